@@ -1,0 +1,180 @@
+"""ctypes bindings to the CPU checkers (test infrastructure only).
+
+* ``Oracle``    -- oracle/_build/liboracle.so, the C restatement of Biovoltron's
+                   PairHMM (pairhmm_oracle.c).
+* ``Reference`` -- oracle/_ref/libref_pairhmm.so, Biovoltron's own kernel
+                   (lib/intel_native/pairhmm) compiled from its sources by
+                   oracle/Makefile; absent where the reference tree is absent
+                   and nothing was prebuilt.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs use this
+module; the product library never loads it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_pairhmm.so")
+
+
+class Testcase(C.Structure):
+    """Layout of ``testcase`` (lib/intel_native/pairhmm/pairhmm_common.h:20-24)."""
+
+    _fields_ = [
+        ("rslen", C.c_int), ("haplen", C.c_int),
+        ("q", C.c_void_p), ("i", C.c_void_p), ("d", C.c_void_p), ("c", C.c_void_p),
+        ("hap", C.c_void_p), ("rs", C.c_void_p),
+    ]
+
+
+class TestcaseArray:
+    """Testcases pointing into a RegionBatch's arrays (which must stay alive)."""
+
+    def __init__(self, batch, reads: np.ndarray, haps: np.ndarray):
+        self.batch = batch
+        n = len(reads)
+        self.n = n
+        self.arr = (Testcase * max(n, 1))()
+        ro, ho = batch.read_offsets, batch.hap_offsets
+        base = {k: getattr(batch, k).ctypes.data for k in ("read_bases", "read_q", "read_i", "read_d", "read_c", "hap_bases")}
+        for k in range(n):
+            r, h = int(reads[k]), int(haps[k])
+            a = int(ro[r])
+            tc = self.arr[k]
+            tc.rslen = int(ro[r + 1] - a)
+            tc.haplen = int(ho[h + 1] - ho[h])
+            tc.q = base["read_q"] + a
+            tc.i = base["read_i"] + a
+            tc.d = base["read_d"] + a
+            tc.c = base["read_c"] + a
+            tc.rs = base["read_bases"] + a
+            tc.hap = base["hap_bases"] + int(ho[h])
+
+    @classmethod
+    def for_batch(cls, batch, limit: Optional[int] = None, sel: Optional[np.ndarray] = None):
+        r, h = batch.pair_index()
+        if sel is not None:
+            r, h = r[sel], h[sel]
+        if limit is not None:
+            r, h = r[:limit], h[:limit]
+        return cls(batch, r, h)
+
+
+def _bind(lib, name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+class Oracle:
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library missing: {path} (run `make -C oracle`)")
+        self.lib = C.CDLL(path)
+        L = self.lib
+        P = C.POINTER(Testcase)
+        self._f32 = _bind(L, "orc_prob_f32", C.c_float, [P])
+        self._f64 = _bind(L, "orc_prob_f64", C.c_double, [P])
+        self._rule = _bind(L, "orc_log10_reference_rule", C.c_double, [P, C.POINTER(C.c_int)])
+        self._resc = _bind(L, "orc_log10_rescaled", C.c_double, [P])
+        self._scalar = _bind(L, "orc_scalar_log10", C.c_double,
+                             [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_void_p])
+        self._b_rule = _bind(L, "orc_batch_reference_rule", None, [C.c_long, P, C.c_void_p, C.c_void_p, C.c_int])
+        self._b_resc = _bind(L, "orc_batch_rescaled", None, [C.c_long, P, C.c_void_p, C.c_int])
+        self._b_f32 = _bind(L, "orc_batch_prob_f32", None, [C.c_long, P, C.c_void_p, C.c_int])
+        self._b_f64 = _bind(L, "orc_batch_prob_f64", None, [C.c_long, P, C.c_void_p, C.c_int])
+        for nm, t in (("orc_table_ph2pr_f32", C.c_float), ("orc_table_ph2pr_f64", C.c_double),
+                      ("orc_table_mm_f32", C.c_float), ("orc_table_mm_f64", C.c_double)):
+            _bind(L, nm, C.POINTER(t), [])
+        _bind(L, "orc_table_mm_size", C.c_int, [])
+
+    # batch forms ------------------------------------------------------------
+    def log10_reference_rule(self, tcs: TestcaseArray, threads: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+        out = np.zeros(tcs.n, np.float64)
+        used = np.zeros(tcs.n, np.int32)
+        self._b_rule(tcs.n, tcs.arr, out.ctypes.data, used.ctypes.data, threads)
+        return out, used.astype(bool)
+
+    def log10_rescaled(self, tcs: TestcaseArray, threads: int = 0) -> np.ndarray:
+        out = np.zeros(tcs.n, np.float64)
+        self._b_resc(tcs.n, tcs.arr, out.ctypes.data, threads)
+        return out
+
+    def prob_f32(self, tcs: TestcaseArray, threads: int = 0) -> np.ndarray:
+        out = np.zeros(tcs.n, np.float32)
+        self._b_f32(tcs.n, tcs.arr, out.ctypes.data, threads)
+        return out
+
+    def prob_f64(self, tcs: TestcaseArray, threads: int = 0) -> np.ndarray:
+        out = np.zeros(tcs.n, np.float64)
+        self._b_f64(tcs.n, tcs.arr, out.ctypes.data, threads)
+        return out
+
+    def scalar_log10(self, read: bytes, qual: bytes, hap: bytes, trans: Optional[Sequence[float]] = None) -> float:
+        t = None
+        if trans is not None:
+            buf = (C.c_double * 7)(*trans)
+            t = C.cast(buf, C.c_void_p)
+        return self._scalar(read, qual, len(read), hap, len(hap), t)
+
+    def tables(self):
+        L = self.lib
+        n = L.orc_table_mm_size()
+        return {
+            "ph2pr_f32": np.ctypeslib.as_array(L.orc_table_ph2pr_f32(), (128,)).copy(),
+            "ph2pr_f64": np.ctypeslib.as_array(L.orc_table_ph2pr_f64(), (128,)).copy(),
+            "mm_f32": np.ctypeslib.as_array(L.orc_table_mm_f32(), (n,)).copy(),
+            "mm_f64": np.ctypeslib.as_array(L.orc_table_mm_f64(), (n,)).copy(),
+        }
+
+
+class Reference:
+    """Biovoltron's own PairHMM kernel, called as AvxPairHMM calls it."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference kernel not built: {path}")
+        self.lib = C.CDLL(path)
+        L = self.lib
+        P = C.POINTER(Testcase)
+        self._f32 = _bind(L, "ref_prob_f32", C.c_float, [P])
+        self._f64 = _bind(L, "ref_prob_f64", C.c_double, [P])
+        self._batch = _bind(L, "ref_batch_log10", None, [C.c_long, P, C.c_void_p, C.c_void_p, C.c_int])
+        self.threads = _bind(L, "ref_threads", C.c_int, [])
+        for nm, t in (("ref_table_ph2pr_f32", C.c_float), ("ref_table_ph2pr_f64", C.c_double),
+                      ("ref_table_mm_f32", C.c_float), ("ref_table_mm_f64", C.c_double)):
+            _bind(L, nm, C.POINTER(t), [])
+        _bind(L, "ref_table_mm_size", C.c_int, [])
+
+    @staticmethod
+    def available(path: str = REF_SO) -> bool:
+        return os.path.exists(path)
+
+    def log10(self, tcs: TestcaseArray, threads: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+        out = np.zeros(tcs.n, np.float64)
+        used = np.zeros(tcs.n, np.int32)
+        self._batch(tcs.n, tcs.arr, out.ctypes.data, used.ctypes.data, threads)
+        return out, used.astype(bool)
+
+    def prob_f32(self, tcs: TestcaseArray) -> np.ndarray:
+        return np.array([self._f32(C.byref(tcs.arr[k])) for k in range(tcs.n)], np.float32)
+
+    def prob_f64(self, tcs: TestcaseArray) -> np.ndarray:
+        return np.array([self._f64(C.byref(tcs.arr[k])) for k in range(tcs.n)], np.float64)
+
+    def tables(self):
+        L = self.lib
+        n = L.ref_table_mm_size()
+        return {
+            "ph2pr_f32": np.ctypeslib.as_array(L.ref_table_ph2pr_f32(), (128,)).copy(),
+            "ph2pr_f64": np.ctypeslib.as_array(L.ref_table_ph2pr_f64(), (128,)).copy(),
+            "mm_f32": np.ctypeslib.as_array(L.ref_table_mm_f32(), (n,)).copy(),
+            "mm_f64": np.ctypeslib.as_array(L.ref_table_mm_f64(), (n,)).copy(),
+        }
