@@ -1,0 +1,245 @@
+// phmm_capi.cpp -- extern "C" entry points declared in include/bv_pairhmm.h.
+//
+// Nothing crosses the C boundary as an exception: every entry point catches
+// and maps failures to a bv_status.
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bv_pairhmm.h"
+#include "phmm_engine.h"
+
+struct bv_phmm_ctx {
+  bvphmm::Engine engine;
+  explicit bv_phmm_ctx(const bv_phmm_options& o) : engine(o) {}
+};
+
+namespace {
+
+// Flattens testcases into one region per run of consecutive testcases that
+// share a read, which is how AvxPairHMM::getData lays them out
+// ([read][hap], pairhmm_avx.hpp:57-79).
+struct Flat {
+  std::vector<int64_t> region_reads{0}, region_haps{0}, read_off{0}, hap_off{0};
+  std::vector<uint8_t> rb, rq, ri, rd, rc, hb;
+  std::vector<int64_t> slot_of;  // testcase k -> result slot
+  bv_region_batch view() const {
+    bv_region_batch b{};
+    b.num_regions = (int64_t)region_reads.size() - 1;
+    b.region_reads = region_reads.data();
+    b.region_haps = region_haps.data();
+    b.num_reads = (int64_t)read_off.size() - 1;
+    b.read_offsets = read_off.data();
+    b.read_bases = rb.data();
+    b.read_q = rq.data();
+    b.read_i = ri.data();
+    b.read_d = rd.data();
+    b.read_c = rc.data();
+    b.num_haps = (int64_t)hap_off.size() - 1;
+    b.hap_offsets = hap_off.data();
+    b.hap_bases = hb.data();
+    return b;
+  }
+  void add_read(int len, const char* s, const char* q, const char* i, const char* d, const char* c) {
+    rb.insert(rb.end(), s, s + len);
+    rq.insert(rq.end(), q, q + len);
+    ri.insert(ri.end(), i, i + len);
+    rd.insert(rd.end(), d, d + len);
+    rc.insert(rc.end(), c, c + len);
+    read_off.push_back((int64_t)rb.size());
+  }
+  void add_hap(int len, const char* s) {
+    hb.insert(hb.end(), s, s + len);
+    hap_off.push_back((int64_t)hb.size());
+  }
+};
+
+bv_status guard(bv_phmm_ctx* ctx, auto&& fn) {
+  try {
+    return fn();
+  } catch (const std::bad_alloc&) {
+    if (ctx) ctx->engine.fail(BV_ERR_OOM, "host allocation failed");
+    return BV_ERR_OOM;
+  } catch (...) {
+    if (ctx) ctx->engine.fail(BV_ERR_INTERNAL, "unexpected exception");
+    return BV_ERR_INTERNAL;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void bv_phmm_default_options(bv_phmm_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->struct_size = (int32_t)sizeof(*o);
+  o->device = 0;
+  o->precision = BV_PRECISION_AUTO;
+  o->mode = BV_MODE_FULL;
+  o->rescue_threshold = bvphmm::kMinAccepted;
+  o->haps_per_unit = 8;
+}
+
+int bv_phmm_abi_version(void) { return BV_PHMM_ABI_VERSION; }
+
+const char* bv_phmm_status_string(bv_status s) {
+  switch (s) {
+    case BV_OK: return "ok";
+    case BV_ERR_INVALID_ARG: return "invalid argument";
+    case BV_ERR_OOM: return "out of memory";
+    case BV_ERR_CUDA: return "CUDA error";
+    case BV_ERR_TIMEOUT: return "timeout";
+    case BV_ERR_NO_DEVICE: return "no CUDA device";
+    case BV_ERR_INTERNAL: return "internal error";
+    case BV_ERR_UNSUPPORTED: return "unsupported";
+  }
+  return "unknown status";
+}
+
+bv_status bv_phmm_create(const bv_phmm_options* opts, bv_phmm_ctx** out) {
+  if (!out) return BV_ERR_INVALID_ARG;
+  *out = nullptr;
+  bv_phmm_options o;
+  bv_phmm_default_options(&o);
+  if (opts) {
+    if (opts->struct_size != (int32_t)sizeof(bv_phmm_options)) return BV_ERR_INVALID_ARG;
+    o = *opts;
+  }
+  if (o.precision != BV_PRECISION_AUTO && o.precision != BV_PRECISION_F64) return BV_ERR_INVALID_ARG;
+  if (o.mode != BV_MODE_FULL && o.mode != BV_MODE_BAND) return BV_ERR_INVALID_ARG;
+  if (o.mode == BV_MODE_BAND) return BV_ERR_UNSUPPORTED;
+  if (o.rescue_threshold != bvphmm::kMinAccepted) return BV_ERR_UNSUPPORTED;
+  bv_phmm_ctx* c = new (std::nothrow) bv_phmm_ctx(o);
+  if (!c) return BV_ERR_OOM;
+  bv_status s = guard(c, [&] { return c->engine.init(); });
+  if (s != BV_OK) {
+    delete c;
+    return s;
+  }
+  *out = c;
+  return BV_OK;
+}
+
+void bv_phmm_destroy(bv_phmm_ctx* ctx) { delete ctx; }
+
+const char* bv_phmm_last_error(const bv_phmm_ctx* ctx) { return ctx ? ctx->engine.last_error() : "null context"; }
+
+int64_t bv_phmm_region_results(const bv_region_batch* b) {
+  if (!b || b->num_regions <= 0 || !b->region_reads || !b->region_haps) return 0;
+  int64_t n = 0;
+  for (int64_t g = 0; g < b->num_regions; ++g)
+    n += (b->region_reads[g + 1] - b->region_reads[g]) * (b->region_haps[g + 1] - b->region_haps[g]);
+  return n;
+}
+
+bv_status bv_phmm_compute_regions(bv_phmm_ctx* ctx, const bv_region_batch* batch, double* out, bv_phmm_stats* stats) {
+  if (!ctx || !batch) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.compute(*batch, out, stats); });
+}
+
+bv_status bv_phmm_stage_regions(bv_phmm_ctx* ctx, const bv_region_batch* batch) {
+  if (!ctx || !batch) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.stage(*batch); });
+}
+
+bv_status bv_phmm_run_staged(bv_phmm_ctx* ctx, bv_phmm_stats* stats) {
+  if (!ctx) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.run(stats); });
+}
+
+bv_status bv_phmm_fetch_results(bv_phmm_ctx* ctx, double* out, int64_t n) {
+  if (!ctx) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.fetch(out, n); });
+}
+
+bv_status bv_phmm_compute_testcases(bv_phmm_ctx* ctx, const bv_testcase* tcs, int64_t n, double* out,
+                                    bv_phmm_stats* stats) {
+  if (!ctx || n < 0 || (n > 0 && (!tcs || !out))) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&]() -> bv_status {
+    Flat f;
+    for (int64_t k = 0; k < n; ++k) {
+      const bv_testcase& t = tcs[k];
+      if (t.rslen < 0 || t.haplen < 0) return ctx->engine.fail(BV_ERR_INVALID_ARG, "negative testcase length");
+      if ((t.rslen > 0 && (!t.rs || !t.q || !t.i || !t.d || !t.c)) || (t.haplen > 0 && !t.hap))
+        return ctx->engine.fail(BV_ERR_INVALID_ARG, "null testcase array");
+      const bool same_read = k > 0 && tcs[k - 1].rs == t.rs && tcs[k - 1].rslen == t.rslen &&
+                             tcs[k - 1].q == t.q && tcs[k - 1].i == t.i && tcs[k - 1].d == t.d && tcs[k - 1].c == t.c;
+      if (!same_read) {
+        if (k > 0) {
+          f.region_reads.push_back((int64_t)f.read_off.size() - 1);
+          f.region_haps.push_back((int64_t)f.hap_off.size() - 1);
+        }
+        f.add_read(t.rslen, t.rs, t.q, t.i, t.d, t.c);
+      }
+      f.add_hap(t.haplen, t.hap);
+    }
+    if (n > 0) {
+      f.region_reads.push_back((int64_t)f.read_off.size() - 1);
+      f.region_haps.push_back((int64_t)f.hap_off.size() - 1);
+    }
+    // Each region holds one read, so result slots follow testcase order.
+    const bv_region_batch b = f.view();
+    return ctx->engine.compute(b, out, stats);
+  });
+}
+
+bv_status bv_phmm_shacc_calculate(bv_phmm_ctx* ctx, bv_shacc_batch* batch) {
+  if (!ctx || !batch || batch->num_reads < 0 || batch->num_haps < 0) return BV_ERR_INVALID_ARG;
+  if ((batch->num_reads > 0 && !batch->reads) || (batch->num_haps > 0 && !batch->haps) ||
+      (batch->num_reads > 0 && batch->num_haps > 0 && !batch->results))
+    return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&]() -> bv_status {
+    Flat f;
+    for (int r = 0; r < batch->num_reads; ++r) {
+      const bv_shacc_read& rd = batch->reads[r];
+      if (rd.length < 0 || (rd.length > 0 && (!rd.bases || !rd.q || !rd.i || !rd.d || !rd.c)))
+        return ctx->engine.fail(BV_ERR_INVALID_ARG, "bad shacc read");
+      f.add_read(rd.length, rd.bases, rd.q, rd.i, rd.d, rd.c);
+    }
+    for (int h = 0; h < batch->num_haps; ++h) {
+      const bv_shacc_hap& hp = batch->haps[h];
+      if (hp.length < 0 || (hp.length > 0 && !hp.bases)) return ctx->engine.fail(BV_ERR_INVALID_ARG, "bad shacc hap");
+      f.add_hap(hp.length, hp.bases);
+    }
+    f.region_reads.push_back(batch->num_reads);
+    f.region_haps.push_back(batch->num_haps);
+    const int64_t n = (int64_t)batch->num_reads * batch->num_haps;
+    std::vector<double> tmp((size_t)std::max<int64_t>(n, 1));
+    const bv_region_batch b = f.view();
+    bv_status s = ctx->engine.compute(b, tmp.data(), nullptr);
+    if (s != BV_OK) return s;
+    for (int64_t k = 0; k < n; ++k) batch->results[k] = (float)tmp[k];
+    return BV_OK;
+  });
+}
+
+int bv_phmm_debug_tables(float* pf, double* pd, float* mf, double* md, int n) {
+  if (n != bvphmm::kMMEntries || !pf || !pd || !mf || !md) return -1;
+  auto t = std::make_unique<bvphmm::Tables>();
+  bvphmm::build_tables(t.get());
+  std::memcpy(pf, t->ph2pr_f, sizeof(t->ph2pr_f));
+  std::memcpy(pd, t->ph2pr_d, sizeof(t->ph2pr_d));
+  std::memcpy(mf, t->mm_f, sizeof(t->mm_f));
+  std::memcpy(md, t->mm_d, sizeof(t->mm_d));
+  return 0;
+}
+
+bv_status bv_phmm_host_register(bv_phmm_ctx* ctx, void* ptr, size_t bytes) {
+  if (!ctx || !ptr || bytes == 0) return BV_ERR_INVALID_ARG;
+  cudaError_t e = cudaSetDevice(ctx->engine.device());
+  if (e == cudaSuccess) e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+  if (e != cudaSuccess) return ctx->engine.cuda_fail(e, "cudaHostRegister");
+  return BV_OK;
+}
+
+bv_status bv_phmm_host_unregister(bv_phmm_ctx* ctx, void* ptr) {
+  if (!ctx || !ptr) return BV_ERR_INVALID_ARG;
+  cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) return ctx->engine.cuda_fail(e, "cudaHostUnregister");
+  return BV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,463 @@
+// phmm_engine.cpp -- host engine: validation, work planning, staging,
+// launches, FP64 rescue, timing and graph replay.
+//
+// Work layout.  A result slot is one (read, haplotype) pair of one region,
+// numbered region by region in read-major order, which is the layout of the
+// [read][hap] matrix that AvxPairHMM::compute_likelihoods returns
+// (include/biovoltron/algo/align/inexact_match/pairhmm_avx.hpp:160-171).
+// A unit is one read scored against up to `haps_per_unit` consecutive
+// haplotypes of its region, so the read's per-row constants and emission table
+// are built once per unit.  Units are bucketed by kernel variant (rows per
+// lane = ceil((read_len + 1) / 32), multi-strip above 256 rows); each bucket is
+// one persistent launch whose warps pull units from a device work-queue head.
+// The FP64 launch follows on the same stream and drains the list of pairs the
+// FP32 launches flagged.
+#include "phmm_engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <string>
+
+namespace bvphmm {
+
+cudaError_t DevBuf::reserve(size_t bytes) {
+  if (bytes <= cap_ && p_) return cudaSuccess;
+  release();
+  size_t want = std::max<size_t>(bytes, 256);
+  cudaError_t e = cudaMalloc(&p_, want);
+  if (e != cudaSuccess) {
+    p_ = nullptr;
+    cap_ = 0;
+    return e;
+  }
+  cap_ = want;
+  return cudaSuccess;
+}
+
+void DevBuf::release() {
+  if (p_) cudaFree(p_);
+  p_ = nullptr;
+  cap_ = 0;
+}
+
+namespace {
+constexpr int kMaxRowsPerLane = 8;
+constexpr int kRescaleTarget = 1000;  // FP64 boundary rows are scaled to ~2^1000
+
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+int hap_bytes_for(int max_hap, int chunk) {
+  return (int)round_up((int64_t)max_hap + (kWarp - 1) + chunk + kHapLead + 16, 16);
+}
+long long bnd_cols_for(int max_hap) { return round_up((int64_t)max_hap + kWarp - 1, 32) + 128; }
+}  // namespace
+
+Engine::Engine(const bv_phmm_options& opt) : opt_(opt) {}
+
+Engine::~Engine() {
+  destroy_graph();
+  if (stream_) {
+    cudaStreamSynchronize(stream_);
+    for (auto& e : ev_)
+      if (e) cudaEventDestroy(e);
+    cudaStreamDestroy(stream_);
+  }
+}
+
+bv_status Engine::fail(bv_status s, const std::string& msg) {
+  err_ = msg;
+  return s;
+}
+
+bv_status Engine::cuda_fail(cudaError_t e, const char* what) {
+  err_ = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return BV_ERR_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInvalidDevice) return BV_ERR_NO_DEVICE;
+  return BV_ERR_CUDA;
+}
+
+#define BV_CUDA(call, what)                         \
+  do {                                              \
+    cudaError_t e__ = (call);                       \
+    if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+  } while (0)
+
+bv_status Engine::init() {
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(BV_ERR_NO_DEVICE, "no CUDA device available");
+  if (opt_.device < 0 || opt_.device >= ndev) return fail(BV_ERR_NO_DEVICE, "device ordinal out of range");
+  BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");
+  BV_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, opt_.device), "SM count");
+  BV_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  for (auto& ev : ev_) BV_CUDA(cudaEventCreate(&ev), "event");
+  Tables host{};
+  build_tables(&host);
+  BV_CUDA(d_tables_.reserve(sizeof(Tables)), "tables alloc");
+  BV_CUDA(cudaMemcpyAsync(d_tables_.get(), &host, sizeof(Tables), cudaMemcpyHostToDevice, stream_), "tables copy");
+  BV_CUDA(d_counters_.reserve(sizeof(Counters)), "counters alloc");
+  BV_CUDA(cudaStreamSynchronize(stream_), "init sync");
+  return BV_OK;
+}
+
+bv_status Engine::validate(const bv_region_batch& b) {
+  if (b.num_regions < 0 || b.num_reads < 0 || b.num_haps < 0) return fail(BV_ERR_INVALID_ARG, "negative count");
+  if (b.num_regions > 0 && (!b.region_reads || !b.region_haps))
+    return fail(BV_ERR_INVALID_ARG, "region offsets missing");
+  if (b.num_reads > 0 && (!b.read_offsets)) return fail(BV_ERR_INVALID_ARG, "read offsets missing");
+  if (b.num_haps > 0 && (!b.hap_offsets)) return fail(BV_ERR_INVALID_ARG, "hap offsets missing");
+  if (b.num_reads >= INT32_MAX || b.num_haps >= INT32_MAX) return fail(BV_ERR_INVALID_ARG, "too many reads or haps");
+  for (int64_t g = 0; g < b.num_regions; ++g) {
+    if (b.region_reads[g] > b.region_reads[g + 1] || b.region_haps[g] > b.region_haps[g + 1])
+      return fail(BV_ERR_INVALID_ARG, "region offsets decrease");
+  }
+  if (b.num_regions > 0) {
+    if (b.region_reads[0] < 0 || b.region_haps[0] < 0 || b.region_reads[b.num_regions] > b.num_reads ||
+        b.region_haps[b.num_regions] > b.num_haps)
+      return fail(BV_ERR_INVALID_ARG, "region offsets out of range");
+  }
+  if (b.num_reads > 0) {
+    if (b.read_offsets[0] < 0) return fail(BV_ERR_INVALID_ARG, "read offset negative");
+    for (int64_t r = 0; r < b.num_reads; ++r) {
+      const int64_t l = b.read_offsets[r + 1] - b.read_offsets[r];
+      if (l < 0) return fail(BV_ERR_INVALID_ARG, "read offsets decrease");
+      if (l > BV_PHMM_MAX_READ_LEN) return fail(BV_ERR_INVALID_ARG, "read longer than BV_PHMM_MAX_READ_LEN");
+    }
+    if (b.read_offsets[b.num_reads] > 0 &&
+        (!b.read_bases || !b.read_q || !b.read_i || !b.read_d || !b.read_c))
+      return fail(BV_ERR_INVALID_ARG, "read arrays missing");
+  }
+  if (b.num_haps > 0) {
+    if (b.hap_offsets[0] < 0) return fail(BV_ERR_INVALID_ARG, "hap offset negative");
+    for (int64_t h = 0; h < b.num_haps; ++h) {
+      const int64_t l = b.hap_offsets[h + 1] - b.hap_offsets[h];
+      if (l < 0) return fail(BV_ERR_INVALID_ARG, "hap offsets decrease");
+      if (l > BV_PHMM_MAX_HAP_LEN) return fail(BV_ERR_INVALID_ARG, "haplotype longer than BV_PHMM_MAX_HAP_LEN");
+    }
+    if (b.hap_offsets[b.num_haps] > 0 && !b.hap_bases) return fail(BV_ERR_INVALID_ARG, "hap bases missing");
+  }
+  return BV_OK;
+}
+
+bv_status Engine::plan(const bv_region_batch& b) {
+  units_.clear();
+  f64_items_.clear();
+  plans_.clear();
+  n_results_ = 0;
+  n_cells_ = 0;
+  max_hap_ = 0;
+  const int per_unit = std::max(1, opt_.haps_per_unit > 0 ? opt_.haps_per_unit : 8);
+  const bool all_f64 = opt_.precision == BV_PRECISION_F64;
+  const int nvar_single = kMaxRowsPerLane;  // variants 0..7: rows per lane 1..8
+  const int v_multi = variant_index(false, 8, true);
+  std::vector<int64_t> count(16, 0);
+  std::vector<int> var_max_hap(16, 0);
+  // pass 1: count units per variant
+  std::vector<int> region_max_hap(std::max<int64_t>(b.num_regions, 1), 0);
+  for (int64_t g = 0; g < b.num_regions; ++g) {
+    int mh = 0;
+    for (int64_t h = b.region_haps[g]; h < b.region_haps[g + 1]; ++h)
+      mh = std::max<int>(mh, (int)(b.hap_offsets[h + 1] - b.hap_offsets[h]));
+    region_max_hap[g] = mh;
+    max_hap_ = std::max(max_hap_, mh);
+  }
+  auto variant_of = [&](int64_t rlen) {
+    const int64_t rows = rlen + 1;
+    const int64_t rt = (rows + kWarp - 1) / kWarp;
+    return rt <= kMaxRowsPerLane ? variant_index(false, (int)rt, false) : v_multi;
+  };
+  for (int64_t g = 0; g < b.num_regions; ++g) {
+    const int64_t nh = b.region_haps[g + 1] - b.region_haps[g];
+    const int64_t nr = b.region_reads[g + 1] - b.region_reads[g];
+    if (nh == 0 || nr == 0) continue;
+    const int64_t chunks = (nh + per_unit - 1) / per_unit;
+    for (int64_t r = b.region_reads[g]; r < b.region_reads[g + 1]; ++r) {
+      const int v = variant_of(b.read_offsets[r + 1] - b.read_offsets[r]);
+      count[v] += chunks;
+      var_max_hap[v] = std::max(var_max_hap[v], region_max_hap[g]);
+    }
+  }
+  (void)nvar_single;
+  std::vector<int64_t> start(17, 0);
+  for (int v = 0; v < 16; ++v) start[v + 1] = start[v] + count[v];
+  if (!all_f64) units_.resize(start[16]);
+  std::vector<int64_t> fill(start.begin(), start.end() - 1);
+  // pass 2: fill units (or FP64 items) in result order within each bucket
+  int64_t res = 0;
+  for (int64_t g = 0; g < b.num_regions; ++g) {
+    const int64_t h0 = b.region_haps[g], nh = b.region_haps[g + 1] - h0;
+    const int64_t r0 = b.region_reads[g], nr = b.region_reads[g + 1] - r0;
+    for (int64_t r = r0; r < r0 + nr; ++r) {
+      const int64_t rl = b.read_offsets[r + 1] - b.read_offsets[r];
+      for (int64_t h = h0; h < h0 + nh; ++h) n_cells_ += rl * (b.hap_offsets[h + 1] - b.hap_offsets[h]);
+      if (all_f64) {
+        for (int64_t k = 0; k < nh; ++k)
+          f64_items_.push_back(PairRef{(int32_t)r, (int32_t)(h0 + k), res + (r - r0) * nh + k});
+        continue;
+      }
+      const int v = variant_of(rl);
+      for (int64_t k = 0; k < nh; k += per_unit) {
+        Unit u{};
+        u.read = (int32_t)r;
+        u.hap0 = (int32_t)(h0 + k);
+        u.nh = (int32_t)std::min<int64_t>(per_unit, nh - k);
+        u.out0 = res + (r - r0) * nh + k;
+        units_[fill[v]++] = u;
+      }
+    }
+    res += nr * nh;
+  }
+  n_results_ = res;
+  // launch plans
+  int slot = 0;
+  for (int v = 0; v < 16 && !all_f64; ++v) {
+    if (count[v] == 0) continue;
+    LaunchPlan lp;
+    lp.variant = v;
+    lp.slot = slot++;
+    lp.unit_base = start[v];
+    lp.n_units = count[v];
+    lp.multi = (v == v_multi);
+    lp.f64 = false;
+    lp.hap_bytes = hap_bytes_for(var_max_hap[v], lp.multi ? 32 : 8);
+    lp.warp_smem = warp_smem_bytes(v, lp.hap_bytes);
+    const int smem_block = lp.warp_smem * (kThreadsPerBlock / kWarp);
+    if (smem_block > 227 * 1024) return fail(BV_ERR_INVALID_ARG, "haplotype too long for shared-memory staging");
+    BV_CUDA(prepare_variant(v, smem_block), "kernel attribute");
+    const int bps = std::max(1, blocks_per_sm(v, smem_block));
+    const int64_t need = (count[v] + (kThreadsPerBlock / kWarp) - 1) / (kThreadsPerBlock / kWarp);
+    lp.grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms_ * bps));
+    lp.bnd_cols = lp.multi ? bnd_cols_for(var_max_hap[v]) : 0;
+    plans_.push_back(lp);
+  }
+  // FP64 launch: persistent over the whole device, whatever the FP32 passes flag
+  LaunchPlan rp;
+  rp.variant = variant_index(true, 4, true);
+  rp.slot = 15;
+  rp.multi = true;
+  rp.f64 = true;
+  rp.hap_bytes = hap_bytes_for(std::max(max_hap_, 1), 32);
+  rp.warp_smem = warp_smem_bytes(rp.variant, rp.hap_bytes);
+  const int smem_block = rp.warp_smem * (kThreadsPerBlock / kWarp);
+  if (smem_block > 227 * 1024) return fail(BV_ERR_INVALID_ARG, "haplotype too long for shared-memory staging");
+  BV_CUDA(prepare_variant(rp.variant, smem_block), "kernel attribute");
+  const int bps = std::max(1, blocks_per_sm(rp.variant, smem_block));
+  rp.grid = sms_ * bps;
+  rp.bnd_cols = bnd_cols_for(std::max(max_hap_, 1));
+  rescue_plan_ = rp;
+  return BV_OK;
+}
+
+bv_status Engine::upload(const bv_region_batch& b) {
+  n_reads_ = b.num_reads;
+  n_haps_ = b.num_haps;
+  n_read_bytes_ = b.num_reads > 0 ? b.read_offsets[b.num_reads] : 0;
+  n_hap_bytes_ = b.num_haps > 0 ? b.hap_offsets[b.num_haps] : 0;
+  const size_t rb = (size_t)std::max<int64_t>(n_read_bytes_, 1);
+  BV_CUDA(d_read_bases_.reserve(rb), "alloc reads");
+  BV_CUDA(d_q_.reserve(rb), "alloc q");
+  BV_CUDA(d_i_.reserve(rb), "alloc i");
+  BV_CUDA(d_d_.reserve(rb), "alloc d");
+  BV_CUDA(d_c_.reserve(rb), "alloc c");
+  BV_CUDA(d_quals4_.reserve(rb * 4), "alloc quals");
+  BV_CUDA(d_read_off_.reserve(sizeof(int64_t) * (n_reads_ + 1)), "alloc read offsets");
+  BV_CUDA(d_hap_bases_.reserve((size_t)std::max<int64_t>(n_hap_bytes_, 1)), "alloc haps");
+  BV_CUDA(d_hap_off_.reserve(sizeof(int64_t) * (n_haps_ + 1)), "alloc hap offsets");
+  BV_CUDA(d_units_.reserve(sizeof(Unit) * std::max<size_t>(units_.size(), 1)), "alloc units");
+  BV_CUDA(d_out_.reserve(sizeof(double) * (size_t)std::max<int64_t>(n_results_, 1)), "alloc results");
+  BV_CUDA(d_rescue_.reserve(sizeof(PairRef) * (size_t)std::max<int64_t>(n_results_, 1)), "alloc rescue list");
+  // strip-boundary buffers for the multi-strip launches
+  size_t need32 = 0;
+  for (const auto& lp : plans_)
+    if (lp.multi) need32 = std::max<size_t>(need32, (size_t)lp.grid * (kThreadsPerBlock / kWarp) * (size_t)lp.bnd_cols * 4 * sizeof(float));
+  if (need32) BV_CUDA(d_bnd32_.reserve(need32), "alloc boundary buffers");
+  const size_t need64 = (size_t)rescue_plan_.grid * (kThreadsPerBlock / kWarp) * (size_t)rescue_plan_.bnd_cols * 4 * sizeof(double);
+  BV_CUDA(d_bnd64_.reserve(need64), "alloc FP64 boundary buffers");
+
+  BV_CUDA(cudaEventRecord(ev_[0], stream_), "event");
+  const int64_t r0 = b.num_reads > 0 ? b.read_offsets[0] : 0;
+  // Offsets are copied verbatim; the byte arrays are copied from index 0 so
+  // offsets index them directly.
+  (void)r0;
+  if (n_read_bytes_ > 0) {
+    BV_CUDA(cudaMemcpyAsync(d_read_bases_.get(), b.read_bases, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+    BV_CUDA(cudaMemcpyAsync(d_q_.get(), b.read_q, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+    BV_CUDA(cudaMemcpyAsync(d_i_.get(), b.read_i, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+    BV_CUDA(cudaMemcpyAsync(d_d_.get(), b.read_d, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+    BV_CUDA(cudaMemcpyAsync(d_c_.get(), b.read_c, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+  }
+  if (n_reads_ > 0)
+    BV_CUDA(cudaMemcpyAsync(d_read_off_.get(), b.read_offsets, sizeof(int64_t) * (n_reads_ + 1), cudaMemcpyHostToDevice,
+                            stream_), "H2D");
+  if (n_hap_bytes_ > 0)
+    BV_CUDA(cudaMemcpyAsync(d_hap_bases_.get(), b.hap_bases, n_hap_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+  if (n_haps_ > 0)
+    BV_CUDA(cudaMemcpyAsync(d_hap_off_.get(), b.hap_offsets, sizeof(int64_t) * (n_haps_ + 1), cudaMemcpyHostToDevice,
+                            stream_), "H2D");
+  if (!units_.empty())
+    BV_CUDA(cudaMemcpyAsync(d_units_.get(), units_.data(), sizeof(Unit) * units_.size(), cudaMemcpyHostToDevice,
+                            stream_), "H2D");
+  if (!f64_items_.empty())
+    BV_CUDA(cudaMemcpyAsync(d_rescue_.get(), f64_items_.data(), sizeof(PairRef) * f64_items_.size(),
+                            cudaMemcpyHostToDevice, stream_), "H2D");
+  BV_CUDA(launch_pack_quals(d_q_.as<uint8_t>(), d_i_.as<uint8_t>(), d_d_.as<uint8_t>(), d_c_.as<uint8_t>(),
+                            d_quals4_.as<uchar4>(), n_read_bytes_, sms_, stream_), "pack quals");
+  BV_CUDA(cudaEventRecord(ev_[1], stream_), "event");
+  BV_CUDA(cudaStreamSynchronize(stream_), "stage sync");
+  BV_CUDA(cudaEventElapsedTime(&ms_h2d_, ev_[0], ev_[1]), "event time");
+  return BV_OK;
+}
+
+bv_status Engine::stage(const bv_region_batch& b) {
+  staged_ = false;
+  destroy_graph();
+  BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");
+  bv_status s = validate(b);
+  if (s != BV_OK) return s;
+  s = plan(b);
+  if (s != BV_OK) return s;
+  s = upload(b);
+  if (s != BV_OK) return s;
+  staged_ = true;
+  runs_since_stage_ = 0;
+  return BV_OK;
+}
+
+bv_status Engine::enqueue_kernels() {
+  BV_CUDA(cudaMemsetAsync(d_counters_.get(), 0, sizeof(Counters), stream_), "memset counters");
+  if (!f64_items_.empty()) {
+    BV_CUDA(launch_set_u64(&d_counters_.as<Counters>()->rescue_count, (unsigned long long)f64_items_.size(), stream_),
+            "set FP64 count");
+  }
+  KernelParams p{};
+  p.batch.read_bases = d_read_bases_.as<uint8_t>();
+  p.batch.read_quals = d_quals4_.as<uchar4>();
+  p.batch.read_off = d_read_off_.as<int64_t>();
+  p.batch.hap_bases = d_hap_bases_.as<uint8_t>();
+  p.batch.hap_off = d_hap_off_.as<int64_t>();
+  p.tables = d_tables_.as<Tables>();
+  p.units = d_units_.as<Unit>();
+  p.ctr = d_counters_.as<Counters>();
+  p.out = d_out_.as<double>();
+  p.rescue = d_rescue_.as<PairRef>();
+  p.rescue_cap = std::max<int64_t>(n_results_, 1);
+  BV_CUDA(cudaEventRecord(ev_[2], stream_), "event");
+  for (const auto& lp : plans_) {
+    p.unit_base = lp.unit_base;
+    p.n_units = lp.n_units;
+    p.slot = lp.slot;
+    p.from_rescue = 0;
+    p.hap_bytes = lp.hap_bytes;
+    p.warp_smem_bytes = lp.warp_smem;
+    p.bnd = lp.multi ? d_bnd32_.get() : nullptr;
+    p.bnd_cols = lp.bnd_cols;
+    p.rescale = 0;
+    p.rescale_target = 0;
+    BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP32 forward launch");
+  }
+  BV_CUDA(cudaEventRecord(ev_[3], stream_), "event");
+  {
+    const LaunchPlan& lp = rescue_plan_;
+    p.unit_base = 0;
+    p.n_units = 0;
+    p.slot = lp.slot;
+    p.from_rescue = 1;
+    p.hap_bytes = lp.hap_bytes;
+    p.warp_smem_bytes = lp.warp_smem;
+    p.bnd = d_bnd64_.get();
+    p.bnd_cols = lp.bnd_cols;
+    p.rescale = 1;
+    p.rescale_target = kRescaleTarget;
+    BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP64 forward launch");
+  }
+  BV_CUDA(cudaEventRecord(ev_[4], stream_), "event");
+  return BV_OK;
+}
+
+void Engine::destroy_graph() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  graph_exec_ = nullptr;
+  graph_ = nullptr;
+}
+
+bv_status Engine::run(bv_phmm_stats* stats) {
+  if (!staged_) return fail(BV_ERR_INVALID_ARG, "no staged batch");
+  BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");
+  const auto t0 = std::chrono::steady_clock::now();
+  // The first run of a staged batch launches directly; later runs replay a
+  // captured graph of the same launch sequence.
+  if (runs_since_stage_ == 0 || !graph_exec_) {
+    if (runs_since_stage_ >= 1 && !graph_exec_) {
+      BV_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+      bv_status s = enqueue_kernels();
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+      if (s != BV_OK) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+      }
+      BV_CUDA(ce, "end capture");
+      graph_ = g;
+      BV_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
+      BV_CUDA(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+    } else {
+      bv_status s = enqueue_kernels();
+      if (s != BV_OK) return s;
+    }
+  } else {
+    BV_CUDA(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
+  }
+  ++runs_since_stage_;
+  Counters c{};
+  BV_CUDA(cudaMemcpyAsync(&c, d_counters_.get(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_), "counters D2H");
+  BV_CUDA(cudaStreamSynchronize(stream_), "run sync");
+  if (c.status != 0) return fail(BV_ERR_INTERNAL, "kernel reported an inconsistent state");
+  if (stats) {
+    float ms32 = 0, ms64 = 0;
+    cudaEventElapsedTime(&ms32, ev_[2], ev_[3]);
+    cudaEventElapsedTime(&ms64, ev_[3], ev_[4]);
+    stats->pairs = n_results_;
+    stats->cells = n_cells_;
+    stats->rescued = (int64_t)c.rescue_count;
+    stats->underflow = (int64_t)c.underflow_count;
+    stats->kernel_launches = (int64_t)plans_.size() + 1;
+    stats->ms_fp32 = ms32;
+    stats->ms_fp64 = ms64;
+    stats->ms_h2d = ms_h2d_;
+    stats->ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return BV_OK;
+}
+
+bv_status Engine::fetch(double* out, int64_t n) {
+  if (!staged_) return fail(BV_ERR_INVALID_ARG, "no staged batch");
+  if (n < 0 || n > n_results_) return fail(BV_ERR_INVALID_ARG, "fetch size exceeds staged results");
+  if (n == 0) return BV_OK;
+  if (!out) return fail(BV_ERR_INVALID_ARG, "null output");
+  BV_CUDA(cudaMemcpyAsync(out, d_out_.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, stream_), "results D2H");
+  BV_CUDA(cudaStreamSynchronize(stream_), "fetch sync");
+  return BV_OK;
+}
+
+bv_status Engine::compute(const bv_region_batch& b, double* out, bv_phmm_stats* stats) {
+  const auto t0 = std::chrono::steady_clock::now();
+  bv_status s = stage(b);
+  if (s != BV_OK) return s;
+  if (n_results_ > 0 && !out) return fail(BV_ERR_INVALID_ARG, "null output");
+  s = run(stats);
+  if (s != BV_OK) return s;
+  const auto t1 = std::chrono::steady_clock::now();
+  s = fetch(out, n_results_);
+  if (s != BV_OK) return s;
+  if (stats) {
+    const auto t2 = std::chrono::steady_clock::now();
+    stats->ms_d2h = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    stats->ms_total = std::chrono::duration<double, std::milli>(t2 - t0).count();
+  }
+  return BV_OK;
+}
+
+}  // namespace bvphmm

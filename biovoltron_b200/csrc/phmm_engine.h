@@ -1,0 +1,100 @@
+// phmm_engine.h -- host engine behind the C ABI (C++20).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "bv_pairhmm.h"
+#include "phmm_common.h"
+#include "phmm_kernels.h"
+
+namespace bvphmm {
+
+// Grow-only device allocation.
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  cudaError_t reserve(size_t bytes);
+  void release();
+  void* get() const { return p_; }
+  template <typename T> T* as() const { return static_cast<T*>(p_); }
+  size_t capacity() const { return cap_; }
+
+ private:
+  void* p_ = nullptr;
+  size_t cap_ = 0;
+};
+
+struct LaunchPlan {
+  int variant = -1;
+  int slot = 0;
+  long long unit_base = 0;
+  long long n_units = 0;
+  int hap_bytes = 0;
+  int warp_smem = 0;
+  int grid = 0;
+  long long bnd_cols = 0;
+  bool multi = false;
+  bool f64 = false;
+};
+
+class Engine {
+ public:
+  explicit Engine(const bv_phmm_options& opt);
+  ~Engine();
+  bv_status init();
+
+  bv_status stage(const bv_region_batch& b);
+  bv_status run(bv_phmm_stats* stats);
+  bv_status fetch(double* out, int64_t n);
+  bv_status compute(const bv_region_batch& b, double* out, bv_phmm_stats* stats);
+
+  const char* last_error() const { return err_.c_str(); }
+  bv_status fail(bv_status s, const std::string& msg);
+  bv_status cuda_fail(cudaError_t e, const char* what);
+  int64_t staged_results() const { return n_results_; }
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return opt_.device; }
+
+ private:
+  bv_status validate(const bv_region_batch& b);
+  bv_status plan(const bv_region_batch& b);
+  bv_status upload(const bv_region_batch& b);
+  bv_status enqueue_kernels();
+  void destroy_graph();
+
+  bv_phmm_options opt_;
+  int sms_ = 0;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev_[8] = {};
+  std::string err_;
+
+  DevBuf d_tables_, d_read_bases_, d_q_, d_i_, d_d_, d_c_, d_quals4_, d_read_off_, d_hap_bases_, d_hap_off_;
+  DevBuf d_units_, d_out_, d_rescue_, d_counters_, d_bnd32_, d_bnd64_, d_f64_items_;
+
+  // staged batch
+  std::vector<Unit> units_;
+  std::vector<PairRef> f64_items_;  // pairs sent straight to FP64 (precision F64)
+  std::vector<LaunchPlan> plans_;
+  LaunchPlan rescue_plan_;
+  int64_t n_results_ = 0;
+  int64_t n_cells_ = 0;
+  int64_t n_read_bytes_ = 0;
+  int64_t n_hap_bytes_ = 0;
+  int64_t n_reads_ = 0;
+  int64_t n_haps_ = 0;
+  int max_hap_ = 0;
+  bool staged_ = false;
+  float ms_h2d_ = 0;
+
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  int runs_since_stage_ = 0;
+};
+
+}  // namespace bvphmm

@@ -1,0 +1,48 @@
+// phmm_kernels.h -- launch interface between the host engine and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "phmm_common.h"
+
+namespace bvphmm {
+
+constexpr int kThreadsPerBlock = 128;
+
+struct KernelParams {
+  DeviceBatch batch;
+  const Tables* tables;
+  const Unit* units;
+  long long unit_base;
+  long long n_units;
+  int slot;               // work-queue head used by this launch
+  int from_rescue;        // 1: items come from the FP64 list
+  Counters* ctr;
+  double* out;            // log10 likelihoods, one per result slot
+  PairRef* rescue;
+  long long rescue_cap;
+  int hap_bytes;          // per-warp bytes for staged haplotype codes
+  int warp_smem_bytes;    // per-warp dynamic shared memory
+  void* bnd;              // per-warp strip-boundary buffers (multi-strip variants)
+  long long bnd_cols;     // rows of 4 values per warp buffer
+  int rescale;            // renormalise between strips (FP64 variants)
+  int rescale_target;     // binary exponent the boundary maximum is scaled to
+};
+
+// Variant table: (precision, rows per lane, multi-strip).
+int variant_index(bool f64, int rows_per_lane, bool multi);
+int warp_smem_bytes(int variant, int hap_bytes);
+int blocks_per_sm(int variant, int smem_per_block);
+// Sets the variant's dynamic shared-memory limit; call before launching or capturing it.
+cudaError_t prepare_variant(int variant, int smem_per_block);
+cudaError_t launch_forward(int variant, const KernelParams& p, int grid, cudaStream_t st);
+cudaError_t launch_pack_quals(const uint8_t* q, const uint8_t* i, const uint8_t* d, const uint8_t* c, uchar4* out,
+                              long long n, int sms, cudaStream_t st);
+
+// Writes one 64-bit value on the device (graph-capturable).
+cudaError_t launch_set_u64(unsigned long long* dst, unsigned long long v, cudaStream_t st);
+
+// Host-side construction of the reference's probability tables (Context.h).
+void build_tables(Tables* t);
+
+}  // namespace bvphmm

@@ -1,0 +1,259 @@
+"""Host-side interface mirroring Biovoltron's PairHMM call, over the C ABI.
+
+``GpuPairHMM.compute_likelihoods(haplotypes, reads)`` has the signature,
+result layout and side effects of ``AvxPairHMM::compute_likelihoods``
+(include/biovoltron/algo/align/inexact_match/pairhmm_avx.hpp:160-171): it
+returns a ``[read][hap]`` list of log10 likelihoods, caps each row at
+``best - 4.5`` (``PairHMM::normalize_likelihoods``, pairhmm.hpp:83-93) and
+keeps only the reads whose best likelihood is *below*
+``min(2, ceil(0.02 * len)) * -4`` (``filter_poorly_modeled_reads``,
+pairhmm.hpp:95-114 -- the reference's comparison, kept as is), removing the
+other reads from ``reads`` in place.
+
+``PairHMMEngine`` exposes the batched entry points (regions, testcases, the
+shacc batch hook and the device-resident stage/run/fetch cycle).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import native as N
+from .workloads import RegionBatch
+
+__all__ = ["PairHMMEngine", "GpuPairHMM", "Haplotype", "SamRecord", "normalize_likelihoods",
+           "filter_poorly_modeled_reads"]
+
+# pairhmm.hpp:27-31
+MAXIMUM_BEST_ALT_LIKELIHOOD_DIFFERENCE = -4.5
+EXPECTED_ERROR_RATE_PER_BASE = 0.02
+LOG10_QUALITY_PER_BASE = -4.0
+MAXIMUM_EXPECTED_ERROR_PER_READ = 2.0
+# sam.hpp:19-31: gap-open 40 and gap-continuation 10 as '!'-offset characters,
+# consumed raw by the kernel.
+GAP_OPEN_PENALTY_BYTE = 40 + ord("!")
+GAP_CONTINUATION_PENALTY_BYTE = 10 + ord("!")
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data if a.size else 0
+
+
+class _BatchView:
+    """Keeps the numpy arrays of a RegionBatch alive behind a C struct."""
+
+    def __init__(self, b: RegionBatch):
+        self.b = b
+        self.arrs = [np.ascontiguousarray(x) for x in (
+            b.region_reads.astype(np.int64), b.region_haps.astype(np.int64), b.read_offsets.astype(np.int64),
+            b.read_bases, b.read_q, b.read_i, b.read_d, b.read_c, b.hap_offsets.astype(np.int64), b.hap_bases)]
+        rr, rh, ro, rb, rq, ri, rd, rc, ho, hb = self.arrs
+        self.c = N.RegionBatchC(
+            num_regions=b.n_regions, region_reads=_ptr(rr), region_haps=_ptr(rh),
+            num_reads=b.n_reads, read_offsets=_ptr(ro), read_bases=_ptr(rb), read_q=_ptr(rq), read_i=_ptr(ri),
+            read_d=_ptr(rd), read_c=_ptr(rc), num_haps=b.n_haps, hap_offsets=_ptr(ho), hap_bases=_ptr(hb))
+
+
+class PairHMMEngine:
+    """One ``bv_phmm_ctx`` (a CUDA stream and its device buffers on one GPU)."""
+
+    def __init__(self, device: int = 0, precision: str = "auto", mode: str = "full", haps_per_unit: int = 8):
+        self.lib = N.load()
+        o = N.Options()
+        self.lib.bv_phmm_default_options(C.byref(o))
+        o.device = device
+        o.precision = {"auto": N.BV_PRECISION_AUTO, "f64": N.BV_PRECISION_F64}[precision]
+        o.mode = {"full": N.BV_MODE_FULL, "band": N.BV_MODE_BAND}[mode]
+        o.haps_per_unit = haps_per_unit
+        h = C.c_void_p()
+        st = self.lib.bv_phmm_create(C.byref(o), C.byref(h))
+        if st != N.BV_OK:
+            raise N.NativeError(st, self.lib.bv_phmm_status_string(st).decode())
+        self.h = h
+        self._staged: Optional[_BatchView] = None
+        self._staged_n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bv_phmm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int):
+        if st != N.BV_OK:
+            msg = self.lib.bv_phmm_last_error(self.h)
+            raise N.NativeError(st, (msg or b"").decode())
+
+    # --- batched entry points ---------------------------------------------
+    def compute_regions(self, batch: RegionBatch, out: Optional[np.ndarray] = None, with_stats: bool = False):
+        v = _BatchView(batch)
+        n = int(self.lib.bv_phmm_region_results(C.byref(v.c)))
+        if out is None:
+            out = np.empty(max(n, 1), np.float64)
+        st = N.Stats()
+        self._check(self.lib.bv_phmm_compute_regions(self.h, C.byref(v.c), _ptr(out), C.byref(st)))
+        res = out[:n]
+        return (res, st.as_dict()) if with_stats else res
+
+    def stage(self, batch: RegionBatch) -> int:
+        v = _BatchView(batch)
+        self._check(self.lib.bv_phmm_stage_regions(self.h, C.byref(v.c)))
+        self._staged = v
+        self._staged_n = int(self.lib.bv_phmm_region_results(C.byref(v.c)))
+        return self._staged_n
+
+    def run(self) -> dict:
+        st = N.Stats()
+        self._check(self.lib.bv_phmm_run_staged(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def fetch(self, n: Optional[int] = None, out: Optional[np.ndarray] = None) -> np.ndarray:
+        n = self._staged_n if n is None else n
+        if out is None:
+            out = np.empty(max(n, 1), np.float64)
+        self._check(self.lib.bv_phmm_fetch_results(self.h, _ptr(out), n))
+        return out[:n]
+
+    def host_register(self, arr: np.ndarray):
+        self._check(self.lib.bv_phmm_host_register(self.h, _ptr(arr), arr.nbytes))
+
+    def host_unregister(self, arr: np.ndarray):
+        self._check(self.lib.bv_phmm_host_unregister(self.h, _ptr(arr)))
+
+    def compute_testcases(self, tcs: Sequence[tuple]) -> np.ndarray:
+        """tcs: (read, q, i, d, c, hap) byte strings; returns log10 per testcase."""
+        keep = []
+        arr = (N.TestcaseC * max(len(tcs), 1))()
+        cache = {}
+        def buf(b: bytes):
+            key = id(b)
+            if key not in cache:
+                a = np.frombuffer(bytes(b), dtype=np.uint8).copy()
+                cache[key] = a
+                keep.append(a)
+            return _ptr(cache[key])
+        for k, (rs, q, i, d, c, hap) in enumerate(tcs):
+            t = arr[k]
+            t.rslen, t.haplen = len(rs), len(hap)
+            t.rs, t.q, t.i, t.d, t.c, t.hap = buf(rs), buf(q), buf(i), buf(d), buf(c), buf(hap)
+        out = np.empty(max(len(tcs), 1), np.float64)
+        self._check(self.lib.bv_phmm_compute_testcases(self.h, arr, len(tcs), _ptr(out), None))
+        return out[: len(tcs)]
+
+    def shacc_calculate(self, reads: Sequence[tuple], haps: Sequence[bytes]) -> np.ndarray:
+        """reads: (bases, q, i, d, c) byte strings; returns float32 [reads, haps] log10."""
+        keep = []
+        def b(x):
+            a = np.frombuffer(bytes(x), dtype=np.uint8).copy()
+            keep.append(a)
+            return _ptr(a)
+        ra = (N.ShaccRead * max(len(reads), 1))()
+        for k, (s, q, i, d, c) in enumerate(reads):
+            ra[k] = N.ShaccRead(len(s), b(s), b(q), b(i), b(d), b(c))
+        ha = (N.ShaccHap * max(len(haps), 1))()
+        for k, s in enumerate(haps):
+            ha[k] = N.ShaccHap(len(s), b(s))
+        res = np.zeros(max(len(reads) * len(haps), 1), np.float32)
+        cells = sum(len(r[0]) for r in reads) * sum(len(h) for h in haps)
+        bt = N.ShaccBatch(len(reads), len(haps), cells, ra, ha, res.ctypes.data_as(C.POINTER(C.c_float)))
+        self._check(self.lib.bv_phmm_shacc_calculate(self.h, C.byref(bt)))
+        return res[: len(reads) * len(haps)].reshape(len(reads), len(haps))
+
+
+# --- reference-shaped objects ------------------------------------------------
+class Haplotype:
+    """The field of ``biovoltron::Haplotype`` the PairHMM reads (haplotype.hpp:12)."""
+
+    def __init__(self, seq):
+        self.seq = seq.encode() if isinstance(seq, str) else bytes(seq)
+
+
+class SamRecord:
+    """The fields and penalty views of ``SamRecord`` the PairHMM reads (sam.hpp:186-475).
+
+    The reference's ``insertion_gop()``/``deletion_gop()``/``overall_gcp()``
+    return views of 256-byte static strings and overrun them for longer reads;
+    here they have the read's length, filled with the same bytes.
+    """
+
+    def __init__(self, seq, qual):
+        self.seq = seq.encode() if isinstance(seq, str) else bytes(seq)
+        self.qual = qual.encode() if isinstance(qual, str) else bytes(qual)
+
+    def size(self) -> int:
+        return len(self.seq)
+
+    def insertion_gop(self) -> bytes:
+        return bytes([GAP_OPEN_PENALTY_BYTE]) * len(self.seq)
+
+    def deletion_gop(self) -> bytes:
+        return bytes([GAP_OPEN_PENALTY_BYTE]) * len(self.seq)
+
+    def overall_gcp(self) -> bytes:
+        return bytes([GAP_CONTINUATION_PENALTY_BYTE]) * len(self.seq)
+
+
+def normalize_likelihoods(ll: List[List[float]]) -> None:
+    """PairHMM::normalize_likelihoods (pairhmm.hpp:83-93), in place."""
+    for row in ll:
+        if not row:
+            continue
+        cap = max(row) + MAXIMUM_BEST_ALT_LIKELIHOOD_DIFFERENCE
+        for k, v in enumerate(row):
+            if v < cap:
+                row[k] = cap
+
+
+def filter_poorly_modeled_reads(reads: list, ll: List[List[float]]) -> None:
+    """PairHMM::filter_poorly_modeled_reads (pairhmm.hpp:95-114), in place.
+
+    Keeps the rows whose best likelihood is below the threshold, exactly as
+    the reference compares.
+    """
+    kept_r, kept_l = [], []
+    for r, row in zip(reads, ll):
+        best = max(row)
+        thr = min(MAXIMUM_EXPECTED_ERROR_PER_READ, math.ceil(r.size() * EXPECTED_ERROR_RATE_PER_BASE)) * LOG10_QUALITY_PER_BASE
+        if best < thr:
+            kept_r.append(r)
+            kept_l.append(row)
+    reads[:] = kept_r
+    ll[:] = kept_l
+
+
+class GpuPairHMM:
+    """Drop-in for ``AvxPairHMM`` (pairhmm_avx.hpp:24-172) on one GPU."""
+
+    def __init__(self, device: int = 0, use_double: bool = False, engine: Optional[PairHMMEngine] = None):
+        self.engine = engine or PairHMMEngine(device=device, precision="f64" if use_double else "auto")
+
+    def compute_likelihoods(self, haplotypes: Sequence[Haplotype], reads: list) -> List[List[float]]:
+        nr, nh = len(reads), len(haplotypes)
+        if nr == 0:
+            return []
+        tcs = []
+        for r in reads:
+            ins, dele, gcp = r.insertion_gop(), r.deletion_gop(), r.overall_gcp()
+            for h in haplotypes:
+                tcs.append((r.seq, r.qual, ins, dele, gcp, h.seq))
+        flat = self.engine.compute_testcases(tcs) if tcs else np.zeros(0)
+        ll = [list(map(float, flat[k * nh:(k + 1) * nh])) for k in range(nr)]
+        if nh == 0:
+            return ll
+        normalize_likelihoods(ll)
+        filter_poorly_modeled_reads(reads, ll)
+        return ll

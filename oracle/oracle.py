@@ -33,28 +33,40 @@ class Testcase(C.Structure):
     ]
 
 
+TESTCASE_DTYPE = np.dtype([("rslen", np.int32), ("haplen", np.int32), ("q", np.uint64), ("i", np.uint64),
+                           ("d", np.uint64), ("c", np.uint64), ("hap", np.uint64), ("rs", np.uint64)])
+assert TESTCASE_DTYPE.itemsize == C.sizeof(Testcase)
+
+
 class TestcaseArray:
-    """Testcases pointing into a RegionBatch's arrays (which must stay alive)."""
+    """Testcases pointing into a RegionBatch's arrays (which must stay alive).
+
+    Built with numpy in the C struct's layout, so millions of pairs cost
+    milliseconds."""
+
+    __test__ = False
 
     def __init__(self, batch, reads: np.ndarray, haps: np.ndarray):
         self.batch = batch
+        reads = np.asarray(reads, np.int64)
+        haps = np.asarray(haps, np.int64)
         n = len(reads)
         self.n = n
-        self.arr = (Testcase * max(n, 1))()
-        ro, ho = batch.read_offsets, batch.hap_offsets
-        base = {k: getattr(batch, k).ctypes.data for k in ("read_bases", "read_q", "read_i", "read_d", "read_c", "hap_bases")}
-        for k in range(n):
-            r, h = int(reads[k]), int(haps[k])
-            a = int(ro[r])
-            tc = self.arr[k]
-            tc.rslen = int(ro[r + 1] - a)
-            tc.haplen = int(ho[h + 1] - ho[h])
-            tc.q = base["read_q"] + a
-            tc.i = base["read_i"] + a
-            tc.d = base["read_d"] + a
-            tc.c = base["read_c"] + a
-            tc.rs = base["read_bases"] + a
-            tc.hap = base["hap_bases"] + int(ho[h])
+        ro, ho = batch.read_offsets.astype(np.int64), batch.hap_offsets.astype(np.int64)
+        a = np.zeros(max(n, 1), TESTCASE_DTYPE)
+        if n:
+            start = ro[reads]
+            a["rslen"][:n] = (ro[reads + 1] - start).astype(np.int32)
+            a["haplen"][:n] = (ho[haps + 1] - ho[haps]).astype(np.int32)
+            for f, arr in (("q", batch.read_q), ("i", batch.read_i), ("d", batch.read_d), ("c", batch.read_c),
+                           ("rs", batch.read_bases)):
+                a[f][:n] = np.uint64(arr.ctypes.data) + start.astype(np.uint64)
+            a["hap"][:n] = np.uint64(batch.hap_bases.ctypes.data) + ho[haps].astype(np.uint64)
+        self.np = a
+        self.arr = a.ctypes.data_as(C.POINTER(Testcase))
+
+    def __getitem__(self, k):
+        return self.arr[k]
 
     @classmethod
     def for_batch(cls, batch, limit: Optional[int] = None, sel: Optional[np.ndarray] = None):
@@ -164,10 +176,10 @@ class Reference:
         return out, used.astype(bool)
 
     def prob_f32(self, tcs: TestcaseArray) -> np.ndarray:
-        return np.array([self._f32(C.byref(tcs.arr[k])) for k in range(tcs.n)], np.float32)
+        return np.array([self._f32(C.pointer(tcs.arr[k])) for k in range(tcs.n)], np.float32)
 
     def prob_f64(self, tcs: TestcaseArray) -> np.ndarray:
-        return np.array([self._f64(C.byref(tcs.arr[k])) for k in range(tcs.n)], np.float64)
+        return np.array([self._f64(C.pointer(tcs.arr[k])) for k in range(tcs.n)], np.float64)
 
     def tables(self):
         L = self.lib

@@ -1,0 +1,150 @@
+"""CUDA path vs the oracle and the reference's golden vectors, through the C ABI.
+
+Tolerances: the FP32 path differs from the reference's FP32 kernel by
+single-precision rounding (different operation order, fused multiply-adds);
+log10 likelihoods are asserted within 1e-4 where the reference is finite and
+within 1e-3 (the contract) against the FP64 oracle everywhere.
+"""
+import numpy as np
+import pytest
+
+from biovoltron_b200 import workloads as W
+from conftest import FIXTURES, load_golden
+from oracle.oracle import TestcaseArray
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP32 = 1e-4
+TOL_CONTRACT = 1e-3
+
+
+def _check(got, ref_log10, truth, tol=TOL_FP32):
+    got = np.asarray(got)
+    fin = np.isfinite(truth)
+    assert np.all(np.isfinite(got[fin])), "GPU result not finite where the FP64 oracle is"
+    assert np.max(np.abs(got[fin] - truth[fin]), initial=0) <= TOL_CONTRACT
+    rf = np.isfinite(ref_log10)
+    assert np.max(np.abs(got[rf] - ref_log10[rf]), initial=0) <= tol
+    # where the oracle says the likelihood is exactly zero, so does the GPU
+    assert np.all(np.isneginf(got[~fin]))
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_golden_fixtures(engine, name):
+    b, exp = load_golden(name)
+    got, st = engine.compute_regions(b, with_stats=True)
+    assert st["pairs"] == b.n_pairs
+    _check(got, exp["ref_log10"], exp["oracle_rescaled"])
+
+
+@pytest.mark.parametrize("name", ["config0", "edge_cases"])
+def test_fp64_mode_matches_reference_fp64(name):
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    b, exp = load_golden(name)
+    with PairHMMEngine(precision="f64") as e:
+        got = e.compute_regions(b)
+    pd = exp["ref_prob_f64"].astype(np.float64)
+    with np.errstate(divide="ignore"):
+        ref = np.log10(pd) - 1020 * np.log10(2.0)
+    fin = np.isfinite(ref)
+    assert np.max(np.abs(got[fin] - ref[fin])) < 1e-9
+    _check(got, exp["ref_log10"], exp["oracle_rescaled"], tol=TOL_FP32)
+
+
+def test_rescue_flags_match_reference_rule(engine):
+    b, exp = load_golden("edge_cases")
+    _, st = engine.compute_regions(b, with_stats=True)
+    # every pair the reference sends to FP64 is far below the threshold here,
+    # so the GPU rescues the same pairs (and reports them)
+    assert st["rescued"] == int(exp["ref_used_f64"].sum())
+
+
+def test_config1_sample_vs_oracle(engine, oracle):
+    b = W.config1(seed=77, n_regions=24)
+    got = engine.compute_regions(b)
+    truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
+    ref, _ = oracle.log10_reference_rule(TestcaseArray.for_batch(b))
+    _check(got, ref, truth)
+
+
+def test_config2_long_reads_vs_rescaled_oracle(engine, oracle):
+    b = W.config2(seed=21, n_pairs=8, max_read=3000, max_hap=4000)
+    got, st = engine.compute_regions(b, with_stats=True)
+    truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
+    assert np.all(np.isfinite(got))
+    assert np.max(np.abs(got - truth)) <= TOL_CONTRACT
+    assert st["rescued"] == b.n_pairs  # all far below 1e-28 (log10 ~ -hundreds)
+
+
+def test_staged_graph_replay_is_deterministic(engine):
+    b = W.config1(seed=3, n_regions=16)
+    direct = engine.compute_regions(b)
+    n = engine.stage(b)
+    outs = []
+    for _ in range(3):  # first run launches, later runs replay the captured graph
+        engine.run()
+        outs.append(engine.fetch(n).copy())
+    for o in outs:
+        assert np.array_equal(o, direct)
+
+
+def test_testcase_and_shacc_entry_points_agree(engine):
+    b, exp = load_golden("config0")
+    r, h = b.pair_index()
+    tcs = []
+    for k in range(len(r)):
+        rd = b.read(int(r[k]))
+        tcs.append((rd[0], rd[1], rd[2], rd[3], rd[4], b.hap(int(h[k]))))
+    got_tc = engine.compute_testcases(tcs)
+    reads = [b.read(k) for k in range(b.n_reads)]
+    haps = [b.hap(k) for k in range(b.n_haps)]
+    got_sh = engine.shacc_calculate(reads, haps)
+    got_rg = engine.compute_regions(b)
+    assert np.array_equal(got_tc, got_rg)
+    assert np.array_equal(got_sh.reshape(-1), got_rg.astype(np.float32))
+
+
+def test_gpu_pairhmm_drop_in(engine):
+    from biovoltron_b200.pairhmm import GpuPairHMM, Haplotype, SamRecord
+    b, exp = load_golden("ref_test")
+    haps = [Haplotype(b.hap(k)) for k in range(8)]
+    reads = [SamRecord(b.read(k)[0], b.read(k)[1]) for k in range(3)]
+    w = GpuPairHMM(engine=engine)
+    ll = w.compute_likelihoods(haps, reads)
+    raw = exp["ref_log10"].reshape(3, 8)
+    for row in ll:
+        assert len(row) == 8
+    # rows kept are those whose best is below -8 (the reference's filter)
+    kept = [k for k in range(3) if raw[k].max() < -8]
+    assert len(ll) == len(kept)
+    for row, k in zip(ll, kept):
+        capped = np.maximum(raw[k], raw[k].max() - 4.5)
+        assert np.max(np.abs(np.array(row) - capped)) < TOL_FP32
+
+
+def test_empty_and_ragged_inputs(engine):
+    # empty batch
+    e = W.from_pairs([])
+    assert engine.compute_regions(e).size == 0
+    # regions with zero reads / zero haps, empty reads and haps
+    parts = [(b"", b"", b"", b"", b"", b"ACGT"), (b"ACGT", b"IIII", b"----", b"----", b"++++", b""),
+             (b"A", b"I", b"-", b"-", b"+", b"A")]
+    b = W.from_pairs(parts)
+    got = engine.compute_regions(b)
+    assert np.isneginf(got[0]) and np.isneginf(got[1]) and np.isfinite(got[2])
+
+
+def test_invalid_arguments_are_rejected(engine):
+    from biovoltron_b200.native import NativeError
+    b = W.config0(0)
+    bad = W.RegionBatch(**{k: getattr(b, k) for k in ("read_bases", "read_q", "read_i", "read_d", "read_c",
+                                                       "read_offsets", "hap_bases", "hap_offsets",
+                                                       "region_reads")}, region_haps=np.array([0, 99], np.int64))
+    with pytest.raises(NativeError) as ei:
+        engine.compute_regions(bad)
+    assert ei.value.status == 1
+    long_hap = W.from_pairs([(b"ACGT", b"IIII", b"----", b"----", b"++++", b"A" * 40000)])
+    with pytest.raises(NativeError):
+        engine.compute_regions(long_hap)
+    # the context still works afterwards
+    assert np.isfinite(engine.compute_regions(W.config0(0))).all()

@@ -1,0 +1,109 @@
+"""Host-side logic: the normalise/filter step of the reference call, the
+GpuPairHMM wrapper's layout and side effects (driven by the oracle through a
+stand-in engine, no GPU), and the workload generators."""
+import math
+
+import numpy as np
+
+from biovoltron_b200 import workloads as W
+from biovoltron_b200.pairhmm import (GpuPairHMM, Haplotype, SamRecord, filter_poorly_modeled_reads,
+                                     normalize_likelihoods)
+from oracle.oracle import TestcaseArray
+
+
+def test_normalize_caps_at_best_minus_4_5():
+    ll = [[-10.0, -20.0, -12.0], [-3.0, -3.0, -100.0]]
+    normalize_likelihoods(ll)
+    assert ll == [[-10.0, -14.5, -12.0], [-3.0, -3.0, -7.5]]
+
+
+def test_filter_keeps_rows_below_threshold_like_the_reference():
+    # threshold = min(2, ceil(0.02 * len)) * -4: -8 for reads of >= 51 bases,
+    # -4 for reads of <= 50; the reference keeps rows whose best is BELOW it.
+    reads = [SamRecord("A" * 100, "I" * 100), SamRecord("A" * 100, "I" * 100), SamRecord("A" * 40, "I" * 40),
+             SamRecord("A" * 40, "I" * 40)]
+    ll = [[-7.0, -9.0], [-8.5, -30.0], [-3.9, -5.0], [-4.1, -6.0]]
+    filter_poorly_modeled_reads(reads, ll)
+    assert ll == [[-8.5, -30.0], [-4.1, -6.0]]
+    assert [r.size() for r in reads] == [100, 40]
+
+
+class _OracleEngine:
+    """Stand-in for PairHMMEngine that scores testcases with the CPU oracle."""
+
+    def __init__(self, oracle):
+        self.oracle = oracle
+
+    def compute_testcases(self, tcs):
+        b = W.from_pairs(tcs)
+        out, _ = self.oracle.log10_reference_rule(TestcaseArray.for_batch(b))
+        return out
+
+
+def test_gpu_pairhmm_wrapper_semantics(oracle):
+    rng = np.random.default_rng(1)
+    base = bytes(W._random_seq(rng, 400))
+    haps = [Haplotype(base), Haplotype(base[:200] + b"A" + base[200:]), Haplotype(bytes(W._random_seq(rng, 400)))]
+    reads = [SamRecord(base[50:150], b";" * 100), SamRecord(base[100:260], b"5" * 160),
+             SamRecord(bytes(W._random_seq(rng, 120)), b"+" * 120)]
+    orig = list(reads)
+    w = GpuPairHMM(engine=_OracleEngine(oracle))
+    ll = w.compute_likelihoods(haps, reads)
+    # recompute by hand: testcases in [read][hap] order with SAM penalty bytes
+    raw = []
+    for r in orig:
+        row = []
+        for h in haps:
+            tc = (r.seq, r.qual, bytes([73]) * r.size(), bytes([73]) * r.size(), bytes([43]) * r.size(), h.seq)
+            b = W.from_pairs([tc])
+            row.append(float(oracle.log10_reference_rule(TestcaseArray.for_batch(b))[0][0]))
+        raw.append(row)
+    normalize_likelihoods(raw)
+    exp_reads = list(orig)
+    filter_poorly_modeled_reads(exp_reads, raw)
+    assert ll == raw
+    assert [r.seq for r in reads] == [r.seq for r in exp_reads]
+
+
+def test_sam_penalty_views_have_read_length():
+    r = SamRecord("ACGT" * 100, "I" * 400)
+    assert r.insertion_gop() == bytes([73]) * 400
+    assert r.deletion_gop() == bytes([73]) * 400
+    assert r.overall_gcp() == bytes([43]) * 400
+
+
+def test_config0_shape():
+    b = W.config0(0)
+    assert b.n_regions == 1 and b.n_reads == 64 and b.n_haps == 8
+    assert set(b.read_lengths()) == {150}
+    hl = b.hap_lengths()
+    assert hl.min() >= 280 and hl.max() <= 320
+    q = b.read_q
+    assert q.min() >= 10 and q.max() <= 40
+    assert set(np.unique(b.read_i)) == {45} and set(np.unique(b.read_c)) == {10}
+    assert set(np.unique(b.read_bases)) <= set(b"ACGT")
+    r, h = b.pair_index()
+    assert len(r) == 512 and r[0] == 0 and h[:8].tolist() == list(range(8))
+
+
+def test_config1_distribution_small():
+    b = W.config1(seed=9, n_regions=64)
+    nr = np.diff(b.region_reads)
+    nh = np.diff(b.region_haps)
+    assert nr.min() >= 20 and nr.max() <= 500
+    assert nh.min() >= 2 and nh.max() <= 32
+    rl = b.read_lengths()
+    assert rl.min() >= 50 and rl.max() <= 250
+    assert b.n_pairs == int((nr * nh).sum())
+
+
+def test_config2_shape():
+    b = W.config2(seed=2, n_pairs=4, max_read=3000, max_hap=4000)
+    rl, hl = b.read_lengths(), b.hap_lengths()
+    assert (hl >= rl + 500).all()
+    assert b.read_q.min() >= 5 and b.read_q.max() <= 30
+
+
+def test_generators_are_seeded():
+    a, b = W.config1(seed=4, n_regions=3), W.config1(seed=4, n_regions=3)
+    assert np.array_equal(a.read_bases, b.read_bases) and np.array_equal(a.hap_bases, b.hap_bases)
