@@ -324,7 +324,12 @@ bv_status Engine::stage(const bv_region_batch& b) {
   return BV_OK;
 }
 
-bv_status Engine::enqueue_kernels() {
+bv_status Engine::enqueue_kernels(bool capturing) {
+  // Inside stream capture, timing events become event-record nodes of the
+  // graph only when recorded as external events.
+  auto rec = [&](cudaEvent_t ev) {
+    return capturing ? cudaEventRecordWithFlags(ev, stream_, cudaEventRecordExternal) : cudaEventRecord(ev, stream_);
+  };
   BV_CUDA(cudaMemsetAsync(d_counters_.get(), 0, sizeof(Counters), stream_), "memset counters");
   if (!f64_items_.empty()) {
     BV_CUDA(launch_set_u64(&d_counters_.as<Counters>()->rescue_count, (unsigned long long)f64_items_.size(), stream_),
@@ -342,7 +347,7 @@ bv_status Engine::enqueue_kernels() {
   p.out = d_out_.as<double>();
   p.rescue = d_rescue_.as<PairRef>();
   p.rescue_cap = std::max<int64_t>(n_results_, 1);
-  BV_CUDA(cudaEventRecord(ev_[2], stream_), "event");
+  BV_CUDA(rec(ev_[2]), "event");
   for (const auto& lp : plans_) {
     p.unit_base = lp.unit_base;
     p.n_units = lp.n_units;
@@ -356,7 +361,7 @@ bv_status Engine::enqueue_kernels() {
     p.rescale_target = 0;
     BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP32 forward launch");
   }
-  BV_CUDA(cudaEventRecord(ev_[3], stream_), "event");
+  BV_CUDA(rec(ev_[3]), "event");
   {
     const LaunchPlan& lp = rescue_plan_;
     p.unit_base = 0;
@@ -371,7 +376,7 @@ bv_status Engine::enqueue_kernels() {
     p.rescale_target = kRescaleTarget;
     BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP64 forward launch");
   }
-  BV_CUDA(cudaEventRecord(ev_[4], stream_), "event");
+  BV_CUDA(rec(ev_[4]), "event");
   return BV_OK;
 }
 
@@ -391,7 +396,7 @@ bv_status Engine::run(bv_phmm_stats* stats) {
   if (runs_since_stage_ == 0 || !graph_exec_) {
     if (runs_since_stage_ >= 1 && !graph_exec_) {
       BV_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-      bv_status s = enqueue_kernels();
+      bv_status s = enqueue_kernels(true);
       cudaGraph_t g = nullptr;
       cudaError_t ce = cudaStreamEndCapture(stream_, &g);
       if (s != BV_OK) {
@@ -403,7 +408,7 @@ bv_status Engine::run(bv_phmm_stats* stats) {
       BV_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0), "graph instantiate");
       BV_CUDA(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
     } else {
-      bv_status s = enqueue_kernels();
+      bv_status s = enqueue_kernels(false);
       if (s != BV_OK) return s;
     }
   } else {

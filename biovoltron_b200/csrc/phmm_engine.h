@@ -65,7 +65,7 @@ class Engine {
   bv_status validate(const bv_region_batch& b);
   bv_status plan(const bv_region_batch& b);
   bv_status upload(const bv_region_batch& b);
-  bv_status enqueue_kernels();
+  bv_status enqueue_kernels(bool capturing);
   void destroy_graph();
 
   bv_phmm_options opt_;

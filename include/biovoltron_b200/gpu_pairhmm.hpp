@@ -1,0 +1,128 @@
+// gpu_pairhmm.hpp -- C++20 drop-in for biovoltron::AvxPairHMM / PairHMM.
+//
+// GpuPairHMM::compute_likelihoods(haplotypes, reads) has the signature, the
+// [read][hap] result layout and the side effects of
+// AvxPairHMM::compute_likelihoods (include/biovoltron/algo/align/
+// inexact_match/pairhmm_avx.hpp:160-171), which HaplotypeCaller calls through
+// PairHMM::compute_likelihoods (haplotypecaller.hpp:90):
+//   1. testcases are built as AvxPairHMM::getData builds them (:38-81): read
+//      bases, qual, insertion_gop(), deletion_gop(), overall_gcp() and each
+//      haplotype's seq, borrowed for the call;
+//   2. log10 likelihoods come from the GPU (FP32, FP64 below 1e-28);
+//   3. PairHMM::normalize_likelihoods (pairhmm.hpp:83-93) caps every value at
+//      the row's best - 4.5;
+//   4. PairHMM::filter_poorly_modeled_reads (pairhmm.hpp:95-114) keeps the
+//      reads whose best likelihood is below min(2, ceil(0.02 len)) * -4 --
+//      the reference's comparison, unchanged -- and removes the others from
+//      `reads`.
+// Read and haplotype types are template parameters, so Biovoltron's
+// SamRecord<> / Haplotype work unchanged (they provide .seq, .qual and the
+// three penalty views), as do any types with the same members.
+//
+// Errors from the C ABI are thrown as std::runtime_error.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "bv_pairhmm.h"
+
+namespace biovoltron_b200 {
+
+class GpuPairHMM {
+ public:
+  static constexpr double kMaximumBestAltLikelihoodDifference = -4.5;  // pairhmm.hpp:28
+  static constexpr double kExpectedErrorRatePerBase = 0.02;             // pairhmm.hpp:29
+  static constexpr double kLog10QualityPerBase = -4.0;                  // pairhmm.hpp:30
+  static constexpr double kMaximumExpectedErrorPerRead = 2.0;           // pairhmm.hpp:31
+
+  explicit GpuPairHMM(int device = 0, bool use_double = false) {
+    bv_phmm_options o;
+    bv_phmm_default_options(&o);
+    o.device = device;
+    o.precision = use_double ? BV_PRECISION_F64 : BV_PRECISION_AUTO;
+    check(bv_phmm_create(&o, &ctx_), "bv_phmm_create");
+  }
+  ~GpuPairHMM() { bv_phmm_destroy(ctx_); }
+  GpuPairHMM(const GpuPairHMM&) = delete;
+  GpuPairHMM& operator=(const GpuPairHMM&) = delete;
+
+  template <class HapVec, class ReadVec>
+  std::vector<std::vector<double>> compute_likelihoods(const HapVec& haplotypes, ReadVec& reads) {
+    const size_t nr = reads.size(), nh = haplotypes.size();
+    std::vector<std::vector<double>> ll(nr, std::vector<double>(nh, 0.0));
+    if (nr == 0 || nh == 0) return ll;
+    std::vector<bv_testcase> tcs;
+    tcs.reserve(nr * nh);
+    for (const auto& r : reads) {
+      const int len = static_cast<int>(r.seq.size());
+      const char* ins = r.insertion_gop().data();
+      const char* del = r.deletion_gop().data();
+      const char* gcp = r.overall_gcp().data();
+      for (const auto& h : haplotypes) {
+        bv_testcase t{};
+        t.rslen = len;
+        t.haplen = static_cast<int>(h.seq.size());
+        t.q = r.qual.data();
+        t.i = ins;
+        t.d = del;
+        t.c = gcp;
+        t.hap = h.seq.data();
+        t.rs = r.seq.data();
+        tcs.push_back(t);
+      }
+    }
+    std::vector<double> flat(nr * nh);
+    check(bv_phmm_compute_testcases(ctx_, tcs.data(), static_cast<int64_t>(tcs.size()), flat.data(), nullptr),
+          "bv_phmm_compute_testcases");
+    for (size_t r = 0; r < nr; ++r)
+      std::copy(flat.begin() + r * nh, flat.begin() + (r + 1) * nh, ll[r].begin());
+    normalize_likelihoods(ll);
+    filter_poorly_modeled_reads(reads, ll);
+    return ll;
+  }
+
+  static void normalize_likelihoods(std::vector<std::vector<double>>& log_likelihoods) {
+    for (auto& row : log_likelihoods) {
+      if (row.empty()) continue;
+      const double cap = *std::max_element(row.begin(), row.end()) + kMaximumBestAltLikelihoodDifference;
+      for (auto& v : row)
+        if (v < cap) v = cap;
+    }
+  }
+
+  template <class ReadVec>
+  static void filter_poorly_modeled_reads(ReadVec& reads, std::vector<std::vector<double>>& log_likelihoods) {
+    ReadVec kept_reads;
+    std::vector<std::vector<double>> kept;
+    for (size_t i = 0; i < log_likelihoods.size(); ++i) {
+      const double best = *std::max_element(log_likelihoods[i].begin(), log_likelihoods[i].end());
+      const double thr = std::min(kMaximumExpectedErrorPerRead,
+                                  std::ceil(reads[i].seq.size() * kExpectedErrorRatePerBase)) *
+                         kLog10QualityPerBase;
+      if (best < thr) {
+        kept_reads.push_back(std::move(reads[i]));
+        kept.push_back(std::move(log_likelihoods[i]));
+      }
+    }
+    reads.swap(kept_reads);
+    log_likelihoods.swap(kept);
+  }
+
+  bv_phmm_ctx* context() const { return ctx_; }
+
+ private:
+  void check(bv_status s, const char* what) {
+    if (s != BV_OK) {
+      std::string msg = std::string(what) + ": " + bv_phmm_status_string(s);
+      if (ctx_) msg += std::string(" (") + bv_phmm_last_error(ctx_) + ")";
+      throw std::runtime_error(msg);
+    }
+  }
+  bv_phmm_ctx* ctx_ = nullptr;
+};
+
+}  // namespace biovoltron_b200

@@ -1,0 +1,59 @@
+// adapter_check.cpp -- drives include/biovoltron_b200/gpu_pairhmm.hpp with
+// record types shaped like Biovoltron's SamRecord<> / Haplotype.
+// Input (stdin): lines "H <bases>" and "R <bases> <quals>"; quals are raw
+// bytes given as printable characters.  Output: the kept reads' indices and
+// the [read][hap] log10 matrix after normalize/filter, one row per line.
+#include <cstdio>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <string_view>
+#include <vector>
+
+#include "biovoltron_b200/gpu_pairhmm.hpp"
+
+struct Haplotype {
+  std::string seq;
+};
+
+struct SamRecord {
+  std::string seq, qual;
+  int id = 0;
+  std::string gop, gcp;  // full-length penalty strings ('!'+40, '!'+10)
+  std::string_view insertion_gop() const { return gop; }
+  std::string_view deletion_gop() const { return gop; }
+  std::string_view overall_gcp() const { return gcp; }
+};
+
+int main() {
+  std::vector<Haplotype> haps;
+  std::vector<SamRecord> reads;
+  std::string line;
+  while (std::getline(std::cin, line)) {
+    std::istringstream ss(line);
+    std::string tag;
+    ss >> tag;
+    if (tag == "H") {
+      Haplotype h;
+      ss >> h.seq;
+      haps.push_back(h);
+    } else if (tag == "R") {
+      SamRecord r;
+      ss >> r.seq >> r.qual;
+      r.id = (int)reads.size();
+      r.gop.assign(r.seq.size(), (char)(40 + '!'));
+      r.gcp.assign(r.seq.size(), (char)(10 + '!'));
+      reads.push_back(r);
+    }
+  }
+  biovoltron_b200::GpuPairHMM hmm(0);
+  auto ll = hmm.compute_likelihoods(haps, reads);
+  std::printf("kept");
+  for (const auto& r : reads) std::printf(" %d", r.id);
+  std::printf("\n");
+  for (const auto& row : ll) {
+    for (size_t j = 0; j < row.size(); ++j) std::printf(j ? " %.9f" : "%.9f", row[j]);
+    std::printf("\n");
+  }
+  return 0;
+}

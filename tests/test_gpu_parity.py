@@ -82,7 +82,8 @@ def test_staged_graph_replay_is_deterministic(engine):
     n = engine.stage(b)
     outs = []
     for _ in range(3):  # first run launches, later runs replay the captured graph
-        engine.run()
+        st = engine.run()
+        assert st["ms_fp32"] > 0 and st["ms_fp64"] > 0  # event nodes replay with the graph
         outs.append(engine.fetch(n).copy())
     for o in outs:
         assert np.array_equal(o, direct)
