@@ -42,408 +42,14 @@
 //   FP64 kernel renormalises the strip boundary row by an exact power of two
 //   so reads of many kilobases stay finite.
 #include <cuda_runtime.h>
-#include <cuda_pipeline.h>
 #include <cstdint>
 #include <cmath>
 
 #include "phmm_common.h"
+#include "phmm_device.cuh"
 #include "phmm_kernels.h"
 
 namespace bvphmm {
-
-template <typename T> struct Vec16;
-template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
-template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
-
-__device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
-
-template <typename T> __device__ __forceinline__ const T* ph2pr_tab(const Tables* t);
-template <> __device__ __forceinline__ const float* ph2pr_tab<float>(const Tables* t) { return t->ph2pr_f; }
-template <> __device__ __forceinline__ const double* ph2pr_tab<double>(const Tables* t) { return t->ph2pr_d; }
-template <typename T> __device__ __forceinline__ const T* mm_tab(const Tables* t);
-template <> __device__ __forceinline__ const float* mm_tab<float>(const Tables* t) { return t->mm_f; }
-template <> __device__ __forceinline__ const double* mm_tab<double>(const Tables* t) { return t->mm_d; }
-
-__device__ __forceinline__ uint32_t base_code(uint32_t b) {
-  // ConvertChar (pairhmm_common.h:26-44): A0 C1 T2 G3 N4, anything else 0.
-  return b == 'C' ? 1u : b == 'T' ? 2u : b == 'G' ? 3u : b == 'N' ? 4u : 0u;
-}
-
-__device__ __forceinline__ int mm_index(int ins, int del) {
-  const int mx = ins > del ? ins : del;
-  const int mn = ins > del ? del : ins;
-  return ((mx * (mx + 1)) >> 1) + mn;
-}
-
-// Shared-memory layout of one warp's slice.
-template <typename T, int RT>
-struct WarpSmem {
-  static constexpr int VPC = Vec16<T>::n;                 // values per 16-byte chunk
-  static constexpr int RTP = (RT + VPC - 1) / VPC * VPC;   // rows rounded to chunks
-  static constexpr int NCH = RTP / VPC;                    // chunks per code
-  static constexpr int kCodeStride = NCH * kWarp * 16;     // bytes per code
-  static constexpr int kEtabBytes = kCodes * kCodeStride;
-  static constexpr int kRingInCols = 64;
-  static constexpr int kRingOutCols = 32;
-  static constexpr int kColBytes = 4 * (int)sizeof(T);     // M, Xh, Yh, unused
-  static constexpr int kRingBytes = (kRingInCols + kRingOutCols) * kColBytes;
-};
-
-// Per-lane row constants for one strip.
-// FP32 keeps X and Y divided by pMX / pMY (one FMA each, see above).  FP64,
-// the rescue path, uses the reference's unscaled form: X/pMX can exceed the
-// exponent range when insertion qualities jump between rows, and the FP64
-// boundary rows are renormalised close to the top of the range.
-template <typename T> struct ScaledXY { static constexpr bool value = sizeof(T) == 4; };
-
-// Per-lane row constants for one strip.  Scaled form: mm = pMM, cx = pGAPM *
-// pMX(r-1), cy = pGAPM * pMY(r-1), kap = pXX pMX(r-1)/pMX(r), g = pYY.
-// Unscaled form: mm = pMM, cx = pGAPM, kap = pMX, my = pMY, g = pXX = pYY.
-template <typename T, int RT>
-struct Rows {
-  T mm[RT], cx[RT], cy[RT], kap[RT], my[RT], g[RT], y0[RT];
-  T pmx_bottom;
-};
-
-// Computes the lane's row constants for the rows [rbase, rbase+RT) (real row
-// numbers, row 0 = initial row, negative = padding) and writes the lane's
-// emission-table column.  initializeVectors (avx-pairhmm-template.h:108-127)
-// and stripeINITIALIZATION (:150-158) give the per-row probabilities.
-template <typename T, int RT>
-__device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const uchar4* __restrict__ quals,
-                                           const uint8_t* __restrict__ bases, int rbase, T init_y,
-                                           Rows<T, RT>& rw, unsigned char* etab_lane) {
-  using S = WarpSmem<T, RT>;
-  using V = typename Vec16<T>::type;
-  const T* ph = ph2pr_tab<T>(tb);
-  const T* mmt = mm_tab<T>(tb);
-  T em[S::RTP], ex[S::RTP];
-  uint32_t rc[S::RTP];
-  bool valid[S::RTP];
-#pragma unroll
-  for (int j = 0; j < S::RTP; ++j) { em[j] = T(0); ex[j] = T(0); rc[j] = 0; valid[j] = false; }
-  rw.pmx_bottom = T(1);
-#pragma unroll
-  for (int j = 0; j < RT; ++j) {
-    const int r = rbase + j;
-    if (r >= 1) {
-      const uchar4 qv = quals[r - 1];
-      const int qq = qv.x & kQualMask, qi = qv.y & kQualMask, qd = qv.z & kQualMask, qc = qv.w & kQualMask;
-      const T pmx = ph[qi], pmy = ph[qd], g = ph[qc];
-      const T gp = T(1) - g;
-      T ap = T(1), bp = T(1);  // scale of the row above: pMX/pMY, or 1 for row 0
-      if (ScaledXY<T>::value && r >= 2) {
-        const uchar4 pv = quals[r - 2];
-        ap = ph[pv.y & kQualMask];
-        bp = ph[pv.z & kQualMask];
-      }
-      rw.mm[j] = mmt[mm_index(qi, qd)];
-      if constexpr (ScaledXY<T>::value) {
-        rw.cx[j] = gp * ap;
-        rw.cy[j] = gp * bp;
-        rw.kap[j] = g * ap / pmx;
-        rw.my[j] = T(0);
-        if (j == RT - 1) rw.pmx_bottom = pmx;
-      } else {
-        rw.cx[j] = gp;
-        rw.cy[j] = T(0);
-        rw.kap[j] = pmx;
-        rw.my[j] = pmy;
-      }
-      rw.g[j] = g;
-      rw.y0[j] = T(0);
-      const T eps = ph[qq];
-      em[j] = T(1) - eps;
-      ex[j] = eps / T(3);
-      rc[j] = base_code(bases[r - 1]);
-      valid[j] = true;
-    } else {
-      // padding rows and row 0: M = 0, X = 0, Y carried unchanged
-      rw.mm[j] = T(0); rw.cx[j] = T(0); rw.cy[j] = T(0); rw.kap[j] = T(0); rw.my[j] = T(0);
-      rw.g[j] = T(1);
-      rw.y0[j] = (r == 0) ? init_y : T(0);
-    }
-  }
-  // Emission table: for haplotype code h, row j: 1-eps on a match, eps/3 on a
-  // mismatch (a read or haplotype N matches everything), 0 for padding.
-#pragma unroll
-  for (int h = 0; h < kCodes; ++h) {
-#pragma unroll
-    for (int ch = 0; ch < S::NCH; ++ch) {
-      T v[Vec16<T>::n];
-#pragma unroll
-      for (int t = 0; t < Vec16<T>::n; ++t) {
-        const int j = ch * Vec16<T>::n + t;
-        const bool match = (rc[j] == (uint32_t)h) || rc[j] == 4u || h == 4;
-        v[t] = (valid[j] && h != kPadCode) ? (match ? em[j] : ex[j]) : T(0);
-      }
-      V vv;
-      if constexpr (Vec16<T>::n == 4) vv = make_float4(v[0], v[1], v[2], v[3]);
-      else vv = make_double2(v[0], v[1]);
-      *reinterpret_cast<V*>(etab_lane + h * S::kCodeStride + ch * (kWarp * 16)) = vv;
-    }
-  }
-}
-
-// Stages a haplotype as column codes: code[kHapLead + c - 1] for c = 1..H,
-// kPadCode everywhere else in [0, n_total).
-__device__ __forceinline__ void stage_hap(const uint8_t* __restrict__ hap, int H, unsigned char* hc, int n_total,
-                                          int lane) {
-  for (int x = lane; x < n_total; x += kWarp) {
-    const int c = x - kHapLead + 1;
-    hc[x] = (c >= 1 && c <= H) ? (unsigned char)base_code(hap[c - 1]) : (unsigned char)kPadCode;
-  }
-}
-
-// One strip of the wavefront.  MULTI: lane 0 reads the row above the strip
-// from `bnd` (the previous strip's bottom row, or zeros for the first strip)
-// and lane 31 writes this strip's bottom row back to `bnd`, both through
-// shared-memory rings.  Column c of the boundary row is buffer row c + 31.
-// Returns, in lane 31, the sums of M and Xh over the bottom row and the
-// largest bottom-row value (for renormalisation between strips).
-template <typename T, int RT, bool MULTI, int CH>
-__device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned char* __restrict__ etab_lane,
-                                          const unsigned char* __restrict__ hc_lane, int nsteps, int lane,
-                                          T* __restrict__ bnd, unsigned char* ring, T in_scale, T& sumM,
-                                          T& sumX, T& bmax) {
-  using S = WarpSmem<T, RT>;
-  using V = typename Vec16<T>::type;
-  constexpr bool kScale = sizeof(T) == 8;  // only the FP64 path renormalises
-  T M[RT], X[RT], Y[RT];
-#pragma unroll
-  for (int j = 0; j < RT; ++j) { M[j] = T(0); X[j] = T(0); Y[j] = rw.y0[j]; }
-  sumM = T(0); sumX = T(0); bmax = T(0);
-  // Values the lane above publishes before step 0: its bottom row at
-  // "column <= 0", i.e. the column-0 boundary state.
-  T upM = __shfl_up_sync(0xffffffffu, M[RT - 1], 1);
-  T upX = __shfl_up_sync(0xffffffffu, X[RT - 1], 1);
-  T upY = __shfl_up_sync(0xffffffffu, Y[RT - 1], 1);
-  T dM = upM, dX = upX, dY = upY;
-  T* ring_in = reinterpret_cast<T*>(ring);
-  T* ring_out = reinterpret_cast<T*>(ring + S::kRingInCols * S::kColBytes);
-  if constexpr (MULTI) {
-    static_assert(CH == 32, "multi-strip runs 32-step chunks");
-    // Lane 0 needs, at step s, buffer row s + 32 (column s + 1); those rows
-    // are streamed into a 64-row ring: chunk k (steps 32k..32k+31) uses ring
-    // half k&1, prefetched during chunk k-1.  Step 0's diagonal is row 31.
-    const T* src = bnd + (size_t)(32 + lane) * 4;
-    __pipeline_memcpy_async(ring_in + lane * 4, src, 16);
-    if constexpr (sizeof(T) == 8) __pipeline_memcpy_async(ring_in + lane * 4 + 2, src + 2, 16);
-    __pipeline_commit();
-    if (lane == 0) {
-      dM = bnd[31 * 4 + 0]; dX = bnd[31 * 4 + 1]; dY = bnd[31 * 4 + 2];
-      if constexpr (kScale) { dM *= in_scale; dX *= in_scale; dY *= in_scale; }
-    }
-    __pipeline_wait_prior(0);
-    __syncwarp();
-  } else {
-    if (lane == 0) { upM = T(0); dM = T(0); }
-  }
-
-  for (int s0 = 0; s0 < nsteps; s0 += CH) {
-    if constexpr (MULTI) {
-      const int nk = s0 / 32 + 1;
-      const T* src = bnd + (size_t)(32 * nk + 32 + lane) * 4;
-      T* dst = ring_in + ((nk & 1) * 32 + lane) * 4;
-      __pipeline_memcpy_async(dst, src, 16);
-      if constexpr (sizeof(T) == 8) __pipeline_memcpy_async(dst + 2, src + 2, 16);
-      __pipeline_commit();
-    }
-#pragma unroll
-    for (int u = 0; u < CH; ++u) {
-      const int s = s0 + u;
-      if constexpr (MULTI) {
-        if (lane == 0) {
-          const T* rin = ring_in + ((((s0 >> 5) & 1) * 32) + u) * 4;
-          upM = rin[0]; upX = rin[1]; upY = rin[2];
-          if constexpr (kScale) { upM *= in_scale; upX *= in_scale; upY *= in_scale; }
-        }
-      }
-      const unsigned code = hc_lane[s];
-      const unsigned char* ep = etab_lane + code * S::kCodeStride;
-      T e[S::RTP];
-#pragma unroll
-      for (int ch = 0; ch < S::NCH; ++ch) {
-        const V v = *reinterpret_cast<const V*>(ep + ch * (kWarp * 16));
-        if constexpr (Vec16<T>::n == 4) {
-          e[ch * 4 + 0] = v.x; e[ch * 4 + 1] = v.y; e[ch * 4 + 2] = v.z; e[ch * 4 + 3] = v.w;
-        } else {
-          e[ch * 2 + 0] = v.x; e[ch * 2 + 1] = v.y;
-        }
-      }
-      T um = upM, ux = upX;
-      T dm = dM, dx = dX, dy = dY;
-#pragma unroll
-      for (int j = 0; j < RT; ++j) {
-        T mn, xn, yn;
-        if constexpr (ScaledXY<T>::value) {
-          mn = e[j] * fma_(rw.mm[j], dm, fma_(rw.cx[j], dx, rw.cy[j] * dy));
-          xn = fma_(rw.kap[j], ux, um);
-          yn = fma_(rw.g[j], Y[j], M[j]);
-        } else {
-          mn = e[j] * fma_(rw.mm[j], dm, rw.cx[j] * (dx + dy));
-          xn = fma_(rw.g[j], ux, rw.kap[j] * um);
-          yn = fma_(rw.g[j], Y[j], rw.my[j] * M[j]);
-        }
-        dm = M[j]; dx = X[j]; dy = Y[j];
-        um = mn; ux = xn;
-        M[j] = mn; X[j] = xn; Y[j] = yn;
-      }
-      sumM += M[RT - 1];
-      sumX += X[RT - 1];
-      const T nM = __shfl_up_sync(0xffffffffu, M[RT - 1], 1);
-      const T nX = __shfl_up_sync(0xffffffffu, X[RT - 1], 1);
-      const T nY = __shfl_up_sync(0xffffffffu, Y[RT - 1], 1);
-      if constexpr (MULTI) {
-        if (lane == kWarp - 1) {
-          T* ro = ring_out + u * 4;
-          ro[0] = M[RT - 1]; ro[1] = X[RT - 1]; ro[2] = Y[RT - 1];
-          if constexpr (kScale) bmax = fmax(bmax, fmax(M[RT - 1], fmax(X[RT - 1], Y[RT - 1])));
-        }
-      }
-      dM = upM; dX = upX; dY = upY;
-      upM = nM; upX = nX; upY = nY;
-      if constexpr (!MULTI) {
-        if (lane == 0) upM = T(0);
-      }
-    }
-    if constexpr (MULTI) {
-      // End of a 32-step chunk: flush its bottom row (buffer rows s0+1 ..
-      // s0+32; ring slot u holds step s0+u, i.e. column s0+u-30) and make the
-      // prefetched chunk visible.
-      __syncwarp();
-      T* dstb = bnd + (size_t)(s0 + 1 + lane) * 4;
-      const T* srco = ring_out + lane * 4;
-      if constexpr (sizeof(T) == 4) {
-        *reinterpret_cast<float4*>(dstb) = *reinterpret_cast<const float4*>(srco);
-      } else {
-        reinterpret_cast<double2*>(dstb)[0] = reinterpret_cast<const double2*>(srco)[0];
-        reinterpret_cast<double2*>(dstb)[1] = reinterpret_cast<const double2*>(srco)[1];
-      }
-      __threadfence_block();
-      __pipeline_wait_prior(0);
-      __syncwarp();
-    }
-  }
-}
-
-template <typename T> __device__ __forceinline__ T log10_(T v);
-template <> __device__ __forceinline__ float log10_(float v) { return log10f(v); }
-template <> __device__ __forceinline__ double log10_(double v) { return log10(v); }
-
-// Work items: full-DP units (a read against consecutive haplotypes) or single
-// pairs from the FP64 list.
-struct Item {
-  int read, hap0, nh;
-  long long out0;
-};
-
-template <typename T, int RT, bool MULTI>
-__device__ void process_item(const KernelParams& p, const Item& it, unsigned char* wsm, int lane, T* bnd) {
-  using S = WarpSmem<T, RT>;
-  const DeviceBatch& b = p.batch;
-  const int64_t ro = b.read_off[it.read];
-  const int R = (int)(b.read_off[it.read + 1] - ro);
-  const uchar4* quals = b.read_quals + ro;
-  const uint8_t* bases = b.read_bases + ro;
-  const int rows = R + 1;
-  const int strip_rows = kWarp * RT;
-  const int nstrips = (rows + strip_rows - 1) / strip_rows;
-  const int pad = nstrips * strip_rows - rows;
-  unsigned char* hc = wsm;
-  unsigned char* etab = wsm + p.hap_bytes;
-  unsigned char* etab_lane = etab + lane * 16;
-  unsigned char* ring = etab + S::kEtabBytes;
-  const bool is_f64 = sizeof(T) == 8;
-  Rows<T, RT> rw;
-  if (!MULTI) {
-    // single strip: rows and emission table are shared by all haplotypes
-    setup_rows<T, RT>(p.tables, quals, bases, lane * RT - pad, T(0), rw, etab_lane);
-  }
-  for (int k = 0; k < it.nh; ++k) {
-    const int h = it.hap0 + k;
-    const int64_t ho = b.hap_off[h];
-    const int H = (int)(b.hap_off[h + 1] - ho);
-    if (H == 0 || R == 0) {
-      // An empty read or haplotype has no alignment: likelihood 0.
-      if (lane == kWarp - 1) p.out[it.out0 + k] = -INFINITY;
-      continue;
-    }
-    const T init = is_f64 ? (T)p.tables->init_d : (T)p.tables->init_f;
-    const T init_y = init / (T)H;
-    const int CHK = MULTI ? 32 : 8;
-    const int nsteps = (H + kWarp - 1 + CHK - 1) / CHK * CHK;
-    __syncwarp();
-    stage_hap(b.hap_bases + ho, H, hc, nsteps + kHapLead, lane);
-    if (!MULTI) {
-      // the initial row's Y depends on the haplotype length
-      const int r0j = pad - lane * RT;  // j of row 0 within this lane, if here
-#pragma unroll
-      for (int j = 0; j < RT; ++j) rw.y0[j] = (j == r0j) ? init_y : T(0);
-    }
-    __syncwarp();
-    T sumM, sumX, bmax;
-    long long kexp = 0;  // stored values are true values * 2^-kexp
-    if constexpr (MULTI) {
-      // boundary row of "strip -1": all zero
-      for (int x = lane; x < nsteps + 96; x += kWarp) {
-        bnd[(size_t)x * 4 + 0] = T(0); bnd[(size_t)x * 4 + 1] = T(0); bnd[(size_t)x * 4 + 2] = T(0);
-      }
-      T in_scale = T(1);
-      for (int st = 0; st < nstrips; ++st) {
-        __syncwarp();
-        setup_rows<T, RT>(p.tables, quals, bases, st * strip_rows + lane * RT - pad, init_y, rw, etab_lane);
-        __syncwarp();
-        run_strip<T, RT, true, 32>(rw, etab_lane, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, sumM,
-                                   sumX, bmax);
-        __syncwarp();
-        in_scale = T(1);
-        if (p.rescale && st + 1 < nstrips) {
-          const T m = __shfl_sync(0xffffffffu, bmax, kWarp - 1);
-          if (m > T(0)) {
-            int e2;
-            frexp((double)m, &e2);
-            // keep the row maximum near 2^(target) so the next strip has headroom
-            const int shift = e2 - p.rescale_target;
-            kexp += shift;
-            in_scale = (T)ldexp(1.0, -shift);
-          }
-        }
-      }
-    } else {
-      run_strip<T, RT, false, 8>(rw, etab_lane, hc + kHapLead - lane, nsteps, lane, nullptr, nullptr, T(1), sumM,
-                                 sumX, bmax);
-    }
-    if (lane == kWarp - 1) {
-      const T res = sumM + rw.pmx_bottom * sumX;
-      const long long o = it.out0 + k;
-      if (!is_f64) {
-        if (!(res >= (T)kMinAccepted) || isinf((double)res)) {
-          const unsigned long long slot = atomicAdd(&p.ctr->rescue_count, 1ull);
-          if (slot < (unsigned long long)p.rescue_cap) {
-            p.rescue[slot].read = it.read;
-            p.rescue[slot].hap = h;
-            p.rescue[slot].out = o;
-          } else {
-            atomicOr(&p.ctr->status, 1ull);
-          }
-          p.out[o] = __longlong_as_double(0x7ff8000000000000ll);
-        } else {
-          p.out[o] = (double)(log10_((float)res) - p.tables->log10_init_f);
-        }
-      } else {
-        const double rd = (double)res;
-        if (rd > 0.0 && isfinite(rd)) {
-          p.out[o] = log10(rd) + (double)kexp * 0.30102999566398119521 - p.tables->log10_init_d;
-        } else {
-          atomicAdd(&p.ctr->underflow_count, 1ull);
-          p.out[o] = -INFINITY;
-        }
-      }
-    }
-  }
-}
 
 template <typename T, int RT, bool MULTI>
 __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
