@@ -191,6 +191,50 @@ bv_status bv_phmm_fetch_results(bv_phmm_ctx* ctx, double* out_log10, int64_t n);
 bv_status bv_phmm_host_register(bv_phmm_ctx* ctx, void* ptr, size_t bytes);
 bv_status bv_phmm_host_unregister(bv_phmm_ctx* ctx, void* ptr);
 
+/* --- scoring without any allocation (no counterpart in the reference) ----
+ * For callers that cannot call cudaMalloc when they need scores: e.g. a
+ * haplotype caller inside a GPU pipeline whose framework's caching allocator
+ * already holds nearly all device memory (a new allocation fails or stalls the
+ * whole device), or code running under a no-new-allocations policy.  They
+ * pass device-resident inputs and a device output array; the library uses
+ * only a fixed scratch array compiled into it (about 4.6 MB per GPU that
+ * loads the library, held until exit) and allocates nothing, host or device.
+ *
+ * Computes, for each pair {int32 read; int32 hap; int64 out} (16 bytes each,
+ * 8-byte aligned), log10 likelihood into out_log10[out] with the FP64 forward
+ * pass -- the values bv_phmm_compute_regions gives with BV_PRECISION_F64.
+ * Inputs are device pointers: read_quals holds 4 bytes per read position
+ * (q, i, d, c; 4-byte aligned); offsets are prefix sums (n+1 entries).
+ * Limits: haplotypes of at most BV_PHMM_NOALLOC_MAX_HAP_LEN bases (the caller
+ * states its bound in max_hap_len; larger values are rejected with
+ * BV_ERR_INVALID_ARG, and a pair whose haplotype is longer than the maximum
+ * or whose indices are out of range gets NaN and makes the call return
+ * BV_ERR_INVALID_ARG); reads of any length.
+ * The call runs on `stream` (a cudaStream_t, NULL = legacy default stream)
+ * and returns after the stream has finished it.  The first call on a device
+ * sets that device up (finds the scratch array's device address, copies the
+ * probability tables into it, synchronously): make it before any stream
+ * capture.  All calls share the one scratch array and it keeps the last
+ * call's contents (the call clears what must start at zero); calls that
+ * overlap on the GPU -- from two host threads or on two streams -- race. */
+#define BV_PHMM_NOALLOC_MAX_HAP_LEN 2048
+
+typedef struct bv_phmm_device_pairs {
+  int64_t num_pairs;
+  const void* pairs;
+  int64_t num_reads;
+  const int64_t* read_offsets;
+  const uint8_t* read_bases;
+  const uint8_t* read_quals;
+  int64_t num_haps;
+  const int64_t* hap_offsets;
+  const uint8_t* hap_bases;
+  int32_t max_hap_len;
+} bv_phmm_device_pairs;
+
+bv_status bv_phmm_forward_f64_noalloc(int device, const bv_phmm_device_pairs* pairs, double* out_log10,
+                                      int64_t num_out, void* stream);
+
 /* Diagnostics: writes the probability tables a context uploads (ph2pr for
  * quals 0..127 and the match-to-match triangle for quals <= 127, both
  * precisions; Context.h:42-175).  Host-only, needs no device.  Returns 0, or
