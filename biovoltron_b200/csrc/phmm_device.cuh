@@ -7,16 +7,62 @@
 #include <cuda_pipeline.h>
 #include <cstdint>
 #include <cmath>
+#include <type_traits>
 
 #include "phmm_common.h"
 #include "phmm_kernels.h"
+#include "phmm_rows.h"
 
 namespace bvphmm {
 
 
-template <typename T> struct Vec16;
-template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
-template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
+// Emission-table chunk: the widest shared-memory load whose lanes fall in
+// distinct banks for the rows a lane owns (4, 8 or 16 bytes per lane).
+template <typename T, int RT> struct EChunk;
+template <int RT> struct EChunk<float, RT> {
+  static constexpr int n = RT >= 3 ? 4 : RT;
+  using type = typename std::conditional<n == 4, float4, typename std::conditional<n == 2, float2, float>::type>::type;
+};
+template <int RT> struct EChunk<double, RT> {
+  static constexpr int n = RT >= 2 ? 2 : 1;
+  using type = typename std::conditional<n == 2, double2, double>::type;
+};
+
+template <typename V, typename T> __device__ __forceinline__ void unpack(const V& v, T* e);
+template <> __device__ __forceinline__ void unpack(const float4& v, float* e) { e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w; }
+template <> __device__ __forceinline__ void unpack(const float2& v, float* e) { e[0] = v.x; e[1] = v.y; }
+template <> __device__ __forceinline__ void unpack(const float& v, float* e) { e[0] = v; }
+template <> __device__ __forceinline__ void unpack(const double2& v, double* e) { e[0] = v.x; e[1] = v.y; }
+template <> __device__ __forceinline__ void unpack(const double& v, double* e) { e[0] = v; }
+// Full-width shared-memory loads of an emission-table chunk.  Written in PTX
+// so the compiler cannot narrow a 16-byte load whose upper values a variant
+// does not use (a narrowed load keeps the 16-byte lane stride and conflicts).
+template <typename V> __device__ __forceinline__ V lds_chunk(const void* p);
+template <> __device__ __forceinline__ float4 lds_chunk<float4>(const void* p) {
+  float4 v;
+  asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "r"((unsigned)__cvta_generic_to_shared(p)));
+  return v;
+}
+template <> __device__ __forceinline__ float2 lds_chunk<float2>(const void* p) {
+  float2 v;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"((unsigned)__cvta_generic_to_shared(p)));
+  return v;
+}
+template <> __device__ __forceinline__ float lds_chunk<float>(const void* p) { return *static_cast<const float*>(p); }
+template <> __device__ __forceinline__ double2 lds_chunk<double2>(const void* p) {
+  double2 v;
+  asm("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"((unsigned)__cvta_generic_to_shared(p)));
+  return v;
+}
+template <> __device__ __forceinline__ double lds_chunk<double>(const void* p) { return *static_cast<const double*>(p); }
+
+__device__ __forceinline__ float4 pack4(const float* v, float4*) { return make_float4(v[0], v[1], v[2], v[3]); }
+__device__ __forceinline__ float2 pack4(const float* v, float2*) { return make_float2(v[0], v[1]); }
+__device__ __forceinline__ float pack4(const float* v, float*) { return v[0]; }
+__device__ __forceinline__ double2 pack4(const double* v, double2*) { return make_double2(v[0], v[1]); }
+__device__ __forceinline__ double pack4(const double* v, double*) { return v[0]; }
 
 __device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
@@ -42,16 +88,30 @@ __device__ __forceinline__ int mm_index(int ins, int del) {
 // Shared-memory layout of one warp's slice.
 template <typename T, int RT>
 struct WarpSmem {
-  static constexpr int VPC = Vec16<T>::n;                 // values per 16-byte chunk
+  static constexpr int VPC = EChunk<T, RT>::n;             // emission values per chunk
+  static constexpr int CB = VPC * (int)sizeof(T);          // chunk bytes = lane stride
   static constexpr int RTP = (RT + VPC - 1) / VPC * VPC;   // rows rounded to chunks
   static constexpr int NCH = RTP / VPC;                    // chunks per code
-  static constexpr int kCodeStride = NCH * kWarp * 16;     // bytes per code
+  static constexpr int kChunkStride = kWarp * CB;          // bytes between a lane's chunks
+  static constexpr int kCodeStride = NCH * kChunkStride;   // bytes per code
   static constexpr int kEtabBytes = kCodes * kCodeStride;
   static constexpr int kRingInCols = 64;
   static constexpr int kRingOutCols = 32;
   static constexpr int kColBytes = 4 * (int)sizeof(T);     // M, Xh, Yh, unused
   static constexpr int kRingBytes = (kRingInCols + kRingOutCols) * kColBytes;
 };
+
+// FP32 adds a summing row below the read's last row: with e = 1, pMM = 1,
+// the X coefficient = pMX(R) (undoing the X/pMX scaling) and pYY = 1, its M is
+// M(R,c-1) + X(R,c-1) and its Y accumulates those, so after the last column
+// its Y + M is the reference's sum over the last row of M + X
+// (avx-pairhmm-template.h:328-343) -- computed with the cell arithmetic
+// instead of two extra adds per step.  The single-strip FP32 kernel also keeps
+// at least one padding row on top: then lane 0's top row may read its own
+// bottom row through the shuffle, because a padding row's outputs reach the
+// rows below only through zero coefficients.
+template <typename T> struct SumRow { static constexpr bool value = sizeof(T) == 4; };
+
 
 // Per-lane row constants for one strip.
 // FP32 keeps X and Y divided by pMX / pMY (one FMA each, see above).  FP64,
@@ -66,7 +126,6 @@ template <typename T> struct ScaledXY { static constexpr bool value = sizeof(T) 
 template <typename T, int RT>
 struct Rows {
   T mm[RT], cx[RT], cy[RT], kap[RT], my[RT], g[RT], y0[RT];
-  T pmx_bottom;
 };
 
 // Computes the lane's row constants for the rows [rbase, rbase+RT) (real row
@@ -75,22 +134,28 @@ struct Rows {
 // and stripeINITIALIZATION (:150-158) give the per-row probabilities.
 template <typename T, int RT>
 __device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const uchar4* __restrict__ quals,
-                                           const uint8_t* __restrict__ bases, int rbase, T init_y,
+                                           const uint8_t* __restrict__ bases, int R, int rbase, T init_y,
                                            Rows<T, RT>& rw, unsigned char* etab_lane) {
   using S = WarpSmem<T, RT>;
-  using V = typename Vec16<T>::type;
+  using V = typename EChunk<T, RT>::type;
   const T* ph = ph2pr_tab<T>(tb);
   const T* mmt = mm_tab<T>(tb);
   T em[S::RTP], ex[S::RTP];
   uint32_t rc[S::RTP];
-  bool valid[S::RTP];
+  bool valid[S::RTP], sumrow[S::RTP];
 #pragma unroll
-  for (int j = 0; j < S::RTP; ++j) { em[j] = T(0); ex[j] = T(0); rc[j] = 0; valid[j] = false; }
-  rw.pmx_bottom = T(1);
+  for (int j = 0; j < S::RTP; ++j) { em[j] = T(0); ex[j] = T(0); rc[j] = 0; valid[j] = false; sumrow[j] = false; }
 #pragma unroll
   for (int j = 0; j < RT; ++j) {
     const int r = rbase + j;
-    if (r >= 1) {
+    if (SumRow<T>::value && r == R + 1 && R >= 1) {
+      rw.mm[j] = T(1);
+      rw.cx[j] = ph[quals[R - 1].y & kQualMask];  // pMX(R): Xh(R) * pMX(R) = X(R)
+      rw.cy[j] = T(0); rw.kap[j] = T(0); rw.my[j] = T(0);
+      rw.g[j] = T(1);
+      rw.y0[j] = T(0);
+      sumrow[j] = true;
+    } else if (r >= 1 && r <= R) {
       const uchar4 qv = quals[r - 1];
       const int qq = qv.x & kQualMask, qi = qv.y & kQualMask, qd = qv.z & kQualMask, qc = qv.w & kQualMask;
       const T pmx = ph[qi], pmy = ph[qd], g = ph[qc];
@@ -107,7 +172,6 @@ __device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const 
         rw.cy[j] = gp * bp;
         rw.kap[j] = g * ap / pmx;
         rw.my[j] = T(0);
-        if (j == RT - 1) rw.pmx_bottom = pmx;
       } else {
         rw.cx[j] = gp;
         rw.cy[j] = T(0);
@@ -134,17 +198,14 @@ __device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const 
   for (int h = 0; h < kCodes; ++h) {
 #pragma unroll
     for (int ch = 0; ch < S::NCH; ++ch) {
-      T v[Vec16<T>::n];
+      T v[4];
 #pragma unroll
-      for (int t = 0; t < Vec16<T>::n; ++t) {
-        const int j = ch * Vec16<T>::n + t;
+      for (int t = 0; t < S::VPC; ++t) {
+        const int j = ch * S::VPC + t;
         const bool match = (rc[j] == (uint32_t)h) || rc[j] == 4u || h == 4;
-        v[t] = (valid[j] && h != kPadCode) ? (match ? em[j] : ex[j]) : T(0);
+        v[t] = sumrow[j] ? T(1) : (valid[j] && h != kPadCode) ? (match ? em[j] : ex[j]) : T(0);
       }
-      V vv;
-      if constexpr (Vec16<T>::n == 4) vv = make_float4(v[0], v[1], v[2], v[3]);
-      else vv = make_double2(v[0], v[1]);
-      *reinterpret_cast<V*>(etab_lane + h * S::kCodeStride + ch * (kWarp * 16)) = vv;
+      *reinterpret_cast<V*>(etab_lane + h * S::kCodeStride + ch * S::kChunkStride) = pack4(v, (V*)nullptr);
     }
   }
 }
@@ -163,16 +224,19 @@ __device__ __forceinline__ void stage_hap(const uint8_t* __restrict__ hap, int H
 // from `bnd` (the previous strip's bottom row, or zeros for the first strip)
 // and lane 31 writes this strip's bottom row back to `bnd`, both through
 // shared-memory rings.  Column c of the boundary row is buffer row c + 31.
-// Returns, in lane 31, the sums of M and Xh over the bottom row and the
-// largest bottom-row value (for renormalisation between strips).
+// On return, lane 31 holds its bottom row's final M and Y (the summing row's
+// result for FP32), the per-step sums of M and X over the bottom row (FP64,
+// which has no summing row) and the largest bottom-row value (FP64, for
+// renormalisation between strips).
 template <typename T, int RT, bool MULTI, int CH>
 __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned char* __restrict__ etab_lane,
                                           const unsigned char* __restrict__ hc_lane, int nsteps, int lane,
-                                          T* __restrict__ bnd, unsigned char* ring, T in_scale, T& sumM,
-                                          T& sumX, T& bmax) {
+                                          T* __restrict__ bnd, unsigned char* ring, T in_scale, T& lastM,
+                                          T& lastY, T& sumM, T& sumX, T& bmax) {
   using S = WarpSmem<T, RT>;
-  using V = typename Vec16<T>::type;
+  using V = typename EChunk<T, RT>::type;
   constexpr bool kScale = sizeof(T) == 8;  // only the FP64 path renormalises
+  constexpr bool kSums = !SumRow<T>::value;
   T M[RT], X[RT], Y[RT];
 #pragma unroll
   for (int j = 0; j < RT; ++j) { M[j] = T(0); X[j] = T(0); Y[j] = rw.y0[j]; }
@@ -200,7 +264,7 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned 
     }
     __pipeline_wait_prior(0);
     __syncwarp();
-  } else {
+  } else if constexpr (!SumRow<T>::value) {
     if (lane == 0) { upM = T(0); dM = T(0); }
   }
 
@@ -228,12 +292,8 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned 
       T e[S::RTP];
 #pragma unroll
       for (int ch = 0; ch < S::NCH; ++ch) {
-        const V v = *reinterpret_cast<const V*>(ep + ch * (kWarp * 16));
-        if constexpr (Vec16<T>::n == 4) {
-          e[ch * 4 + 0] = v.x; e[ch * 4 + 1] = v.y; e[ch * 4 + 2] = v.z; e[ch * 4 + 3] = v.w;
-        } else {
-          e[ch * 2 + 0] = v.x; e[ch * 2 + 1] = v.y;
-        }
+        const V v = lds_chunk<V>(ep + ch * S::kChunkStride);
+        unpack(v, e + ch * S::VPC);
       }
       T um = upM, ux = upX;
       T dm = dM, dx = dX, dy = dY;
@@ -253,8 +313,10 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned 
         um = mn; ux = xn;
         M[j] = mn; X[j] = xn; Y[j] = yn;
       }
-      sumM += M[RT - 1];
-      sumX += X[RT - 1];
+      if constexpr (kSums) {
+        sumM += M[RT - 1];
+        sumX += X[RT - 1];
+      }
       const T nM = __shfl_up_sync(0xffffffffu, M[RT - 1], 1);
       const T nX = __shfl_up_sync(0xffffffffu, X[RT - 1], 1);
       const T nY = __shfl_up_sync(0xffffffffu, Y[RT - 1], 1);
@@ -267,7 +329,7 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned 
       }
       dM = upM; dX = upX; dY = upY;
       upM = nM; upX = nX; upY = nY;
-      if constexpr (!MULTI) {
+      if constexpr (!MULTI && !SumRow<T>::value) {
         if (lane == 0) upM = T(0);
       }
     }
@@ -289,6 +351,8 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned 
       __syncwarp();
     }
   }
+  lastM = M[RT - 1];
+  lastY = Y[RT - 1];
 }
 
 template <typename T> __device__ __forceinline__ T log10_(T v);
@@ -310,19 +374,22 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
   const int R = (int)(b.read_off[it.read + 1] - ro);
   const uchar4* quals = b.read_quals + ro;
   const uint8_t* bases = b.read_bases + ro;
-  const int rows = R + 1;
+  // Padded row space: padding rows on top, row 0, rows 1..R, and (FP32) the
+  // summing row; the host chose RT so that single-strip FP32 keeps >= 1
+  // padding row on top.
+  const int rows = R + 1 + (SumRow<T>::value ? 1 : 0);
   const int strip_rows = kWarp * RT;
-  const int nstrips = (rows + strip_rows - 1) / strip_rows;
+  const int nstrips = (rows_needed(R, SumRow<T>::value, !MULTI) + strip_rows - 1) / strip_rows;
   const int pad = nstrips * strip_rows - rows;
   unsigned char* hc = wsm;
   unsigned char* etab = wsm + p.hap_bytes;
-  unsigned char* etab_lane = etab + lane * 16;
+  unsigned char* etab_lane = etab + lane * S::CB;
   unsigned char* ring = etab + S::kEtabBytes;
   const bool is_f64 = sizeof(T) == 8;
   Rows<T, RT> rw;
   if (!MULTI) {
     // single strip: rows and emission table are shared by all haplotypes
-    setup_rows<T, RT>(p.tables, quals, bases, lane * RT - pad, T(0), rw, etab_lane);
+    setup_rows<T, RT>(p.tables, quals, bases, R, lane * RT - pad, T(0), rw, etab_lane);
   }
   for (int k = 0; k < it.nh; ++k) {
     const int h = it.hap0 + k;
@@ -336,7 +403,9 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
     const T init = is_f64 ? (T)p.tables->init_d : (T)p.tables->init_f;
     const T init_y = init / (T)H;
     const int CHK = MULTI ? 32 : 8;
-    const int nsteps = (H + kWarp - 1 + CHK - 1) / CHK * CHK;
+    // lane 31 reaches column H at step H+30; the FP32 summing row trails the
+    // last read row by one column, so FP32 runs one step more.
+    const int nsteps = (H + kWarp - 1 + (SumRow<T>::value ? 1 : 0) + CHK - 1) / CHK * CHK;
     __syncwarp();
     stage_hap(b.hap_bases + ho, H, hc, nsteps + kHapLead, lane);
     if (!MULTI) {
@@ -346,7 +415,7 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
       for (int j = 0; j < RT; ++j) rw.y0[j] = (j == r0j) ? init_y : T(0);
     }
     __syncwarp();
-    T sumM, sumX, bmax;
+    T lastM, lastY, sumM, sumX, bmax;
     long long kexp = 0;  // stored values are true values * 2^-kexp
     if constexpr (MULTI) {
       // boundary row of "strip -1": all zero
@@ -356,10 +425,10 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
       T in_scale = T(1);
       for (int st = 0; st < nstrips; ++st) {
         __syncwarp();
-        setup_rows<T, RT>(p.tables, quals, bases, st * strip_rows + lane * RT - pad, init_y, rw, etab_lane);
+        setup_rows<T, RT>(p.tables, quals, bases, R, st * strip_rows + lane * RT - pad, init_y, rw, etab_lane);
         __syncwarp();
-        run_strip<T, RT, true, 32>(rw, etab_lane, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, sumM,
-                                   sumX, bmax);
+        run_strip<T, RT, true, 32>(rw, etab_lane, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
+                                   lastY, sumM, sumX, bmax);
         __syncwarp();
         in_scale = T(1);
         if (p.rescale && st + 1 < nstrips) {
@@ -375,11 +444,12 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
         }
       }
     } else {
-      run_strip<T, RT, false, 8>(rw, etab_lane, hc + kHapLead - lane, nsteps, lane, nullptr, nullptr, T(1), sumM,
-                                 sumX, bmax);
+      run_strip<T, RT, false, 8>(rw, etab_lane, hc + kHapLead - lane, nsteps, lane, nullptr, nullptr, T(1), lastM,
+                                 lastY, sumM, sumX, bmax);
     }
     if (lane == kWarp - 1) {
-      const T res = sumM + rw.pmx_bottom * sumX;
+      // FP32: the summing row's Y + M; FP64: the accumulated last-row sums.
+      const T res = SumRow<T>::value ? lastY + lastM : sumM + sumX;
       const long long o = it.out0 + k;
       if (!is_f64) {
         if (!(res >= (T)kMinAccepted) || isinf((double)res)) {

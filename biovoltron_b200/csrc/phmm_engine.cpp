@@ -14,6 +14,8 @@
 // FP32 launches flagged.
 #include "phmm_engine.h"
 
+#include "phmm_rows.h"
+
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -50,7 +52,7 @@ int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 int hap_bytes_for(int max_hap, int chunk) {
   return (int)round_up((int64_t)max_hap + (kWarp - 1) + chunk + kHapLead + 16, 16);
 }
-long long bnd_cols_for(int max_hap) { return round_up((int64_t)max_hap + kWarp - 1, 32) + 128; }
+long long bnd_cols_for(int max_hap) { return round_up((int64_t)max_hap + kWarp, 32) + 160; }
 }  // namespace
 
 Engine::Engine(const bv_phmm_options& opt) : opt_(opt) {}
@@ -163,7 +165,9 @@ bv_status Engine::plan(const bv_region_batch& b) {
     max_hap_ = std::max(max_hap_, mh);
   }
   auto variant_of = [&](int64_t rlen) {
-    const int64_t rows = rlen + 1;
+    // rows of the single-strip FP32 kernel: row 0, the read, the summing row
+    // and one padding row on top (phmm_device.cuh, rows_needed)
+    const int64_t rows = rows_needed((int)std::min<int64_t>(rlen, 1 << 24), true, true);
     const int64_t rt = (rows + kWarp - 1) / kWarp;
     return rt <= kMaxRowsPerLane ? variant_index(false, (int)rt, false) : v_multi;
   };

@@ -149,3 +149,22 @@ def test_invalid_arguments_are_rejected(engine):
         engine.compute_regions(long_hap)
     # the context still works afterwards
     assert np.isfinite(engine.compute_regions(W.config0(0))).all()
+
+
+def test_alignment_ending_at_last_haplotype_base(engine, oracle):
+    # The last column must be reached whatever haplotype length mod the
+    # kernel's step chunking (8 single-strip, 32 multi-strip); reads here end
+    # exactly at the haplotype's last base, so that column carries the mass.
+    rng = np.random.default_rng(17)
+    pairs = []
+    for H in list(range(220, 236)) + list(range(985, 995)):
+        hap = bytes(W._random_seq(rng, H))
+        for n in (100, 300):
+            read = hap[H - n:]
+            pairs.append((read, bytes(rng.integers(20, 41, size=n).astype(np.uint8)), bytes([45]) * n,
+                          bytes([45]) * n, bytes([10]) * n, hap))
+    b = W.from_pairs(pairs)
+    got = engine.compute_regions(b)
+    truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
+    ref, _ = oracle.log10_reference_rule(TestcaseArray.for_batch(b))
+    _check(got, ref, truth)
