@@ -1,0 +1,824 @@
+// phmm_band.cu -- learned-band PairHMM path (see phmm_band.h for the pipeline).
+//
+// The reference computes every pair over its full read x haplotype matrix
+// (avx-pairhmm-template.h:210-346).  Here a pair whose alignment is confined
+// to a narrow diagonal band is scored on that band only: cells with diagonal
+// d = c - r in [d_lo, d_lo + W) follow the reference recurrence, cells outside
+// are zero.  The band comes from the 11-mer seed diagonal d* of the pair and
+// from a small MLP that predicts the band's lower and upper edge relative to
+// d*; the full DP takes every pair the band path cannot vouch for.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+
+#include "phmm_band.h"
+#include "phmm_common.h"
+#include "phmm_kernels.h"
+#include "phmm_rows.h"
+
+namespace bvphmm {
+namespace {
+
+constexpr uint64_t kNoKey = ~0ull;
+
+__device__ __forceinline__ int kmer_code(uint8_t b) {
+  // 2-bit code for A C T G (ConvertChar's order); -1 for anything else.
+  return b == 'A' ? 0 : b == 'C' ? 1 : b == 'T' ? 2 : b == 'G' ? 3 : -1;
+}
+
+// One-hot nibble used by the banded kernel's match test: a read or haplotype
+// N matches everything (0xF), other unknown bytes read as A (ConvertChar).
+__device__ __forceinline__ uint32_t onehot(uint8_t b) {
+  return b == 'C' ? 2u : b == 'T' ? 4u : b == 'G' ? 8u : b == 'N' ? 15u : 1u;
+}
+
+__global__ void k_pairs_from_units(const Unit* __restrict__ units, long long n_units, int32_t* pair_read,
+                                   int32_t* pair_hap) {
+  for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < n_units;
+       u += (long long)gridDim.x * blockDim.x) {
+    const Unit un = units[u];
+    for (int k = 0; k < un.nh; ++k) {
+      pair_read[un.out0 + k] = un.read;
+      pair_hap[un.out0 + k] = un.hap0 + k;
+    }
+  }
+}
+
+// Per haplotype: keys (code << 32 | position) of every 11-mer made of A/C/G/T,
+// sorted ascending by a block-wide bitonic sort; other slots hold kNoKey.
+__global__ void __launch_bounds__(256) k_hap_kmers(const uint8_t* __restrict__ hap_bases,
+                                                   const int64_t* __restrict__ hap_off, long long n_haps,
+                                                   uint64_t* __restrict__ keys) {
+  __shared__ uint64_t sk[kBandMaxHap];
+  __shared__ uint8_t sb[kBandMaxHap];
+  for (long long h = blockIdx.x; h < n_haps; h += gridDim.x) {
+    const int64_t off = hap_off[h];
+    const int H = (int)(hap_off[h + 1] - off);
+    if (H > kBandMaxHap) {
+      for (int x = threadIdx.x; x < H; x += blockDim.x) keys[off + x] = kNoKey;
+      continue;
+    }
+    int n = 1;
+    while (n < H) n <<= 1;
+    __syncthreads();
+    for (int x = threadIdx.x; x < H; x += blockDim.x) sb[x] = hap_bases[off + x];
+    __syncthreads();
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+      uint64_t key = kNoKey;
+      if (x + kK <= H) {
+        uint32_t code = 0;
+        bool ok = true;
+        for (int t = 0; t < kK; ++t) {
+          const int c = kmer_code(sb[x + t]);
+          ok &= c >= 0;
+          code = (code << 2) | (uint32_t)(c & 3);
+        }
+        if (ok) key = ((uint64_t)code << 32) | (uint32_t)x;
+      }
+      sk[x] = key;
+    }
+    __syncthreads();
+    for (int size = 2; size <= n; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int x = threadIdx.x; x < n; x += blockDim.x) {
+          const int y = x ^ stride;
+          if (y > x) {
+            const bool up = (x & size) == 0;
+            const uint64_t a = sk[x], b = sk[y];
+            if ((a > b) == up) { sk[x] = b; sk[y] = a; }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int x = threadIdx.x; x < H; x += blockDim.x) keys[off + x] = sk[x];
+  }
+}
+
+// Per read: the 2-bit code of the 11-mer starting at each position (or
+// kNoCode when it holds a byte other than A/C/G/T), computed once per read
+// rather than once per pair.
+constexpr uint32_t kNoCode = 0xffffffffu;
+
+__global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n_bytes, uint32_t* __restrict__ codes) {
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n_bytes;
+       x += (long long)gridDim.x * blockDim.x) {
+    uint32_t code = 0;
+    bool ok = x + kK <= n_bytes;
+    for (int t = 0; t < kK && ok; ++t) {
+      const int c = kmer_code(read_bases[x + t]);
+      ok &= c >= 0;
+      code = (code << 2) | (uint32_t)(c & 3);
+    }
+    codes[x] = ok ? code : kNoCode;  // positions too close to a read's end are masked by the caller
+  }
+}
+
+// One warp per pair.  The haplotype's sorted 11-mer keys are staged in
+// shared memory; every read 11-mer is binary-searched there and each shared
+// occurrence votes for diagonal d = j - i in a per-warp histogram.  d* is the
+// most voted diagonal (smallest on ties); the features are the 64 bins
+// d* - 32 .. d* + 31 and a few scalars, all divided by the number of read
+// 11-mers; kmin/kmax are the extreme voted diagonals.
+constexpr int kFeatWarps = 4;
+constexpr int kHitCap = 512;
+
+__global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  uint64_t* skeys = reinterpret_cast<uint64_t*>(smem) + (size_t)wib * kBandMaxHap;
+  int* hist = reinterpret_cast<int*>(smem + (size_t)kFeatWarps * kBandMaxHap * 8) + (size_t)wib * kBandMaxSpan;
+  int* hits = reinterpret_cast<int*>(smem + (size_t)kFeatWarps * kBandMaxHap * 8) + (size_t)kFeatWarps * kBandMaxSpan +
+              (size_t)wib * (kHitCap + 1);
+  int* nhit = hits + kHitCap;
+  for (int x = lane; x < kBandMaxSpan; x += 32) hist[x] = 0;
+  const long long nwarps = (long long)gridDim.x * kFeatWarps;
+  int staged_hap = -1;
+  for (long long pi = blockIdx.x * (long long)kFeatWarps + wib; pi < p.n_pairs; pi += nwarps) {
+    const int r = p.pair_read[pi], h = p.pair_hap[pi];
+    const int64_t ro = p.batch.read_off[r], ho = p.batch.hap_off[h];
+    const int R = (int)(p.batch.read_off[r + 1] - ro), H = (int)(p.batch.hap_off[h + 1] - ho);
+    __nv_bfloat16* f = p.feat + pi * kFeat;
+    if (R < kK || H < kK || H > kBandMaxHap || R + H + 1 >= kBandMaxSpan) {
+      if (lane == 0) { p.dstar[pi] = INT32_MIN; p.kmin[pi] = INT32_MIN; p.kmax[pi] = INT32_MAX; }
+      for (int x = lane; x < kFeat; x += 32) f[x] = __float2bfloat16(0.f);
+      continue;
+    }
+    const int nk_hap = H - kK + 1;
+    if (h != staged_hap) {
+      __syncwarp();
+      for (int x = lane; x < nk_hap; x += 32) skeys[x] = p.hap_kmers[ho + x];
+      staged_hap = h;
+    }
+    if (lane == 0) *nhit = 0;
+    __syncwarp();
+    const uint32_t* rcode = p.read_kmers + ro;
+    const int nk_read = R - kK + 1;
+    for (int i0 = 0; i0 < nk_read; i0 += 32) {
+      const int i = i0 + lane;
+      const uint32_t code = i < nk_read ? rcode[i] : kNoCode;
+      int m = nk_hap;
+      if (code != kNoCode) {
+        const uint64_t lo_key = (uint64_t)code << 32;
+        int a = 0, b = nk_hap;  // first key >= lo_key
+        while (a < b) {
+          const int mid = (a + b) >> 1;
+          if (skeys[mid] < lo_key) a = mid + 1; else b = mid;
+        }
+        m = a;
+      }
+      // one vote per occurrence; lanes voting for the same diagonal are
+      // combined so each histogram slot takes one atomic per round
+      for (;;) {
+        int slot = -1;
+        if (m < nk_hap) {
+          const uint64_t key = skeys[m];
+          if ((key >> 32) == code) slot = (int)(key & 0xffffffffu) - i + R;  // d + R
+          else m = nk_hap;
+        }
+        const unsigned active = __ballot_sync(0xffffffffu, slot >= 0);
+        if (active == 0u) break;
+        if (slot >= 0) {
+          const unsigned peers = __match_any_sync(active, slot);
+          if ((__ffs(peers) - 1) == lane) {
+            if (atomicAdd(&hist[slot], __popc(peers)) == 0) {
+              const int q = atomicAdd(nhit, 1);
+              if (q < kHitCap) hits[q] = slot;
+            }
+          }
+          ++m;
+        }
+      }
+    }
+    __syncwarp();
+    const int nh = min(*nhit, kHitCap);
+    const bool overflow = *nhit > kHitCap;
+    // mode: highest count, smallest diagonal on ties
+    int best_cnt = 0, best_slot = 0x7fffffff, smin = 0x7fffffff, smax = -1;
+    for (int x = lane; x < nh; x += 32) {
+      const int s = hits[x], c = hist[s];
+      if (c > best_cnt || (c == best_cnt && s < best_slot)) { best_cnt = c; best_slot = s; }
+      smin = min(smin, s);
+      smax = max(smax, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+      smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+    }
+    if (lane == 0) {
+      // extent of the shared 11-mer diagonals (a hit list overflow widens it to everything)
+      p.kmin[pi] = overflow ? INT32_MIN : smin - R;
+      p.kmax[pi] = overflow ? INT32_MAX : smax - R;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const int oc = __shfl_xor_sync(0xffffffffu, best_cnt, o), os = __shfl_xor_sync(0xffffffffu, best_slot, o);
+      if (oc > best_cnt || (oc == best_cnt && os < best_slot)) { best_cnt = oc; best_slot = os; }
+    }
+    const float inv = 1.f / (float)(R - kK + 1);
+    if (best_cnt == 0) {
+      if (lane == 0) p.dstar[pi] = INT32_MIN;
+      for (int x = lane; x < kFeat; x += 32) f[x] = __float2bfloat16(0.f);
+    } else {
+      const int ds = best_slot - R;
+      int total = 0;
+      for (int x = lane; x < nh; x += 32) total += hist[hits[x]];
+      int win = 0, nonzero = 0, peak = 0;
+      float binv[2];
+      for (int t = 0; t < 2; ++t) {
+        const int bin = lane + 32 * t;
+        const int s = best_slot - kHistBins / 2 + bin;
+        const int c = (s >= 0 && s < R + H) ? hist[s] : 0;
+        win += c;
+        nonzero += c > 0;
+        peak = max(peak, c);
+        binv[t] = (float)c * inv;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        total += __shfl_xor_sync(0xffffffffu, total, o);
+        win += __shfl_xor_sync(0xffffffffu, win, o);
+        nonzero += __shfl_xor_sync(0xffffffffu, nonzero, o);
+        peak = max(peak, __shfl_xor_sync(0xffffffffu, peak, o));
+      }
+      if (overflow) total = max(total, win);
+      f[lane] = __float2bfloat16(binv[0]);
+      f[lane + 32] = __float2bfloat16(binv[1]);
+      if (lane < kFeat - kHistBins) {
+        float v = 0.f;
+        switch (lane) {
+          case 0: v = (float)total * inv; break;
+          case 1: v = (float)(total - win) * inv; break;
+          case 2: v = (float)R / 256.f; break;
+          case 3: v = (float)H / 1024.f; break;
+          case 4: v = (float)(ds + R) / (float)(R + H); break;
+          case 5: v = 1.f; break;
+          case 6: v = (float)peak * inv; break;
+          case 7: v = (float)nonzero / (float)kHistBins; break;
+          default: v = 0.f;
+        }
+        f[kHistBins + lane] = __float2bfloat16(v);
+      }
+      if (lane == 0) p.dstar[pi] = ds;
+    }
+    __syncwarp();
+    if (overflow) {
+      for (int x = lane; x < R + H; x += 32) hist[x] = 0;
+    } else {
+      for (int x = lane; x < nh; x += 32) hist[hits[x]] = 0;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MLP forward on tensor cores: mma.sync m16n8k16, BF16 operands, FP32
+// accumulation.  One warp scores 16 pairs per pass; the weights live in shared
+// memory transposed ([out][in]) so B fragments load with ldmatrix directly.
+// ---------------------------------------------------------------------------
+constexpr int kMlpWarps = 8;
+constexpr int kLdF = kFeat + 8;   // padded row strides (bf16 elements) against bank conflicts
+constexpr int kLdH = kHid + 8;
+
+struct MlpSmem {
+  __nv_bfloat16 w1t[kHid * kLdF];
+  __nv_bfloat16 w2t[kHid * kLdH];
+  __nv_bfloat16 w3t[8 * kLdH];
+  float b1[kHid], b2[kHid], b3[8];
+  __nv_bfloat16 act[kMlpWarps][16 * kLdH];  // per-warp 16-row activation tile
+};
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3, const void* p) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
+}
+__device__ __forceinline__ void ldmatrix_x2(uint32_t& r0, uint32_t& r1, const void* p) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0, %1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(a));
+}
+__device__ __forceinline__ void mma_bf16(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// acc[nt][4] += A[16 x K] (smem, row stride lda) * Bt[N x K]^T (smem, row stride ldb)
+template <int K, int NT>
+__device__ __forceinline__ void warp_gemm(float (*acc)[4], const __nv_bfloat16* A, int lda, const __nv_bfloat16* Bt,
+                                          int ldb, int lane) {
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    uint32_t a0, a1, a2, a3;
+    {
+      const int m = lane >> 3, rr = (lane & 7) + 8 * (m & 1), cc = k0 + 8 * (m >> 1);
+      ldmatrix_x4(a0, a1, a2, a3, A + rr * lda + cc);
+    }
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      uint32_t b0, b1;
+      const int l = lane & 15;
+      ldmatrix_x2(b0, b1, Bt + (nt * 8 + (l & 7)) * ldb + k0 + 8 * (l >> 3));
+      mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
+    }
+  }
+}
+
+// bias + ReLU, write the 16 x (8*NT) tile back as bf16 (row stride kLdH)
+template <int NT>
+__device__ __forceinline__ void store_hidden(float (*acc)[4], const float* bias, __nv_bfloat16* out, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    const int col = nt * 8 + 2 * t;
+    const float v0 = fmaxf(acc[nt][0] + bias[col], 0.f), v1 = fmaxf(acc[nt][1] + bias[col + 1], 0.f);
+    const float v2 = fmaxf(acc[nt][2] + bias[col], 0.f), v3 = fmaxf(acc[nt][3] + bias[col + 1], 0.f);
+    *reinterpret_cast<__nv_bfloat162*>(out + g * kLdH + col) = __floats2bfloat162_rn(v0, v1);
+    *reinterpret_cast<__nv_bfloat162*>(out + (g + 8) * kLdH + col) = __floats2bfloat162_rn(v2, v3);
+  }
+}
+
+__global__ void __launch_bounds__(kMlpWarps * 32) k_mlp_forward(BandParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  MlpSmem& s = *reinterpret_cast<MlpSmem*>(smem_raw);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const MlpParams* W = p.mlp;
+  for (int x = threadIdx.x; x < kHid * kFeat; x += blockDim.x) s.w1t[(x / kFeat) * kLdF + x % kFeat] = W->w1[x];
+  for (int x = threadIdx.x; x < kHid * kHid; x += blockDim.x) s.w2t[(x / kHid) * kLdH + x % kHid] = W->w2[x];
+  for (int x = threadIdx.x; x < 8 * kHid; x += blockDim.x)
+    s.w3t[(x / kHid) * kLdH + x % kHid] = (x / kHid) < kOut ? W->w3[x] : __float2bfloat16(0.f);
+  for (int x = threadIdx.x; x < kHid; x += blockDim.x) { s.b1[x] = W->b1[x]; s.b2[x] = W->b2[x]; }
+  if (threadIdx.x < 8) s.b3[threadIdx.x] = threadIdx.x < kOut ? W->b3[threadIdx.x] : 0.f;
+  __syncthreads();
+  __nv_bfloat16* act = s.act[wib];
+  const long long ntiles = (p.n_pairs + 15) / 16;
+  for (long long tile = blockIdx.x * (long long)kMlpWarps + wib; tile < ntiles; tile += (long long)gridDim.x * kMlpWarps) {
+    const long long row0 = tile * 16;
+    // input tile: 16 pairs x kFeat, zero rows past the end
+    for (int x = lane; x < 16 * kFeat / 8; x += 32) {
+      const int rr = x / (kFeat / 8), cc = (x % (kFeat / 8)) * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (row0 + rr < p.n_pairs) v = *reinterpret_cast<const uint4*>(p.feat + (row0 + rr) * kFeat + cc);
+      *reinterpret_cast<uint4*>(act + rr * kLdH + cc) = v;
+    }
+    __syncwarp();
+    float acc[16][4];
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+    warp_gemm<kFeat, 16>(acc, act, kLdH, s.w1t, kLdF, lane);
+    __syncwarp();
+    store_hidden<16>(acc, s.b1, act, lane);
+    __syncwarp();
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+    warp_gemm<kHid, 16>(acc, act, kLdH, s.w2t, kLdH, lane);
+    __syncwarp();
+    store_hidden<16>(acc, s.b2, act, lane);
+    __syncwarp();
+    float o[1][4] = {{0.f, 0.f, 0.f, 0.f}};
+    warp_gemm<kHid, 1>(o, act, kLdH, s.w3t, kLdH, lane);
+    const int g = lane >> 2, t = lane & 3;
+    if (t == 0) {
+      if (row0 + g < p.n_pairs) {
+        p.mlp_out[(row0 + g) * kOut + 0] = o[0][0] + s.b3[0];
+        p.mlp_out[(row0 + g) * kOut + 1] = o[0][1] + s.b3[1];
+      }
+      if (row0 + g + 8 < p.n_pairs) {
+        p.mlp_out[(row0 + g + 8) * kOut + 0] = o[0][2] + s.b3[0];
+        p.mlp_out[(row0 + g + 8) * kOut + 1] = o[0][3] + s.b3[1];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Routing.  Pass 0 counts band items per (width class, read-length bucket)
+// and writes full-DP fallback units; pass 1 places band items at their
+// bucket's offset so that each warp of the banded kernel gets reads of nearly
+// equal length.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int full_variant(int R) {
+  const int rt = (rows_needed(R, true, true) + 31) / 32;
+  return rt <= 8 ? rt - 1 : 8;  // k_forward<float, rt, single> or the multi-strip variant
+}
+
+__device__ __forceinline__ bool route_band(const BandParams& p, long long pi, int R, int H, int& cls, int& d_lo) {
+  const int ds = p.dstar[pi];
+  if (ds == INT32_MIN || R > kBandMaxRead || R == 0 || H == 0) return false;
+  float lo, hi;
+  if (p.use_mlp) {
+    lo = p.mlp_out[pi * kOut + 0];
+    hi = p.mlp_out[pi * kOut + 1];
+    if (!(lo <= hi) || !isfinite(lo) || !isfinite(hi)) return false;
+  } else {
+    lo = -(float)p.fixed_half;
+    hi = (float)p.fixed_half;
+  }
+  // band in absolute diagonals, widened to hold every shared 11-mer diagonal
+  const int km = p.kmin[pi], kx = p.kmax[pi];
+  if (km == INT32_MIN || kx == INT32_MAX) return false;
+  const int blo = min(ds + (int)floorf(lo) - p.margin, km), bhi = max(ds + (int)ceilf(hi) + p.margin, kx);
+  const int width = bhi - blo + 1;
+  if (width > band_width(kBandWidths - 1) || width < 1) return false;
+  cls = width <= band_width(0) ? 0 : 1;
+  d_lo = blo - (band_width(cls) - width) / 2;
+  return true;
+}
+
+// Block-aggregated: per-block shared counters, one global atomic per
+// (counter, block); pass 1 reserves each bucket's range for the block at once.
+__global__ void __launch_bounds__(256) k_band_route(BandParams p, int pass) {
+  __shared__ unsigned int cnt[kBandWidths * kRBuckets + 9];
+  __shared__ unsigned long long base[kBandWidths * kRBuckets + 9];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long pi0 = blockIdx.x * (long long)blockDim.x; pi0 < p.n_pairs; pi0 += stride) {
+    for (int x = threadIdx.x; x < kBandWidths * kRBuckets + 9; x += blockDim.x) cnt[x] = 0;
+    __syncthreads();
+    const long long pi = pi0 + threadIdx.x;
+    int slot_idx = -1;
+    unsigned local = 0;
+    int r = 0, h = 0, d_lo = 0, R = 0;
+    bool band = false;
+    if (pi < p.n_pairs) {
+      r = p.pair_read[pi];
+      h = p.pair_hap[pi];
+      R = (int)(p.batch.read_off[r + 1] - p.batch.read_off[r]);
+      const int H = (int)(p.batch.hap_off[h + 1] - p.batch.hap_off[h]);
+      int cls = 0;
+      band = route_band(p, pi, R, H, cls, d_lo);
+      const int bucket = min(R / kRBucketRows, kRBuckets - 1);
+      slot_idx = band ? cls * kRBuckets + bucket : kBandWidths * kRBuckets + full_variant(R);
+      if (pass == 0 || band) local = atomicAdd(&cnt[slot_idx], 1u);
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < kBandWidths * kRBuckets + 9; x += blockDim.x) {
+      const unsigned c = cnt[x];
+      if (c == 0) continue;
+      if (x < kBandWidths * kRBuckets) {
+        const int cls = x / kRBuckets, bucket = x % kRBuckets;
+        if (pass == 0) atomicAdd(&p.bctr->band_count[cls][bucket], (unsigned long long)c);
+        else base[x] = atomicAdd(&p.bctr->band_fill[cls][bucket], (unsigned long long)c);
+      } else if (pass == 0) {
+        base[x] = atomicAdd(&p.bctr->full_count[x - kBandWidths * kRBuckets], (unsigned long long)c);
+        atomicAdd(&p.bctr->fallback_route, (unsigned long long)c);
+      }
+    }
+    __syncthreads();
+    if (pi < p.n_pairs) {
+      if (band && pass == 1) {
+        BandItem it;
+        it.read = r; it.hap = h; it.out = pi; it.d_lo = d_lo; it.pad_ = 0;
+        const int cls = slot_idx / kRBuckets;
+        p.items[(size_t)cls * p.item_cap + base[slot_idx] + local] = it;
+      } else if (!band && pass == 0) {
+        const int v = slot_idx - kBandWidths * kRBuckets;
+        const unsigned long long q = base[slot_idx] + local;
+        if (q < (unsigned long long)p.full_cap) {
+          Unit u{};
+          u.read = r; u.hap0 = h; u.nh = 1; u.out0 = pi;
+          p.full_items[(size_t)v * p.full_cap + q] = u;
+        } else {
+          atomicOr(&p.ctr->status, 4ull);
+        }
+      }
+      if (band && pass == 0 && p.audit_period > 0 && pi % p.audit_period == 0) {
+        const unsigned long long a = atomicAdd(&p.bctr->audit_count, 1ull);
+        if (a < (unsigned long long)p.audit_cap) p.audit_pairs[a] = pi;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// exclusive prefix over buckets, per width class
+__global__ void k_band_scan(BandCounters* c) {
+  if (threadIdx.x < kBandWidths) {
+    unsigned long long acc = 0;
+    for (int b = 0; b < kRBuckets; ++b) {
+      c->band_fill[threadIdx.x][b] = acc;
+      acc += c->band_count[threadIdx.x][b];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Banded forward-backward: one thread per pair, the band's state in
+// registers, rows swept top to bottom (forward) then bottom to top
+// (backward).  In band coordinates k = d - d_lo,
+//   forward   M(r,k) <- (r-1,k)   X(r,k) <- (r-1,k+1)   Y(r,k) <- (r,k-1)
+//   backward  B(r,k) <- B(r+1,k) via M, B(r+1,k-1) via X, B(r,k+1) via Y
+// with the FP32 scaled forward recurrence of the full kernel.  Cells left of
+// column 1 stay exactly zero in the forward (their inputs are zero); cells
+// right of column H never feed a cell inside the matrix in the forward and
+// are exactly zero in the backward (their successors lie right of H too).
+// The haplotype window is W one-hot nibbles, shifted one column per row; a
+// match is one AND against the read base's replicated nibble.
+//
+// Fallback test: the posterior mass on the band's two edge diagonals,
+//   sum_r [A(r,0) Bmax(r,0) + A(r,W-1) Bmax(r,W-1)] / L_band,
+// with A = M + X + Y forward and Bmax = max(B_M, B_X, B_Y) -- an upper bound on
+// sum_s F_s B_s at the cell.  The forward keeps A at the two edge cells per
+// row as a pair of BF16 in a per-thread slab (row r at slab[r * nthreads]).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float mm_of(const Tables* tb, int qi, int qd) {
+  const int mx = max(qi, qd), mn = min(qi, qd);
+  return tb->mm_f[((mx * (mx + 1)) >> 1) + mn];
+}
+
+template <int W>
+__global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
+  constexpr int NW = W / 8;
+  const Tables* tb = p.tables;
+  const unsigned long long total = [&] {
+    unsigned long long s = 0;
+    for (int b = 0; b < kRBuckets; ++b) s += p.bctr->band_count[cls][b];
+    return s;
+  }();
+  const BandItem* items = p.items + (size_t)cls * p.item_cap;
+  const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  uint32_t* slab = p.edge_slab + tid;
+  unsigned long long cells = 0;
+  for (unsigned long long ii = tid; ii < total; ii += nthreads) {
+    const BandItem it = items[ii];
+    const int64_t ro = p.batch.read_off[it.read], ho = p.batch.hap_off[it.hap];
+    const int R = (int)(p.batch.read_off[it.read + 1] - ro), H = (int)(p.batch.hap_off[it.hap + 1] - ho);
+    const uchar4* quals = p.batch.read_quals + ro;
+    const uint8_t* rbase = p.batch.read_bases + ro;
+    const uint8_t* hap = p.batch.hap_bases + ho;
+    const int d_lo = it.d_lo;
+    float M[W], X[W], Y[W];
+    const float init_y = tb->init_f / (float)H;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const int c = d_lo + k;
+      M[k] = 0.f; X[k] = 0.f;
+      Y[k] = (c >= 0 && c <= H) ? init_y : 0.f;
+    }
+    uint32_t win[NW];  // row 1: columns d_lo + 1 + k
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      uint32_t v = 0;
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int c = d_lo + 1 + w * 8 + t;
+        v |= ((c >= 1 && c <= H) ? onehot(hap[c - 1]) : 0u) << (4 * t);
+      }
+      win[w] = v;
+    }
+    float ap = 1.f, bp = 1.f;  // pMX / pMY of the row above (1 for row 0)
+    float pmx_last = 1.f;
+    for (int r = 1; r <= R; ++r) {
+      const uchar4 qv = quals[r - 1];
+      const int qi = qv.y & kQualMask, qd = qv.z & kQualMask;
+      const float pmx = tb->ph2pr_f[qi], pmy = tb->ph2pr_f[qd];
+      const float g = tb->ph2pr_f[qv.w & kQualMask], gp = 1.f - g;
+      const float eps = tb->ph2pr_f[qv.x & kQualMask];
+      const float mm = mm_of(tb, qi, qd);
+      const float cx = gp * ap, cy = gp * bp, kap = g * ap / pmx;
+      const float em = 1.f - eps, ex = eps / 3.f;
+      const uint32_t rb = onehot(rbase[r - 1]) * 0x11111111u;
+      float lm = 0.f, ly = 0.f;
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const bool match = (win[k >> 3] & rb & (0xFu << (4 * (k & 7)))) != 0u;
+        const float e = match ? em : ex;
+        const float upm = (k + 1 < W) ? M[k + 1] : 0.f;
+        const float upx = (k + 1 < W) ? X[k + 1] : 0.f;
+        const float mn = e * __fmaf_rn(mm, M[k], __fmaf_rn(cx, X[k], cy * Y[k]));
+        const float xn = __fmaf_rn(kap, upx, upm);
+        const float yn = __fmaf_rn(g, ly, lm);
+        M[k] = mn; X[k] = xn; Y[k] = yn;
+        lm = mn; ly = yn;
+      }
+      // edge cells' A = M + X + Y (true X, Y) for the backward's posterior test
+      const float a0 = M[0] + pmx * X[0] + pmy * Y[0];
+      const float a1 = M[W - 1] + pmx * X[W - 1] + pmy * Y[W - 1];
+      const __nv_bfloat162 pk = __floats2bfloat162_rn(a0, a1);
+      slab[(size_t)r * nthreads] = *reinterpret_cast<const uint32_t*>(&pk);
+      const int cn = r + 1 + d_lo + W - 1;  // next row's window: shift, append column cn
+      const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hap[cn - 1]) : 0u;
+#pragma unroll
+      for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
+      win[NW - 1] = (win[NW - 1] >> 4) | (nib << 28);
+      ap = pmx; bp = pmy;
+      pmx_last = pmx;
+    }
+    float tot = 0.f;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const int c = R + d_lo + k;
+      tot += (c >= 1 && c <= H) ? M[k] + pmx_last * X[k] : 0.f;
+    }
+    cells += (unsigned long long)R * W;
+    bool fall_back = !(tot > 0.f);
+    const bool rescue = !fall_back && (!(tot >= (float)kMinAccepted) || isinf(tot));
+    if (!fall_back && !rescue) {
+      // ---- backward: B in registers, renormalised by powers of two ----
+      float BM[W], BX[W], BY[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const int c = R + d_lo + k;
+        const float v = (c >= 1 && c <= H) ? 1.f : 0.f;
+        BM[k] = v; BX[k] = v; BY[k] = 0.f;
+      }
+      double acc = 0.0;
+      int bexp = 0;  // true B = stored B * 2^bexp
+      {
+        const __nv_bfloat162 pk = *reinterpret_cast<const __nv_bfloat162*>(&slab[(size_t)R * nthreads]);
+        acc += (double)__low2float(pk) * fmaxf(BM[0], BX[0]) + (double)__high2float(pk) * fmaxf(BM[W - 1], BX[W - 1]);
+      }
+      // window to row R's columns (R + d_lo + k): shift back one column
+      {
+        const int c0 = R + d_lo;
+        const uint32_t nib = (c0 >= 1 && c0 <= H) ? onehot(hap[c0 - 1]) : 0u;
+#pragma unroll
+        for (int w = NW - 1; w > 0; --w) win[w] = __funnelshift_l(win[w - 1], win[w], 4);
+        win[0] = (win[0] << 4) | nib;
+      }
+      uchar4 q1 = quals[R - 1];
+      for (int r = R - 1; r >= 1; --r) {
+        const uchar4 q0 = quals[r - 1];  // row r; q1 is row r+1
+        const int qi1 = q1.y & kQualMask, qd1 = q1.z & kQualMask;
+        const float mm1 = mm_of(tb, qi1, qd1), mx1 = tb->ph2pr_f[qi1];
+        const float g1 = tb->ph2pr_f[q1.w & kQualMask], gp1 = 1.f - g1;
+        const float eps1 = tb->ph2pr_f[q1.x & kQualMask];
+        const float em1 = 1.f - eps1, ex1 = eps1 / 3.f;
+        const float my0 = tb->ph2pr_f[q0.z & kQualMask], g0 = tb->ph2pr_f[q0.w & kQualMask];
+        const uint32_t rb1 = onehot(rbase[r]) * 0x11111111u;
+        float byn = 0.f;  // B_Y(r, k+1)
+#pragma unroll
+        for (int k = W - 1; k >= 0; --k) {
+          const bool match = (win[k >> 3] & rb1 & (0xFu << (4 * (k & 7)))) != 0u;
+          const float e = match ? em1 : ex1;
+          const float emb = e * BM[k];
+          const float bxk = (k > 0) ? BX[k - 1] : 0.f;
+          const float nbm = __fmaf_rn(mm1, emb, __fmaf_rn(mx1, bxk, my0 * byn));
+          const float nbx = __fmaf_rn(gp1, emb, g1 * bxk);
+          const float nby = __fmaf_rn(gp1, emb, g0 * byn);
+          BM[k] = nbm; BX[k] = nbx; BY[k] = nby;
+          byn = nby;
+        }
+        const __nv_bfloat162 pk = *reinterpret_cast<const __nv_bfloat162*>(&slab[(size_t)r * nthreads]);
+        const float b0 = fmaxf(BM[0], fmaxf(BX[0], BY[0])), b1 = fmaxf(BM[W - 1], fmaxf(BX[W - 1], BY[W - 1]));
+        acc += ((double)__low2float(pk) * b0 + (double)__high2float(pk) * b1) * ldexp(1.0, bexp);
+        if ((r & 7) == 0) {
+          float m = 0.f;
+#pragma unroll
+          for (int k = 0; k < W; ++k) m = fmaxf(m, fmaxf(BM[k], BX[k]));
+          if (m > 0.f && (m < 0x1p-60f || m > 0x1p60f)) {
+            int e2;
+            frexpf(m, &e2);
+            const float sc = ldexpf(1.f, -e2);
+#pragma unroll
+            for (int k = 0; k < W; ++k) { BM[k] *= sc; BX[k] *= sc; BY[k] *= sc; }
+            bexp += e2;
+          }
+        }
+        // window to row r's columns: shift back one column, new k = 0 is column r + d_lo
+        const int c0 = r + d_lo;
+        const uint32_t nib = (c0 >= 1 && c0 <= H) ? onehot(hap[c0 - 1]) : 0u;
+#pragma unroll
+        for (int w = NW - 1; w > 0; --w) win[w] = __funnelshift_l(win[w - 1], win[w], 4);
+        win[0] = (win[0] << 4) | nib;
+        q1 = q0;
+      }
+      cells += (unsigned long long)R * W;
+      const double edge = acc / (double)tot;
+      fall_back = !(edge <= (double)p.edge_threshold);
+    }
+    if (fall_back) {
+      const int v = full_variant(R);
+      const unsigned long long q = atomicAdd(&p.bctr->full_count[v], 1ull);
+      atomicAdd(&p.bctr->fallback_edge, 1ull);
+      if (q < (unsigned long long)p.full_cap) {
+        Unit u{};
+        u.read = it.read; u.hap0 = it.hap; u.nh = 1; u.out0 = it.out;
+        p.full_items[(size_t)v * p.full_cap + q] = u;
+      } else {
+        atomicOr(&p.ctr->status, 4ull);
+      }
+    } else if (rescue) {
+      const unsigned long long slot = atomicAdd(&p.ctr->rescue_count, 1ull);
+      if (slot < (unsigned long long)p.rescue_cap) {
+        p.rescue[slot].read = it.read;
+        p.rescue[slot].hap = it.hap;
+        p.rescue[slot].out = it.out;
+      } else {
+        atomicOr(&p.ctr->status, 1ull);
+      }
+      p.out[it.out] = __longlong_as_double(0x7ff8000000000000ll);
+    } else {
+      p.out[it.out] = (double)(log10f(tot) - tb->log10_init_f);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
+  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(&p.bctr->band_cells, cells);
+}
+
+__global__ void k_audit_units(BandParams p, Unit* units) {
+  const unsigned long long n = min(p.bctr->audit_count, (unsigned long long)p.audit_cap);
+  for (unsigned long long a = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; a < n;
+       a += (unsigned long long)gridDim.x * blockDim.x) {
+    const long long pi = p.audit_pairs[a];
+    Unit u{};
+    u.read = p.pair_read[pi]; u.hap0 = p.pair_hap[pi]; u.nh = 1; u.out0 = (long long)a;
+    units[a] = u;
+  }
+}
+
+__global__ void k_audit_compare(BandParams p, double* err) {
+  const unsigned long long n = min(p.bctr->audit_count, (unsigned long long)p.audit_cap);
+  for (unsigned long long a = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; a < n;
+       a += (unsigned long long)gridDim.x * blockDim.x) {
+    const double b = p.out[p.audit_pairs[a]], f = p.audit_out[a];
+    // NaN where the full DP's FP32 value needed the FP64 pass (not audited)
+    err[a] = (isfinite(b) && isfinite(f)) ? fabs(b - f) : (isinf(b) && isinf(f) ? 0.0 : __longlong_as_double(0x7ff8000000000000ll));
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_audit_units(const BandParams& p, Unit* units, cudaStream_t st) {
+  k_audit_units<<<64, 256, 0, st>>>(p, units);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_audit_compare(const BandParams& p, double* err, cudaStream_t st) {
+  k_audit_compare<<<64, 256, 0, st>>>(p, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pairs_from_units(const Unit* units, long long n_units, int32_t* pair_read, int32_t* pair_hap,
+                                    int sms, cudaStream_t st) {
+  if (n_units <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((n_units + 255) / 256, (long long)sms * 8);
+  k_pairs_from_units<<<(int)blocks, 256, 0, st>>>(units, n_units, pair_read, pair_hap);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint32_t* codes, int sms, cudaStream_t st) {
+  if (n_bytes <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((n_bytes + 255) / 256, (long long)sms * 16);
+  k_read_kmers<<<(int)blocks, 256, 0, st>>>(read_bases, n_bytes, codes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hap_kmers(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint64_t* keys,
+                             cudaStream_t st) {
+  if (n_haps <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>(n_haps, 148 * 16);
+  k_hap_kmers<<<(int)blocks, 256, 0, st>>>(hap_bases, hap_off, n_haps, keys);
+  return cudaGetLastError();
+}
+
+constexpr int kFeatSmem = kFeatWarps * kBandMaxHap * 8 + kFeatWarps * kBandMaxSpan * 4 + kFeatWarps * (kHitCap + 1) * 4;
+
+cudaError_t prepare_band_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(k_featurize, cudaFuncAttributeMaxDynamicSharedMemorySize, kFeatSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+}
+
+cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
+  if (p.n_pairs <= 0) return cudaSuccess;
+  const int smem = kFeatSmem;
+  const long long blocks = std::min<long long>((p.n_pairs + kFeatWarps - 1) / kFeatWarps, (long long)sms * 3);
+  k_featurize<<<(int)blocks, kFeatWarps * 32, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st) {
+  if (p.n_pairs <= 0) return cudaSuccess;
+  const int smem = (int)sizeof(MlpSmem);
+  const long long tiles = (p.n_pairs + 15) / 16;
+  const long long blocks = std::min<long long>((tiles + kMlpWarps - 1) / kMlpWarps, (long long)sms * 2);
+  k_mlp_forward<<<(int)blocks, kMlpWarps * 32, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st) {
+  if (p.n_pairs <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((p.n_pairs + 255) / 256, (long long)sms * 8);
+  k_band_route<<<(int)blocks, 256, 0, st>>>(p, pass);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st) {
+  k_band_scan<<<1, 32, 0, st>>>(c);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_band_dp(const BandParams& p, int cls, int sms, cudaStream_t st) {
+  const int blocks = band_dp_blocks(sms);
+  if (cls == 0) k_band_f32<16><<<blocks, 128, 0, st>>>(p, 0);
+  else k_band_f32<32><<<blocks, 128, 0, st>>>(p, 1);
+  return cudaGetLastError();
+}
+
+}  // namespace bvphmm

@@ -1,0 +1,120 @@
+// phmm_band.h -- learned-band path: launch interface (host <-> kernels).
+//
+// Pipeline, all on the context's stream:
+//   k_pairs_from_units  expand work units into one (read, hap) per result slot
+//   k_hap_kmers         per haplotype: sorted (11-mer code, position) keys
+//   k_featurize         per pair: shared 11-mer diagonal histogram -> features,
+//                       seed diagonal d* (the histogram's mode)
+//   k_mlp_forward       per pair: BF16 MLP 80-128-128-2 (FP32 accumulation) ->
+//                       lower and upper band edge relative to d*
+//   k_band_route        band (by width class and read-length bucket) or full DP
+//   k_band_f32<W>       banded forward, one thread per pair, edge-mass check
+// Pairs that leave the band path go to the full-DP kernels through per-variant
+// device lists; FP32 results below 1e-28 go to the FP64 list as before.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "phmm_common.h"
+
+namespace bvphmm {
+
+constexpr int kK = 11;                 // k-mer length of the featuriser
+constexpr int kFeat = 80;              // MLP input width (64 histogram bins + 16 scalars, zero padded)
+constexpr int kHid = 128;              // hidden width
+constexpr int kOut = 2;                // outputs: lower and upper band edge (diagonals, relative to d*)
+constexpr int kHistBins = 64;          // histogram window: d* - 32 .. d* + 31
+constexpr int kBandMaxSpan = 2048;     // read_len + hap_len limit of the featuriser (per-warp histogram)
+constexpr int kBandMaxHap = 1024;      // haplotype limit of the k-mer sort and the featuriser's staging
+constexpr int kBandWidths = 2;         // width classes of the banded kernel
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+constexpr int band_width(int cls) { return cls == 0 ? 16 : 32; }
+constexpr int kRBuckets = 64;          // read-length buckets (8 rows each) for warp-uniform band launches
+constexpr int kRBucketRows = 8;
+constexpr int kBandMaxRead = kRBuckets * kRBucketRows - 1;
+
+// MLP parameters, device layout: weights as [out][in] (row = output unit).
+struct MlpParams {
+  __nv_bfloat16 w1[kHid * kFeat];
+  __nv_bfloat16 w2[kHid * kHid];
+  __nv_bfloat16 w3[kOut * kHid];
+  float b1[kHid];
+  float b2[kHid];
+  float b3[kOut];
+};
+
+// One banded-DP work item.
+struct BandItem {
+  int32_t read;
+  int32_t hap;
+  int64_t out;
+  int32_t d_lo;  // first diagonal of the band (c - r)
+  int32_t pad_;
+};
+
+struct BandCounters {
+  unsigned long long band_count[kBandWidths][kRBuckets];  // items per (width, bucket)
+  unsigned long long band_fill[kBandWidths][kRBuckets];
+  unsigned long long band_next[kBandWidths];              // work-queue heads of the band launches
+  unsigned long long full_count[16];                      // fallback items per full-DP variant
+  unsigned long long audit_count;
+  unsigned long long fallback_edge;                       // pairs sent back by the edge check
+  unsigned long long fallback_route;                      // pairs routed to the full DP up front
+  unsigned long long band_cells;
+};
+
+struct BandParams {
+  DeviceBatch batch;
+  const Tables* tables;
+  long long n_pairs;
+  const int32_t* pair_read;   // [n_pairs]
+  const int32_t* pair_hap;    // [n_pairs]
+  const uint64_t* hap_kmers;  // sorted keys, one slot per haplotype base
+  const uint32_t* read_kmers; // 11-mer code per read position
+  int32_t* dstar;             // [n_pairs] seed diagonal (INT32_MIN: no seed)
+  int32_t* kmin;              // [n_pairs] lowest / highest diagonal of a shared 11-mer
+  int32_t* kmax;
+  __nv_bfloat16* feat;        // [n_pairs, kFeat]
+  float* mlp_out;             // [n_pairs, kOut]
+  const MlpParams* mlp;
+  int use_mlp;                // 0: fixed band half-width `fixed_half` around d*
+  int fixed_half;
+  int margin;                 // diagonals added on both sides of the predicted band
+  float edge_threshold;       // fallback when the posterior band-edge mass exceeds it
+  uint32_t* edge_slab;        // [kBandMaxRead + 1][band_dp_blocks * 128] forward edge cells (BF16 pairs)
+  int audit_period;           // every audit_period-th pair is also scored by the full DP (0: off)
+  BandCounters* bctr;
+  Counters* ctr;
+  BandItem* items;            // [kBandWidths][capacity]
+  long long item_cap;
+  Unit* full_items;           // [16][capacity] fallback units (nh = 1), per full-DP variant
+  long long full_cap;
+  int64_t* audit_pairs;       // [audit capacity]
+  long long audit_cap;
+  double* out;                // log10 per result slot
+  double* audit_out;          // full-DP log10 of the audit pairs
+  PairRef* rescue;
+  long long rescue_cap;
+};
+
+cudaError_t launch_pairs_from_units(const Unit* units, long long n_units, int32_t* pair_read, int32_t* pair_hap,
+                                    int sms, cudaStream_t st);
+cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint32_t* codes, int sms, cudaStream_t st);
+cudaError_t launch_hap_kmers(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint64_t* keys,
+                             cudaStream_t st);
+cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st);
+cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st);
+cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st);
+cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st);
+cudaError_t launch_band_dp(const BandParams& p, int width_class, int sms, cudaStream_t st);
+inline int band_dp_blocks(int sms) { return sms * 4; }
+// Sets the dynamic shared-memory limits of the band kernels (before any capture).
+cudaError_t prepare_band_kernels();
+// audit: full-DP units for the sampled pairs (out = audit slot), then the differences
+cudaError_t launch_audit_units(const BandParams& p, Unit* units, cudaStream_t st);
+cudaError_t launch_audit_compare(const BandParams& p, double* err, cudaStream_t st);
+
+}  // namespace bvphmm

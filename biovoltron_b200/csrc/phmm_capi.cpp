@@ -10,6 +10,7 @@
 
 #include "bv_pairhmm.h"
 #include "phmm_engine.h"
+#include "phmm_mlp.h"
 
 struct bv_phmm_ctx {
   bvphmm::Engine engine;
@@ -110,7 +111,6 @@ bv_status bv_phmm_create(const bv_phmm_options* opts, bv_phmm_ctx** out) {
   }
   if (o.precision != BV_PRECISION_AUTO && o.precision != BV_PRECISION_F64) return BV_ERR_INVALID_ARG;
   if (o.mode != BV_MODE_FULL && o.mode != BV_MODE_BAND) return BV_ERR_INVALID_ARG;
-  if (o.mode == BV_MODE_BAND) return BV_ERR_UNSUPPORTED;
   if (o.rescue_threshold != bvphmm::kMinAccepted) return BV_ERR_UNSUPPORTED;
   bv_phmm_ctx* c = new (std::nothrow) bv_phmm_ctx(o);
   if (!c) return BV_ERR_OOM;
@@ -225,6 +225,82 @@ int bv_phmm_debug_tables(float* pf, double* pd, float* mf, double* md, int n) {
   std::memcpy(mf, t->mm_f, sizeof(t->mm_f));
   std::memcpy(md, t->mm_d, sizeof(t->mm_d));
   return 0;
+}
+
+void bv_phmm_default_band_options(bv_band_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->struct_size = (int32_t)sizeof(*o);
+  o->enabled = 1;
+  o->use_mlp = 0;
+  o->fixed_half = 8;
+  o->margin = 2;
+  o->audit_period = 0;
+  o->edge_threshold = 1e-3;
+}
+
+bv_status bv_phmm_set_band_options(bv_phmm_ctx* ctx, const bv_band_options* o) {
+  if (!ctx || !o) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.set_band_options(*o); });
+}
+
+void bv_phmm_default_band_train_options(bv_band_train_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->struct_size = (int32_t)sizeof(*o);
+  o->epochs = 8;
+  o->batch = 1024;
+  o->lr = 2e-3f;
+  o->alpha = 8.f;
+  o->tau = 1e-4f;
+  o->clip = 20.f;
+  o->margin = 2;
+  o->seed = 1234;
+}
+
+bv_status bv_phmm_band_train(bv_phmm_ctx* ctx, const bv_region_batch* train, const bv_band_train_options* o,
+                             bv_band_train_report* report) {
+  if (!ctx || !train || !o) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] {
+    bv_band_train_report r{};
+    const bv_status s = ctx->engine.band_train(*train, *o, &r);
+    if (report) *report = r;
+    return s;
+  });
+}
+
+bv_status bv_phmm_band_labels(bv_phmm_ctx* ctx, const bv_region_batch* batch, float tau, int32_t* dstar, int32_t* lo,
+                              int32_t* hi, float* features) {
+  if (!ctx || !batch || !dstar || !lo || !hi) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.band_labels(*batch, tau, dstar, lo, hi, features); });
+}
+
+int64_t bv_phmm_band_param_count(void) { return bvphmm::kMlpParamCount; }
+
+bv_status bv_phmm_band_get_weights(bv_phmm_ctx* ctx, float* w, int64_t n) {
+  if (!ctx || !w) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.band_get_weights(w, n); });
+}
+
+bv_status bv_phmm_band_set_weights(bv_phmm_ctx* ctx, const float* w, int64_t n) {
+  if (!ctx || !w) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.band_set_weights(w, n); });
+}
+
+bv_status bv_phmm_band_save(bv_phmm_ctx* ctx, const char* path) {
+  if (!ctx || !path) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.band_save(path); });
+}
+
+bv_status bv_phmm_band_load(bv_phmm_ctx* ctx, const char* path) {
+  if (!ctx || !path) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.band_load(path); });
+}
+
+bv_status bv_phmm_band_mlp_eval(bv_phmm_ctx* ctx, const float* w, const float* x, const float* targets, int64_t n,
+                                float alpha, float* out, float* loss, float* grad) {
+  if (!ctx || !w || !x || !targets || !out || !loss || n <= 0) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.band_mlp_eval(w, x, targets, n, alpha, out, loss, grad); });
 }
 
 bv_status bv_phmm_host_register(bv_phmm_ctx* ctx, void* ptr, size_t bytes) {

@@ -452,7 +452,9 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
       const T res = SumRow<T>::value ? lastY + lastM : sumM + sumX;
       const long long o = it.out0 + k;
       if (!is_f64) {
-        if (!(res >= (T)kMinAccepted) || isinf((double)res)) {
+        if (!p.rescue && (!(res >= (T)kMinAccepted) || isinf((double)res))) {
+          p.out[o] = __longlong_as_double(0x7ff8000000000000ll);
+        } else if (!(res >= (T)kMinAccepted) || isinf((double)res)) {
           const unsigned long long slot = atomicAdd(&p.ctr->rescue_count, 1ull);
           if (slot < (unsigned long long)p.rescue_cap) {
             p.rescue[slot].read = it.read;

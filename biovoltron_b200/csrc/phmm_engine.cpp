@@ -55,7 +55,17 @@ int hap_bytes_for(int max_hap, int chunk) {
 long long bnd_cols_for(int max_hap) { return round_up((int64_t)max_hap + kWarp, 32) + 160; }
 }  // namespace
 
-Engine::Engine(const bv_phmm_options& opt) : opt_(opt) {}
+Engine::Engine(const bv_phmm_options& opt) : opt_(opt) {
+  // BV_MODE_BAND at creation: the band path with its default options (a fixed
+  // band around the seed until MLP weights are trained or loaded).
+  band_opt_.struct_size = (int32_t)sizeof(bv_band_options);
+  band_opt_.enabled = opt.mode == BV_MODE_BAND;
+  band_opt_.use_mlp = 0;
+  band_opt_.fixed_half = 8;
+  band_opt_.margin = 2;
+  band_opt_.audit_period = 0;
+  band_opt_.edge_threshold = 1e-3;
+}
 
 Engine::~Engine() {
   destroy_graph();
@@ -323,6 +333,10 @@ bv_status Engine::stage(const bv_region_batch& b) {
   if (s != BV_OK) return s;
   s = upload(b);
   if (s != BV_OK) return s;
+  if (band_enabled()) {
+    s = band_prepare();
+    if (s != BV_OK) return s;
+  }
   staged_ = true;
   runs_since_stage_ = 0;
   return BV_OK;
@@ -352,7 +366,12 @@ bv_status Engine::enqueue_kernels(bool capturing) {
   p.rescue = d_rescue_.as<PairRef>();
   p.rescue_cap = std::max<int64_t>(n_results_, 1);
   BV_CUDA(rec(ev_[2]), "event");
+  if (band_enabled()) {
+    bv_status bs = enqueue_band(capturing, p);
+    if (bs != BV_OK) return bs;
+  }
   for (const auto& lp : plans_) {
+    if (band_enabled()) break;
     p.unit_base = lp.unit_base;
     p.n_units = lp.n_units;
     p.slot = lp.slot;
@@ -381,6 +400,9 @@ bv_status Engine::enqueue_kernels(bool capturing) {
     BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP64 forward launch");
   }
   BV_CUDA(rec(ev_[4]), "event");
+  if (band_enabled() && band_opt_.audit_period > 0) {
+    BV_CUDA(launch_audit_compare(band_params(), d_audit_err_.as<double>(), stream_), "audit compare");
+  }
   return BV_OK;
 }
 
@@ -423,6 +445,11 @@ bv_status Engine::run(bv_phmm_stats* stats) {
   BV_CUDA(cudaMemcpyAsync(&c, d_counters_.get(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_), "counters D2H");
   BV_CUDA(cudaStreamSynchronize(stream_), "run sync");
   if (c.status != 0) return fail(BV_ERR_INTERNAL, "kernel reported an inconsistent state");
+  if (stats) *stats = bv_phmm_stats{};
+  if (stats && band_enabled()) {
+    bv_status bs = band_stats(stats);
+    if (bs != BV_OK) return bs;
+  }
   if (stats) {
     float ms32 = 0, ms64 = 0;
     cudaEventElapsedTime(&ms32, ev_[2], ev_[3]);
@@ -431,7 +458,10 @@ bv_status Engine::run(bv_phmm_stats* stats) {
     stats->cells = n_cells_;
     stats->rescued = (int64_t)c.rescue_count;
     stats->underflow = (int64_t)c.underflow_count;
-    stats->kernel_launches = (int64_t)plans_.size() + 1;
+    stats->kernel_launches = band_enabled()
+                                 ? 6 + (band_opt_.use_mlp ? 1 : 0) + kBandWidths + 9 +
+                                       (band_opt_.audit_period > 0 ? 3 : 0) + 1
+                                 : (int64_t)plans_.size() + 1;
     stats->ms_fp32 = ms32;
     stats->ms_fp64 = ms64;
     stats->ms_h2d = ms_h2d_;

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "bv_pairhmm.h"
+#include "phmm_band.h"
 #include "phmm_common.h"
 #include "phmm_kernels.h"
 
@@ -60,12 +61,25 @@ class Engine {
   int64_t staged_results() const { return n_results_; }
   cudaStream_t stream() const { return stream_; }
   int device() const { return opt_.device; }
+  bv_status set_band_options(const bv_band_options& o);
+  bool band_enabled() const { return band_opt_.enabled != 0; }
+  bv_status band_train(const bv_region_batch& b, const bv_band_train_options& o, bv_band_train_report* rep);
+  bv_status band_labels(const bv_region_batch& b, float tau, int32_t* dstar, int32_t* lo, int32_t* hi, float* feat);
+  bv_status band_get_weights(float* w, int64_t n);
+  bv_status band_set_weights(const float* w, int64_t n);
+  bv_status band_save(const char* path);
+  bv_status band_load(const char* path);
+  bv_status band_mlp_eval(const float* w, const float* x, const float* t, int64_t n, float alpha, float* out,
+                          float* loss, float* grad);
 
  private:
   bv_status validate(const bv_region_batch& b);
   bv_status plan(const bv_region_batch& b);
   bv_status upload(const bv_region_batch& b);
   bv_status enqueue_kernels(bool capturing);
+  bv_status band_prepare();
+  bv_status enqueue_band(bool capturing, KernelParams& p);
+  bv_status band_stats(bv_phmm_stats* stats);
   void destroy_graph();
 
   bv_phmm_options opt_;
@@ -91,6 +105,22 @@ class Engine {
   int max_hap_ = 0;
   bool staged_ = false;
   float ms_h2d_ = 0;
+
+  // learned band
+  bv_band_options band_opt_{};
+  bool mlp_ready_ = false;
+  DevBuf d_pair_read_, d_pair_hap_, d_hap_kmers_, d_dstar_, d_feat_, d_mlp_out_, d_mlp_, d_bctr_;
+  DevBuf d_kmin_, d_kmax_, d_edge_slab_, d_read_kmers_;
+  DevBuf d_band_items_, d_full_items_, d_audit_pairs_, d_audit_units_, d_audit_out_, d_audit_err_;
+  long long item_cap_ = 0, full_cap_ = 0, audit_cap_ = 0;
+  LaunchPlan full_plans_[9];
+  BandParams band_params() const;
+  // training
+  bv_status stage_for_labels(const bv_region_batch& b);
+  bv_status compute_labels(const bv_region_batch& b, float tau, float* ms);
+  bv_status install_weights(const float* w_host);
+  std::vector<float> mlp_w_;  // FP32 master weights of the installed MLP
+  DevBuf d_lab_lo_, d_lab_hi_, d_lab_fbuf_, d_mlp_w_;
 
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;

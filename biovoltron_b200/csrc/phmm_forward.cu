@@ -59,7 +59,8 @@ __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
   const int warp_global = blockIdx.x * (kThreadsPerBlock / kWarp) + wib;
   unsigned char* wsm = smem + (size_t)wib * p.warp_smem_bytes;
   T* bnd = MULTI ? reinterpret_cast<T*>(p.bnd) + (size_t)warp_global * p.bnd_cols * 4 : nullptr;
-  const unsigned long long n = p.from_rescue ? p.ctr->rescue_count : (unsigned long long)p.n_units;
+  const unsigned long long n = p.from_rescue ? p.ctr->rescue_count
+                               : p.n_units_dev ? *p.n_units_dev : (unsigned long long)p.n_units;
   const unsigned long long n_eff = p.from_rescue && n > (unsigned long long)p.rescue_cap ? p.rescue_cap : n;
   unsigned long long* next = p.from_rescue ? &p.ctr->rescue_next : &p.ctr->unit_next[p.slot];
   for (;;) {

@@ -15,11 +15,12 @@ struct KernelParams {
   const Unit* units;
   long long unit_base;
   long long n_units;
+  const unsigned long long* n_units_dev;  // if set, the unit count is read from device memory
   int slot;               // work-queue head used by this launch
   int from_rescue;        // 1: items come from the FP64 list
   Counters* ctr;
   double* out;            // log10 likelihoods, one per result slot
-  PairRef* rescue;
+  PairRef* rescue;        // null: pairs below the FP32 threshold get NaN (audit runs)
   long long rescue_cap;
   int hap_bytes;          // per-warp bytes for staged haplotype codes
   int warp_smem_bytes;    // per-warp dynamic shared memory

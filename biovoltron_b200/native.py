@@ -44,7 +44,30 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_int64),
         ("ms_h2d", C.c_double), ("ms_fp32", C.c_double), ("ms_fp64", C.c_double), ("ms_band", C.c_double),
         ("ms_d2h", C.c_double), ("ms_total", C.c_double),
+        ("band_routed_full", C.c_int64), ("audit_pairs", C.c_int64), ("audit_max_err", C.c_double),
+        ("audit_p99_err", C.c_double),
     ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BandOptions(C.Structure):
+    _fields_ = [("struct_size", C.c_int32), ("enabled", C.c_int32), ("use_mlp", C.c_int32),
+                ("fixed_half", C.c_int32), ("margin", C.c_int32), ("audit_period", C.c_int32),
+                ("edge_threshold", C.c_double), ("reserved", C.c_int32 * 6)]
+
+
+class BandTrainOptions(C.Structure):
+    _fields_ = [("struct_size", C.c_int32), ("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float),
+                ("alpha", C.c_float), ("tau", C.c_float), ("clip", C.c_float), ("margin", C.c_int32),
+                ("seed", C.c_uint64), ("reserved", C.c_int32 * 4)]
+
+
+class BandTrainReport(C.Structure):
+    _fields_ = [("pairs", C.c_int64), ("labelled", C.c_int64), ("steps", C.c_int32), ("first_loss", C.c_float),
+                ("last_loss", C.c_float), ("cover_frac", C.c_double), ("band_frac", C.c_double),
+                ("ms_labels", C.c_double), ("ms_train", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -117,7 +140,18 @@ def load() -> C.CDLL:
         "bv_phmm_host_register": (C.c_int, [V, V, C.c_size_t]),
         "bv_phmm_host_unregister": (C.c_int, [V, V]),
         "bv_phmm_debug_tables": (C.c_int, [V, V, V, V, C.c_int]),
+        "bv_phmm_default_band_options": (None, [P(BandOptions)]),
+        "bv_phmm_set_band_options": (C.c_int, [V, P(BandOptions)]),
         "bv_phmm_measure_fp32_peak": (C.c_int, [C.c_int, P(C.c_double)]),
+        "bv_phmm_default_band_train_options": (None, [P(BandTrainOptions)]),
+        "bv_phmm_band_train": (C.c_int, [V, P(RegionBatchC), P(BandTrainOptions), P(BandTrainReport)]),
+        "bv_phmm_band_labels": (C.c_int, [V, P(RegionBatchC), C.c_float, V, V, V, V]),
+        "bv_phmm_band_param_count": (C.c_int64, []),
+        "bv_phmm_band_get_weights": (C.c_int, [V, V, C.c_int64]),
+        "bv_phmm_band_set_weights": (C.c_int, [V, V, C.c_int64]),
+        "bv_phmm_band_save": (C.c_int, [V, C.c_char_p]),
+        "bv_phmm_band_load": (C.c_int, [V, C.c_char_p]),
+        "bv_phmm_band_mlp_eval": (C.c_int, [V, V, V, V, C.c_int64, C.c_float, V, V, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

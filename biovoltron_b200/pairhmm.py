@@ -16,6 +16,7 @@ shacc batch hook and the device-resident stage/run/fetch cycle).
 from __future__ import annotations
 
 import ctypes as C
+import os
 import math
 from typing import List, Optional, Sequence
 
@@ -127,6 +128,71 @@ class PairHMMEngine:
             out = np.empty(max(n, 1), np.float64)
         self._check(self.lib.bv_phmm_fetch_results(self.h, _ptr(out), n))
         return out[:n]
+
+    def set_band_options(self, enabled: bool = True, use_mlp: bool = False, fixed_half: int = 8, margin: int = 2,
+                         audit_period: int = 0, edge_threshold: float = 1e-3):
+        """Routes pairs through the banded kernel (see bv_band_options)."""
+        o = N.BandOptions()
+        self.lib.bv_phmm_default_band_options(C.byref(o))
+        o.enabled, o.use_mlp, o.fixed_half, o.margin = int(enabled), int(use_mlp), fixed_half, margin
+        o.audit_period, o.edge_threshold = audit_period, edge_threshold
+        self._check(self.lib.bv_phmm_set_band_options(self.h, C.byref(o)))
+
+    # --- learned band: training and weights ---------------------------------
+    def band_train(self, batch: RegionBatch, epochs: int = 8, batch_size: int = 1024, lr: float = 2e-3,
+                   alpha: float = 8.0, tau: float = 1e-4, clip: float = 20.0, margin: int = 2,
+                   seed: int = 1234) -> dict:
+        """Labels `batch` on the GPU and trains the band MLP (bv_phmm_band_train)."""
+        o = N.BandTrainOptions()
+        self.lib.bv_phmm_default_band_train_options(C.byref(o))
+        o.epochs, o.batch, o.lr, o.alpha, o.tau, o.clip, o.margin, o.seed = (
+            epochs, batch_size, lr, alpha, tau, clip, margin, seed)
+        v = _BatchView(batch)
+        rep = N.BandTrainReport()
+        self._check(self.lib.bv_phmm_band_train(self.h, C.byref(v.c), C.byref(o), C.byref(rep)))
+        self._staged = None
+        return rep.as_dict()
+
+    def band_labels(self, batch: RegionBatch, tau: float = 1e-4, features: bool = False):
+        """Seed diagonal, label spread lo/hi (absolute diagonals) and optionally
+        the MLP inputs of every result slot."""
+        v = _BatchView(batch)
+        n = int(self.lib.bv_phmm_region_results(C.byref(v.c)))
+        ds, lo, hi = (np.empty(max(n, 1), np.int32) for _ in range(3))
+        feat = np.empty((max(n, 1), 80), np.float32) if features else None
+        self._check(self.lib.bv_phmm_band_labels(self.h, C.byref(v.c), tau, _ptr(ds), _ptr(lo), _ptr(hi),
+                                                 _ptr(feat) if features else None))
+        self._staged = None
+        out = (ds[:n], lo[:n], hi[:n])
+        return out + (feat[:n],) if features else out
+
+    def band_weights(self) -> np.ndarray:
+        w = np.empty(int(self.lib.bv_phmm_band_param_count()), np.float32)
+        self._check(self.lib.bv_phmm_band_get_weights(self.h, _ptr(w), w.size))
+        return w
+
+    def set_band_weights(self, w: np.ndarray):
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(self.lib.bv_phmm_band_set_weights(self.h, _ptr(w), w.size))
+
+    def band_save(self, path: str):
+        self._check(self.lib.bv_phmm_band_save(self.h, os.fsencode(path)))
+
+    def band_load(self, path: str):
+        self._check(self.lib.bv_phmm_band_load(self.h, os.fsencode(path)))
+
+    def band_mlp_eval(self, w: np.ndarray, x: np.ndarray, targets: np.ndarray, alpha: float, grad: bool = True):
+        """Training objective on the GPU: (outputs [n, 2], loss, gradient or None)."""
+        w = np.ascontiguousarray(w, np.float32)
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        n = x.shape[0]
+        out = np.empty((n, 2), np.float32)
+        loss = np.zeros(1, np.float32)
+        g = np.empty_like(w) if grad else None
+        self._check(self.lib.bv_phmm_band_mlp_eval(self.h, _ptr(w), _ptr(x), _ptr(t), n, alpha, _ptr(out),
+                                                   _ptr(loss), _ptr(g) if grad else None))
+        return out, float(loss[0]), g
 
     def host_register(self, arr: np.ndarray):
         self._check(self.lib.bv_phmm_host_register(self.h, _ptr(arr), arr.nbytes))

@@ -86,6 +86,10 @@ typedef struct bv_phmm_stats {
   double ms_band;         /* featurise + band MLP + banded DP kernels */
   double ms_d2h;          /* device->host copy of the results */
   double ms_total;        /* whole call, host wall clock */
+  int64_t band_routed_full; /* pairs the router sent to the full DP (no seed, too wide, too long) */
+  int64_t audit_pairs;      /* banded pairs also scored by the full DP */
+  double audit_max_err;     /* max |log10 band - log10 full| over the audit pairs */
+  double audit_p99_err;     /* 99th percentile of the same */
 } bv_phmm_stats;
 
 typedef struct bv_phmm_ctx bv_phmm_ctx;
@@ -101,6 +105,30 @@ bv_status bv_phmm_create(const bv_phmm_options* opts, bv_phmm_ctx** out);
 void bv_phmm_destroy(bv_phmm_ctx* ctx);
 /* Message describing the last failure on this context ("" if none). */
 const char* bv_phmm_last_error(const bv_phmm_ctx* ctx);
+
+/* --- learned band --------------------------------------------------------
+ * With `enabled`, every pair is first scored on a diagonal band around its
+ * 11-mer seed diagonal: [seed + lo - margin, seed + hi + margin], where lo/hi
+ * come from the band MLP (use_mlp, weights from bv_phmm_band_train or
+ * bv_phmm_band_load) or are -fixed_half/+fixed_half.  Pairs without a seed,
+ * with a band wider than 32 diagonals or reads longer than 511 bases, and
+ * pairs whose band-edge mass exceeds edge_threshold are scored by the full DP.
+ * Every audit_period-th banded pair is also scored by the full DP and the
+ * differences are reported in bv_phmm_stats.  No counterpart in the reference
+ * (its PairHMM always computes the full matrix). */
+typedef struct bv_band_options {
+  int32_t struct_size;    /* sizeof(bv_band_options) */
+  int32_t enabled;
+  int32_t use_mlp;
+  int32_t fixed_half;
+  int32_t margin;
+  int32_t audit_period;
+  double edge_threshold;
+  int32_t reserved[6];
+} bv_band_options;
+
+void bv_phmm_default_band_options(bv_band_options* opts);
+bv_status bv_phmm_set_band_options(bv_phmm_ctx* ctx, const bv_band_options* opts);
 
 /* --- seam 1/2: the per-pair testcase --------------------------------------
  * Layout of `testcase` (lib/intel_native/pairhmm/pairhmm_common.h:20-24).
@@ -190,6 +218,68 @@ bv_status bv_phmm_fetch_results(bv_phmm_ctx* ctx, double* out_log10, int64_t n);
  * at full bandwidth (cudaHostRegister); unregister before freeing it. */
 bv_status bv_phmm_host_register(bv_phmm_ctx* ctx, void* ptr, size_t bytes);
 bv_status bv_phmm_host_unregister(bv_phmm_ctx* ctx, void* ptr);
+
+/* --- learned band: training and weights ---------------------------------- */
+/* Band MLP training, on this context's GPU.  Labels: for every pair of
+ * `train` the full-DP forward-backward gives the posterior of each cell,
+ * normalised per read row; the label is the lowest and highest diagonal
+ * whose largest per-row posterior reaches `tau`, relative to the pair's
+ * 11-mer seed diagonal.  Pairs without a seed or with reads longer than 511
+ * bases are not used.  The MLP (80-128-128-2, ReLU, BF16 weights as the
+ * inference kernel uses them) is trained with Adam on an asymmetric squared
+ * loss that weights a band narrower than the label by `alpha`.  On success
+ * the weights are installed (use_mlp may be set).  Replaces the previous
+ * staged batch (stage again before bv_phmm_run).  No counterpart in the
+ * reference. */
+typedef struct bv_band_train_options {
+  int32_t struct_size;  /* sizeof(bv_band_train_options) */
+  int32_t epochs;
+  int32_t batch;        /* pairs per Adam step */
+  float lr;             /* peak learning rate (cosine decay to 0) */
+  float alpha;          /* loss weight of under-covering errors */
+  float tau;            /* posterior threshold of the label spread */
+  float clip;           /* labels are clipped to [-clip, clip] diagonals */
+  int32_t margin;       /* margin used for the coverage figures of the report */
+  uint64_t seed;        /* weight initialisation and shuffling */
+  int32_t reserved[4];
+} bv_band_train_options;
+
+typedef struct bv_band_train_report {
+  int64_t pairs;          /* pairs in the training batch */
+  int64_t labelled;       /* pairs with a seed and a label */
+  int32_t steps;          /* Adam steps taken */
+  float first_loss;       /* loss of the first and of the last epoch (mean over steps) */
+  float last_loss;
+  double cover_frac;      /* labelled pairs whose routed band (margin, 11-mer extent) covers the label */
+  double band_frac;       /* labelled pairs whose routed band fits the banded kernel (<= 32 diagonals) */
+  double ms_labels;       /* label kernel time */
+  double ms_train;        /* training loop time */
+} bv_band_train_report;
+
+void bv_phmm_default_band_train_options(bv_band_train_options* opts);
+bv_status bv_phmm_band_train(bv_phmm_ctx* ctx, const bv_region_batch* train, const bv_band_train_options* opts,
+                             bv_band_train_report* report);
+/* Labels and features of a batch, as training sees them (testing and
+ * analysis): per result slot the seed diagonal (INT32_MIN: none), the label
+ * spread lo/hi in absolute diagonals (INT32_MIN: none) and, if `features` is
+ * not NULL, the 80 MLP inputs.  Replaces the staged batch. */
+bv_status bv_phmm_band_labels(bv_phmm_ctx* ctx, const bv_region_batch* batch, float tau, int32_t* dstar, int32_t* lo,
+                              int32_t* hi, float* features);
+/* Number of FP32 MLP parameters: W1[128][80], b1[128], W2[128][128], b2[128],
+ * W3[2][128], b3[2], weights as [output][input], in that order. */
+int64_t bv_phmm_band_param_count(void);
+bv_status bv_phmm_band_get_weights(bv_phmm_ctx* ctx, float* w, int64_t n);
+bv_status bv_phmm_band_set_weights(bv_phmm_ctx* ctx, const float* w, int64_t n);
+/* Weight file: 8-byte magic "BVBANDW\0", u32 version (1), u32 80, u32 128,
+ * u32 2, u32 parameter count, FP32 parameters (little endian). */
+bv_status bv_phmm_band_save(bv_phmm_ctx* ctx, const char* path);
+bv_status bv_phmm_band_load(bv_phmm_ctx* ctx, const char* path);
+/* One evaluation of the training objective on the GPU with the given FP32
+ * weights (rounded to BF16 as in training): outputs [n][2], the loss and, if
+ * `grad` is not NULL, its gradient (bv_phmm_band_param_count floats).  x is
+ * [n][80], targets [n][2].  For gradient checks. */
+bv_status bv_phmm_band_mlp_eval(bv_phmm_ctx* ctx, const float* w, const float* x, const float* targets, int64_t n,
+                                float alpha, float* out, float* loss, float* grad);
 
 /* --- scoring without any allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc when they need scores: e.g. a

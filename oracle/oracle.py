@@ -106,6 +106,45 @@ class Oracle:
                       ("orc_table_mm_f32", C.c_float), ("orc_table_mm_f64", C.c_double)):
             _bind(L, nm, C.POINTER(t), [])
         _bind(L, "orc_table_mm_size", C.c_int, [])
+        self._band = _bind(L, "orc_band_log10", C.c_double, [P, C.c_int, C.c_int])
+        self._post = _bind(L, "orc_posterior_diag", C.c_int, [P, C.c_void_p])
+        self._leak = _bind(L, "orc_band_leak_bound", C.c_double, [])
+        self.set_rho = _bind(L, "orc_band_set_rho", None, [C.c_double])
+        self.set_r0 = _bind(L, "orc_band_set_r0", None, [C.c_int])
+        self._pedge = _bind(L, "orc_band_posterior_edge", C.c_double, [P, C.c_int, C.c_int])
+        self._bdet = _bind(L, "orc_band_detail", C.c_double,
+                           [P, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)])
+
+    # banded DP and posterior spread (learned-band path) ---------------------
+    def band_log10(self, tcs: TestcaseArray, d_lo, W) -> np.ndarray:
+        d_lo = np.broadcast_to(np.asarray(d_lo, np.int64), (tcs.n,))
+        W = np.broadcast_to(np.asarray(W, np.int64), (tcs.n,))
+        return np.array([self._band(C.pointer(tcs.arr[k]), int(d_lo[k]), int(W[k])) for k in range(tcs.n)])
+
+    def band_detail(self, tcs: TestcaseArray, d_lo, W):
+        """Banded log10 plus the kernel's edge statistics (row_ratio, end_frac)."""
+        d_lo = np.broadcast_to(np.asarray(d_lo, np.int64), (tcs.n,))
+        W = np.broadcast_to(np.asarray(W, np.int64), (tcs.n,))
+        out = np.zeros((tcs.n, 4))
+        a, b = C.c_double(), C.c_double()
+        for k in range(tcs.n):
+            out[k, 0] = self._bdet(C.pointer(tcs.arr[k]), int(d_lo[k]), int(W[k]), C.byref(a), C.byref(b))
+            out[k, 1], out[k, 2] = a.value, b.value
+            out[k, 3] = self._leak()
+        return out
+
+    def band_posterior_edge(self, tcs: TestcaseArray, d_lo, W) -> np.ndarray:
+        """Upper bound on the posterior mass of the band's two edge diagonals."""
+        d_lo = np.broadcast_to(np.asarray(d_lo, np.int64), (tcs.n,))
+        W = np.broadcast_to(np.asarray(W, np.int64), (tcs.n,))
+        return np.array([self._pedge(C.pointer(tcs.arr[k]), int(d_lo[k]), int(W[k])) for k in range(tcs.n)])
+
+    def posterior_diag(self, tcs: TestcaseArray, k: int):
+        """Per-diagonal max-over-rows posterior for pair k: (dmin, pstar array)."""
+        t = tcs.arr[k]
+        out = np.zeros(t.rslen + t.haplen - 1, np.float64)
+        st = self._post(C.pointer(t), out.ctypes.data)
+        return (1 - t.rslen, out) if st == 0 else (1 - t.rslen, None)
 
     # batch forms ------------------------------------------------------------
     def log10_reference_rule(self, tcs: TestcaseArray, threads: int = 0) -> Tuple[np.ndarray, np.ndarray]:
@@ -190,3 +229,37 @@ class Reference:
             "mm_f32": np.ctypeslib.as_array(L.ref_table_mm_f32(), (n,)).copy(),
             "mm_f64": np.ctypeslib.as_array(L.ref_table_mm_f64(), (n,)).copy(),
         }
+
+
+def seed_diagonal(read: bytes, hap: bytes, k: int = 11):
+    """The featuriser's seed diagonal: the most frequent j - i over shared
+    k-mers (read position i, haplotype position j, A/C/G/T only), smallest on
+    ties; None without a shared k-mer."""
+    if len(read) < k or len(hap) < k:
+        return None
+    idx = {}
+    for j in range(len(hap) - k + 1):
+        s = hap[j:j + k]
+        if all(c in b"ACGT" for c in s):
+            idx.setdefault(s, []).append(j)
+    counts = {}
+    for i in range(len(read) - k + 1):
+        for j in idx.get(read[i:i + k], ()):
+            counts[j - i] = counts.get(j - i, 0) + 1
+    if not counts:
+        return None
+    best = max(counts.values())
+    return min(d for d, c in counts.items() if c == best)
+
+
+def seed_extent(read: bytes, hap: bytes, k: int = 11):
+    """Lowest and highest diagonal j - i of a shared k-mer, or None."""
+    if len(read) < k or len(hap) < k:
+        return None
+    idx = {}
+    for j in range(len(hap) - k + 1):
+        s = hap[j:j + k]
+        if all(c in b"ACGT" for c in s):
+            idx.setdefault(s, []).append(j)
+    ds = [j - i for i in range(len(read) - k + 1) for j in idx.get(read[i:i + k], ())]
+    return (min(ds), max(ds)) if ds else None

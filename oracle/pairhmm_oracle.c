@@ -45,7 +45,7 @@
 #define ORC_JAC_TOL 8.0
 #define ORC_JAC_STEP 0.0001
 #define ORC_JAC_INV_STEP (1.0 / ORC_JAC_STEP)
-#define ORC_JAC_SIZE ((int)(ORC_JAC_TOL / ORC_JAC_STEP) + 1)
+#define ORC_JAC_SIZE 80001 /* (int)(ORC_JAC_TOL / ORC_JAC_STEP) + 1, Context.h:10 */
 #define ORC_MM_SIZE (((ORC_MAX_QUAL + 1) * (ORC_MAX_QUAL + 2)) >> 1)
 #define ORC_MIN_ACCEPTED 1e-28f
 
@@ -375,3 +375,317 @@ const double *orc_table_ph2pr_f64(void) { orc_init(); return ph2pr_d; }
 const float *orc_table_mm_f32(void) { orc_init(); return mm_f; }
 const double *orc_table_mm_f64(void) { orc_init(); return mm_d; }
 int orc_table_mm_size(void) { return ORC_MM_SIZE; }
+
+/* ------------------------------------------------------------------------ *
+ * Learned-band support (the reference has no banded PairHMM; these define
+ * the banded DP and the training labels the B200 path computes).
+ *
+ * Band: diagonals d = c - r in [d_lo, d_lo + W).  Row 0 carries
+ * Y = 1/H on its band cells with 0 <= c <= H; in rows r >= 1 cells outside the
+ * band or outside 1 <= c <= H are zero; in-band cells follow the reference
+ * recurrence (avx-pairhmm-template.h:183-198) with out-of-band neighbours
+ * zero.  Result: log10 of the sum over the last row's band cells with
+ * 1 <= c <= H of M + X, rows renormalised by powers of two as in
+ * orc_log10_rescaled.
+ * ------------------------------------------------------------------------ */
+double orc_band_log10(const orc_testcase *tc, int d_lo, int W) {
+    orc_init();
+    const int R = tc->rslen, H = tc->haplen;
+    if (R == 0 || H == 0 || W <= 0) return -INFINITY;
+    double *buf = (double *)calloc((size_t)6 * W, sizeof(double));
+    double *Mp = buf, *Xp = buf + W, *Yp = buf + 2 * W, *Mc = buf + 3 * W, *Xc = buf + 4 * W, *Yc = buf + 5 * W;
+    for (int k = 0; k < W; k++) {
+        const int c = d_lo + k;
+        Yp[k] = (c >= 0 && c <= H) ? 1.0 / (double)H : 0.0;
+    }
+    long long e2sum = 0;
+    for (int r = 1; r <= R; r++) {
+        const int qi = tc->i[r - 1] & 127, qd = tc->d[r - 1] & 127;
+        const int qc = tc->c[r - 1] & 127, qq = tc->q[r - 1] & 127;
+        const double pMM = set_mm_prob_d(qi, qd), gp = 1.0 - ph2pr_d[qc];
+        const double pMX = ph2pr_d[qi], pMY = ph2pr_d[qd], g = ph2pr_d[qc];
+        const double eps = ph2pr_d[qq], one_m = 1.0 - eps, mis = eps / 3.0;
+        const uint8_t rc = base_code[(uint8_t)tc->rs[r - 1]];
+        double mx = 0;
+        for (int k = 0; k < W; k++) {
+            const int c = r + d_lo + k;
+            if (c < 1 || c > H) { Mc[k] = Xc[k] = Yc[k] = 0; continue; }
+            const double e = is_match(rc, base_code[(uint8_t)tc->hap[c - 1]]) ? one_m : mis;
+            Mc[k] = e * (pMM * Mp[k] + gp * Xp[k] + gp * Yp[k]);
+            Xc[k] = (k + 1 < W) ? pMX * Mp[k + 1] + g * Xp[k + 1] : 0.0;
+            Yc[k] = (k > 0) ? pMY * Mc[k - 1] + g * Yc[k - 1] : 0.0;
+            double m = Mc[k] > Xc[k] ? Mc[k] : Xc[k];
+            m = m > Yc[k] ? m : Yc[k];
+            mx = mx > m ? mx : m;
+        }
+        if (mx > 0) {
+            int e2; frexp(mx, &e2);
+            const double s = ldexp(1.0, -e2);
+            for (int k = 0; k < W; k++) { Mc[k] *= s; Xc[k] *= s; Yc[k] *= s; }
+            e2sum += e2;
+        }
+        double *t;
+        t = Mp; Mp = Mc; Mc = t; t = Xp; Xp = Xc; Xc = t; t = Yp; Yp = Yc; Yc = t;
+    }
+    double s = 0;
+    for (int k = 0; k < W; k++) {
+        const int c = R + d_lo + k;
+        if (c >= 1 && c <= H) s += Mp[k] + Xp[k];
+    }
+    free(buf);
+    if (!(s > 0)) return -INFINITY;
+    return log10(s) + (double)e2sum * log10(2.0);
+}
+
+/*
+ * Posterior spread over diagonals from the full forward-backward DP.
+ * For each row r >= 1 the posterior of the cells, p_r(c) ~ sum over states
+ * of F_s(r,c) B_s(r,c), is normalised to sum 1 over the row; pstar[d - dmin]
+ * = max over rows of p_r at diagonal d = c - r, for d in [dmin, dmax] =
+ * [1 - R, H - 1].  Returns 0, or -1 when the likelihood is zero.
+ * Backward recurrences (successor weights of the forward):
+ *   B_M(r,c) = mm(r+1) e(r+1,c+1) B_M(r+1,c+1) + mx(r+1) B_X(r+1,c) + my(r) B_Y(r,c+1) + [r==R]
+ *   B_X(r,c) = gp(r+1) e(r+1,c+1) B_M(r+1,c+1) + g(r+1) B_X(r+1,c) + [r==R]
+ *   B_Y(r,c) = gp(r+1) e(r+1,c+1) B_M(r+1,c+1) + g(r) B_Y(r,c+1)
+ * Every row is renormalised by a power of two in both passes; the per-row
+ * normalisation of p_r makes those scales cancel.
+ */
+int orc_posterior_diag(const orc_testcase *tc, double *pstar) {
+    orc_init();
+    const int R = tc->rslen, H = tc->haplen;
+    if (R == 0 || H == 0) return -1;
+    const size_t W = (size_t)H + 2;
+    double *F = (double *)calloc((size_t)3 * (R + 1) * W, sizeof(double));
+    double *B = (double *)calloc((size_t)3 * (R + 2) * W, sizeof(double));
+    double *mm = malloc(sizeof(double) * (R + 2)), *gp = malloc(sizeof(double) * (R + 2));
+    double *mx = malloc(sizeof(double) * (R + 2)), *my = malloc(sizeof(double) * (R + 2));
+    double *gg = malloc(sizeof(double) * (R + 2)), *em = malloc(sizeof(double) * (R + 2));
+    double *ex = malloc(sizeof(double) * (R + 2));
+    uint8_t *rc = malloc((size_t)R + 2), *hc = malloc((size_t)H + 2);
+    for (int c = 1; c <= H; c++) hc[c] = base_code[(uint8_t)tc->hap[c - 1]];
+    for (int r = 1; r <= R; r++) {
+        const int qi = tc->i[r - 1] & 127, qd = tc->d[r - 1] & 127, qc = tc->c[r - 1] & 127, qq = tc->q[r - 1] & 127;
+        mm[r] = set_mm_prob_d(qi, qd); gp[r] = 1.0 - ph2pr_d[qc]; mx[r] = ph2pr_d[qi]; my[r] = ph2pr_d[qd];
+        gg[r] = ph2pr_d[qc]; em[r] = 1.0 - ph2pr_d[qq]; ex[r] = ph2pr_d[qq] / 3.0;
+        rc[r] = base_code[(uint8_t)tc->rs[r - 1]];
+    }
+#define FM(r, c) F[((size_t)3 * (r)) * W + (c)]
+#define FX(r, c) F[((size_t)3 * (r) + 1) * W + (c)]
+#define FY(r, c) F[((size_t)3 * (r) + 2) * W + (c)]
+#define BM(r, c) B[((size_t)3 * (r)) * W + (c)]
+#define BX(r, c) B[((size_t)3 * (r) + 1) * W + (c)]
+#define BY(r, c) B[((size_t)3 * (r) + 2) * W + (c)]
+#define EM(r, c) (is_match(rc[r], hc[c]) ? em[r] : ex[r])
+    for (int c = 0; c <= H; c++) FY(0, c) = 1.0 / H;
+    for (int r = 1; r <= R; r++) {
+        double m = 0;
+        for (int c = 1; c <= H; c++) {
+            FM(r, c) = EM(r, c) * (mm[r] * FM(r - 1, c - 1) + gp[r] * (FX(r - 1, c - 1) + FY(r - 1, c - 1)));
+            FX(r, c) = mx[r] * FM(r - 1, c) + gg[r] * FX(r - 1, c);
+            FY(r, c) = my[r] * FM(r, c - 1) + gg[r] * FY(r, c - 1);
+            double v = FM(r, c) > FX(r, c) ? FM(r, c) : FX(r, c);
+            v = v > FY(r, c) ? v : FY(r, c);
+            m = m > v ? m : v;
+        }
+        if (m > 0) { int e2; frexp(m, &e2); double s = ldexp(1.0, -e2);
+            for (int c = 0; c <= H; c++) { FM(r, c) *= s; FX(r, c) *= s; FY(r, c) *= s; } }
+    }
+    for (int r = R; r >= 1; r--) {
+        double m = 0;
+        for (int c = H; c >= 1; c--) {
+            double nm = 0, bx = 0, by = 0, bm = 0;
+            if (r < R && c < H) nm = EM(r + 1, c + 1) * BM(r + 1, c + 1);
+            if (r < R) { bm += mm[r + 1] * nm + mx[r + 1] * BX(r + 1, c); bx += gp[r + 1] * nm + gg[r + 1] * BX(r + 1, c); }
+            else { bm += 1.0; bx += 1.0; }
+            by = (r < R ? gp[r + 1] * nm : 0.0) + (c < H ? gg[r] * BY(r, c + 1) : 0.0);
+            if (c < H) bm += my[r] * BY(r, c + 1);
+            BM(r, c) = bm; BX(r, c) = bx; BY(r, c) = by;
+            double v = bm > bx ? bm : bx; v = v > by ? v : by; m = m > v ? m : v;
+        }
+        if (m > 0 && r > 1) { int e2; frexp(m, &e2); double s = ldexp(1.0, -e2);
+            for (int c = 1; c <= H; c++) { BM(r, c) *= s; BX(r, c) *= s; BY(r, c) *= s; } }
+    }
+    int ok = 0;
+    const int dmin = 1 - R;
+    for (int d = 0; d < R + H - 1; d++) pstar[d] = 0;
+    for (int r = 1; r <= R; r++) {
+        double tot = 0;
+        for (int c = 1; c <= H; c++) tot += FM(r, c) * BM(r, c) + FX(r, c) * BX(r, c) + FY(r, c) * BY(r, c);
+        if (!(tot > 0)) continue;
+        ok = 1;
+        for (int c = 1; c <= H; c++) {
+            const double p = (FM(r, c) * BM(r, c) + FX(r, c) * BX(r, c) + FY(r, c) * BY(r, c)) / tot;
+            const int d = c - r - dmin;
+            if (p > pstar[d]) pstar[d] = p;
+        }
+    }
+#undef FM
+#undef FX
+#undef FY
+#undef BM
+#undef BX
+#undef BY
+#undef EM
+    free(F); free(B); free(mm); free(gp); free(mx); free(my); free(gg); free(em); free(ex); free(rc); free(hc);
+    return ok ? 0 : -1;
+}
+
+/*
+ * Banded DP as orc_band_log10, also returning the two edge statistics the
+ * banded kernel uses for its fallback decision:
+ *   row_ratio  max over rows r >= 8, r = 0 mod 4, of (A(r,0) + A(r,W-1)) / max_k A(r,k)
+ *              with A = M + X + Y (true, unscaled values)
+ *   end_frac   share of the last row's M + X on the band's two outer diagonals of each side
+ */
+/* leak_bound: sum over rows of the forward mass leaving the band (an
+ * insertion step off the left edge, a deletion step off the right edge) times
+ * the suffix's perfect-match probability prod_{r' > r} (1 - eps_r'), divided
+ * by the band likelihood -- an upper bound, up to the sum over suffix paths,
+ * on the relative mass the band loses. */
+static double g_leak_bound;
+static int g_r0 = 8; /* first row the edge ratio looks at */
+void orc_band_set_r0(int r0) { g_r0 = r0; }
+static double g_rho = 1.0; /* continuation discount per 11 bases (k-mer exclusion); 1 = none */
+void orc_band_set_rho(double rho) { g_rho = rho; }
+double orc_band_leak_bound(void) { return g_leak_bound; }
+
+double orc_band_detail(const orc_testcase *tc, int d_lo, int W, double *row_ratio, double *end_frac) {
+    orc_init();
+    const int R = tc->rslen, H = tc->haplen;
+    *row_ratio = 0; *end_frac = 0;
+    if (R == 0 || H == 0 || W <= 0) return -INFINITY;
+    double *buf = (double *)calloc((size_t)6 * W, sizeof(double));
+    double *Mp = buf, *Xp = buf + W, *Yp = buf + 2 * W, *Mc = buf + 3 * W, *Xc = buf + 4 * W, *Yc = buf + 5 * W;
+    for (int k = 0; k < W; k++) { const int c = d_lo + k; Yp[k] = (c >= 0 && c <= H) ? 1.0 / (double)H : 0.0; }
+    long long e2sum = 0;
+    double rr = 0;
+    double leak_sum = 0, pre = 1;  /* sum leak(r) * 2^e2sum(r) / prod_{r' <= r}(1-eps), in row-scaled units */
+    for (int r = 1; r <= R; r++) {
+        const int qi = tc->i[r - 1] & 127, qd = tc->d[r - 1] & 127, qc = tc->c[r - 1] & 127, qq = tc->q[r - 1] & 127;
+        const double pMM = set_mm_prob_d(qi, qd), gp = 1.0 - ph2pr_d[qc];
+        const double pMX = ph2pr_d[qi], pMY = ph2pr_d[qd], g = ph2pr_d[qc];
+        const double eps = ph2pr_d[qq], one_m = 1.0 - eps, mis = eps / 3.0;
+        const uint8_t rc = base_code[(uint8_t)tc->rs[r - 1]];
+        /* mass of row r-1 leaving through the left edge into row r's X */
+        const double leak_l = pMX * Mp[0] + g * Xp[0];
+        pre *= one_m;
+        double mx = 0;
+        for (int k = 0; k < W; k++) {
+            const int c = r + d_lo + k;
+            if (c < 1 || c > H) { Mc[k] = Xc[k] = Yc[k] = 0; continue; }
+            const double e = is_match(rc, base_code[(uint8_t)tc->hap[c - 1]]) ? one_m : mis;
+            Mc[k] = e * (pMM * Mp[k] + gp * Xp[k] + gp * Yp[k]);
+            Xc[k] = (k + 1 < W) ? pMX * Mp[k + 1] + g * Xp[k + 1] : 0.0;
+            Yc[k] = (k > 0) ? pMY * Mc[k - 1] + g * Yc[k - 1] : 0.0;
+            double m = Mc[k] > Xc[k] ? Mc[k] : Xc[k]; m = m > Yc[k] ? m : Yc[k]; mx = mx > m ? mx : m;
+        }
+        /* mass of row r leaving through the right edge into Y */
+        const double leak_r = pMY * Mc[W - 1] + g * Yc[W - 1];
+        leak_sum += (leak_l + leak_r) * ldexp(1.0, (int)e2sum) / pre * pow(g_rho, (double)((R - r) / 11));
+        if (r >= g_r0 && (r & 3) == 0) {
+            double peak = 0;
+            for (int k = 0; k < W; k++) { const double a = Mc[k] + Xc[k] + Yc[k]; peak = peak > a ? peak : a; }
+            const double edge = Mc[0] + Xc[0] + Yc[0] + Mc[W - 1] + Xc[W - 1] + Yc[W - 1];
+            if (edge > 0) { const double q = peak > 0 ? edge / peak : 1e300; rr = rr > q ? rr : q; }
+        }
+        if (mx > 0) { int e2; frexp(mx, &e2); const double s = ldexp(1.0, -e2);
+            for (int k = 0; k < W; k++) { Mc[k] *= s; Xc[k] *= s; Yc[k] *= s; } e2sum += e2; }
+        double *t; t = Mp; Mp = Mc; Mc = t; t = Xp; Xp = Xc; Xc = t; t = Yp; Yp = Yc; Yc = t;
+    }
+    double s = 0, outer = 0;
+    for (int k = 0; k < W; k++) {
+        const int c = R + d_lo + k;
+        if (c >= 1 && c <= H) { s += Mp[k] + Xp[k]; if (k < 2 || k >= W - 2) outer += Mp[k] + Xp[k]; }
+    }
+    free(buf);
+    *row_ratio = rr;
+    *end_frac = s > 0 ? outer / s : 1.0;
+    g_leak_bound = s > 0 ? leak_sum * pre / (s * ldexp(1.0, (int)e2sum)) : 1e300;
+    if (!(s > 0)) return -INFINITY;
+    return log10(s) + (double)e2sum * log10(2.0);
+}
+
+/*
+ * Posterior mass on the band's two edge diagonals, from a banded
+ * forward-backward pass (FP64, rows renormalised in both passes):
+ *   edge = sum_r [ A_F(r,0) Bmax(r,0) + A_F(r,W-1) Bmax(r,W-1) ] / L_band
+ * with A_F = M + X + Y forward and Bmax = max(B_M, B_X, B_Y) backward at the
+ * cell (an upper bound on sum_s F_s B_s there).  Backward, band coordinates:
+ *   B_M(r,k) = mm(r+1) e(r+1,k) B_M(r+1,k) + mx(r+1) B_X(r+1,k-1) + my(r) B_Y(r,k+1) + [r==R]
+ *   B_X(r,k) = gp(r+1) e(r+1,k) B_M(r+1,k) + g(r+1) B_X(r+1,k-1) + [r==R]
+ *   B_Y(r,k) = gp(r+1) e(r+1,k) B_M(r+1,k) + g(r) B_Y(r,k+1)
+ * out-of-band or out-of-matrix successors contributing zero.
+ */
+double orc_band_posterior_edge(const orc_testcase *tc, int d_lo, int W) {
+    orc_init();
+    const int R = tc->rslen, H = tc->haplen;
+    if (R == 0 || H == 0 || W <= 0) return 1.0;
+    double *Af0 = calloc((size_t)R + 2, sizeof(double)), *Af1 = calloc((size_t)R + 2, sizeof(double));
+    double *fs = calloc((size_t)R + 2, sizeof(double));  /* log2 scale of forward row r */
+    double *mm = malloc(sizeof(double) * (R + 2)), *gp = malloc(sizeof(double) * (R + 2));
+    double *mxp = malloc(sizeof(double) * (R + 2)), *myp = malloc(sizeof(double) * (R + 2));
+    double *gg = malloc(sizeof(double) * (R + 2)), *em = malloc(sizeof(double) * (R + 2)), *ex = malloc(sizeof(double) * (R + 2));
+    uint8_t *rc = malloc((size_t)R + 2);
+    for (int r = 1; r <= R; r++) {
+        const int qi = tc->i[r - 1] & 127, qd = tc->d[r - 1] & 127, qc = tc->c[r - 1] & 127, qq = tc->q[r - 1] & 127;
+        mm[r] = set_mm_prob_d(qi, qd); gp[r] = 1.0 - ph2pr_d[qc]; mxp[r] = ph2pr_d[qi]; myp[r] = ph2pr_d[qd];
+        gg[r] = ph2pr_d[qc]; em[r] = 1.0 - ph2pr_d[qq]; ex[r] = ph2pr_d[qq] / 3.0; rc[r] = base_code[(uint8_t)tc->rs[r - 1]];
+    }
+#define EMIS(r, k) ((r + d_lo + (k) >= 1 && r + d_lo + (k) <= H) ? (is_match(rc[r], base_code[(uint8_t)tc->hap[r + d_lo + (k) - 1]]) ? em[r] : ex[r]) : 0.0)
+    double *buf = calloc((size_t)6 * W, sizeof(double));
+    double *Mp = buf, *Xp = buf + W, *Yp = buf + 2 * W, *Mc = buf + 3 * W, *Xc = buf + 4 * W, *Yc = buf + 5 * W;
+    for (int k = 0; k < W; k++) { const int c = d_lo + k; Yp[k] = (c >= 0 && c <= H) ? 1.0 / (double)H : 0.0; }
+    double lsc = 0;
+    for (int r = 1; r <= R; r++) {
+        double m = 0;
+        for (int k = 0; k < W; k++) {
+            const int c = r + d_lo + k;
+            if (c < 1 || c > H) { Mc[k] = Xc[k] = Yc[k] = 0; continue; }
+            Mc[k] = EMIS(r, k) * (mm[r] * Mp[k] + gp[r] * (Xp[k] + Yp[k]));
+            Xc[k] = (k + 1 < W) ? mxp[r] * Mp[k + 1] + gg[r] * Xp[k + 1] : 0.0;
+            Yc[k] = (k > 0) ? myp[r] * Mc[k - 1] + gg[r] * Yc[k - 1] : 0.0;
+            const double v = Mc[k] + Xc[k] + Yc[k]; m = m > v ? m : v;
+        }
+        Af0[r] = Mc[0] + Xc[0] + Yc[0]; Af1[r] = Mc[W - 1] + Xc[W - 1] + Yc[W - 1]; fs[r] = lsc;
+        if (m > 0) { int e2; frexp(m, &e2); const double s = ldexp(1.0, -e2);
+            for (int k = 0; k < W; k++) { Mc[k] *= s; Xc[k] *= s; Yc[k] *= s; } lsc += e2; }
+        double *t; t = Mp; Mp = Mc; Mc = t; t = Xp; Xp = Xc; Xc = t; t = Yp; Yp = Yc; Yc = t;
+    }
+    double L = 0;
+    for (int k = 0; k < W; k++) { const int c = R + d_lo + k; if (c >= 1 && c <= H) L += Mp[k] + Xp[k]; }
+    const double lscL = lsc;  /* L_true = L * 2^lscL; A_F(r) true = Af(r) * 2^fs[r] */
+    /* backward */
+    double *BM = calloc(W, sizeof(double)), *BX = calloc(W, sizeof(double)), *BY = calloc(W, sizeof(double));
+    double bls = 0, edge = 0;
+    for (int r = R; r >= 1; r--) {
+        double nBM[256], nBX[256], nBY[256];
+        for (int k = W - 1; k >= 0; k--) {
+            const int c = r + d_lo + k;
+            if (c < 1 || c > H) { nBM[k] = nBX[k] = nBY[k] = 0; continue; }
+            double tM = 0, tX = 0, tY = 0;
+            if (r < R) {
+                const double em1 = (c + 1 <= H) ? EMIS(r + 1, k) * BM[k] : 0.0;
+                const double bxk = (k - 1 >= 0) ? BX[k - 1] : 0.0;
+                tM = mm[r + 1] * em1 + mxp[r + 1] * bxk;
+                tX = gp[r + 1] * em1 + gg[r + 1] * bxk;
+                tY = gp[r + 1] * em1;
+            } else { tM = 1.0 * ldexp(1.0, -(int)bls); tX = tM; tY = 0; }
+            const double byk1 = (k + 1 < W && c + 1 <= H) ? nBY[k + 1] : 0.0;
+            nBM[k] = tM + myp[r] * byk1;
+            nBX[k] = tX;
+            nBY[k] = tY + gg[r] * byk1;
+        }
+        double m = 0;
+        for (int k = 0; k < W; k++) { BM[k] = nBM[k]; BX[k] = nBX[k]; BY[k] = nBY[k];
+            const double v = BM[k] > BX[k] ? BM[k] : BX[k]; m = m > v ? m : v; }
+        /* posterior bound at the edges: A_F(r) * Bmax(r) / L  (all in true units) */
+        const double b0 = fmax(BM[0], fmax(BX[0], BY[0])), b1 = fmax(BM[W - 1], fmax(BX[W - 1], BY[W - 1]));
+        edge += (Af0[r] * b0 + Af1[r] * b1) * ldexp(1.0, (int)(fs[r] + bls - lscL));
+        if (m > 0) { int e2; frexp(m, &e2); const double s = ldexp(1.0, -e2);
+            for (int k = 0; k < W; k++) { BM[k] *= s; BX[k] *= s; BY[k] *= s; } bls += e2; }
+    }
+#undef EMIS
+    free(BM); free(BX); free(BY); free(buf); free(Af0); free(Af1); free(fs);
+    free(mm); free(gp); free(mxp); free(myp); free(gg); free(em); free(ex); free(rc);
+    return L > 0 ? edge / L : 1.0;
+}

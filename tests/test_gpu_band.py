@@ -1,0 +1,96 @@
+"""The banded path on the GPU.
+
+* With a fixed band around the 11-mer seed diagonal, every banded pair's
+  result equals the oracle's banded DP on the same band (FP32 tolerance).
+* Routed-out and fallback pairs equal the full DP.
+* The audit compares banded against full results on a sample.
+"""
+import numpy as np
+import pytest
+
+from biovoltron_b200 import workloads as W
+from oracle.oracle import TestcaseArray, seed_diagonal, seed_extent
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP32 = 1e-4
+TOL_CONTRACT = 1e-3
+
+
+def _band_engine(**kw):
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    e = PairHMMEngine(device=0)
+    e.set_band_options(**kw)
+    return e
+
+
+def test_fixed_band_matches_oracle_band(oracle):
+    b = W.config1(seed=31, n_regions=6)
+    half, margin = 6, 1
+    with _band_engine(fixed_half=half, margin=margin, edge_threshold=1e30) as e:
+        got, st = e.compute_regions(b, with_stats=True)
+    assert st["band_pairs"] > 0.8 * b.n_pairs
+    r, h = b.pair_index()
+    tcs = TestcaseArray.for_batch(b)
+    d_lo, wcls, sel = [], [], []
+    for k in range(len(r)):
+        rd, hp = b.read(int(r[k]))[0], b.hap(int(h[k]))
+        ds = seed_diagonal(rd, hp)
+        if ds is None or b.read_lengths()[r[k]] > 511:
+            continue
+        km, kx = seed_extent(rd, hp)
+        blo, bhi = min(ds - half - margin, km), max(ds + half + margin, kx)
+        width = bhi - blo + 1
+        if width > 32:
+            continue
+        W_cls = 16 if width <= 16 else 32
+        d_lo.append(blo - (W_cls - width) // 2)
+        wcls.append(W_cls)
+        sel.append(k)
+    sel = np.array(sel)
+    sub = TestcaseArray(b, r[sel], h[sel])
+    exp = oracle.band_log10(sub, np.array(d_lo), np.array(wcls))
+    fin = np.isfinite(exp) & (exp > -60)
+    assert np.max(np.abs(got[sel][fin] - exp[fin])) <= TOL_FP32
+
+
+def test_fixed_band_audit_reports_banded_error(oracle):
+    # The fixed band is the ablation of the learned band: it may leave the
+    # contract on pairs whose alignment spreads beyond it.  The audit must
+    # see exactly the banded-vs-full differences of its sampled pairs.
+    b = W.config1(seed=32, n_regions=8)
+    period = 7
+    with _band_engine(fixed_half=8, margin=2, edge_threshold=1e-3, audit_period=period) as e:
+        got, st = e.compute_regions(b, with_stats=True)
+    truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
+    assert np.all(np.isfinite(got))
+    err = np.abs(got - truth)
+    sampled = err[::period]
+    assert st["audit_pairs"] > 0
+    assert st["audit_max_err"] <= sampled.max() + 1e-4
+    assert st["band_pairs"] + st["band_routed_full"] == b.n_pairs
+
+
+def test_band_mode_edge_cases_equal_full(engine):
+    # no shared 11-mer, short reads and long reads all go to the full DP
+    from conftest import load_golden
+    for name in ("edge_cases", "long_pairs", "config0"):
+        b, exp = load_golden(name)
+        full = engine.compute_regions(b)
+        with _band_engine(fixed_half=8, margin=2) as e:
+            got, st = e.compute_regions(b, with_stats=True)
+        truth = exp["oracle_rescaled"]
+        fin = np.isfinite(truth)
+        assert np.all(np.isneginf(got[~fin]))
+        assert np.max(np.abs(got[fin] - truth[fin])) <= TOL_CONTRACT
+
+
+def test_band_staged_replay_is_deterministic():
+    b = W.config1(seed=33, n_regions=10)
+    with _band_engine(fixed_half=8, margin=2, audit_period=5) as e:
+        direct = e.compute_regions(b)
+        n = e.stage(b)
+        for _ in range(3):
+            st = e.run()
+            assert st["band_pairs"] > 0
+            assert np.array_equal(e.fetch(n), direct)

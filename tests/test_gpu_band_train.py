@@ -1,0 +1,121 @@
+"""Band MLP training on the GPU: labels against the oracle's posterior,
+the training objective against its CPU restatement, weight I/O, and the
+learned band against the full DP (with the fixed band as the ablation)."""
+import numpy as np
+import pytest
+
+from biovoltron_b200 import workloads as W
+from oracle import band_mlp as M
+from oracle.oracle import TestcaseArray, seed_diagonal
+
+pytestmark = pytest.mark.gpu
+
+TOL_CONTRACT = 1e-3
+
+
+def _engine():
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    return PairHMMEngine(device=0)
+
+
+@pytest.fixture(scope="module")
+def trained(tmp_path_factory):
+    """Weights trained once on a config-1-shaped batch of its own seed."""
+    path = str(tmp_path_factory.mktemp("band") / "band.bvw")
+    train = W.config1(seed=200, n_regions=24)
+    with _engine() as e:
+        rep = e.band_train(train, epochs=6, seed=7)
+        e.band_save(path)
+    print("train report", rep)
+    return path, rep
+
+
+def test_labels_match_oracle_posterior(oracle):
+    b = W.config1(seed=41, n_regions=2)
+    tau = 1e-4
+    with _engine() as e:
+        ds, lo, hi, feat = e.band_labels(b, tau=tau, features=True)
+    assert feat.shape == (b.n_pairs, 80) and np.all(np.isfinite(feat))
+    r, h = b.pair_index()
+    rng = np.random.default_rng(0)
+    picks = rng.choice(b.n_pairs, 40, replace=False)
+    tcs = TestcaseArray(b, r[picks], h[picks])
+    checked = 0
+    for j, k in enumerate(picks):
+        rd, hp = b.read(int(r[k]))[0], b.hap(int(h[k]))
+        exp_ds = seed_diagonal(rd, hp)
+        assert ds[k] == (np.iinfo(np.int32).min if exp_ds is None else exp_ds), k
+        dmin, pstar = oracle.posterior_diag(tcs, j)
+        assert pstar is not None
+        d = np.arange(len(pstar)) + dmin
+        strict, loose = d[pstar >= tau * 1.05], d[pstar >= tau * 0.95]
+        assert loose.min() <= lo[k] <= strict.min(), (k, lo[k], loose.min(), strict.min())
+        assert strict.max() <= hi[k] <= loose.max(), (k, hi[k], strict.max(), loose.max())
+        checked += 1
+    assert checked == 40
+
+
+def test_objective_matches_cpu_restatement():
+    rng = np.random.default_rng(5)
+    n = 48
+    w = M.init_weights(11, out_scale=1.0)
+    x = rng.uniform(0, 1, (n, M.FEAT)).astype(np.float32)
+    t = rng.normal(0, 4, (n, 2)).astype(np.float32)
+    with _engine() as e:
+        out, loss, g = e.band_mlp_eval(w, x, t, alpha=8.0)
+    eo, el, eg = M.objective(w.astype(np.float64), x, t, 8.0, rounding=True)
+    assert np.max(np.abs(out - eo)) <= 1e-3 * max(1.0, np.max(np.abs(eo)))
+    assert abs(loss - el) <= 1e-3 * el
+    assert np.linalg.norm(g - eg) <= 2e-3 * np.linalg.norm(eg)
+
+
+def test_training_reduces_loss_and_covers_labels(trained):
+    _, rep = trained
+    assert rep["labelled"] >= 0.9 * rep["pairs"]
+    assert rep["last_loss"] < 0.5 * rep["first_loss"]
+    assert rep["band_frac"] >= 0.8 and rep["cover_frac"] >= 0.98, rep
+
+
+def test_weights_roundtrip(trained, tmp_path):
+    path, _ = trained
+    with _engine() as e:
+        with pytest.raises(RuntimeError):
+            e.band_weights()  # nothing installed yet
+        e.band_load(path)
+        w = e.band_weights()
+        assert w.size == M.N_PARAMS and np.all(np.isfinite(w))
+        e.set_band_weights(w * 0.5)
+        assert np.array_equal(e.band_weights(), (w * 0.5).astype(np.float32))
+        p2 = str(tmp_path / "w2.bvw")
+        e.band_save(p2)
+        e.band_load(path)
+        assert np.array_equal(e.band_weights(), w)
+        e.band_load(p2)
+        assert np.array_equal(e.band_weights(), (w * 0.5).astype(np.float32))
+        bad = tmp_path / "bad.bvw"
+        bad.write_bytes(b"not a weight file")
+        with pytest.raises(RuntimeError):
+            e.band_load(str(bad))
+
+
+def test_learned_band_within_contract_and_ablation(trained, oracle):
+    path, _ = trained
+    b = W.config1(seed=32, n_regions=8)
+    truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
+    res = {}
+    for use_mlp in (True, False):
+        with _engine() as e:
+            if use_mlp:
+                e.band_load(path)
+            e.set_band_options(use_mlp=use_mlp, fixed_half=8, margin=2, edge_threshold=1e-3, audit_period=5)
+            got, st = e.compute_regions(b, with_stats=True)
+        res[use_mlp] = (float(np.max(np.abs(got - truth))), st)
+    err_mlp, st_mlp = res[True]
+    err_fixed, st_fixed = res[False]
+    print("learned", err_mlp, st_mlp)
+    print("fixed", err_fixed, st_fixed)
+    assert err_mlp <= TOL_CONTRACT, st_mlp
+    assert st_mlp["audit_max_err"] <= TOL_CONTRACT
+    assert st_mlp["band_pairs"] >= 0.7 * b.n_pairs
+    # ablation: the fixed band of the same budget does worse on error or coverage
+    assert err_fixed > err_mlp or st_fixed["band_pairs"] < st_mlp["band_pairs"]
