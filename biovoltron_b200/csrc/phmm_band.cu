@@ -34,6 +34,7 @@ __device__ __forceinline__ int kmer_code(uint8_t b) {
 __device__ __forceinline__ uint32_t onehot(uint8_t b) {
   return b == 'C' ? 2u : b == 'T' ? 4u : b == 'G' ? 8u : b == 'N' ? 15u : 1u;
 }
+__device__ __forceinline__ bool bases_match(uint8_t a, uint8_t b) { return (onehot(a) & onehot(b)) != 0u; }
 
 __global__ void k_pairs_from_units(const Unit* __restrict__ units, long long n_units, int32_t* pair_read,
                                    int32_t* pair_hap) {
@@ -121,10 +122,19 @@ __global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n
 // shared memory; every read 11-mer is binary-searched there and each shared
 // occurrence votes for diagonal d = j - i in a per-warp histogram.  d* is the
 // most voted diagonal (smallest on ties); the features are the 64 bins
-// d* - 32 .. d* + 31 and a few scalars, all divided by the number of read
-// 11-mers; kmin/kmax are the extreme voted diagonals.
+// d* - 32 .. d* + 31 divided by the number of read 11-mers, and 16 scalars:
+// vote totals, lengths, d*'s position, the uncovered read ends (t_pre, t_suf),
+// the diagonals of the first and last hit relative to d*, the mismatches of
+// the first and last 16 read bases along those diagonals, and the voted
+// extent relative to d*.  kmin/kmax are the extreme voted diagonals widened
+// by the read ends' triangles: an insertion run in a read end moves the
+// alignment one diagonal per row, so below a diagonal whose last hit leaves
+// t read bases uncovered (t <= kEndRows, or any t for the read's last hit)
+// the band reaches t diagonals down, and likewise up from a diagonal whose
+// first hit starts h bases into the read.
 constexpr int kFeatWarps = 4;
 constexpr int kHitCap = 512;
+constexpr int kEndRows = 24;  // horizon of the per-diagonal end triangles
 
 __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -134,6 +144,9 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
   int* hits = reinterpret_cast<int*>(smem + (size_t)kFeatWarps * kBandMaxHap * 8) + (size_t)kFeatWarps * kBandMaxSpan +
               (size_t)wib * (kHitCap + 1);
   int* nhit = hits + kHitCap;
+  // per voted diagonal: first (high 16 bits) and last (low 16 bits) read position
+  int* pos = reinterpret_cast<int*>(smem + (size_t)kFeatWarps * kBandMaxHap * 8) + (size_t)kFeatWarps * kBandMaxSpan +
+             (size_t)kFeatWarps * (kHitCap + 1) + (size_t)wib * kBandMaxSpan;
   for (int x = lane; x < kBandMaxSpan; x += 32) hist[x] = 0;
   const long long nwarps = (long long)gridDim.x * kFeatWarps;
   int staged_hap = -1;
@@ -157,6 +170,8 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
     __syncwarp();
     const uint32_t* rcode = p.read_kmers + ro;
     const int nk_read = R - kK + 1;
+    // first and last read position with a shared 11-mer, with that hit's slot
+    int first_i = INT32_MAX, first_s = 0, last_i = -1, last_s = 0;
     for (int i0 = 0; i0 < nk_read; i0 += 32) {
       const int i = i0 + lane;
       const uint32_t code = i < nk_read ? rcode[i] : kNoCode;
@@ -182,15 +197,24 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
         const unsigned active = __ballot_sync(0xffffffffu, slot >= 0);
         if (active == 0u) break;
         if (slot >= 0) {
+          if (i < first_i) { first_i = i; first_s = slot; }
+          if (i > last_i) { last_i = i; last_s = slot; }
           const unsigned peers = __match_any_sync(active, slot);
           if ((__ffs(peers) - 1) == lane) {
+            // peers share the slot; their read positions are i0 + (lanes of peers)
+            const int i_hi = i0 + 31 - __clz(peers);
             if (atomicAdd(&hist[slot], __popc(peers)) == 0) {
+              pos[slot] = (i << 16) | i_hi;
               const int q = atomicAdd(nhit, 1);
               if (q < kHitCap) hits[q] = slot;
+            } else {  // repeats can revisit a slot out of order within a chunk
+              const int ps = pos[slot];
+              pos[slot] = (min(ps >> 16, i) << 16) | max(ps & 0xffff, i_hi);
             }
           }
           ++m;
         }
+        __syncwarp();
       }
     }
     __syncwarp();
@@ -208,10 +232,52 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
       smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
       smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
     }
+    for (int o = 16; o > 0; o >>= 1) {
+      const int fi = __shfl_xor_sync(0xffffffffu, first_i, o), fs = __shfl_xor_sync(0xffffffffu, first_s, o);
+      const int li = __shfl_xor_sync(0xffffffffu, last_i, o), ls = __shfl_xor_sync(0xffffffffu, last_s, o);
+      if (fi < first_i || (fi == first_i && fs < first_s)) { first_i = fi; first_s = fs; }
+      if (li > last_i || (li == last_i && ls < last_s)) { last_i = li; last_s = ls; }
+    }
+    // read ends not covered by a shared 11-mer: t_pre bases before the first
+    // hit, t_suf after the last.  An insertion run in a read end moves the
+    // alignment one diagonal per row, so the end rows may sit up to t_pre
+    // diagonals above the first hit's diagonal and t_suf below the last one.
+    const int t_pre = last_i >= 0 ? first_i : 0, t_suf = last_i >= 0 ? R - kK - last_i : 0;
+    const int d_first = first_s - R, d_last = last_s - R;
+    // mismatches of the first / last 16 read bases along those diagonals
+    int mis_pre = 0, mis_suf = 0;
+    if (last_i >= 0) {
+      const int nb = min(16, R);
+      const uint8_t* rb = p.batch.read_bases + ro;
+      const uint8_t* hb = p.batch.hap_bases + ho;
+      bool mp = false, ms = false;
+      if (lane < nb) {
+        const int ip = lane, jp = ip + d_first;
+        const int is = R - 1 - lane, js = is + d_last;
+        mp = jp < 0 || jp >= H || !bases_match(rb[ip], hb[jp]);
+        ms = js < 0 || js >= H || !bases_match(rb[is], hb[js]);
+      }
+      mis_pre = __popc(__ballot_sync(0xffffffffu, mp));
+      mis_suf = __popc(__ballot_sync(0xffffffffu, ms));
+    }
+    // end triangles of every voted diagonal whose hits come within kEndRows
+    // rows of a read end
+    int tri_lo = d_last - t_suf, tri_hi = d_first + t_pre;
+    for (int x = lane; x < nh; x += 32) {
+      const int s = hits[x], ps = pos[s], d = s - R;
+      const int tail = R - kK - (ps & 0xffff), head = ps >> 16;
+      if (tail <= kEndRows) tri_lo = min(tri_lo, d - tail);
+      if (head <= kEndRows) tri_hi = max(tri_hi, d + head);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      tri_lo = min(tri_lo, __shfl_xor_sync(0xffffffffu, tri_lo, o));
+      tri_hi = max(tri_hi, __shfl_xor_sync(0xffffffffu, tri_hi, o));
+    }
     if (lane == 0) {
-      // extent of the shared 11-mer diagonals (a hit list overflow widens it to everything)
-      p.kmin[pi] = overflow ? INT32_MIN : smin - R;
-      p.kmax[pi] = overflow ? INT32_MAX : smax - R;
+      // extent of the shared 11-mer diagonals and the end triangles (a hit
+      // list overflow widens it to everything)
+      p.kmin[pi] = overflow ? INT32_MIN : min(smin - R, tri_lo);
+      p.kmax[pi] = overflow ? INT32_MAX : max(smax - R, tri_hi);
     }
     for (int o = 16; o > 0; o >>= 1) {
       const int oc = __shfl_xor_sync(0xffffffffu, best_cnt, o), os = __shfl_xor_sync(0xffffffffu, best_slot, o);
@@ -256,6 +322,14 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
           case 5: v = 1.f; break;
           case 6: v = (float)peak * inv; break;
           case 7: v = (float)nonzero / (float)kHistBins; break;
+          case 8: v = (float)t_pre / 32.f; break;
+          case 9: v = (float)t_suf / 32.f; break;
+          case 10: v = (float)(d_first - ds) / 32.f; break;
+          case 11: v = (float)(d_last - ds) / 32.f; break;
+          case 12: v = (float)mis_pre / 16.f; break;
+          case 13: v = (float)mis_suf / 16.f; break;
+          case 14: v = overflow ? -2.f : fmaxf((float)(smin - R - ds) / 32.f, -2.f); break;
+          case 15: v = overflow ? 2.f : fminf((float)(smax - R - ds) / 32.f, 2.f); break;
           default: v = 0.f;
         }
         f[kHistBins + lane] = __float2bfloat16(v);
@@ -777,7 +851,8 @@ cudaError_t launch_hap_kmers(const uint8_t* hap_bases, const int64_t* hap_off, l
   return cudaGetLastError();
 }
 
-constexpr int kFeatSmem = kFeatWarps * kBandMaxHap * 8 + kFeatWarps * kBandMaxSpan * 4 + kFeatWarps * (kHitCap + 1) * 4;
+constexpr int kFeatSmem =
+    kFeatWarps * kBandMaxHap * 8 + 2 * kFeatWarps * kBandMaxSpan * 4 + kFeatWarps * (kHitCap + 1) * 4;
 
 cudaError_t prepare_band_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_featurize, cudaFuncAttributeMaxDynamicSharedMemorySize, kFeatSmem);
@@ -788,7 +863,7 @@ cudaError_t prepare_band_kernels() {
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
   if (p.n_pairs <= 0) return cudaSuccess;
   const int smem = kFeatSmem;
-  const long long blocks = std::min<long long>((p.n_pairs + kFeatWarps - 1) / kFeatWarps, (long long)sms * 3);
+  const long long blocks = std::min<long long>((p.n_pairs + kFeatWarps - 1) / kFeatWarps, (long long)sms * 2);
   k_featurize<<<(int)blocks, kFeatWarps * 32, smem, st>>>(p);
   return cudaGetLastError();
 }

@@ -248,10 +248,10 @@ void bv_phmm_default_band_train_options(bv_band_train_options* o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
   o->struct_size = (int32_t)sizeof(*o);
-  o->epochs = 8;
+  o->epochs = 20;
   o->batch = 1024;
   o->lr = 2e-3f;
-  o->alpha = 8.f;
+  o->alpha = 16.f;
   o->tau = 1e-4f;
   o->clip = 20.f;
   o->margin = 2;
@@ -270,9 +270,14 @@ bv_status bv_phmm_band_train(bv_phmm_ctx* ctx, const bv_region_batch* train, con
 }
 
 bv_status bv_phmm_band_labels(bv_phmm_ctx* ctx, const bv_region_batch* batch, float tau, int32_t* dstar, int32_t* lo,
-                              int32_t* hi, float* features) {
+                              int32_t* hi, float* features, int32_t* kmin, int32_t* kmax) {
   if (!ctx || !batch || !dstar || !lo || !hi) return BV_ERR_INVALID_ARG;
-  return guard(ctx, [&] { return ctx->engine.band_labels(*batch, tau, dstar, lo, hi, features); });
+  return guard(ctx, [&] { return ctx->engine.band_labels(*batch, tau, dstar, lo, hi, features, kmin, kmax); });
+}
+
+bv_status bv_phmm_band_routes(bv_phmm_ctx* ctx, int64_t n, int32_t* d_lo, int32_t* width, int32_t* route) {
+  if (!ctx || !d_lo || !width || !route || n < 0) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.band_routes(n, d_lo, width, route); });
 }
 
 int64_t bv_phmm_band_param_count(void) { return bvphmm::kMlpParamCount; }

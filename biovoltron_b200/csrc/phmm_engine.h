@@ -64,7 +64,9 @@ class Engine {
   bv_status set_band_options(const bv_band_options& o);
   bool band_enabled() const { return band_opt_.enabled != 0; }
   bv_status band_train(const bv_region_batch& b, const bv_band_train_options& o, bv_band_train_report* rep);
-  bv_status band_labels(const bv_region_batch& b, float tau, int32_t* dstar, int32_t* lo, int32_t* hi, float* feat);
+  bv_status band_labels(const bv_region_batch& b, float tau, int32_t* dstar, int32_t* lo, int32_t* hi, float* feat,
+                        int32_t* kmin, int32_t* kmax);
+  bv_status band_routes(int64_t n, int32_t* d_lo, int32_t* width, int32_t* route);
   bv_status band_get_weights(float* w, int64_t n);
   bv_status band_set_weights(const float* w, int64_t n);
   bv_status band_save(const char* path);

@@ -200,4 +200,44 @@ bv_status Engine::band_stats(bv_phmm_stats* st) {
   return BV_OK;
 }
 
+bv_status Engine::band_routes(int64_t n, int32_t* d_lo, int32_t* width, int32_t* route) {
+  if (!band_enabled() || !staged_) return fail(BV_ERR_INVALID_ARG, "no band-mode batch has run");
+  if (n != n_results_) return fail(BV_ERR_INVALID_ARG, "result count");
+  BandCounters bc{};
+  Counters cc{};
+  BV_CUDA(cudaMemcpy(&bc, d_bctr_.get(), sizeof(bc), cudaMemcpyDeviceToHost), "band counters");
+  BV_CUDA(cudaMemcpy(&cc, d_counters_.get(), sizeof(cc), cudaMemcpyDeviceToHost), "counters");
+  std::fill(d_lo, d_lo + n, 0);
+  std::fill(width, width + n, 0);
+  std::fill(route, route + n, 1);
+  for (int c = 0; c < kBandWidths; ++c) {
+    unsigned long long cnt = 0;
+    for (int b = 0; b < kRBuckets; ++b) cnt += bc.band_count[c][b];
+    cnt = std::min<unsigned long long>(cnt, (unsigned long long)item_cap_);
+    std::vector<BandItem> it(cnt);
+    if (cnt) BV_CUDA(cudaMemcpy(it.data(), d_band_items_.as<BandItem>() + (size_t)c * item_cap_, sizeof(BandItem) * cnt,
+                                cudaMemcpyDeviceToHost), "band items");
+    for (const auto& x : it) {
+      if (x.out < 0 || x.out >= n) continue;
+      d_lo[x.out] = x.d_lo;
+      width[x.out] = band_width(c);
+      route[x.out] = 0;
+    }
+  }
+  for (int v = 0; v < 9; ++v) {
+    const unsigned long long cnt = std::min<unsigned long long>(bc.full_count[v], (unsigned long long)full_cap_);
+    std::vector<Unit> u(cnt);
+    if (cnt) BV_CUDA(cudaMemcpy(u.data(), d_full_items_.as<Unit>() + (size_t)v * full_cap_, sizeof(Unit) * cnt,
+                                cudaMemcpyDeviceToHost), "fallback units");
+    for (const auto& x : u)
+      if (x.out0 >= 0 && x.out0 < n && route[x.out0] == 0) route[x.out0] = 2;
+  }
+  const unsigned long long nr = std::min<unsigned long long>(cc.rescue_count, (unsigned long long)std::max<int64_t>(n_results_, 1));
+  std::vector<PairRef> rl(nr);
+  if (nr) BV_CUDA(cudaMemcpy(rl.data(), d_rescue_.get(), sizeof(PairRef) * nr, cudaMemcpyDeviceToHost), "rescue list");
+  for (const auto& x : rl)
+    if (x.out >= 0 && x.out < n && route[x.out] == 0) route[x.out] = 3;
+  return BV_OK;
+}
+
 }  // namespace bvphmm

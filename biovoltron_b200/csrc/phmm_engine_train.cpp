@@ -120,7 +120,7 @@ bv_status Engine::compute_labels(const bv_region_batch& b, float tau, float* ms)
 }
 
 bv_status Engine::band_labels(const bv_region_batch& b, float tau, int32_t* dstar, int32_t* lo, int32_t* hi,
-                              float* feat) {
+                              float* feat, int32_t* kmin, int32_t* kmax) {
   bv_status s = stage_for_labels(b);
   if (s != BV_OK) return s;
   s = compute_labels(b, tau, nullptr);
@@ -130,6 +130,8 @@ bv_status Engine::band_labels(const bv_region_batch& b, float tau, int32_t* dsta
   BV_CUDA(cudaMemcpy(dstar, d_dstar_.get(), n * 4, cudaMemcpyDeviceToHost), "D2H");
   BV_CUDA(cudaMemcpy(lo, d_lab_lo_.get(), n * 4, cudaMemcpyDeviceToHost), "D2H");
   BV_CUDA(cudaMemcpy(hi, d_lab_hi_.get(), n * 4, cudaMemcpyDeviceToHost), "D2H");
+  if (kmin) BV_CUDA(cudaMemcpy(kmin, d_kmin_.get(), n * 4, cudaMemcpyDeviceToHost), "D2H");
+  if (kmax) BV_CUDA(cudaMemcpy(kmax, d_kmax_.get(), n * 4, cudaMemcpyDeviceToHost), "D2H");
   if (feat) {
     std::vector<uint16_t> f(n * kFeat);
     BV_CUDA(cudaMemcpy(f.data(), d_feat_.get(), f.size() * 2, cudaMemcpyDeviceToHost), "D2H");

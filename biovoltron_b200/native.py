@@ -145,7 +145,8 @@ def load() -> C.CDLL:
         "bv_phmm_measure_fp32_peak": (C.c_int, [C.c_int, P(C.c_double)]),
         "bv_phmm_default_band_train_options": (None, [P(BandTrainOptions)]),
         "bv_phmm_band_train": (C.c_int, [V, P(RegionBatchC), P(BandTrainOptions), P(BandTrainReport)]),
-        "bv_phmm_band_labels": (C.c_int, [V, P(RegionBatchC), C.c_float, V, V, V, V]),
+        "bv_phmm_band_labels": (C.c_int, [V, P(RegionBatchC), C.c_float, V, V, V, V, V, V]),
+        "bv_phmm_band_routes": (C.c_int, [V, C.c_int64, V, V, V]),
         "bv_phmm_band_param_count": (C.c_int64, []),
         "bv_phmm_band_get_weights": (C.c_int, [V, V, C.c_int64]),
         "bv_phmm_band_set_weights": (C.c_int, [V, V, C.c_int64]),

@@ -107,6 +107,7 @@ class PairHMMEngine:
             out = np.empty(max(n, 1), np.float64)
         st = N.Stats()
         self._check(self.lib.bv_phmm_compute_regions(self.h, C.byref(v.c), _ptr(out), C.byref(st)))
+        self._staged_n = n
         res = out[:n]
         return (res, st.as_dict()) if with_stats else res
 
@@ -139,8 +140,8 @@ class PairHMMEngine:
         self._check(self.lib.bv_phmm_set_band_options(self.h, C.byref(o)))
 
     # --- learned band: training and weights ---------------------------------
-    def band_train(self, batch: RegionBatch, epochs: int = 8, batch_size: int = 1024, lr: float = 2e-3,
-                   alpha: float = 8.0, tau: float = 1e-4, clip: float = 20.0, margin: int = 2,
+    def band_train(self, batch: RegionBatch, epochs: int = 20, batch_size: int = 1024, lr: float = 2e-3,
+                   alpha: float = 16.0, tau: float = 1e-4, clip: float = 20.0, margin: int = 2,
                    seed: int = 1234) -> dict:
         """Labels `batch` on the GPU and trains the band MLP (bv_phmm_band_train)."""
         o = N.BandTrainOptions()
@@ -153,18 +154,32 @@ class PairHMMEngine:
         self._staged = None
         return rep.as_dict()
 
-    def band_labels(self, batch: RegionBatch, tau: float = 1e-4, features: bool = False):
-        """Seed diagonal, label spread lo/hi (absolute diagonals) and optionally
-        the MLP inputs of every result slot."""
+    def band_labels(self, batch: RegionBatch, tau: float = 1e-4, features: bool = False, extent: bool = False):
+        """Seed diagonal, label spread lo/hi (absolute diagonals) and, on
+        request, the MLP inputs and the shared-11-mer diagonal extent of every
+        result slot."""
         v = _BatchView(batch)
         n = int(self.lib.bv_phmm_region_results(C.byref(v.c)))
-        ds, lo, hi = (np.empty(max(n, 1), np.int32) for _ in range(3))
+        ds, lo, hi, km, kx = (np.empty(max(n, 1), np.int32) for _ in range(5))
         feat = np.empty((max(n, 1), 80), np.float32) if features else None
         self._check(self.lib.bv_phmm_band_labels(self.h, C.byref(v.c), tau, _ptr(ds), _ptr(lo), _ptr(hi),
-                                                 _ptr(feat) if features else None))
+                                                 _ptr(feat) if features else None, _ptr(km), _ptr(kx)))
         self._staged = None
         out = (ds[:n], lo[:n], hi[:n])
-        return out + (feat[:n],) if features else out
+        if features:
+            out = out + (feat[:n],)
+        if extent:
+            out = out + (km[:n], kx[:n])
+        return out
+
+    def band_routes(self):
+        """Route of every result slot of the last band-mode run:
+        (d_lo, width, route), route 0 banded, 1 routed to the full DP,
+        2 edge-check fallback, 3 FP64 recompute."""
+        n = self._staged_n
+        d_lo, width, route = (np.empty(max(n, 1), np.int32) for _ in range(3))
+        self._check(self.lib.bv_phmm_band_routes(self.h, n, _ptr(d_lo), _ptr(width), _ptr(route)))
+        return d_lo[:n], width[:n], route[:n]
 
     def band_weights(self) -> np.ndarray:
         w = np.empty(int(self.lib.bv_phmm_band_param_count()), np.float32)

@@ -261,10 +261,16 @@ bv_status bv_phmm_band_train(bv_phmm_ctx* ctx, const bv_region_batch* train, con
                              bv_band_train_report* report);
 /* Labels and features of a batch, as training sees them (testing and
  * analysis): per result slot the seed diagonal (INT32_MIN: none), the label
- * spread lo/hi in absolute diagonals (INT32_MIN: none) and, if `features` is
- * not NULL, the 80 MLP inputs.  Replaces the staged batch. */
+ * spread lo/hi in absolute diagonals (INT32_MIN: none) and, for the pointers
+ * that are not NULL, the 80 MLP inputs and the lowest / highest diagonal of a
+ * shared 11-mer.  Replaces the staged batch. */
 bv_status bv_phmm_band_labels(bv_phmm_ctx* ctx, const bv_region_batch* batch, float tau, int32_t* dstar, int32_t* lo,
-                              int32_t* hi, float* features);
+                              int32_t* hi, float* features, int32_t* kmin, int32_t* kmax);
+/* After bv_phmm_run_staged in band mode: per result slot the route taken
+ * (0 banded, 1 full DP from the router, 2 banded then sent to the full DP by
+ * the edge check, 3 banded then recomputed in FP64) and, for routes 0, 2 and
+ * 3, the band's first diagonal and width.  For testing and analysis. */
+bv_status bv_phmm_band_routes(bv_phmm_ctx* ctx, int64_t n, int32_t* d_lo, int32_t* width, int32_t* route);
 /* Number of FP32 MLP parameters: W1[128][80], b1[128], W2[128][128], b2[128],
  * W3[2][128], b3[2], weights as [output][input], in that order. */
 int64_t bv_phmm_band_param_count(void);

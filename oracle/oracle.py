@@ -252,8 +252,18 @@ def seed_diagonal(read: bytes, hap: bytes, k: int = 11):
     return min(d for d, c in counts.items() if c == best)
 
 
+END_ROWS = 24
+
+
 def seed_extent(read: bytes, hap: bytes, k: int = 11):
-    """Lowest and highest diagonal j - i of a shared k-mer, or None."""
+    """The featuriser's band extent, or None without a shared k-mer: the
+    lowest and highest diagonal j - i of a shared k-mer, widened by the read
+    ends' triangles -- t_pre = first read position with a hit, t_suf = read
+    bases after the last hit; the first hit's diagonal + t_pre and the last
+    hit's diagonal - t_suf (smallest diagonal where a position has several
+    hits) are included, and so is d - tail (d + head) for every voted
+    diagonal d whose last hit leaves tail <= END_ROWS read bases after it
+    (whose first hit starts head <= END_ROWS bases into the read)."""
     if len(read) < k or len(hap) < k:
         return None
     idx = {}
@@ -261,5 +271,24 @@ def seed_extent(read: bytes, hap: bytes, k: int = 11):
         s = hap[j:j + k]
         if all(c in b"ACGT" for c in s):
             idx.setdefault(s, []).append(j)
-    ds = [j - i for i in range(len(read) - k + 1) for j in idx.get(read[i:i + k], ())]
-    return (min(ds), max(ds)) if ds else None
+    hits = [(i, j - i) for i in range(len(read) - k + 1) for j in idx.get(read[i:i + k], ())]
+    if not hits:
+        return None
+    ds = [d for _, d in hits]
+    i0 = min(i for i, _ in hits)
+    i1 = max(i for i, _ in hits)
+    d0 = min(d for i, d in hits if i == i0)
+    d1 = min(d for i, d in hits if i == i1)
+    t_pre, t_suf = i0, len(read) - k - i1
+    lo, hi = min(min(ds), d1 - t_suf), max(max(ds), d0 + t_pre)
+    first, last = {}, {}
+    for i, d in hits:
+        first[d] = min(first.get(d, i), i)
+        last[d] = max(last.get(d, i), i)
+    for d in first:
+        tail, head = len(read) - k - last[d], first[d]
+        if tail <= END_ROWS:
+            lo = min(lo, d - tail)
+        if head <= END_ROWS:
+            hi = max(hi, d + head)
+    return lo, hi
