@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 
@@ -22,7 +23,7 @@
 namespace bvphmm {
 namespace {
 
-constexpr uint64_t kNoKey = ~0ull;
+constexpr uint32_t kEmpty = 0xffffffffu;  // free hash-table slot
 
 __device__ __forceinline__ int kmer_code(uint8_t b) {
   // 2-bit code for A C T G (ConvertChar's order); -1 for anything else.
@@ -48,54 +49,49 @@ __global__ void k_pairs_from_units(const Unit* __restrict__ units, long long n_u
   }
 }
 
-// Per haplotype: keys (code << 32 | position) of every 11-mer made of A/C/G/T,
-// sorted ascending by a block-wide bitonic sort; other slots hold kNoKey.
-__global__ void __launch_bounds__(256) k_hap_kmers(const uint8_t* __restrict__ hap_bases,
+// Per haplotype h: a bucketed hash table of its 11-mers at
+// table + tbl_base(h): (H + 1) / 2 buckets of 4 slots (load factor <= 1/2);
+// a key lives in its hash bucket or, when that is full, in the next bucket
+// with a free slot.  An entry is (code << 10) | position; kEmpty marks a free
+// slot.  Built in shared memory, written out coalesced.  Haplotypes longer
+// than kBandMaxHap get no table (the featuriser routes their pairs to the
+// full DP).
+__device__ __forceinline__ int64_t tbl_base(int64_t hap_off, long long h) { return 2 * hap_off + 4 * h; }
+__device__ __forceinline__ uint32_t tbl_bucket(uint32_t code, uint32_t nb) {
+  return (uint32_t)(((uint64_t)(code * 0x9E3779B1u) * nb) >> 32);
+}
+
+__global__ void __launch_bounds__(256) k_hap_table(const uint8_t* __restrict__ hap_bases,
                                                    const int64_t* __restrict__ hap_off, long long n_haps,
-                                                   uint64_t* __restrict__ keys) {
-  __shared__ uint64_t sk[kBandMaxHap];
+                                                   uint32_t* __restrict__ table) {
+  __shared__ uint32_t st[2 * kBandMaxHap + 4];
   __shared__ uint8_t sb[kBandMaxHap];
   for (long long h = blockIdx.x; h < n_haps; h += gridDim.x) {
     const int64_t off = hap_off[h];
     const int H = (int)(hap_off[h + 1] - off);
-    if (H > kBandMaxHap) {
-      for (int x = threadIdx.x; x < H; x += blockDim.x) keys[off + x] = kNoKey;
-      continue;
-    }
-    int n = 1;
-    while (n < H) n <<= 1;
+    if (H > kBandMaxHap || H < kK) continue;
+    const uint32_t nb = (uint32_t)(H + 1) / 2;
     __syncthreads();
     for (int x = threadIdx.x; x < H; x += blockDim.x) sb[x] = hap_bases[off + x];
+    for (uint32_t x = threadIdx.x; x < 4 * nb; x += blockDim.x) st[x] = kEmpty;
     __syncthreads();
-    for (int x = threadIdx.x; x < n; x += blockDim.x) {
-      uint64_t key = kNoKey;
-      if (x + kK <= H) {
-        uint32_t code = 0;
-        bool ok = true;
-        for (int t = 0; t < kK; ++t) {
-          const int c = kmer_code(sb[x + t]);
-          ok &= c >= 0;
-          code = (code << 2) | (uint32_t)(c & 3);
-        }
-        if (ok) key = ((uint64_t)code << 32) | (uint32_t)x;
+    for (int x = threadIdx.x; x + kK <= H; x += blockDim.x) {
+      uint32_t code = 0;
+      bool ok = true;
+      for (int t = 0; t < kK; ++t) {
+        const int c = kmer_code(sb[x + t]);
+        ok &= c >= 0;
+        code = (code << 2) | (uint32_t)(c & 3);
       }
-      sk[x] = key;
+      if (!ok) continue;
+      const uint32_t e = (code << 10) | (uint32_t)x;
+      uint32_t bk = tbl_bucket(code, nb);
+      for (bool done = false; !done; bk = bk + 1 == nb ? 0 : bk + 1)
+        for (int t = 0; t < 4 && !done; ++t) done = atomicCAS(&st[4 * bk + t], kEmpty, e) == kEmpty;
     }
     __syncthreads();
-    for (int size = 2; size <= n; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int x = threadIdx.x; x < n; x += blockDim.x) {
-          const int y = x ^ stride;
-          if (y > x) {
-            const bool up = (x & size) == 0;
-            const uint64_t a = sk[x], b = sk[y];
-            if ((a > b) == up) { sk[x] = b; sk[y] = a; }
-          }
-        }
-        __syncthreads();
-      }
-    }
-    for (int x = threadIdx.x; x < H; x += blockDim.x) keys[off + x] = sk[x];
+    uint32_t* dst = table + tbl_base(off, h);
+    for (uint32_t x = threadIdx.x; x < 4 * nb; x += blockDim.x) dst[x] = st[x];
   }
 }
 
@@ -118,10 +114,17 @@ __global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n
   }
 }
 
-// One warp per pair.  The haplotype's sorted 11-mer keys are staged in
-// shared memory; every read 11-mer is binary-searched there and each shared
-// occurrence votes for diagonal d = j - i in a per-warp histogram.  d* is the
-// most voted diagonal (smallest on ties); the features are the 64 bins
+// One block per chunk of kUnitChunk consecutive work units (a read and up
+// to haps_per_unit haplotypes of its region), chunks taken from a device
+// counter.  The chunk's pairs run haplotype by haplotype (units sorted by
+// first haplotype): the block stages the haplotype's 11-mer hash table into
+// shared memory once and its warps share out the reads that meet it, one
+// warp per pair.  The read's
+// 11-mers at positions 0, kSeedStride, 2 kSeedStride, ... and R - 11 are
+// looked up there, and every shared occurrence votes for diagonal d = j - i
+// in a per-warp histogram whose slot also keeps the first and last sampled
+// read position voting for it.  d* is the most
+// voted diagonal (smallest on ties); the features are the 64 bins
 // d* - 32 .. d* + 31 divided by the number of read 11-mers, and 16 scalars:
 // vote totals, lengths, d*'s position, the uncovered read ends (t_pre, t_suf),
 // the diagonals of the first and last hit relative to d*, the mismatches of
@@ -132,217 +135,264 @@ __global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n
 // t read bases uncovered (t <= kEndRows, or any t for the read's last hit)
 // the band reaches t diagonals down, and likewise up from a diagonal whose
 // first hit starts h bases into the read.
-constexpr int kFeatWarps = 4;
-constexpr int kHitCap = 512;
-constexpr int kEndRows = 24;  // horizon of the per-diagonal end triangles
+constexpr int kFeatWarps = 8;
+constexpr int kHitCap = 256;
+constexpr int kEndRows = 24;   // horizon of the per-diagonal end triangles
+constexpr int kUnitChunk = 32;
+constexpr int kHistSlots = kBandMaxRead + kBandMaxHap;  // d + R in [0, R + H)
+// histogram slot: votes << 18 | first read position << 9 | last read position
+// (read positions < 2^9 because reads over kBandMaxRead bases are not banded)
+static_assert(kBandMaxRead < 512, "histogram slot packing");
+
+__device__ __forceinline__ void no_seed(const BandParams& p, long long pi, int lane) {
+  if (lane == 0) { p.dstar[pi] = INT32_MIN; p.kmin[pi] = INT32_MIN; p.kmax[pi] = INT32_MAX; }
+  __nv_bfloat16* f = p.feat + pi * kFeat;
+  for (int x = lane; x < kFeat; x += 32) f[x] = __float2bfloat16(0.f);
+}
+
+__device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, const uint32_t* tbl, uint32_t* hist,
+                               int* hits, int* nhit, int lane) {
+  const int64_t ro = p.batch.read_off[r], ho = p.batch.hap_off[h];
+  const int R = (int)(p.batch.read_off[r + 1] - ro), H = (int)(p.batch.hap_off[h + 1] - ho);
+  __nv_bfloat16* f = p.feat + pi * kFeat;
+  const uint32_t nb = (uint32_t)(H + 1) / 2;
+  if (lane == 0) *nhit = 0;
+  __syncwarp();
+  const uint32_t* rcode = p.read_kmers + ro;
+  const int last_pos = R - kK;
+  const int n_samp = last_pos / kSeedStride + 1 + (last_pos % kSeedStride != 0);
+  for (int t0 = 0; t0 < n_samp; t0 += 32) {
+    const int t = t0 + lane;
+    const int i = min(t * kSeedStride, last_pos);
+    const uint32_t code = t < n_samp ? rcode[i] : kNoCode;
+    int bk = code != kNoCode ? (int)tbl_bucket(code, nb) : -1;
+    for (;;) {
+      uint32_t hitmask = 0u;  // slots of the loaded bucket holding this code
+      uint4 q = make_uint4(0, 0, 0, 0);
+      if (bk >= 0) {
+        q = *reinterpret_cast<const uint4*>(tbl + 4 * bk);
+        hitmask = ((q.x >> 10) == code && q.x != kEmpty ? 1u : 0u) | ((q.y >> 10) == code && q.y != kEmpty ? 2u : 0u) |
+                  ((q.z >> 10) == code && q.z != kEmpty ? 4u : 0u) | ((q.w >> 10) == code && q.w != kEmpty ? 8u : 0u);
+        const bool has_free = q.x == kEmpty || q.y == kEmpty || q.z == kEmpty || q.w == kEmpty;
+        bk = has_free ? -1 : (bk + 1 == (int)nb ? 0 : bk + 1);
+      }
+      while (__any_sync(0xffffffffu, hitmask != 0u)) {
+        int vote = -1;
+        if (hitmask) {
+          const int k = __ffs(hitmask) - 1;
+          hitmask &= hitmask - 1u;
+          const uint32_t e = k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
+          vote = (int)(e & 1023u) - i + R;  // d + R
+        }
+        const unsigned vm = __ballot_sync(0xffffffffu, vote >= 0);
+        if (vote >= 0) {
+          const unsigned peers = __match_any_sync(vm, vote);
+          if ((__ffs(peers) - 1) == lane) {
+            // one leader per slot; peers' sampled positions are those of their lanes
+            const int hl = 31 - __clz(peers);
+            const uint32_t n = (uint32_t)__popc(peers);
+            const uint32_t i_hi = (uint32_t)min((t0 + hl) * kSeedStride, last_pos);
+            const uint32_t old = hist[vote];
+            if (old == 0u) {
+              hist[vote] = (n << 18) | ((uint32_t)i << 9) | i_hi;
+              const int qn = atomicAdd(nhit, 1);
+              if (qn < kHitCap) hits[qn] = vote;
+            } else {
+              const uint32_t fi = min((old >> 9) & 511u, (uint32_t)i), la = max(old & 511u, i_hi);
+              hist[vote] = (((old >> 18) + n) << 18) | (fi << 9) | la;
+            }
+          }
+        }
+        __syncwarp();
+      }
+      if (!__any_sync(0xffffffffu, bk >= 0)) break;
+    }
+  }
+  __syncwarp();
+  const int nh = min(*nhit, kHitCap);
+  const bool overflow = *nhit > kHitCap;
+  // one pass over the voted diagonals: mode (most votes, smallest slot on
+  // ties), voted extent, first and last sampled hit (smallest slot on ties),
+  // per-diagonal end triangles, vote total
+  uint32_t best = 0u, fkey = 0xffffffffu, lkey = 0u;
+  int smin = INT32_MAX, smax = -1, tri_lo = INT32_MAX, tri_hi = INT32_MIN, total = 0;
+  for (int x = lane; x < nh; x += 32) {
+    const int sl = hits[x];
+    const uint32_t v = hist[sl], c = v >> 18, fi = (v >> 9) & 511u, la = v & 511u;
+    best = max(best, (c << 16) | (0xffffu - (uint32_t)sl));
+    fkey = min(fkey, (fi << 16) | (uint32_t)sl);
+    lkey = max(lkey, (la << 16) | (0xffffu - (uint32_t)sl));
+    smin = min(smin, sl);
+    smax = max(smax, sl);
+    const int d = sl - R, tail = R - kK - (int)la, head = (int)fi;
+    if (tail <= kEndRows) tri_lo = min(tri_lo, d - tail);
+    if (head <= kEndRows) tri_hi = max(tri_hi, d + head);
+    total += (int)c;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
+    lkey = max(lkey, __shfl_xor_sync(0xffffffffu, lkey, o));
+    smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+    smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+    tri_lo = min(tri_lo, __shfl_xor_sync(0xffffffffu, tri_lo, o));
+    tri_hi = max(tri_hi, __shfl_xor_sync(0xffffffffu, tri_hi, o));
+    total += __shfl_xor_sync(0xffffffffu, total, o);
+  }
+  if (best == 0u) {
+    no_seed(p, pi, lane);
+  } else {
+    const int best_slot = (int)(0xffffu - (best & 0xffffu));
+    const int ds = best_slot - R;
+    const int first_i = (int)(fkey >> 16), first_s = (int)(fkey & 0xffffu);
+    const int last_i = (int)(lkey >> 16), last_s = (int)(0xffffu - (lkey & 0xffffu));
+    const int t_pre = first_i, t_suf = R - kK - last_i;
+    const int d_first = first_s - R, d_last = last_s - R;
+    tri_lo = min(tri_lo, d_last - t_suf);
+    tri_hi = max(tri_hi, d_first + t_pre);
+    // mismatches of the first / last 16 read bases along those diagonals
+    const int n_end = min(16, R);
+    const uint8_t* rb = p.batch.read_bases + ro;
+    const uint8_t* hb = p.batch.hap_bases + ho;
+    bool mp = false, ms = false;
+    if (lane < n_end) {
+      const int ip = lane, jp = ip + d_first;
+      const int is = R - 1 - lane, js = is + d_last;
+      mp = jp < 0 || jp >= H || !bases_match(rb[ip], hb[jp]);
+      ms = js < 0 || js >= H || !bases_match(rb[is], hb[js]);
+    }
+    const int mis_pre = __popc(__ballot_sync(0xffffffffu, mp));
+    const int mis_suf = __popc(__ballot_sync(0xffffffffu, ms));
+    // 64 histogram bins d* - 32 .. d* + 31, two adjacent bins per lane
+    int win = 0, nonzero = 0, peak = 0;
+    const float inv = 1.f / (float)n_samp;
+    int cb[2];
+    for (int t = 0; t < 2; ++t) {
+      const int s = best_slot - kHistBins / 2 + 2 * lane + t;
+      cb[t] = (s >= 0 && s < R + H) ? (int)(hist[s] >> 18) : 0;
+      win += cb[t];
+      nonzero += cb[t] > 0;
+      peak = max(peak, cb[t]);
+    }
+    *reinterpret_cast<__nv_bfloat162*>(f + 2 * lane) = __floats2bfloat162_rn((float)cb[0] * inv, (float)cb[1] * inv);
+    for (int o = 16; o > 0; o >>= 1) {
+      win += __shfl_xor_sync(0xffffffffu, win, o);
+      nonzero += __shfl_xor_sync(0xffffffffu, nonzero, o);
+      peak = max(peak, __shfl_xor_sync(0xffffffffu, peak, o));
+    }
+    if (overflow) total = max(total, win);
+    if (lane == 0) {
+      // 16 scalars, written as two 16-byte stores
+      const float v[16] = {(float)total * inv,
+                           (float)(total - win) * inv,
+                           (float)R / 256.f,
+                           (float)H / 1024.f,
+                           (float)(ds + R) / (float)(R + H),
+                           1.f,
+                           (float)peak * inv,
+                           (float)nonzero / (float)kHistBins,
+                           (float)t_pre / 32.f,
+                           (float)t_suf / 32.f,
+                           (float)(d_first - ds) / 32.f,
+                           (float)(d_last - ds) / 32.f,
+                           (float)mis_pre / 16.f,
+                           (float)mis_suf / 16.f,
+                           overflow ? -2.f : fmaxf((float)(smin - R - ds) / 32.f, -2.f),
+                           overflow ? 2.f : fminf((float)(smax - R - ds) / 32.f, 2.f)};
+      uint32_t w[8];
+#pragma unroll
+      for (int x = 0; x < 8; ++x) {
+        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * x], v[2 * x + 1]);
+        w[x] = *reinterpret_cast<const uint32_t*>(&b2);
+      }
+      uint4* dst = reinterpret_cast<uint4*>(f + kHistBins);
+      dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+      dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    }
+    if (lane == 0) {
+      p.dstar[pi] = ds;
+      // voted extent and end triangles (a hit list overflow widens it to everything)
+      p.kmin[pi] = overflow ? INT32_MIN : min(smin - R, tri_lo);
+      p.kmax[pi] = overflow ? INT32_MAX : max(smax - R, tri_hi);
+    }
+  }
+  __syncwarp();
+  if (overflow) {
+    for (int x = lane; x < R + H; x += 32) hist[x] = 0u;
+  } else {
+    for (int x = lane; x < nh; x += 32) hist[hits[x]] = 0u;
+  }
+  __syncwarp();
+}
 
 __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  uint64_t* skeys = reinterpret_cast<uint64_t*>(smem) + (size_t)wib * kBandMaxHap;
-  int* hist = reinterpret_cast<int*>(smem + (size_t)kFeatWarps * kBandMaxHap * 8) + (size_t)wib * kBandMaxSpan;
-  int* hits = reinterpret_cast<int*>(smem + (size_t)kFeatWarps * kBandMaxHap * 8) + (size_t)kFeatWarps * kBandMaxSpan +
-              (size_t)wib * (kHitCap + 1);
+  // block-shared: the staged haplotype table and the chunk's units sorted by
+  // first haplotype; per warp: histogram and voted-slot list
+  uint32_t* tbl = reinterpret_cast<uint32_t*>(smem);
+  Unit* su = reinterpret_cast<Unit*>(smem + (size_t)(2 * kBandMaxHap + 4) * 4);
+  int* sctl = reinterpret_cast<int*>(su + kUnitChunk);  // [0] chunk, [1] max nh
+  uint32_t* hist = reinterpret_cast<uint32_t*>(sctl + 4) + (size_t)wib * kHistSlots;
+  int* hits = reinterpret_cast<int*>(sctl + 4) + (size_t)kFeatWarps * kHistSlots + (size_t)wib * (kHitCap + 1);
   int* nhit = hits + kHitCap;
-  // per voted diagonal: first (high 16 bits) and last (low 16 bits) read position
-  int* pos = reinterpret_cast<int*>(smem + (size_t)kFeatWarps * kBandMaxHap * 8) + (size_t)kFeatWarps * kBandMaxSpan +
-             (size_t)kFeatWarps * (kHitCap + 1) + (size_t)wib * kBandMaxSpan;
-  for (int x = lane; x < kBandMaxSpan; x += 32) hist[x] = 0;
-  const long long nwarps = (long long)gridDim.x * kFeatWarps;
-  int staged_hap = -1;
-  for (long long pi = blockIdx.x * (long long)kFeatWarps + wib; pi < p.n_pairs; pi += nwarps) {
-    const int r = p.pair_read[pi], h = p.pair_hap[pi];
-    const int64_t ro = p.batch.read_off[r], ho = p.batch.hap_off[h];
-    const int R = (int)(p.batch.read_off[r + 1] - ro), H = (int)(p.batch.hap_off[h + 1] - ho);
-    __nv_bfloat16* f = p.feat + pi * kFeat;
-    if (R < kK || H < kK || H > kBandMaxHap || R + H + 1 >= kBandMaxSpan) {
-      if (lane == 0) { p.dstar[pi] = INT32_MIN; p.kmin[pi] = INT32_MIN; p.kmax[pi] = INT32_MAX; }
-      for (int x = lane; x < kFeat; x += 32) f[x] = __float2bfloat16(0.f);
-      continue;
+  for (int x = lane; x < kHistSlots; x += 32) hist[x] = 0u;
+  const long long nchunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
+  for (;;) {
+    __syncthreads();  // the previous chunk is done with su / tbl
+    if (threadIdx.x == 0) sctl[0] = (int)min((long long)atomicAdd(&p.bctr->feat_next, 1ull), nchunks);
+    __syncthreads();
+    const long long c = sctl[0];
+    if (c >= nchunks) break;
+    const long long u0 = c * kUnitChunk;
+    const int nu = (int)min((long long)kUnitChunk, p.n_units - u0);
+    if (wib == 0) {
+      Unit un{};
+      if (lane < nu) un = p.units[u0 + lane];
+      const long long key = lane < nu ? ((long long)un.hap0 << 5) | lane : LLONG_MAX;
+      int rank = 0;
+      for (int o = 0; o < 32; ++o) rank += __shfl_sync(0xffffffffu, key, o) < key;
+      if (lane < nu) su[rank] = un;
+      int mx = lane < nu ? un.nh : 0;
+      for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if (lane == 0) sctl[1] = mx;
     }
-    const int nk_hap = H - kK + 1;
-    if (h != staged_hap) {
-      __syncwarp();
-      for (int x = lane; x < nk_hap; x += 32) skeys[x] = p.hap_kmers[ho + x];
-      staged_hap = h;
-    }
-    if (lane == 0) *nhit = 0;
-    __syncwarp();
-    const uint32_t* rcode = p.read_kmers + ro;
-    const int nk_read = R - kK + 1;
-    // first and last read position with a shared 11-mer, with that hit's slot
-    int first_i = INT32_MAX, first_s = 0, last_i = -1, last_s = 0;
-    for (int i0 = 0; i0 < nk_read; i0 += 32) {
-      const int i = i0 + lane;
-      const uint32_t code = i < nk_read ? rcode[i] : kNoCode;
-      int m = nk_hap;
-      if (code != kNoCode) {
-        const uint64_t lo_key = (uint64_t)code << 32;
-        int a = 0, b = nk_hap;  // first key >= lo_key
-        while (a < b) {
-          const int mid = (a + b) >> 1;
-          if (skeys[mid] < lo_key) a = mid + 1; else b = mid;
-        }
-        m = a;
-      }
-      // one vote per occurrence; lanes voting for the same diagonal are
-      // combined so each histogram slot takes one atomic per round
-      for (;;) {
-        int slot = -1;
-        if (m < nk_hap) {
-          const uint64_t key = skeys[m];
-          if ((key >> 32) == code) slot = (int)(key & 0xffffffffu) - i + R;  // d + R
-          else m = nk_hap;
-        }
-        const unsigned active = __ballot_sync(0xffffffffu, slot >= 0);
-        if (active == 0u) break;
-        if (slot >= 0) {
-          if (i < first_i) { first_i = i; first_s = slot; }
-          if (i > last_i) { last_i = i; last_s = slot; }
-          const unsigned peers = __match_any_sync(active, slot);
-          if ((__ffs(peers) - 1) == lane) {
-            // peers share the slot; their read positions are i0 + (lanes of peers)
-            const int i_hi = i0 + 31 - __clz(peers);
-            if (atomicAdd(&hist[slot], __popc(peers)) == 0) {
-              pos[slot] = (i << 16) | i_hi;
-              const int q = atomicAdd(nhit, 1);
-              if (q < kHitCap) hits[q] = slot;
-            } else {  // repeats can revisit a slot out of order within a chunk
-              const int ps = pos[slot];
-              pos[slot] = (min(ps >> 16, i) << 16) | max(ps & 0xffff, i_hi);
-            }
+    __syncthreads();
+    const int max_nh = sctl[1];
+    for (int k = 0; k < max_nh; ++k) {
+      for (int q0 = 0; q0 < nu;) {
+        // a group: consecutive units with the same first haplotype, so one haplotype h
+        const int hap0 = su[q0].hap0;
+        int q1 = q0 + 1;
+        while (q1 < nu && su[q1].hap0 == hap0) ++q1;
+        const int h = hap0 + k;
+        bool any = false;
+        for (int q = q0; q < q1; ++q) any |= k < su[q].nh;
+        if (any) {
+          const int64_t ho = p.batch.hap_off[h];
+          const int H = (int)(p.batch.hap_off[h + 1] - ho);
+          const bool tab = H >= kK && H <= kBandMaxHap;
+          if (tab) {
+            const uint32_t* src_tbl = p.hap_table + tbl_base(ho, h);
+            for (int x = threadIdx.x; x < 4 * ((H + 1) / 2); x += blockDim.x) tbl[x] = src_tbl[x];
           }
-          ++m;
+          __syncthreads();
+          for (int q = q0 + wib; q < q1; q += kFeatWarps) {
+            const Unit un = su[q];
+            if (k >= un.nh) continue;
+            const long long pi = un.out0 + k;
+            const int R = (int)(p.batch.read_off[un.read + 1] - p.batch.read_off[un.read]);
+            if (!tab || R < kK || R > kBandMaxRead) {
+              no_seed(p, pi, lane);
+              continue;
+            }
+            featurize_pair(p, pi, un.read, h, tbl, hist, hits, nhit, lane);
+          }
+          __syncthreads();  // before the table is restaged
         }
-        __syncwarp();
+        q0 = q1;
       }
     }
-    __syncwarp();
-    const int nh = min(*nhit, kHitCap);
-    const bool overflow = *nhit > kHitCap;
-    // mode: highest count, smallest diagonal on ties
-    int best_cnt = 0, best_slot = 0x7fffffff, smin = 0x7fffffff, smax = -1;
-    for (int x = lane; x < nh; x += 32) {
-      const int s = hits[x], c = hist[s];
-      if (c > best_cnt || (c == best_cnt && s < best_slot)) { best_cnt = c; best_slot = s; }
-      smin = min(smin, s);
-      smax = max(smax, s);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
-      smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const int fi = __shfl_xor_sync(0xffffffffu, first_i, o), fs = __shfl_xor_sync(0xffffffffu, first_s, o);
-      const int li = __shfl_xor_sync(0xffffffffu, last_i, o), ls = __shfl_xor_sync(0xffffffffu, last_s, o);
-      if (fi < first_i || (fi == first_i && fs < first_s)) { first_i = fi; first_s = fs; }
-      if (li > last_i || (li == last_i && ls < last_s)) { last_i = li; last_s = ls; }
-    }
-    // read ends not covered by a shared 11-mer: t_pre bases before the first
-    // hit, t_suf after the last.  An insertion run in a read end moves the
-    // alignment one diagonal per row, so the end rows may sit up to t_pre
-    // diagonals above the first hit's diagonal and t_suf below the last one.
-    const int t_pre = last_i >= 0 ? first_i : 0, t_suf = last_i >= 0 ? R - kK - last_i : 0;
-    const int d_first = first_s - R, d_last = last_s - R;
-    // mismatches of the first / last 16 read bases along those diagonals
-    int mis_pre = 0, mis_suf = 0;
-    if (last_i >= 0) {
-      const int nb = min(16, R);
-      const uint8_t* rb = p.batch.read_bases + ro;
-      const uint8_t* hb = p.batch.hap_bases + ho;
-      bool mp = false, ms = false;
-      if (lane < nb) {
-        const int ip = lane, jp = ip + d_first;
-        const int is = R - 1 - lane, js = is + d_last;
-        mp = jp < 0 || jp >= H || !bases_match(rb[ip], hb[jp]);
-        ms = js < 0 || js >= H || !bases_match(rb[is], hb[js]);
-      }
-      mis_pre = __popc(__ballot_sync(0xffffffffu, mp));
-      mis_suf = __popc(__ballot_sync(0xffffffffu, ms));
-    }
-    // end triangles of every voted diagonal whose hits come within kEndRows
-    // rows of a read end
-    int tri_lo = d_last - t_suf, tri_hi = d_first + t_pre;
-    for (int x = lane; x < nh; x += 32) {
-      const int s = hits[x], ps = pos[s], d = s - R;
-      const int tail = R - kK - (ps & 0xffff), head = ps >> 16;
-      if (tail <= kEndRows) tri_lo = min(tri_lo, d - tail);
-      if (head <= kEndRows) tri_hi = max(tri_hi, d + head);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      tri_lo = min(tri_lo, __shfl_xor_sync(0xffffffffu, tri_lo, o));
-      tri_hi = max(tri_hi, __shfl_xor_sync(0xffffffffu, tri_hi, o));
-    }
-    if (lane == 0) {
-      // extent of the shared 11-mer diagonals and the end triangles (a hit
-      // list overflow widens it to everything)
-      p.kmin[pi] = overflow ? INT32_MIN : min(smin - R, tri_lo);
-      p.kmax[pi] = overflow ? INT32_MAX : max(smax - R, tri_hi);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const int oc = __shfl_xor_sync(0xffffffffu, best_cnt, o), os = __shfl_xor_sync(0xffffffffu, best_slot, o);
-      if (oc > best_cnt || (oc == best_cnt && os < best_slot)) { best_cnt = oc; best_slot = os; }
-    }
-    const float inv = 1.f / (float)(R - kK + 1);
-    if (best_cnt == 0) {
-      if (lane == 0) p.dstar[pi] = INT32_MIN;
-      for (int x = lane; x < kFeat; x += 32) f[x] = __float2bfloat16(0.f);
-    } else {
-      const int ds = best_slot - R;
-      int total = 0;
-      for (int x = lane; x < nh; x += 32) total += hist[hits[x]];
-      int win = 0, nonzero = 0, peak = 0;
-      float binv[2];
-      for (int t = 0; t < 2; ++t) {
-        const int bin = lane + 32 * t;
-        const int s = best_slot - kHistBins / 2 + bin;
-        const int c = (s >= 0 && s < R + H) ? hist[s] : 0;
-        win += c;
-        nonzero += c > 0;
-        peak = max(peak, c);
-        binv[t] = (float)c * inv;
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        total += __shfl_xor_sync(0xffffffffu, total, o);
-        win += __shfl_xor_sync(0xffffffffu, win, o);
-        nonzero += __shfl_xor_sync(0xffffffffu, nonzero, o);
-        peak = max(peak, __shfl_xor_sync(0xffffffffu, peak, o));
-      }
-      if (overflow) total = max(total, win);
-      f[lane] = __float2bfloat16(binv[0]);
-      f[lane + 32] = __float2bfloat16(binv[1]);
-      if (lane < kFeat - kHistBins) {
-        float v = 0.f;
-        switch (lane) {
-          case 0: v = (float)total * inv; break;
-          case 1: v = (float)(total - win) * inv; break;
-          case 2: v = (float)R / 256.f; break;
-          case 3: v = (float)H / 1024.f; break;
-          case 4: v = (float)(ds + R) / (float)(R + H); break;
-          case 5: v = 1.f; break;
-          case 6: v = (float)peak * inv; break;
-          case 7: v = (float)nonzero / (float)kHistBins; break;
-          case 8: v = (float)t_pre / 32.f; break;
-          case 9: v = (float)t_suf / 32.f; break;
-          case 10: v = (float)(d_first - ds) / 32.f; break;
-          case 11: v = (float)(d_last - ds) / 32.f; break;
-          case 12: v = (float)mis_pre / 16.f; break;
-          case 13: v = (float)mis_suf / 16.f; break;
-          case 14: v = overflow ? -2.f : fmaxf((float)(smin - R - ds) / 32.f, -2.f); break;
-          case 15: v = overflow ? 2.f : fminf((float)(smax - R - ds) / 32.f, 2.f); break;
-          default: v = 0.f;
-        }
-        f[kHistBins + lane] = __float2bfloat16(v);
-      }
-      if (lane == 0) p.dstar[pi] = ds;
-    }
-    __syncwarp();
-    if (overflow) {
-      for (int x = lane; x < R + H; x += 32) hist[x] = 0;
-    } else {
-      for (int x = lane; x < nh; x += 32) hist[hits[x]] = 0;
-    }
-    __syncwarp();
   }
 }
 
@@ -499,7 +549,7 @@ __device__ __forceinline__ bool route_band(const BandParams& p, long long pi, in
   const int blo = min(ds + (int)floorf(lo) - p.margin, km), bhi = max(ds + (int)ceilf(hi) + p.margin, kx);
   const int width = bhi - blo + 1;
   if (width > band_width(kBandWidths - 1) || width < 1) return false;
-  cls = width <= band_width(0) ? 0 : 1;
+  cls = width <= band_width(0) ? 0 : width <= band_width(1) ? 1 : 2;
   d_lo = blo - (band_width(cls) - width) / 2;
   return true;
 }
@@ -577,6 +627,7 @@ __global__ void k_band_scan(BandCounters* c) {
       c->band_fill[threadIdx.x][b] = acc;
       acc += c->band_count[threadIdx.x][b];
     }
+    c->band_total[threadIdx.x] = acc;
   }
 }
 
@@ -608,11 +659,12 @@ template <int W>
 __global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
   constexpr int NW = W / 8;
   const Tables* tb = p.tables;
-  const unsigned long long total = [&] {
-    unsigned long long s = 0;
-    for (int b = 0; b < kRBuckets; ++b) s += p.bctr->band_count[cls][b];
-    return s;
-  }();
+  __shared__ QProb qp[128];
+  for (int x = threadIdx.x; x < 128; x += blockDim.x) qp[x] = tb->qp[x];
+  __syncthreads();
+  // routed items (bucketed by read length), then items promoted from the next narrower class
+  const unsigned long long total =
+      p.bctr->band_total[cls] + min(p.bctr->promoted[cls], (unsigned long long)p.item_cap - p.bctr->band_total[cls]);
   const BandItem* items = p.items + (size_t)cls * p.item_cap;
   const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
   const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
@@ -650,12 +702,12 @@ __global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
     for (int r = 1; r <= R; ++r) {
       const uchar4 qv = quals[r - 1];
       const int qi = qv.y & kQualMask, qd = qv.z & kQualMask;
-      const float pmx = tb->ph2pr_f[qi], pmy = tb->ph2pr_f[qd];
-      const float g = tb->ph2pr_f[qv.w & kQualMask], gp = 1.f - g;
-      const float eps = tb->ph2pr_f[qv.x & kQualMask];
+      const QProb qpi = qp[qi], qpg = qp[qv.w & kQualMask], qpb = qp[qv.x & kQualMask];
+      const float pmx = qpi.p, pmy = qp[qd].p;
+      const float g = qpg.p, gp = qpg.q;
       const float mm = mm_of(tb, qi, qd);
-      const float cx = gp * ap, cy = gp * bp, kap = g * ap / pmx;
-      const float em = 1.f - eps, ex = eps / 3.f;
+      const float cx = gp * ap, cy = gp * bp, kap = g * ap * qpi.inv;
+      const float em = qpb.q, ex = qpb.third;
       const uint32_t rb = onehot(rbase[r - 1]) * 0x11111111u;
       float lm = 0.f, ly = 0.f;
 #pragma unroll
@@ -702,7 +754,7 @@ __global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
         BM[k] = v; BX[k] = v; BY[k] = 0.f;
       }
       double acc = 0.0;
-      int bexp = 0;  // true B = stored B * 2^bexp
+      double bscale = 1.0;  // true B = stored B * bscale (a power of two)
       {
         const __nv_bfloat162 pk = *reinterpret_cast<const __nv_bfloat162*>(&slab[(size_t)R * nthreads]);
         acc += (double)__low2float(pk) * fmaxf(BM[0], BX[0]) + (double)__high2float(pk) * fmaxf(BM[W - 1], BX[W - 1]);
@@ -716,14 +768,16 @@ __global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
         win[0] = (win[0] << 4) | nib;
       }
       uchar4 q1 = quals[R - 1];
+      QProb qg1 = qp[q1.w & kQualMask];
       for (int r = R - 1; r >= 1; --r) {
         const uchar4 q0 = quals[r - 1];  // row r; q1 is row r+1
         const int qi1 = q1.y & kQualMask, qd1 = q1.z & kQualMask;
-        const float mm1 = mm_of(tb, qi1, qd1), mx1 = tb->ph2pr_f[qi1];
-        const float g1 = tb->ph2pr_f[q1.w & kQualMask], gp1 = 1.f - g1;
-        const float eps1 = tb->ph2pr_f[q1.x & kQualMask];
-        const float em1 = 1.f - eps1, ex1 = eps1 / 3.f;
-        const float my0 = tb->ph2pr_f[q0.z & kQualMask], g0 = tb->ph2pr_f[q0.w & kQualMask];
+        const float mm1 = mm_of(tb, qi1, qd1), mx1 = qp[qi1].p;
+        const float g1 = qg1.p, gp1 = qg1.q;
+        const QProb qb1 = qp[q1.x & kQualMask];
+        const float em1 = qb1.q, ex1 = qb1.third;
+        const QProb qg0 = qp[q0.w & kQualMask];
+        const float my0 = qp[q0.z & kQualMask].p, g0 = qg0.p;
         const uint32_t rb1 = onehot(rbase[r]) * 0x11111111u;
         float byn = 0.f;  // B_Y(r, k+1)
 #pragma unroll
@@ -740,7 +794,7 @@ __global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
         }
         const __nv_bfloat162 pk = *reinterpret_cast<const __nv_bfloat162*>(&slab[(size_t)r * nthreads]);
         const float b0 = fmaxf(BM[0], fmaxf(BX[0], BY[0])), b1 = fmaxf(BM[W - 1], fmaxf(BX[W - 1], BY[W - 1]));
-        acc += ((double)__low2float(pk) * b0 + (double)__high2float(pk) * b1) * ldexp(1.0, bexp);
+        acc += (double)(__low2float(pk) * b0 + __high2float(pk) * b1) * bscale;
         if ((r & 7) == 0) {
           float m = 0.f;
 #pragma unroll
@@ -751,7 +805,7 @@ __global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
             const float sc = ldexpf(1.f, -e2);
 #pragma unroll
             for (int k = 0; k < W; ++k) { BM[k] *= sc; BX[k] *= sc; BY[k] *= sc; }
-            bexp += e2;
+            bscale = ldexp(bscale, e2);
           }
         }
         // window to row r's columns: shift back one column, new k = 0 is column r + d_lo
@@ -761,12 +815,24 @@ __global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
         for (int w = NW - 1; w > 0; --w) win[w] = __funnelshift_l(win[w - 1], win[w], 4);
         win[0] = (win[0] << 4) | nib;
         q1 = q0;
+        qg1 = qg0;
       }
       cells += (unsigned long long)R * W;
       const double edge = acc / (double)tot;
       fall_back = !(edge <= (double)p.edge_threshold);
     }
-    if (fall_back) {
+    if (fall_back && cls + 1 < kBandWidths) {
+      // second chance on the next wider band, centred on this one
+      const unsigned long long q = atomicAdd(&p.bctr->promoted[cls + 1], 1ull);
+      const unsigned long long at = p.bctr->band_total[cls + 1] + q;
+      if (at < (unsigned long long)p.item_cap) {
+        BandItem ni = it;
+        ni.d_lo = it.d_lo - (band_width(cls + 1) - W) / 2;
+        p.items[(size_t)(cls + 1) * p.item_cap + at] = ni;
+      } else {
+        atomicOr(&p.ctr->status, 4ull);
+      }
+    } else if (fall_back) {
       const int v = full_variant(R);
       const unsigned long long q = atomicAdd(&p.bctr->full_count[v], 1ull);
       atomicAdd(&p.bctr->fallback_edge, 1ull);
@@ -843,16 +909,16 @@ cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint
   return cudaGetLastError();
 }
 
-cudaError_t launch_hap_kmers(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint64_t* keys,
-                             cudaStream_t st) {
+cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint32_t* table,
+                             int sms, cudaStream_t st) {
   if (n_haps <= 0) return cudaSuccess;
-  const long long blocks = std::min<long long>(n_haps, 148 * 16);
-  k_hap_kmers<<<(int)blocks, 256, 0, st>>>(hap_bases, hap_off, n_haps, keys);
+  const long long blocks = std::min<long long>(n_haps, (long long)sms * 8);
+  k_hap_table<<<(int)blocks, 256, 0, st>>>(hap_bases, hap_off, n_haps, table);
   return cudaGetLastError();
 }
 
-constexpr int kFeatSmem =
-    kFeatWarps * kBandMaxHap * 8 + 2 * kFeatWarps * kBandMaxSpan * 4 + kFeatWarps * (kHitCap + 1) * 4;
+constexpr int kFeatSmem = (2 * kBandMaxHap + 4) * 4 + kUnitChunk * (int)sizeof(Unit) + 16 +
+                          kFeatWarps * (kHistSlots + kHitCap + 1) * 4;
 
 cudaError_t prepare_band_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_featurize, cudaFuncAttributeMaxDynamicSharedMemorySize, kFeatSmem);
@@ -861,10 +927,10 @@ cudaError_t prepare_band_kernels() {
 }
 
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
-  if (p.n_pairs <= 0) return cudaSuccess;
-  const int smem = kFeatSmem;
-  const long long blocks = std::min<long long>((p.n_pairs + kFeatWarps - 1) / kFeatWarps, (long long)sms * 2);
-  k_featurize<<<(int)blocks, kFeatWarps * 32, smem, st>>>(p);
+  if (p.n_units <= 0) return cudaSuccess;
+  const long long chunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
+  const long long blocks = std::min<long long>(chunks, (long long)sms * 3);
+  k_featurize<<<(int)blocks, kFeatWarps * 32, kFeatSmem, st>>>(p);
   return cudaGetLastError();
 }
 
@@ -891,8 +957,9 @@ cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st) {
 
 cudaError_t launch_band_dp(const BandParams& p, int cls, int sms, cudaStream_t st) {
   const int blocks = band_dp_blocks(sms);
-  if (cls == 0) k_band_f32<16><<<blocks, 128, 0, st>>>(p, 0);
-  else k_band_f32<32><<<blocks, 128, 0, st>>>(p, 1);
+  if (cls == 0) k_band_f32<8><<<blocks, 128, 0, st>>>(p, 0);
+  else if (cls == 1) k_band_f32<16><<<blocks, 128, 0, st>>>(p, 1);
+  else k_band_f32<32><<<blocks, 128, 0, st>>>(p, 2);
   return cudaGetLastError();
 }
 

@@ -2,15 +2,21 @@
 //
 // Pipeline, all on the context's stream:
 //   k_pairs_from_units  expand work units into one (read, hap) per result slot
-//   k_hap_kmers         per haplotype: sorted (11-mer code, position) keys
-//   k_featurize         per pair: shared 11-mer diagonal histogram -> features,
-//                       seed diagonal d* (the histogram's mode)
+//   k_hap_table         per haplotype: 11-mer hash table (code -> positions)
+//   k_read_kmers        per read position: 11-mer code
+//   k_featurize         per pair (units in chunks, haplotype tables staged in
+//                       shared memory): shared 11-mer diagonal histogram ->
+//                       features, seed diagonal d* (the histogram's mode),
+//                       band extent (voted diagonals and read-end triangles)
 //   k_mlp_forward       per pair: BF16 MLP 80-128-128-2 (FP32 accumulation) ->
 //                       lower and upper band edge relative to d*
 //   k_band_route        band (by width class and read-length bucket) or full DP
-//   k_band_f32<W>       banded forward, one thread per pair, edge-mass check
-// Pairs that leave the band path go to the full-DP kernels through per-variant
-// device lists; FP32 results below 1e-28 go to the FP64 list as before.
+//   k_band_f32<W>       banded forward-backward, one thread per pair, edge-mass
+//                       check; W = 8, 16, 32 run in that order, and a pair that
+//                       fails the check is promoted to the next wider band
+// Pairs that leave the band path (routed out, or failing at W = 32) go to the
+// full-DP kernels through per-variant device lists; FP32 results below 1e-28
+// go to the FP64 list as before.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -21,17 +27,18 @@
 namespace bvphmm {
 
 constexpr int kK = 11;                 // k-mer length of the featuriser
+constexpr int kSeedStride = 5;         // read 11-mers sampled every kSeedStride positions (and the last one)
 constexpr int kFeat = 80;              // MLP input width (64 histogram bins + 16 scalars, zero padded)
 constexpr int kHid = 128;              // hidden width
 constexpr int kOut = 2;                // outputs: lower and upper band edge (diagonals, relative to d*)
 constexpr int kHistBins = 64;          // histogram window: d* - 32 .. d* + 31
 constexpr int kBandMaxSpan = 2048;     // read_len + hap_len limit of the featuriser (per-warp histogram)
 constexpr int kBandMaxHap = 1024;      // haplotype limit of the k-mer sort and the featuriser's staging
-constexpr int kBandWidths = 2;         // width classes of the banded kernel
+constexpr int kBandWidths = 3;         // width classes of the banded kernel
 #if defined(__CUDACC__)
 __host__ __device__
 #endif
-constexpr int band_width(int cls) { return cls == 0 ? 16 : 32; }
+constexpr int band_width(int cls) { return cls == 0 ? 8 : cls == 1 ? 16 : 32; }
 constexpr int kRBuckets = 64;          // read-length buckets (8 rows each) for warp-uniform band launches
 constexpr int kRBucketRows = 8;
 constexpr int kBandMaxRead = kRBuckets * kRBucketRows - 1;
@@ -59,11 +66,14 @@ struct BandCounters {
   unsigned long long band_count[kBandWidths][kRBuckets];  // items per (width, bucket)
   unsigned long long band_fill[kBandWidths][kRBuckets];
   unsigned long long band_next[kBandWidths];              // work-queue heads of the band launches
+  unsigned long long band_total[kBandWidths];             // routed items per width class
+  unsigned long long promoted[kBandWidths];               // items promoted from the next narrower class
   unsigned long long full_count[16];                      // fallback items per full-DP variant
   unsigned long long audit_count;
   unsigned long long fallback_edge;                       // pairs sent back by the edge check
   unsigned long long fallback_route;                      // pairs routed to the full DP up front
   unsigned long long band_cells;
+  unsigned long long feat_next;                           // work-queue head of the featuriser
 };
 
 struct BandParams {
@@ -72,7 +82,9 @@ struct BandParams {
   long long n_pairs;
   const int32_t* pair_read;   // [n_pairs]
   const int32_t* pair_hap;    // [n_pairs]
-  const uint64_t* hap_kmers;  // sorted keys, one slot per haplotype base
+  const uint32_t* hap_table;  // 11-mer hash tables, 2 slots per haplotype base + 4 per haplotype
+  const Unit* units;          // work units (featuriser order)
+  long long n_units;
   const uint32_t* read_kmers; // 11-mer code per read position
   int32_t* dstar;             // [n_pairs] seed diagonal (INT32_MIN: no seed)
   int32_t* kmin;              // [n_pairs] lowest / highest diagonal of a shared 11-mer
@@ -103,8 +115,8 @@ struct BandParams {
 cudaError_t launch_pairs_from_units(const Unit* units, long long n_units, int32_t* pair_read, int32_t* pair_hap,
                                     int sms, cudaStream_t st);
 cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint32_t* codes, int sms, cudaStream_t st);
-cudaError_t launch_hap_kmers(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint64_t* keys,
-                             cudaStream_t st);
+cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint32_t* table,
+                             int sms, cudaStream_t st);
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st);
 cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st);
 cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st);

@@ -26,7 +26,14 @@ constexpr int kHapTail = 48;
 // Reference constants (Context.h:104-110, 144-150; pairhmm_common.h:16).
 constexpr double kMinAccepted = 1e-28;
 
+// Per-quality FP32 probabilities for the banded kernel: p = 10^(-q/10),
+// 1 - p, p / 3 and 1 / p, one 16-byte load per quality byte.
+struct alignas(16) QProb {
+  float p, q, third, inv;
+};
+
 struct Tables {
+  QProb qp[128];
   float ph2pr_f[128];
   float mm_f[kMMEntries];
   double ph2pr_d[128];

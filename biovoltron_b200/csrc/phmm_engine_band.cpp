@@ -42,7 +42,9 @@ BandParams Engine::band_params() const {
   p.n_pairs = n_results_;
   p.pair_read = d_pair_read_.as<int32_t>();
   p.pair_hap = d_pair_hap_.as<int32_t>();
-  p.hap_kmers = d_hap_kmers_.as<uint64_t>();
+  p.hap_table = d_hap_table_.as<uint32_t>();
+  p.units = d_units_.as<Unit>();
+  p.n_units = (long long)units_.size();
   p.read_kmers = d_read_kmers_.as<uint32_t>();
   p.dstar = d_dstar_.as<int32_t>();
   p.kmin = d_kmin_.as<int32_t>();
@@ -76,7 +78,7 @@ bv_status Engine::band_prepare() {
   BV_CUDA(prepare_band_kernels(), "band kernel attributes");
   BV_CUDA(d_pair_read_.reserve(sizeof(int32_t) * n), "alloc pairs");
   BV_CUDA(d_pair_hap_.reserve(sizeof(int32_t) * n), "alloc pairs");
-  BV_CUDA(d_hap_kmers_.reserve(sizeof(uint64_t) * std::max<int64_t>(n_hap_bytes_, 1)), "alloc kmers");
+  BV_CUDA(d_hap_table_.reserve(sizeof(uint32_t) * (2 * std::max<int64_t>(n_hap_bytes_, 1) + 4 * n_haps_)), "alloc hap tables");
   BV_CUDA(d_read_kmers_.reserve(sizeof(uint32_t) * std::max<int64_t>(n_read_bytes_, 1)), "alloc kmers");
   BV_CUDA(d_dstar_.reserve(sizeof(int32_t) * n), "alloc seeds");
   BV_CUDA(d_kmin_.reserve(sizeof(int32_t) * n), "alloc seeds");
@@ -125,7 +127,7 @@ bv_status Engine::enqueue_band(bool capturing, KernelParams& kp) {
   (void)capturing;
   BandParams p = band_params();
   BV_CUDA(cudaMemsetAsync(d_bctr_.get(), 0, sizeof(BandCounters), stream_), "memset band counters");
-  BV_CUDA(launch_hap_kmers(p.batch.hap_bases, p.batch.hap_off, n_haps_, d_hap_kmers_.as<uint64_t>(), stream_), "kmers");
+  BV_CUDA(launch_hap_table(p.batch.hap_bases, p.batch.hap_off, n_haps_, d_hap_table_.as<uint32_t>(), sms_, stream_), "hap tables");
   BV_CUDA(launch_read_kmers(p.batch.read_bases, n_read_bytes_, d_read_kmers_.as<uint32_t>(), sms_, stream_), "kmers");
   BV_CUDA(launch_featurize(p, sms_, stream_), "featurize");
   if (p.use_mlp) BV_CUDA(launch_mlp_forward(p, sms_, stream_), "mlp");
@@ -179,6 +181,8 @@ bv_status Engine::band_stats(bv_phmm_stats* st) {
   st->band_fallback = (int64_t)bc.fallback_edge;
   st->band_routed_full = (int64_t)bc.fallback_route;
   st->band_cells = (int64_t)bc.band_cells;
+  st->band_promoted = 0;
+  for (int c = 0; c < kBandWidths; ++c) st->band_promoted += (int64_t)bc.promoted[c];
   const long long na = std::min<long long>((long long)bc.audit_count, audit_cap_);
   st->audit_pairs = band_opt_.audit_period > 0 ? na : 0;
   st->audit_max_err = 0;
@@ -211,8 +215,7 @@ bv_status Engine::band_routes(int64_t n, int32_t* d_lo, int32_t* width, int32_t*
   std::fill(width, width + n, 0);
   std::fill(route, route + n, 1);
   for (int c = 0; c < kBandWidths; ++c) {
-    unsigned long long cnt = 0;
-    for (int b = 0; b < kRBuckets; ++b) cnt += bc.band_count[c][b];
+    unsigned long long cnt = bc.band_total[c] + bc.promoted[c];
     cnt = std::min<unsigned long long>(cnt, (unsigned long long)item_cap_);
     std::vector<BandItem> it(cnt);
     if (cnt) BV_CUDA(cudaMemcpy(it.data(), d_band_items_.as<BandItem>() + (size_t)c * item_cap_, sizeof(BandItem) * cnt,

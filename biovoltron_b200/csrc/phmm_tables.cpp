@@ -66,6 +66,10 @@ void build_tables(Tables* t) {
   for (int x = 0; x < 128; ++x) {
     t->ph2pr_d[x] = std::pow(10.0, -((double)x) / 10.0);
     t->ph2pr_f[x] = powf(10.f, -((float)x) / 10.f);
+    t->qp[x].p = t->ph2pr_f[x];
+    t->qp[x].q = 1.f - t->ph2pr_f[x];
+    t->qp[x].third = t->ph2pr_f[x] / 3.f;
+    t->qp[x].inv = 1.f / t->ph2pr_f[x];
   }
   fill_mm<float>(t->mm_f);
   fill_mm<double>(t->mm_d);

@@ -90,6 +90,7 @@ typedef struct bv_phmm_stats {
   int64_t audit_pairs;      /* banded pairs also scored by the full DP */
   double audit_max_err;     /* max |log10 band - log10 full| over the audit pairs */
   double audit_p99_err;     /* 99th percentile of the same */
+  int64_t band_promoted;    /* banded pairs retried on the next wider band after the edge check */
 } bv_phmm_stats;
 
 typedef struct bv_phmm_ctx bv_phmm_ctx;

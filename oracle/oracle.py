@@ -231,21 +231,37 @@ class Reference:
         }
 
 
-def seed_diagonal(read: bytes, hap: bytes, k: int = 11):
-    """The featuriser's seed diagonal: the most frequent j - i over shared
-    k-mers (read position i, haplotype position j, A/C/G/T only), smallest on
-    ties; None without a shared k-mer."""
-    if len(read) < k or len(hap) < k:
-        return None
+SEED_STRIDE = 5
+
+
+def _sample_positions(read_len: int, k: int):
+    """Read positions whose k-mers the featuriser looks up: 0, SEED_STRIDE,
+    2 SEED_STRIDE, ... and the last one, read_len - k."""
+    last = read_len - k
+    pos = list(range(0, last + 1, SEED_STRIDE))
+    if pos[-1] != last:
+        pos.append(last)
+    return pos
+
+
+def _seed_hits(read: bytes, hap: bytes, k: int):
     idx = {}
     for j in range(len(hap) - k + 1):
         s = hap[j:j + k]
         if all(c in b"ACGT" for c in s):
             idx.setdefault(s, []).append(j)
+    return [(i, j - i) for i in _sample_positions(len(read), k) for j in idx.get(read[i:i + k], ())]
+
+
+def seed_diagonal(read: bytes, hap: bytes, k: int = 11):
+    """The featuriser's seed diagonal: the most frequent j - i over the shared
+    k-mers (haplotype position j, sampled read position i, A/C/G/T only),
+    smallest on ties; None without a shared k-mer."""
+    if len(read) < k or len(hap) < k:
+        return None
     counts = {}
-    for i in range(len(read) - k + 1):
-        for j in idx.get(read[i:i + k], ()):
-            counts[j - i] = counts.get(j - i, 0) + 1
+    for _, d in _seed_hits(read, hap, k):
+        counts[d] = counts.get(d, 0) + 1
     if not counts:
         return None
     best = max(counts.values())
@@ -257,21 +273,16 @@ END_ROWS = 24
 
 def seed_extent(read: bytes, hap: bytes, k: int = 11):
     """The featuriser's band extent, or None without a shared k-mer: the
-    lowest and highest diagonal j - i of a shared k-mer, widened by the read
-    ends' triangles -- t_pre = first read position with a hit, t_suf = read
-    bases after the last hit; the first hit's diagonal + t_pre and the last
+    lowest and highest diagonal j - i of a shared (sampled) k-mer, widened by
+    the read ends' triangles -- t_pre = first sampled read position with a
+    hit, t_suf = read bases after the last sampled hit; the first hit's diagonal + t_pre and the last
     hit's diagonal - t_suf (smallest diagonal where a position has several
     hits) are included, and so is d - tail (d + head) for every voted
     diagonal d whose last hit leaves tail <= END_ROWS read bases after it
     (whose first hit starts head <= END_ROWS bases into the read)."""
     if len(read) < k or len(hap) < k:
         return None
-    idx = {}
-    for j in range(len(hap) - k + 1):
-        s = hap[j:j + k]
-        if all(c in b"ACGT" for c in s):
-            idx.setdefault(s, []).append(j)
-    hits = [(i, j - i) for i in range(len(read) - k + 1) for j in idx.get(read[i:i + k], ())]
+    hits = _seed_hits(read, hap, k)
     if not hits:
         return None
     ds = [d for _, d in hits]
