@@ -139,6 +139,7 @@ constexpr int kFeatWarps = 8;
 constexpr int kHitCap = 256;
 constexpr int kEndRows = 24;   // horizon of the per-diagonal end triangles
 constexpr int kUnitChunk = 32;
+constexpr int kCtlInts = 72;  // chunk control block of the featuriser (ints)
 constexpr int kHistSlots = kBandMaxRead + kBandMaxHap;  // d + R in [0, R + H)
 // histogram slot: votes << 18 | first read position << 9 | last read position
 // (read positions < 2^9 because reads over kBandMaxRead bases are not banded)
@@ -150,21 +151,92 @@ __device__ __forceinline__ void no_seed(const BandParams& p, long long pi, int l
   for (int x = lane; x < kFeat; x += 32) f[x] = __float2bfloat16(0.f);
 }
 
+// Sampling stride of a read of R bases: kSeedStride, or wider so that at
+// most 32 positions (0, stride, 2 stride, ... and R - 11) are sampled.
+__device__ __forceinline__ int seed_stride(int last_pos) { return max(kSeedStride, (last_pos + 30) / 31); }
+
 __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, const uint32_t* tbl, uint32_t* hist,
                                int* hits, int* nhit, int lane) {
   const int64_t ro = p.batch.read_off[r], ho = p.batch.hap_off[h];
   const int R = (int)(p.batch.read_off[r + 1] - ro), H = (int)(p.batch.hap_off[h + 1] - ho);
   __nv_bfloat16* f = p.feat + pi * kFeat;
   const uint32_t nb = (uint32_t)(H + 1) / 2;
-  if (lane == 0) *nhit = 0;
-  __syncwarp();
-  const uint32_t* rcode = p.read_kmers + ro;
   const int last_pos = R - kK;
-  const int n_samp = last_pos / kSeedStride + 1 + (last_pos % kSeedStride != 0);
-  for (int t0 = 0; t0 < n_samp; t0 += 32) {
-    const int t = t0 + lane;
-    const int i = min(t * kSeedStride, last_pos);
-    const uint32_t code = t < n_samp ? rcode[i] : kNoCode;
+  const int stride = seed_stride(last_pos);
+  const int q_s = stride == kSeedStride ? last_pos / kSeedStride : last_pos / stride;
+  const int n_samp = q_s + 1 + (q_s * stride != last_pos);  // <= 32
+  // lane t looks up the 11-mer at sampled position i: every occurrence in
+  // the haplotype is a vote for slot d + R (d = j - i)
+  const int i = min(lane * stride, last_pos);
+  const uint32_t code = lane < n_samp ? p.read_kmers[ro + i] : kNoCode;
+  int v0 = -1, nv = 0;
+  if (code != kNoCode) {
+    uint32_t bk = tbl_bucket(code, nb);
+    for (uint32_t guard = 0; guard < nb; ++guard) {
+      const uint4 q = *reinterpret_cast<const uint4*>(tbl + 4 * bk);
+      const uint32_t e4[4] = {q.x, q.y, q.z, q.w};
+      bool has_free = false;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (e4[k] == kEmpty) { has_free = true; continue; }
+        if ((e4[k] >> 10) == code) {
+          if (nv == 0) v0 = (int)(e4[k] & 1023u) - i + R;
+          ++nv;
+        }
+      }
+      if (has_free) break;
+      bk = bk + 1 == nb ? 0 : bk + 1;
+    }
+  }
+  // summary of the votes: mode (most votes, smallest slot on ties), voted
+  // extent, first and last sampled hit (smallest slot on ties), per-diagonal
+  // end triangles, vote total, and the 64 histogram bins around the mode
+  uint32_t best = 0u, fkey = 0xffffffffu, lkey = 0u;
+  int smin = INT32_MAX, smax = -1, tri_lo = INT32_MAX, tri_hi = INT32_MIN, total = 0;
+  bool overflow = false;
+  int* wbin = hits;  // 64 bins (fast path)
+  const bool fast = !__any_sync(0xffffffffu, nv > 1);
+  if (fast) {
+    // at most one vote per lane: group the lanes by slot
+    const bool valid = nv == 1;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    const unsigned peers = __match_any_sync(0xffffffffu, valid ? v0 : -1);
+    const bool lead = valid && (__ffs(peers) - 1) == lane;
+    if (valid) {
+      const uint32_t c = (uint32_t)__popc(peers);
+      best = (c << 16) | (0xffffu - (uint32_t)v0);
+      fkey = ((uint32_t)i << 16) | (uint32_t)v0;
+      lkey = ((uint32_t)i << 16) | (0xffffu - (uint32_t)v0);
+      smin = smax = v0;
+    }
+    if (lead) {  // the leader is the group's first sampled position, its highest lane the last
+      const int la = min((31 - __clz(peers)) * stride, last_pos);
+      const int d = v0 - R, tail = R - kK - la, head = i;
+      if (tail <= kEndRows) tri_lo = d - tail;
+      if (head <= kEndRows) tri_hi = d + head;
+    }
+    total = __popc(vmask);
+    for (int o = 16; o > 0; o >>= 1) {
+      best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+      fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
+      lkey = max(lkey, __shfl_xor_sync(0xffffffffu, lkey, o));
+      smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+      smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+      tri_lo = min(tri_lo, __shfl_xor_sync(0xffffffffu, tri_lo, o));
+      tri_hi = max(tri_hi, __shfl_xor_sync(0xffffffffu, tri_hi, o));
+    }
+    wbin[lane] = 0;
+    wbin[lane + 32] = 0;
+    __syncwarp();
+    if (lead && best != 0u) {
+      const int b = v0 - ((int)(0xffffu - (best & 0xffffu)) - kHistBins / 2);
+      if (b >= 0 && b < kHistBins) wbin[b] = __popc(peers);
+    }
+    __syncwarp();
+  } else {
+    // repeated 11-mers: per-warp histogram in shared memory
+    if (lane == 0) *nhit = 0;
+    __syncwarp();
     int bk = code != kNoCode ? (int)tbl_bucket(code, nb) : -1;
     for (;;) {
       uint32_t hitmask = 0u;  // slots of the loaded bucket holding this code
@@ -191,7 +263,7 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
             // one leader per slot; peers' sampled positions are those of their lanes
             const int hl = 31 - __clz(peers);
             const uint32_t n = (uint32_t)__popc(peers);
-            const uint32_t i_hi = (uint32_t)min((t0 + hl) * kSeedStride, last_pos);
+            const uint32_t i_hi = (uint32_t)min(hl * stride, last_pos);
             const uint32_t old = hist[vote];
             if (old == 0u) {
               hist[vote] = (n << 18) | ((uint32_t)i << 9) | i_hi;
@@ -207,37 +279,32 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
       }
       if (!__any_sync(0xffffffffu, bk >= 0)) break;
     }
-  }
-  __syncwarp();
-  const int nh = min(*nhit, kHitCap);
-  const bool overflow = *nhit > kHitCap;
-  // one pass over the voted diagonals: mode (most votes, smallest slot on
-  // ties), voted extent, first and last sampled hit (smallest slot on ties),
-  // per-diagonal end triangles, vote total
-  uint32_t best = 0u, fkey = 0xffffffffu, lkey = 0u;
-  int smin = INT32_MAX, smax = -1, tri_lo = INT32_MAX, tri_hi = INT32_MIN, total = 0;
-  for (int x = lane; x < nh; x += 32) {
-    const int sl = hits[x];
-    const uint32_t v = hist[sl], c = v >> 18, fi = (v >> 9) & 511u, la = v & 511u;
-    best = max(best, (c << 16) | (0xffffu - (uint32_t)sl));
-    fkey = min(fkey, (fi << 16) | (uint32_t)sl);
-    lkey = max(lkey, (la << 16) | (0xffffu - (uint32_t)sl));
-    smin = min(smin, sl);
-    smax = max(smax, sl);
-    const int d = sl - R, tail = R - kK - (int)la, head = (int)fi;
-    if (tail <= kEndRows) tri_lo = min(tri_lo, d - tail);
-    if (head <= kEndRows) tri_hi = max(tri_hi, d + head);
-    total += (int)c;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-    fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
-    lkey = max(lkey, __shfl_xor_sync(0xffffffffu, lkey, o));
-    smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
-    smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
-    tri_lo = min(tri_lo, __shfl_xor_sync(0xffffffffu, tri_lo, o));
-    tri_hi = max(tri_hi, __shfl_xor_sync(0xffffffffu, tri_hi, o));
-    total += __shfl_xor_sync(0xffffffffu, total, o);
+    __syncwarp();
+    const int nh = min(*nhit, kHitCap);
+    overflow = *nhit > kHitCap;
+    for (int x = lane; x < nh; x += 32) {
+      const int sl = hits[x];
+      const uint32_t v = hist[sl], c = v >> 18, fi = (v >> 9) & 511u, la = v & 511u;
+      best = max(best, (c << 16) | (0xffffu - (uint32_t)sl));
+      fkey = min(fkey, (fi << 16) | (uint32_t)sl);
+      lkey = max(lkey, (la << 16) | (0xffffu - (uint32_t)sl));
+      smin = min(smin, sl);
+      smax = max(smax, sl);
+      const int d = sl - R, tail = R - kK - (int)la, head = (int)fi;
+      if (tail <= kEndRows) tri_lo = min(tri_lo, d - tail);
+      if (head <= kEndRows) tri_hi = max(tri_hi, d + head);
+      total += (int)c;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+      fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
+      lkey = max(lkey, __shfl_xor_sync(0xffffffffu, lkey, o));
+      smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+      smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+      tri_lo = min(tri_lo, __shfl_xor_sync(0xffffffffu, tri_lo, o));
+      tri_hi = max(tri_hi, __shfl_xor_sync(0xffffffffu, tri_hi, o));
+      total += __shfl_xor_sync(0xffffffffu, total, o);
+    }
   }
   if (best == 0u) {
     no_seed(p, pi, lane);
@@ -265,11 +332,11 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
     const int mis_suf = __popc(__ballot_sync(0xffffffffu, ms));
     // 64 histogram bins d* - 32 .. d* + 31, two adjacent bins per lane
     int win = 0, nonzero = 0, peak = 0;
-    const float inv = 1.f / (float)n_samp;
+    const float inv = __frcp_rn((float)n_samp);
     int cb[2];
     for (int t = 0; t < 2; ++t) {
       const int s = best_slot - kHistBins / 2 + 2 * lane + t;
-      cb[t] = (s >= 0 && s < R + H) ? (int)(hist[s] >> 18) : 0;
+      cb[t] = fast ? wbin[2 * lane + t] : (s >= 0 && s < R + H) ? (int)(hist[s] >> 18) : 0;
       win += cb[t];
       nonzero += cb[t] > 0;
       peak = max(peak, cb[t]);
@@ -287,7 +354,7 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
                            (float)(total - win) * inv,
                            (float)R / 256.f,
                            (float)H / 1024.f,
-                           (float)(ds + R) / (float)(R + H),
+                           __fdividef((float)(ds + R), (float)(R + H)),
                            1.f,
                            (float)peak * inv,
                            (float)nonzero / (float)kHistBins,
@@ -317,10 +384,12 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
     }
   }
   __syncwarp();
-  if (overflow) {
-    for (int x = lane; x < R + H; x += 32) hist[x] = 0u;
-  } else {
-    for (int x = lane; x < nh; x += 32) hist[hits[x]] = 0u;
+  if (!fast) {
+    if (overflow) {
+      for (int x = lane; x < R + H; x += 32) hist[x] = 0u;
+    } else {
+      for (int x = lane, nh = min(*nhit, kHitCap); x < nh; x += 32) hist[hits[x]] = 0u;
+    }
   }
   __syncwarp();
 }
@@ -332,9 +401,10 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
   // first haplotype; per warp: histogram and voted-slot list
   uint32_t* tbl = reinterpret_cast<uint32_t*>(smem);
   Unit* su = reinterpret_cast<Unit*>(smem + (size_t)(2 * kBandMaxHap + 4) * 4);
-  int* sctl = reinterpret_cast<int*>(su + kUnitChunk);  // [0] chunk, [1] max nh
-  uint32_t* hist = reinterpret_cast<uint32_t*>(sctl + 4) + (size_t)wib * kHistSlots;
-  int* hits = reinterpret_cast<int*>(sctl + 4) + (size_t)kFeatWarps * kHistSlots + (size_t)wib * (kHitCap + 1);
+  // [0] chunk, [1] max nh, [2] groups, [3..3+33) group starts, [36..68) group max nh
+  int* sctl = reinterpret_cast<int*>(su + kUnitChunk);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(sctl + kCtlInts) + (size_t)wib * kHistSlots;
+  int* hits = reinterpret_cast<int*>(sctl + kCtlInts) + (size_t)kFeatWarps * kHistSlots + (size_t)wib * (kHitCap + 1);
   int* nhit = hits + kHitCap;
   for (int x = lane; x < kHistSlots; x += 32) hist[x] = 0u;
   const long long nchunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
@@ -347,28 +417,39 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
     const long long u0 = c * kUnitChunk;
     const int nu = (int)min((long long)kUnitChunk, p.n_units - u0);
     if (wib == 0) {
+      // sort the units by first haplotype; groups of equal first haplotype
       Unit un{};
       if (lane < nu) un = p.units[u0 + lane];
       const long long key = lane < nu ? ((long long)un.hap0 << 5) | lane : LLONG_MAX;
       int rank = 0;
       for (int o = 0; o < 32; ++o) rank += __shfl_sync(0xffffffffu, key, o) < key;
       if (lane < nu) su[rank] = un;
-      int mx = lane < nu ? un.nh : 0;
+      __syncwarp();
+      const int hap_r = lane < nu ? su[lane].hap0 : -1, nh_r = lane < nu ? su[lane].nh : 0;
+      // lane q (in sorted order) starts a group when its first haplotype differs from lane q - 1's
+      const int prev = __shfl_up_sync(0xffffffffu, hap_r, 1);
+      const bool start = lane < nu && (lane == 0 || prev != hap_r);
+      const unsigned starts = __ballot_sync(0xffffffffu, start);
+      const int g = __popc(starts & ((2u << lane) - 1u)) - 1;  // group of sorted lane q
+      int gmax = lane < nu ? nh_r : 0;  // max nh within the group (segmented reduction)
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_down_sync(0xffffffffu, gmax, o);
+        const int gv = __shfl_down_sync(0xffffffffu, g, o);
+        if (lane + o < nu && gv == g) gmax = max(gmax, v);
+      }
+      if (start) { sctl[3 + g] = lane; sctl[36 + g] = gmax; }
+      int mx = lane < nu ? nh_r : 0;
       for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      if (lane == 0) sctl[1] = mx;
+      if (lane == 0) { sctl[1] = mx; sctl[2] = __popc(starts); sctl[3 + __popc(starts)] = nu; }
     }
     __syncthreads();
-    const int max_nh = sctl[1];
+    const int max_nh = sctl[1], ngroups = sctl[2];
     for (int k = 0; k < max_nh; ++k) {
-      for (int q0 = 0; q0 < nu;) {
-        // a group: consecutive units with the same first haplotype, so one haplotype h
-        const int hap0 = su[q0].hap0;
-        int q1 = q0 + 1;
-        while (q1 < nu && su[q1].hap0 == hap0) ++q1;
-        const int h = hap0 + k;
-        bool any = false;
-        for (int q = q0; q < q1; ++q) any |= k < su[q].nh;
-        if (any) {
+      for (int gi = 0; gi < ngroups; ++gi) {
+        // a group: consecutive sorted units with the same first haplotype, so one haplotype h
+        const int q0 = sctl[3 + gi], q1 = sctl[4 + gi];
+        const int h = su[q0].hap0 + k;
+        if (k < sctl[36 + gi]) {
           const int64_t ho = p.batch.hap_off[h];
           const int H = (int)(p.batch.hap_off[h + 1] - ho);
           const bool tab = H >= kK && H <= kBandMaxHap;
@@ -390,7 +471,6 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
           }
           __syncthreads();  // before the table is restaged
         }
-        q0 = q1;
       }
     }
   }
@@ -917,7 +997,7 @@ cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, l
   return cudaGetLastError();
 }
 
-constexpr int kFeatSmem = (2 * kBandMaxHap + 4) * 4 + kUnitChunk * (int)sizeof(Unit) + 16 +
+constexpr int kFeatSmem = (2 * kBandMaxHap + 4) * 4 + kUnitChunk * (int)sizeof(Unit) + kCtlInts * 4 +
                           kFeatWarps * (kHistSlots + kHitCap + 1) * 4;
 
 cudaError_t prepare_band_kernels() {

@@ -235,10 +235,12 @@ SEED_STRIDE = 5
 
 
 def _sample_positions(read_len: int, k: int):
-    """Read positions whose k-mers the featuriser looks up: 0, SEED_STRIDE,
-    2 SEED_STRIDE, ... and the last one, read_len - k."""
+    """Read positions whose k-mers the featuriser looks up: 0, s, 2 s, ...
+    and the last one, read_len - k, with s = max(SEED_STRIDE, ceil(last / 31))
+    so that at most 32 positions are sampled."""
     last = read_len - k
-    pos = list(range(0, last + 1, SEED_STRIDE))
+    stride = max(SEED_STRIDE, (last + 30) // 31)
+    pos = list(range(0, last + 1, stride))
     if pos[-1] != last:
         pos.append(last)
     return pos
