@@ -218,6 +218,7 @@ def main():
     ap.add_argument("--regions", type=int, default=0, help="config1 only: fewer regions (profiling cases)")
     ap.add_argument("--ref-seconds", type=float, default=10.0, help="CPU seconds per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--haps-per-warp", type=int, default=0, help="0: engine default, 1 or 2")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -230,7 +231,7 @@ def main():
 
     batch = make_workload(args.workload, args.seed + 1000 * rank, args.regions)
     log(f"[rank {rank}] workload: {batch.name}: {batch.n_pairs} pairs, {batch.n_cells():.3e} cells")
-    eng = PairHMMEngine(device=local)
+    eng = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp)
     lib = load()
     peak = C.c_double(0)
     st = lib.bv_phmm_measure_fp32_peak(local, C.byref(peak))

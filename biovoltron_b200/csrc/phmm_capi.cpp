@@ -112,6 +112,7 @@ bv_status bv_phmm_create(const bv_phmm_options* opts, bv_phmm_ctx** out) {
   if (o.precision != BV_PRECISION_AUTO && o.precision != BV_PRECISION_F64) return BV_ERR_INVALID_ARG;
   if (o.mode != BV_MODE_FULL && o.mode != BV_MODE_BAND) return BV_ERR_INVALID_ARG;
   if (o.rescue_threshold != bvphmm::kMinAccepted) return BV_ERR_UNSUPPORTED;
+  if (o.haps_per_warp < 0 || o.haps_per_warp > 2) return BV_ERR_INVALID_ARG;
   bv_phmm_ctx* c = new (std::nothrow) bv_phmm_ctx(o);
   if (!c) return BV_ERR_OOM;
   bv_status s = guard(c, [&] { return c->engine.init(); });

@@ -16,53 +16,103 @@
 namespace bvphmm {
 
 
-// Emission-table chunk: the widest shared-memory load whose lanes fall in
-// distinct banks for the rows a lane owns (4, 8 or 16 bytes per lane).
-template <typename T, int RT> struct EChunk;
-template <int RT> struct EChunk<float, RT> {
-  static constexpr int n = RT >= 3 ? 4 : RT;
-  using type = typename std::conditional<n == 4, float4, typename std::conditional<n == 2, float2, float>::type>::type;
-};
-template <int RT> struct EChunk<double, RT> {
-  static constexpr int n = RT >= 2 ? 2 : 1;
-  using type = typename std::conditional<n == 2, double2, double>::type;
-};
-
-template <typename V, typename T> __device__ __forceinline__ void unpack(const V& v, T* e);
-template <> __device__ __forceinline__ void unpack(const float4& v, float* e) { e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w; }
-template <> __device__ __forceinline__ void unpack(const float2& v, float* e) { e[0] = v.x; e[1] = v.y; }
-template <> __device__ __forceinline__ void unpack(const float& v, float* e) { e[0] = v; }
-template <> __device__ __forceinline__ void unpack(const double2& v, double* e) { e[0] = v.x; e[1] = v.y; }
-template <> __device__ __forceinline__ void unpack(const double& v, double* e) { e[0] = v; }
-// Full-width shared-memory loads of an emission-table chunk.  Written in PTX
-// so the compiler cannot narrow a 16-byte load whose upper values a variant
-// does not use (a narrowed load keeps the 16-byte lane stride and conflicts).
-template <typename V> __device__ __forceinline__ V lds_chunk(const void* p);
-template <> __device__ __forceinline__ float4 lds_chunk<float4>(const void* p) {
+// Shared-memory loads written in PTX (full vector width).
+__device__ __forceinline__ float4 lds4f(const unsigned char* p) {
   float4 v;
   asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
       : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
       : "r"((unsigned)__cvta_generic_to_shared(p)));
   return v;
 }
-template <> __device__ __forceinline__ float2 lds_chunk<float2>(const void* p) {
+__device__ __forceinline__ float2 lds2f(const unsigned char* p) {
   float2 v;
   asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"((unsigned)__cvta_generic_to_shared(p)));
   return v;
 }
-template <> __device__ __forceinline__ float lds_chunk<float>(const void* p) { return *static_cast<const float*>(p); }
-template <> __device__ __forceinline__ double2 lds_chunk<double2>(const void* p) {
+__device__ __forceinline__ double2 lds2d(const unsigned char* p) {
   double2 v;
   asm("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"((unsigned)__cvta_generic_to_shared(p)));
   return v;
 }
-template <> __device__ __forceinline__ double lds_chunk<double>(const void* p) { return *static_cast<const double*>(p); }
 
-__device__ __forceinline__ float4 pack4(const float* v, float4*) { return make_float4(v[0], v[1], v[2], v[3]); }
-__device__ __forceinline__ float2 pack4(const float* v, float2*) { return make_float2(v[0], v[1]); }
-__device__ __forceinline__ float pack4(const float* v, float*) { return v[0]; }
-__device__ __forceinline__ double2 pack4(const double* v, double2*) { return make_double2(v[0], v[1]); }
-__device__ __forceinline__ double pack4(const double* v, double*) { return v[0]; }
+// Emission table of one warp.  For each haplotype code, a block of
+// 32 * RT values: every lane's RT rows, split into chunks of Wm = 16 /
+// sizeof(T) rows (4 FP32, 2 FP64) and, for the remainder, one chunk of 2
+// and/or one of 1 row.  Chunk region r of width w holds lane l's rows at
+// region + l * w * sizeof(T), so one load per chunk covers 32 * w
+// consecutive words: bank-conflict free, and a lookup of all RT rows moves
+// exactly RT * 128 bytes (RT shared-memory wavefronts for FP32).
+template <typename T, int RT>
+struct ETab {
+  static constexpr int Wm = 16 / (int)sizeof(T);
+  static constexpr int NF = RT / Wm;                                   // full-width chunks
+  static constexpr bool kHalf = Wm == 4 && (RT % Wm) >= 2;            // FP32 only: a 2-row chunk
+  static constexpr bool kOne = (RT % 2) == 1;                          // a 1-row chunk
+  static constexpr int kOffHalf = NF * kWarp * 16;
+  static constexpr int kOffOne = kOffHalf + (kHalf ? kWarp * 2 * (int)sizeof(T) : 0);
+  static constexpr int kCodeStride = kWarp * RT * (int)sizeof(T);
+  static constexpr int kBytes = kCodes * kCodeStride;
+  static_assert(NF * Wm + (kHalf ? 2 : 0) + (kOne ? 1 : 0) == RT, "chunking covers the rows");
+};
+
+// A lane's three chunk bases in the warp's table.
+struct ELane {
+  const unsigned char* full;
+  const unsigned char* half;
+  const unsigned char* one;
+};
+
+template <typename T, int RT>
+__device__ __forceinline__ ELane elane(const unsigned char* etab, int lane) {
+  using E = ETab<T, RT>;
+  return ELane{etab + lane * 16, etab + E::kOffHalf + lane * 2 * (int)sizeof(T),
+               etab + E::kOffOne + lane * (int)sizeof(T)};
+}
+
+// Loads the lane's RT emissions for the code whose block starts at `off`.
+template <typename T, int RT>
+__device__ __forceinline__ void load_emissions(const ELane& el, unsigned off, T* e) {
+  using E = ETab<T, RT>;
+#pragma unroll
+  for (int ch = 0; ch < E::NF; ++ch) {
+    if constexpr (sizeof(T) == 4) {
+      const float4 v = lds4f(el.full + off + ch * kWarp * 16);
+      e[4 * ch] = v.x; e[4 * ch + 1] = v.y; e[4 * ch + 2] = v.z; e[4 * ch + 3] = v.w;
+    } else {
+      const double2 v = lds2d(el.full + off + ch * kWarp * 16);
+      e[2 * ch] = v.x; e[2 * ch + 1] = v.y;
+    }
+  }
+  if constexpr (E::kHalf) {
+    const float2 v = lds2f(el.half + off);
+    e[E::NF * 4] = v.x; e[E::NF * 4 + 1] = v.y;
+  }
+  if constexpr (E::kOne) {
+    e[RT - 1] = *reinterpret_cast<const T*>(el.one + off);
+  }
+}
+
+// Stores the lane's RT emissions of one code (set-up).
+template <typename T, int RT>
+__device__ __forceinline__ void store_emissions(unsigned char* etab, int lane, int code, const T* v) {
+  using E = ETab<T, RT>;
+  unsigned char* blk = etab + code * E::kCodeStride;
+#pragma unroll
+  for (int ch = 0; ch < E::NF; ++ch) {
+    if constexpr (sizeof(T) == 4) {
+      *reinterpret_cast<float4*>(blk + ch * kWarp * 16 + lane * 16) =
+          make_float4(v[4 * ch], v[4 * ch + 1], v[4 * ch + 2], v[4 * ch + 3]);
+    } else {
+      *reinterpret_cast<double2*>(blk + ch * kWarp * 16 + lane * 16) = make_double2(v[2 * ch], v[2 * ch + 1]);
+    }
+  }
+  if constexpr (E::kHalf) {
+    *reinterpret_cast<float2*>(blk + E::kOffHalf + lane * 8) = make_float2(v[E::NF * 4], v[E::NF * 4 + 1]);
+  }
+  if constexpr (E::kOne) {
+    *reinterpret_cast<T*>(blk + E::kOffOne + lane * (int)sizeof(T)) = v[RT - 1];
+  }
+}
 
 __device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
@@ -88,13 +138,8 @@ __device__ __forceinline__ int mm_index(int ins, int del) {
 // Shared-memory layout of one warp's slice.
 template <typename T, int RT>
 struct WarpSmem {
-  static constexpr int VPC = EChunk<T, RT>::n;             // emission values per chunk
-  static constexpr int CB = VPC * (int)sizeof(T);          // chunk bytes = lane stride
-  static constexpr int RTP = (RT + VPC - 1) / VPC * VPC;   // rows rounded to chunks
-  static constexpr int NCH = RTP / VPC;                    // chunks per code
-  static constexpr int kChunkStride = kWarp * CB;          // bytes between a lane's chunks
-  static constexpr int kCodeStride = NCH * kChunkStride;   // bytes per code
-  static constexpr int kEtabBytes = kCodes * kCodeStride;
+  static constexpr int kCodeStride = ETab<T, RT>::kCodeStride;  // bytes per code
+  static constexpr int kEtabBytes = ETab<T, RT>::kBytes;
   static constexpr int kRingInCols = 64;
   static constexpr int kRingOutCols = 32;
   static constexpr int kColBytes = 4 * (int)sizeof(T);     // M, Xh, Yh, unused
@@ -135,16 +180,14 @@ struct Rows {
 template <typename T, int RT>
 __device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const uchar4* __restrict__ quals,
                                            const uint8_t* __restrict__ bases, int R, int rbase, T init_y,
-                                           Rows<T, RT>& rw, unsigned char* etab_lane) {
-  using S = WarpSmem<T, RT>;
-  using V = typename EChunk<T, RT>::type;
+                                           Rows<T, RT>& rw, unsigned char* etab, int lane) {
   const T* ph = ph2pr_tab<T>(tb);
   const T* mmt = mm_tab<T>(tb);
-  T em[S::RTP], ex[S::RTP];
-  uint32_t rc[S::RTP];
-  bool valid[S::RTP], sumrow[S::RTP];
+  T em[RT], ex[RT];
+  uint32_t rc[RT];
+  bool valid[RT], sumrow[RT];
 #pragma unroll
-  for (int j = 0; j < S::RTP; ++j) { em[j] = T(0); ex[j] = T(0); rc[j] = 0; valid[j] = false; sumrow[j] = false; }
+  for (int j = 0; j < RT; ++j) { em[j] = T(0); ex[j] = T(0); rc[j] = 0; valid[j] = false; sumrow[j] = false; }
 #pragma unroll
   for (int j = 0; j < RT; ++j) {
     const int r = rbase + j;
@@ -196,17 +239,13 @@ __device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const 
   // mismatch (a read or haplotype N matches everything), 0 for padding.
 #pragma unroll
   for (int h = 0; h < kCodes; ++h) {
+    T v[RT];
 #pragma unroll
-    for (int ch = 0; ch < S::NCH; ++ch) {
-      T v[4];
-#pragma unroll
-      for (int t = 0; t < S::VPC; ++t) {
-        const int j = ch * S::VPC + t;
-        const bool match = (rc[j] == (uint32_t)h) || rc[j] == 4u || h == 4;
-        v[t] = sumrow[j] ? T(1) : (valid[j] && h != kPadCode) ? (match ? em[j] : ex[j]) : T(0);
-      }
-      *reinterpret_cast<V*>(etab_lane + h * S::kCodeStride + ch * S::kChunkStride) = pack4(v, (V*)nullptr);
+    for (int j = 0; j < RT; ++j) {
+      const bool match = (rc[j] == (uint32_t)h) || rc[j] == 4u || h == 4;
+      v[j] = sumrow[j] ? T(1) : (valid[j] && h != kPadCode) ? (match ? em[j] : ex[j]) : T(0);
     }
+    store_emissions<T, RT>(etab, lane, h, v);
   }
 }
 
@@ -220,6 +259,21 @@ __device__ __forceinline__ void stage_hap(const uint8_t* __restrict__ hap, int H
   }
 }
 
+// Stages two haplotypes for a paired warp: entry x holds the emission-table
+// offsets of both haplotypes' codes at column kHapLead + c - 1 (first in the
+// low 16 bits), so one 32-bit shared load per step serves both.
+template <int STRIDE>
+__device__ __forceinline__ void stage_hap_pair(const uint8_t* __restrict__ ha, int HA, const uint8_t* __restrict__ hb,
+                                               int HB, uint32_t* hcp, int n_total, int lane) {
+  static_assert(kCodes * STRIDE <= 65536, "offsets fit 16 bits");
+  for (int x = lane; x < n_total; x += kWarp) {
+    const int c = x - kHapLead + 1;
+    const uint32_t ca = (c >= 1 && c <= HA) ? base_code(ha[c - 1]) : (uint32_t)kPadCode;
+    const uint32_t cb = (c >= 1 && c <= HB) ? base_code(hb[c - 1]) : (uint32_t)kPadCode;
+    hcp[x] = ca * STRIDE | (cb * STRIDE) << 16;
+  }
+}
+
 // One strip of the wavefront.  MULTI: lane 0 reads the row above the strip
 // from `bnd` (the previous strip's bottom row, or zeros for the first strip)
 // and lane 31 writes this strip's bottom row back to `bnd`, both through
@@ -229,12 +283,11 @@ __device__ __forceinline__ void stage_hap(const uint8_t* __restrict__ hap, int H
 // which has no summing row) and the largest bottom-row value (FP64, for
 // renormalisation between strips).
 template <typename T, int RT, bool MULTI, int CH>
-__device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned char* __restrict__ etab_lane,
+__device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
                                           const unsigned char* __restrict__ hc_lane, int nsteps, int lane,
                                           T* __restrict__ bnd, unsigned char* ring, T in_scale, T& lastM,
                                           T& lastY, T& sumM, T& sumX, T& bmax) {
   using S = WarpSmem<T, RT>;
-  using V = typename EChunk<T, RT>::type;
   constexpr bool kScale = sizeof(T) == 8;  // only the FP64 path renormalises
   constexpr bool kSums = !SumRow<T>::value;
   T M[RT], X[RT], Y[RT];
@@ -287,14 +340,8 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned 
           if constexpr (kScale) { upM *= in_scale; upX *= in_scale; upY *= in_scale; }
         }
       }
-      const unsigned code = hc_lane[s];
-      const unsigned char* ep = etab_lane + code * S::kCodeStride;
-      T e[S::RTP];
-#pragma unroll
-      for (int ch = 0; ch < S::NCH; ++ch) {
-        const V v = lds_chunk<V>(ep + ch * S::kChunkStride);
-        unpack(v, e + ch * S::VPC);
-      }
+      T e[RT];
+      load_emissions<T, RT>(el, (unsigned)hc_lane[s] * S::kCodeStride, e);
       T um = upM, ux = upX;
       T dm = dM, dx = dX, dy = dY;
 #pragma unroll
@@ -355,6 +402,69 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const unsigned 
   lastY = Y[RT - 1];
 }
 
+// Two haplotypes of one read in one warp (FP32 single strip).  Both pairs
+// share the read's row constants and emission table; their states are the
+// two halves of float2 values, so the transition arithmetic runs as packed
+// FP32x2 instructions (fma.rn.f32x2 / mul.rn.f32x2 of sm_100), which halves
+// the issue slots the FP32 pipe needs and leaves them to the shuffles and
+// shared-memory loads.  Each half follows run_strip's operation order
+// exactly, so a paired result equals the single-haplotype result bit for bit.
+__device__ __forceinline__ float2 shfl_up2(float2 v) {
+  return make_float2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
+}
+
+template <int RT>
+__device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const float* __restrict__ y0a,
+                                               const float* __restrict__ y0b, const ELane el,
+                                               const uint32_t* __restrict__ hcp_lane, int nsteps,
+                                               float2& lastM, float2& lastY) {
+  constexpr int CH = 8;
+  float2 mm[RT], cx[RT], cy[RT], kap[RT], g[RT];
+  float2 M[RT], X[RT], Y[RT];
+#pragma unroll
+  for (int j = 0; j < RT; ++j) {
+    mm[j] = make_float2(rw.mm[j], rw.mm[j]);
+    cx[j] = make_float2(rw.cx[j], rw.cx[j]);
+    cy[j] = make_float2(rw.cy[j], rw.cy[j]);
+    kap[j] = make_float2(rw.kap[j], rw.kap[j]);
+    g[j] = make_float2(rw.g[j], rw.g[j]);
+    M[j] = make_float2(0.f, 0.f);
+    X[j] = make_float2(0.f, 0.f);
+    Y[j] = make_float2(y0a[j], y0b[j]);
+  }
+  float2 upM = shfl_up2(M[RT - 1]), upX = shfl_up2(X[RT - 1]), upY = shfl_up2(Y[RT - 1]);
+  float2 dM = upM, dX = upX, dY = upY;
+  for (int s0 = 0; s0 < nsteps; s0 += CH) {
+#pragma unroll
+    for (int u = 0; u < CH; ++u) {
+      const int s = s0 + u;
+      const uint32_t offs = hcp_lane[s];
+      float ea[RT], eb[RT];
+      load_emissions<float, RT>(el, offs & 0xffffu, ea);
+      load_emissions<float, RT>(el, offs >> 16, eb);
+      float2 um = upM, ux = upX;
+      float2 dm = dM, dx = dX, dy = dY;
+#pragma unroll
+      for (int j = 0; j < RT; ++j) {
+        float2 t = __fmul2_rn(cy[j], dy);
+        t = __ffma2_rn(cx[j], dx, t);
+        t = __ffma2_rn(mm[j], dm, t);
+        const float2 mn = make_float2(ea[j] * t.x, eb[j] * t.y);
+        const float2 xn = __ffma2_rn(kap[j], ux, um);
+        const float2 yn = __ffma2_rn(g[j], Y[j], M[j]);
+        dm = M[j]; dx = X[j]; dy = Y[j];
+        um = mn; ux = xn;
+        M[j] = mn; X[j] = xn; Y[j] = yn;
+      }
+      const float2 nM = shfl_up2(M[RT - 1]), nX = shfl_up2(X[RT - 1]), nY = shfl_up2(Y[RT - 1]);
+      dM = upM; dX = upX; dY = upY;
+      upM = nM; upX = nX; upY = nY;
+    }
+  }
+  lastM = M[RT - 1];
+  lastY = Y[RT - 1];
+}
+
 template <typename T> __device__ __forceinline__ T log10_(T v);
 template <> __device__ __forceinline__ float log10_(float v) { return log10f(v); }
 template <> __device__ __forceinline__ double log10_(double v) { return log10(v); }
@@ -366,7 +476,41 @@ struct Item {
   long long out0;
 };
 
-template <typename T, int RT, bool MULTI>
+// Writes one pair's log10 likelihood (lane 31 holds the result).  FP32:
+// values below MIN_ACCEPTED or not finite go to the FP64 list (or NaN when
+// the launch has none); FP64: log10 of the renormalised sum, -inf when it
+// stayed non-positive.
+template <typename T>
+__device__ __forceinline__ void write_result(const KernelParams& p, int read, int hap, long long o, T res,
+                                             long long kexp) {
+  if (sizeof(T) == 4) {
+    if (!p.rescue && (!(res >= (T)kMinAccepted) || isinf((double)res))) {
+      p.out[o] = __longlong_as_double(0x7ff8000000000000ll);
+    } else if (!(res >= (T)kMinAccepted) || isinf((double)res)) {
+      const unsigned long long slot = atomicAdd(&p.ctr->rescue_count, 1ull);
+      if (slot < (unsigned long long)p.rescue_cap) {
+        p.rescue[slot].read = read;
+        p.rescue[slot].hap = hap;
+        p.rescue[slot].out = o;
+      } else {
+        atomicOr(&p.ctr->status, 1ull);
+      }
+      p.out[o] = __longlong_as_double(0x7ff8000000000000ll);
+    } else {
+      p.out[o] = (double)(log10_((float)res) - p.tables->log10_init_f);
+    }
+  } else {
+    const double rd = (double)res;
+    if (rd > 0.0 && isfinite(rd)) {
+      p.out[o] = log10(rd) + (double)kexp * 0.30102999566398119521 - p.tables->log10_init_d;
+    } else {
+      atomicAdd(&p.ctr->underflow_count, 1ull);
+      p.out[o] = -INFINITY;
+    }
+  }
+}
+
+template <typename T, int RT, bool MULTI, bool PAIR = false>
 __device__ void process_item(const KernelParams& p, const Item& it, unsigned char* wsm, int lane, T* bnd) {
   using S = WarpSmem<T, RT>;
   const DeviceBatch& b = p.batch;
@@ -383,18 +527,48 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
   const int pad = nstrips * strip_rows - rows;
   unsigned char* hc = wsm;
   unsigned char* etab = wsm + p.hap_bytes;
-  unsigned char* etab_lane = etab + lane * S::CB;
+  const ELane el = elane<T, RT>(etab, lane);
   unsigned char* ring = etab + S::kEtabBytes;
   const bool is_f64 = sizeof(T) == 8;
   Rows<T, RT> rw;
   if (!MULTI) {
     // single strip: rows and emission table are shared by all haplotypes
-    setup_rows<T, RT>(p.tables, quals, bases, R, lane * RT - pad, T(0), rw, etab_lane);
+    setup_rows<T, RT>(p.tables, quals, bases, R, lane * RT - pad, T(0), rw, etab, lane);
   }
   for (int k = 0; k < it.nh; ++k) {
     const int h = it.hap0 + k;
     const int64_t ho = b.hap_off[h];
     const int H = (int)(b.hap_off[h + 1] - ho);
+    if constexpr (PAIR && !MULTI && sizeof(T) == 4) {
+      if (k + 1 < it.nh && R > 0) {
+        const int64_t ho2 = b.hap_off[h + 1];
+        const int H2 = (int)(b.hap_off[h + 2] - ho2);
+        if (H > 0 && H2 > 0) {
+          const int Hm = H > H2 ? H : H2;
+          const int nsteps = (Hm + kWarp + 7) / 8 * 8;  // as the single path: H + 31 + 1 (summing row), to 8
+          uint32_t* hcp = reinterpret_cast<uint32_t*>(hc);
+          __syncwarp();
+          stage_hap_pair<S::kCodeStride>(b.hap_bases + ho, H, b.hap_bases + ho2, H2, hcp, nsteps + kHapLead, lane);
+          const T init = (T)p.tables->init_f;
+          const int r0j = pad - lane * RT;
+          float y0a[RT], y0b[RT];
+#pragma unroll
+          for (int j = 0; j < RT; ++j) {
+            y0a[j] = (j == r0j) ? init / (T)H : 0.f;
+            y0b[j] = (j == r0j) ? init / (T)H2 : 0.f;
+          }
+          __syncwarp();
+          float2 lastM, lastY;
+          run_strip_pair<RT>(rw, y0a, y0b, el, hcp + kHapLead - lane, nsteps, lastM, lastY);
+          if (lane == kWarp - 1) {
+            write_result<float>(p, it.read, h, it.out0 + k, lastY.x + lastM.x, 0);
+            write_result<float>(p, it.read, h + 1, it.out0 + k + 1, lastY.y + lastM.y, 0);
+          }
+          ++k;
+          continue;
+        }
+      }
+    }
     if (H == 0 || R == 0) {
       // An empty read or haplotype has no alignment: likelihood 0.
       if (lane == kWarp - 1) p.out[it.out0 + k] = -INFINITY;
@@ -425,9 +599,9 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
       T in_scale = T(1);
       for (int st = 0; st < nstrips; ++st) {
         __syncwarp();
-        setup_rows<T, RT>(p.tables, quals, bases, R, st * strip_rows + lane * RT - pad, init_y, rw, etab_lane);
+        setup_rows<T, RT>(p.tables, quals, bases, R, st * strip_rows + lane * RT - pad, init_y, rw, etab, lane);
         __syncwarp();
-        run_strip<T, RT, true, 32>(rw, etab_lane, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
+        run_strip<T, RT, true, 32>(rw, el, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
                                    lastY, sumM, sumX, bmax);
         __syncwarp();
         in_scale = T(1);
@@ -444,38 +618,13 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
         }
       }
     } else {
-      run_strip<T, RT, false, 8>(rw, etab_lane, hc + kHapLead - lane, nsteps, lane, nullptr, nullptr, T(1), lastM,
+      run_strip<T, RT, false, 8>(rw, el, hc + kHapLead - lane, nsteps, lane, nullptr, nullptr, T(1), lastM,
                                  lastY, sumM, sumX, bmax);
     }
     if (lane == kWarp - 1) {
       // FP32: the summing row's Y + M; FP64: the accumulated last-row sums.
       const T res = SumRow<T>::value ? lastY + lastM : sumM + sumX;
-      const long long o = it.out0 + k;
-      if (!is_f64) {
-        if (!p.rescue && (!(res >= (T)kMinAccepted) || isinf((double)res))) {
-          p.out[o] = __longlong_as_double(0x7ff8000000000000ll);
-        } else if (!(res >= (T)kMinAccepted) || isinf((double)res)) {
-          const unsigned long long slot = atomicAdd(&p.ctr->rescue_count, 1ull);
-          if (slot < (unsigned long long)p.rescue_cap) {
-            p.rescue[slot].read = it.read;
-            p.rescue[slot].hap = h;
-            p.rescue[slot].out = o;
-          } else {
-            atomicOr(&p.ctr->status, 1ull);
-          }
-          p.out[o] = __longlong_as_double(0x7ff8000000000000ll);
-        } else {
-          p.out[o] = (double)(log10_((float)res) - p.tables->log10_init_f);
-        }
-      } else {
-        const double rd = (double)res;
-        if (rd > 0.0 && isfinite(rd)) {
-          p.out[o] = log10(rd) + (double)kexp * 0.30102999566398119521 - p.tables->log10_init_d;
-        } else {
-          atomicAdd(&p.ctr->underflow_count, 1ull);
-          p.out[o] = -INFINITY;
-        }
-      }
+      write_result<T>(p, it.read, h, it.out0 + k, res, kexp);
     }
   }
 }

@@ -45,6 +45,7 @@ void DevBuf::release() {
 
 namespace {
 constexpr int kMaxRowsPerLane = 8;
+constexpr int kMaxVariants = 32;
 constexpr int kRescaleTarget = 1000;  // FP64 boundary rows are scaled to ~2^1000
 
 int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
@@ -161,10 +162,9 @@ bv_status Engine::plan(const bv_region_batch& b) {
   max_hap_ = 0;
   const int per_unit = std::max(1, opt_.haps_per_unit > 0 ? opt_.haps_per_unit : 8);
   const bool all_f64 = opt_.precision == BV_PRECISION_F64;
-  const int nvar_single = kMaxRowsPerLane;  // variants 0..7: rows per lane 1..8
   const int v_multi = variant_index(false, 8, true);
-  std::vector<int64_t> count(16, 0);
-  std::vector<int> var_max_hap(16, 0);
+  std::vector<int64_t> count(kMaxVariants, 0);
+  std::vector<int> var_max_hap(kMaxVariants, 0);
   // pass 1: count units per variant
   std::vector<int> region_max_hap(std::max<int64_t>(b.num_regions, 1), 0);
   for (int64_t g = 0; g < b.num_regions; ++g) {
@@ -174,12 +174,14 @@ bv_status Engine::plan(const bv_region_batch& b) {
     region_max_hap[g] = mh;
     max_hap_ = std::max(max_hap_, mh);
   }
+  // two haplotypes per warp (paired variants) unless the options ask for one
+  auto pair_rows = [&](int64_t rt) { return opt_.haps_per_warp != 1 && rt >= 1 && per_unit >= 2; };
   auto variant_of = [&](int64_t rlen) {
     // rows of the single-strip FP32 kernel: row 0, the read, the summing row
     // and one padding row on top (phmm_device.cuh, rows_needed)
     const int64_t rows = rows_needed((int)std::min<int64_t>(rlen, 1 << 24), true, true);
     const int64_t rt = (rows + kWarp - 1) / kWarp;
-    return rt <= kMaxRowsPerLane ? variant_index(false, (int)rt, false) : v_multi;
+    return rt <= kMaxRowsPerLane ? variant_index(false, (int)rt, false, pair_rows(rt)) : v_multi;
   };
   for (int64_t g = 0; g < b.num_regions; ++g) {
     const int64_t nh = b.region_haps[g + 1] - b.region_haps[g];
@@ -192,10 +194,9 @@ bv_status Engine::plan(const bv_region_batch& b) {
       var_max_hap[v] = std::max(var_max_hap[v], region_max_hap[g]);
     }
   }
-  (void)nvar_single;
-  std::vector<int64_t> start(17, 0);
-  for (int v = 0; v < 16; ++v) start[v + 1] = start[v] + count[v];
-  if (!all_f64) units_.resize(start[16]);
+  std::vector<int64_t> start(kMaxVariants + 1, 0);
+  for (int v = 0; v < kMaxVariants; ++v) start[v + 1] = start[v] + count[v];
+  if (!all_f64) units_.resize(start[kMaxVariants]);
   std::vector<int64_t> fill(start.begin(), start.end() - 1);
   // pass 2: fill units (or FP64 items) in result order within each bucket
   int64_t res = 0;
@@ -225,7 +226,7 @@ bv_status Engine::plan(const bv_region_batch& b) {
   n_results_ = res;
   // launch plans
   int slot = 0;
-  for (int v = 0; v < 16 && !all_f64; ++v) {
+  for (int v = 0; v < kMaxVariants && !all_f64; ++v) {
     if (count[v] == 0) continue;
     LaunchPlan lp;
     lp.variant = v;
@@ -234,7 +235,9 @@ bv_status Engine::plan(const bv_region_batch& b) {
     lp.n_units = count[v];
     lp.multi = (v == v_multi);
     lp.f64 = false;
-    lp.hap_bytes = hap_bytes_for(var_max_hap[v], lp.multi ? 32 : 8);
+    lp.code_row_bytes = hap_bytes_for(var_max_hap[v], lp.multi ? 32 : 8);
+    // a paired variant stages one 32-bit entry (both haplotypes' table offsets) per column
+    lp.hap_bytes = variant_paired(v) ? 4 * lp.code_row_bytes : lp.code_row_bytes;
     lp.warp_smem = warp_smem_bytes(v, lp.hap_bytes);
     const int smem_block = lp.warp_smem * (kThreadsPerBlock / kWarp);
     if (smem_block > 227 * 1024) return fail(BV_ERR_INVALID_ARG, "haplotype too long for shared-memory staging");
@@ -377,6 +380,7 @@ bv_status Engine::enqueue_kernels(bool capturing) {
     p.slot = lp.slot;
     p.from_rescue = 0;
     p.hap_bytes = lp.hap_bytes;
+    p.code_row_bytes = lp.code_row_bytes;
     p.warp_smem_bytes = lp.warp_smem;
     p.bnd = lp.multi ? d_bnd32_.get() : nullptr;
     p.bnd_cols = lp.bnd_cols;
@@ -392,6 +396,7 @@ bv_status Engine::enqueue_kernels(bool capturing) {
     p.slot = lp.slot;
     p.from_rescue = 1;
     p.hap_bytes = lp.hap_bytes;
+    p.code_row_bytes = 0;
     p.warp_smem_bytes = lp.warp_smem;
     p.bnd = d_bnd64_.get();
     p.bnd_cols = lp.bnd_cols;

@@ -37,6 +37,7 @@ struct LaunchPlan {
   long long unit_base = 0;
   long long n_units = 0;
   int hap_bytes = 0;
+  int code_row_bytes = 0;
   int warp_smem = 0;
   int grid = 0;
   long long bnd_cols = 0;

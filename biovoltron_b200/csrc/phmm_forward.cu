@@ -51,7 +51,7 @@
 
 namespace bvphmm {
 
-template <typename T, int RT, bool MULTI>
+template <typename T, int RT, bool MULTI, bool PAIR>
 __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & (kWarp - 1);
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
       const Unit u = p.units[p.unit_base + w];
       it.read = u.read; it.hap0 = u.hap0; it.nh = u.nh; it.out0 = u.out0;
     }
-    process_item<T, RT, MULTI>(p, it, wsm, lane, bnd);
+    process_item<T, RT, MULTI, PAIR>(p, it, wsm, lane, bnd);
   }
 }
 
@@ -98,52 +98,67 @@ cudaError_t launch_set_u64(unsigned long long* dst, unsigned long long v, cudaSt
 // ---------------------------------------------------------------------------
 // Host-side launch table
 // ---------------------------------------------------------------------------
-template <typename T, int RT, bool MULTI>
+template <typename T, int RT, bool MULTI, bool PAIR>
 int warp_smem_bytes_for(int hap_bytes) {
   using S = WarpSmem<T, RT>;
   return hap_bytes + S::kEtabBytes + (MULTI ? S::kRingBytes : 0);
 }
 
-template <typename T, int RT, bool MULTI>
+template <typename T, int RT, bool MULTI, bool PAIR>
 static cudaError_t launch_one(const KernelParams& p, int grid, cudaStream_t st) {
   const int smem = (kThreadsPerBlock / kWarp) * p.warp_smem_bytes;
-  k_forward<T, RT, MULTI><<<grid, kThreadsPerBlock, smem, st>>>(p);
+  k_forward<T, RT, MULTI, PAIR><<<grid, kThreadsPerBlock, smem, st>>>(p);
   return cudaGetLastError();
 }
 
-template <typename T, int RT, bool MULTI>
+template <typename T, int RT, bool MULTI, bool PAIR>
 static cudaError_t prepare_one(int smem_per_block) {
-  return cudaFuncSetAttribute(&k_forward<T, RT, MULTI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
+  return cudaFuncSetAttribute(&k_forward<T, RT, MULTI, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              smem_per_block);
 }
 
-template <typename T, int RT, bool MULTI>
+template <typename T, int RT, bool MULTI, bool PAIR>
 static int occupancy_one(int smem_per_block) {
   int nb = 0;
-  auto k = &k_forward<T, RT, MULTI>;
+  auto k = &k_forward<T, RT, MULTI, PAIR>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kThreadsPerBlock, smem_per_block) != cudaSuccess) return 0;
   return nb;
 }
 
+// Variant order: indices 0..7 are FP32 single strip with 1..8 rows per lane
+// and 8 the FP32 multi-strip variant (the band path's fallback buckets use
+// these numbers); then the FP64 variants and the paired FP32 variants.
 #define BV_VARIANTS(X)              \
-  X(float, 1, false) X(float, 2, false) X(float, 3, false) X(float, 4, false) \
-  X(float, 5, false) X(float, 6, false) X(float, 7, false) X(float, 8, false) \
-  X(float, 8, true) X(double, 4, true) X(double, 2, true)
+  X(float, 1, false, false) X(float, 2, false, false) X(float, 3, false, false) X(float, 4, false, false) \
+  X(float, 5, false, false) X(float, 6, false, false) X(float, 7, false, false) X(float, 8, false, false) \
+  X(float, 8, true, false) X(double, 4, true, false) X(double, 2, true, false)                           \
+  X(float, 1, false, true) X(float, 2, false, true) X(float, 3, false, true) X(float, 4, false, true)     \
+  X(float, 5, false, true) X(float, 6, false, true) X(float, 7, false, true) X(float, 8, false, true)
 
-int variant_index(bool f64, int rt, bool multi) {
+int variant_index(bool f64, int rt, bool multi, bool paired) {
   int idx = 0;
-#define BV_IDX(T, RT, MULTI)                                                         \
-  if ((sizeof(T) == 8) == f64 && RT == rt && MULTI == multi) return idx; \
+#define BV_IDX(T, RT, MULTI, PAIR)                                                                 \
+  if ((sizeof(T) == 8) == f64 && RT == rt && MULTI == multi && PAIR == paired) return idx; \
   ++idx;
   BV_VARIANTS(BV_IDX)
 #undef BV_IDX
   return -1;
 }
 
+bool variant_paired(int variant) {
+  int idx = 0;
+#define BV_PAIRED(T, RT, MULTI, PAIR) \
+  if (idx++ == variant) return PAIR;
+  BV_VARIANTS(BV_PAIRED)
+#undef BV_PAIRED
+  return false;
+}
+
 int warp_smem_bytes(int variant, int hap_bytes) {
   int idx = 0;
-#define BV_SM(T, RT, MULTI) \
-  if (idx++ == variant) return warp_smem_bytes_for<T, RT, MULTI>(hap_bytes);
+#define BV_SM(T, RT, MULTI, PAIR) \
+  if (idx++ == variant) return warp_smem_bytes_for<T, RT, MULTI, PAIR>(hap_bytes);
   BV_VARIANTS(BV_SM)
 #undef BV_SM
   return -1;
@@ -151,8 +166,8 @@ int warp_smem_bytes(int variant, int hap_bytes) {
 
 cudaError_t prepare_variant(int variant, int smem_per_block) {
   int idx = 0;
-#define BV_PREP(T, RT, MULTI) \
-  if (idx++ == variant) return prepare_one<T, RT, MULTI>(smem_per_block);
+#define BV_PREP(T, RT, MULTI, PAIR) \
+  if (idx++ == variant) return prepare_one<T, RT, MULTI, PAIR>(smem_per_block);
   BV_VARIANTS(BV_PREP)
 #undef BV_PREP
   return cudaErrorInvalidValue;
@@ -160,8 +175,8 @@ cudaError_t prepare_variant(int variant, int smem_per_block) {
 
 cudaError_t launch_forward(int variant, const KernelParams& p, int grid, cudaStream_t st) {
   int idx = 0;
-#define BV_LAUNCH(T, RT, MULTI) \
-  if (idx++ == variant) return launch_one<T, RT, MULTI>(p, grid, st);
+#define BV_LAUNCH(T, RT, MULTI, PAIR) \
+  if (idx++ == variant) return launch_one<T, RT, MULTI, PAIR>(p, grid, st);
   BV_VARIANTS(BV_LAUNCH)
 #undef BV_LAUNCH
   return cudaErrorInvalidValue;
@@ -169,8 +184,8 @@ cudaError_t launch_forward(int variant, const KernelParams& p, int grid, cudaStr
 
 int blocks_per_sm(int variant, int smem_per_block) {
   int idx = 0;
-#define BV_OCC(T, RT, MULTI) \
-  if (idx++ == variant) return occupancy_one<T, RT, MULTI>(smem_per_block);
+#define BV_OCC(T, RT, MULTI, PAIR) \
+  if (idx++ == variant) return occupancy_one<T, RT, MULTI, PAIR>(smem_per_block);
   BV_VARIANTS(BV_OCC)
 #undef BV_OCC
   return 0;

@@ -23,6 +23,7 @@ struct KernelParams {
   PairRef* rescue;        // null: pairs below the FP32 threshold get NaN (audit runs)
   long long rescue_cap;
   int hap_bytes;          // per-warp bytes for staged haplotype codes
+  int code_row_bytes;     // entries of a staged code row (paired variants stage 4-byte entries)
   int warp_smem_bytes;    // per-warp dynamic shared memory
   void* bnd;              // per-warp strip-boundary buffers (multi-strip variants)
   long long bnd_cols;     // rows of 4 values per warp buffer
@@ -30,8 +31,10 @@ struct KernelParams {
   int rescale_target;     // binary exponent the boundary maximum is scaled to
 };
 
-// Variant table: (precision, rows per lane, multi-strip).
-int variant_index(bool f64, int rows_per_lane, bool multi);
+// Variant table: (precision, rows per lane, multi-strip, two haplotypes per
+// warp).  Paired variants exist for FP32 single strip only.
+int variant_index(bool f64, int rows_per_lane, bool multi, bool paired = false);
+bool variant_paired(int variant);
 int warp_smem_bytes(int variant, int hap_bytes);
 int blocks_per_sm(int variant, int smem_per_block);
 // Sets the variant's dynamic shared-memory limit; call before launching or capturing it.

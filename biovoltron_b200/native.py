@@ -33,7 +33,8 @@ BV_MODE_BAND = 1
 class Options(C.Structure):
     _fields_ = [
         ("struct_size", C.c_int32), ("device", C.c_int32), ("precision", C.c_int32), ("mode", C.c_int32),
-        ("rescue_threshold", C.c_double), ("haps_per_unit", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("rescue_threshold", C.c_double), ("haps_per_unit", C.c_int32), ("haps_per_warp", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

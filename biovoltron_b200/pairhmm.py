@@ -61,7 +61,8 @@ class _BatchView:
 class PairHMMEngine:
     """One ``bv_phmm_ctx`` (a CUDA stream and its device buffers on one GPU)."""
 
-    def __init__(self, device: int = 0, precision: str = "auto", mode: str = "full", haps_per_unit: int = 8):
+    def __init__(self, device: int = 0, precision: str = "auto", mode: str = "full", haps_per_unit: int = 8,
+                 haps_per_warp: int = 0):
         self.lib = N.load()
         o = N.Options()
         self.lib.bv_phmm_default_options(C.byref(o))
@@ -69,6 +70,7 @@ class PairHMMEngine:
         o.precision = {"auto": N.BV_PRECISION_AUTO, "f64": N.BV_PRECISION_F64}[precision]
         o.mode = {"full": N.BV_MODE_FULL, "band": N.BV_MODE_BAND}[mode]
         o.haps_per_unit = haps_per_unit
+        o.haps_per_warp = haps_per_warp
         h = C.c_void_p()
         st = self.lib.bv_phmm_create(C.byref(o), C.byref(h))
         if st != N.BV_OK:

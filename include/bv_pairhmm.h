@@ -68,7 +68,9 @@ typedef struct bv_phmm_options {
   int32_t mode;             /* bv_phmm_mode */
   double rescue_threshold;  /* FP32 value (scaled by 2^120) below which FP64 runs; default 1e-28 */
   int32_t haps_per_unit;    /* haplotypes one warp scores against a read before taking new work; default 8 */
-  int32_t reserved[7];
+  int32_t haps_per_warp;    /* 2: a warp scores two haplotypes of a read at once (packed FP32x2), 1: one;
+                               0 (default): 2 */
+  int32_t reserved[6];
 } bv_phmm_options;
 
 typedef struct bv_phmm_stats {

@@ -168,3 +168,18 @@ def test_alignment_ending_at_last_haplotype_base(engine, oracle):
     truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
     ref, _ = oracle.log10_reference_rule(TestcaseArray.for_batch(b))
     _check(got, ref, truth)
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_paired_haplotypes_bit_identical_to_single(seed):
+    """Two haplotypes per warp (packed FP32x2) run each pair's arithmetic in
+    the single-haplotype order: identical results, including the FP64-rescued
+    pairs and odd haplotype counts."""
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    b = W.config1(seed=seed, n_regions=24)
+    with PairHMMEngine(haps_per_warp=1) as e1:
+        one, st1 = e1.compute_regions(b, with_stats=True)
+    with PairHMMEngine(haps_per_warp=2) as e2:
+        two, st2 = e2.compute_regions(b, with_stats=True)
+    assert st1["rescued"] == st2["rescued"]
+    assert np.array_equal(one, two)
