@@ -413,6 +413,15 @@ __device__ __forceinline__ float2 shfl_up2(float2 v) {
   return make_float2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
 }
 
+// The lane above sends, instead of its bottom row's M, X and Y, the two sums
+// this lane's top row r consumes (two shuffles per haplotype and step
+// instead of three):
+//   zx = kap(r) Xh(r-1,c) + M(r-1,c)                              (X of row r)
+//   zm = pMM(r) M(r-1,c-1) + cx(r) Xh(r-1,c-1) + cy(r) Yh(r-1,c-1)  (M of row r / e)
+// computed from the row-r constants the lane above holds (mmN, cxN, cyN,
+// kapN), with the operations and operands of the top row's own update.
+// Lane 0 receives its own sums: its top row is padding (e = 0) and the row
+// below has zero X coefficient, so they reach no real row.
 template <int RT>
 __device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const float* __restrict__ y0a,
                                                const float* __restrict__ y0b, const ELane el,
@@ -432,8 +441,14 @@ __device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const 
     X[j] = make_float2(0.f, 0.f);
     Y[j] = make_float2(y0a[j], y0b[j]);
   }
-  float2 upM = shfl_up2(M[RT - 1]), upX = shfl_up2(X[RT - 1]), upY = shfl_up2(Y[RT - 1]);
-  float2 dM = upM, dX = upX, dY = upY;
+  // the next lane's top-row constants
+  const float mmN1 = __shfl_down_sync(0xffffffffu, rw.mm[0], 1), cxN1 = __shfl_down_sync(0xffffffffu, rw.cx[0], 1);
+  const float cyN1 = __shfl_down_sync(0xffffffffu, rw.cy[0], 1), kapN1 = __shfl_down_sync(0xffffffffu, rw.kap[0], 1);
+  const float2 mmN = make_float2(mmN1, mmN1), cxN = make_float2(cxN1, cxN1);
+  const float2 cyN = make_float2(cyN1, cyN1), kapN = make_float2(kapN1, kapN1);
+  // sums for step 0 from the column-0 boundary state (M = X = 0, Y = y0)
+  float2 zx = shfl_up2(__ffma2_rn(kapN, X[RT - 1], M[RT - 1]));
+  float2 zm = shfl_up2(__ffma2_rn(mmN, M[RT - 1], __ffma2_rn(cxN, X[RT - 1], __fmul2_rn(cyN, Y[RT - 1]))));
   for (int s0 = 0; s0 < nsteps; s0 += CH) {
 #pragma unroll
     for (int u = 0; u < CH; ++u) {
@@ -442,10 +457,14 @@ __device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const 
       float ea[RT], eb[RT];
       load_emissions<float, RT>(el, offs & 0xffffu, ea);
       load_emissions<float, RT>(el, offs >> 16, eb);
-      float2 um = upM, ux = upX;
-      float2 dm = dM, dx = dX, dy = dY;
+      // top row from the lane above's sums
+      const float2 mn0 = make_float2(ea[0] * zm.x, eb[0] * zm.y);
+      const float2 yn0 = __ffma2_rn(g[0], Y[0], M[0]);
+      float2 dm = M[0], dx = X[0], dy = Y[0];
+      float2 um = mn0, ux = zx;
+      M[0] = mn0; X[0] = zx; Y[0] = yn0;
 #pragma unroll
-      for (int j = 0; j < RT; ++j) {
+      for (int j = 1; j < RT; ++j) {
         float2 t = __fmul2_rn(cy[j], dy);
         t = __ffma2_rn(cx[j], dx, t);
         t = __ffma2_rn(mm[j], dm, t);
@@ -456,9 +475,9 @@ __device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const 
         um = mn; ux = xn;
         M[j] = mn; X[j] = xn; Y[j] = yn;
       }
-      const float2 nM = shfl_up2(M[RT - 1]), nX = shfl_up2(X[RT - 1]), nY = shfl_up2(Y[RT - 1]);
-      dM = upM; dX = upX; dY = upY;
-      upM = nM; upX = nX; upY = nY;
+      // dm/dx/dy: the bottom row at column c-1; M/X/Y[RT-1]: at column c
+      zx = shfl_up2(__ffma2_rn(kapN, X[RT - 1], M[RT - 1]));
+      zm = shfl_up2(__ffma2_rn(mmN, dm, __ffma2_rn(cxN, dx, __fmul2_rn(cyN, dy))));
     }
   }
   lastM = M[RT - 1];
