@@ -1,26 +1,40 @@
 #!/usr/bin/env python3
 """PairHMM forward-pass benchmark (one JSON line on rank 0).
 
-Workload (default): 4096 uneven active regions -- reads per region lognormal
-(median 60, sigma 0.75, 20-500), read length U(50, 250), 2-32 haplotypes of
-U(200, 700) bp per region, 1% SNVs and 0-2 indels per haplotype, 1% read
-substitutions, q ~ U(10, 40), i = d = 45, c = 10 -- seeded synthetic data.
-A step scores every read against every haplotype of its region: ~5.4 M pairs,
-~3.7e11 DP cells.
+Default workload (config 4, the headline): 200,000 active regions of 300 bp
+over a 60 Mb uniform-ACGT synthetic reference, 30x coverage of 150 bp reads
+(1% substitutions, 0.1% indels), 2-16 haplotypes per region spanning the
+region +-75 bp with SNV/indel alleles at 1/1000 bp; q ~ U(10, 40), i = d =
+45, c = 10.  Every read is scored against every haplotype of its region:
+~1.08e8 pairs, ~7.3e12 DP cells.  Seeded synthetic data (no dataset).
 
-* value    pairs/s with the batch resident in HBM (staged once), device time of
-           the step's kernels from CUDA events on the engine's stream; the
-           inputs (~274 MB) exceed the 126 MB L2, so nothing is flushed.
-* e2e      pairs/s through bv_phmm_compute_regions with host buffers (page-
-           locked): validation and planning, host->device copies, kernels and
-           the device->host copy of the log10 results inside the timed region.
-* roofline the FP32 forward kernels against the measured FP32 FMA peak (12
-           algorithmic flops per DP cell, the reference's computeMXY count).
-* cpu_baseline  Biovoltron's own AVX PairHMM kernel (oracle/_ref, compiled
-           from the reference sources) on all host cores, on a seeded sample of
-           the same regions.
+The full chosen form runs: the band MLP is first trained on the GPU (labels
+from the full DP's posterior spreads, 1M pairs drawn from config 1's
+distribution, its own seed); then every step scores the whole batch with the
+learned band (featuriser, BF16 MLP, banded forward-backward with edge-mass
+fallback to the full DP, sampled audit) and FP32 with FP64 rescue.  The plain
+full-DP kernels score the same batch in the same run for the comparison.
+
+* value        pairs/s of the full chosen form with the batch resident in HBM
+               (device time from CUDA events on the engine's stream; inputs of
+               ~9.9 GB exceed the 126 MB L2, so nothing is flushed).
+* plain        the same for the plain full DP (FP32 + FP64 rescue).
+* e2e          pairs/s through bv_phmm_compute_regions in band mode with
+               page-locked host buffers: validation, planning, host->device
+               copies, all kernels and the device->host copy of the results.
+* accuracy     max / p99 |dlog10L| of both forms against the FP64 oracle on a
+               seeded sample of pairs, and of the band against the full DP on
+               every pair.
+* roofline     the dominant kernel (the banded forward-backward) against the
+               measured FP32 FMA peak, 12 algorithmic flops per band-cell
+               update; roofline_plain the full-DP kernels, 12 flops per cell
+               (the reference's computeMXY count).
+* cpu_baseline Biovoltron's own AVX PairHMM kernel (oracle/_ref, compiled from
+               the reference sources) on all host cores, on a seeded sample of
+               the same regions.
 
 --impl reference times that CPU kernel alone, on the same workload.
+--workload config0|config1|config2 --form plain|band run the other configs.
 Multi-GPU (torchrun): every rank scores its own batch (different seed) on its
 own GPU, no data-path collective (weak scaling); time is the max over ranks.
 """
@@ -56,7 +70,7 @@ def make_workload(name: str, seed: int, regions: int = 0) -> W.RegionBatch:
     if name == "config2":
         return W.config2(seed=seed)
     if name == "config4":
-        return W.config4(seed=seed)
+        return W.config4(seed=seed, n_regions=regions or 200_000)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -86,8 +100,18 @@ class ClockSampler:
         self.proc.terminate()
         out, _ = self.proc.communicate(timeout=10)
         rows = [r.split(", ") for r in out.strip().splitlines() if r.strip()]
-        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        rows = [r for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return 0.0
+        # under load: samples drawing at least half of the highest power seen
+        pmax = max([num(r[3]) for r in rows], default=0.0)
+        loaded = [r for r in rows if num(r[3]) >= 0.5 * pmax] or rows
+        sm = [float(r[1]) for r in loaded]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
@@ -97,7 +121,8 @@ class ClockSampler:
                 if r[5 + k].strip() == "Active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(sm),
+                "power_w_max": pmax}
 
 
 def cpu_reference_rate(batch: W.RegionBatch, target_s: float, seed: int = 0):
@@ -207,115 +232,232 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def train_band(eng, args, local_seed: int) -> dict:
+    """Trains the band MLP on the GPU (or loads --weights) and installs it."""
+    if args.weights:
+        eng.band_load(args.weights)
+        return {"weights": args.weights}
+    # 1M pairs drawn from config 1's distribution (regions added until the pair count is reached)
+    per_region = 5_388_348 / 4096
+    n_reg = max(8, int(round(args.train_pairs / per_region)))
+    tb = W.config1(seed=7000 + local_seed, n_regions=n_reg)
+    rep = eng.band_train(tb, epochs=args.train_epochs, seed=1234 + local_seed)
+    rep["train_workload"] = tb.name
+    return rep
+
+
+def time_form(eng, batch, args, pg, band: bool):
+    """Stages the batch once; returns per-step stats, device ms and results."""
+    n = eng.stage(batch)
+    for _ in range(args.warmup):
+        eng.run()
+    barrier(pg)
+    steps = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        steps.append(eng.run())
+    wall = time.perf_counter() - t0
+    barrier(pg)
+    res = eng.fetch(n)
+    return n, steps, wall, res
+
+
+def accuracy(batch, got_band, got_plain, n_sample: int, seed: int):
+    """max / p99 |dlog10| against the FP64 oracle on a seeded sample of pairs."""
+    from oracle.oracle import Oracle, TestcaseArray
+    rng = np.random.default_rng(seed)
+    sel = np.sort(rng.choice(batch.n_pairs, size=min(n_sample, batch.n_pairs), replace=False))
+    truth = Oracle().log10_rescaled(TestcaseArray.for_batch(batch, sel=sel))
+    out = {"oracle_sample_pairs": int(sel.size)}
+    for name, got in (("band", got_band), ("plain", got_plain)):
+        if got is None:
+            continue
+        g = got[sel]
+        fin = np.isfinite(truth)
+        err = np.abs(g[fin] - truth[fin])
+        out[name] = {"max_abs_dlog10_vs_fp64_oracle": float(err.max(initial=0)),
+                     "p99_abs_dlog10_vs_fp64_oracle": float(np.quantile(err, 0.99)) if err.size else 0.0,
+                     "nonfinite_mismatch": int(np.sum(np.isfinite(g[~fin])) + np.sum(~np.isfinite(g[fin])))}
+    if got_band is not None and got_plain is not None:
+        both = np.isfinite(got_band) & np.isfinite(got_plain)
+        d = np.abs(got_band[both] - got_plain[both])
+        out["band_vs_full_dp_all_pairs"] = {"max": float(d.max(initial=0)),
+                                            "p99": float(np.quantile(d, 0.99)) if d.size else 0.0,
+                                            "over_1e-3": int(np.sum(d > 1e-3)), "pairs": int(both.sum())}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="config1")
+    ap.add_argument("--workload", default="config4")
+    ap.add_argument("--form", choices=["band", "plain"], default=None,
+                    help="band: learned band + batched (default for config4/config1); plain: full DP only")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--regions", type=int, default=0, help="config1 only: fewer regions (profiling cases)")
+    ap.add_argument("--regions", type=int, default=0, help="config1/config4: fewer regions (profiling cases)")
     ap.add_argument("--ref-seconds", type=float, default=10.0, help="CPU seconds per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="band form only (profiling)")
     ap.add_argument("--haps-per-warp", type=int, default=0, help="0: engine default, 1 or 2")
+    ap.add_argument("--train-pairs", type=int, default=1_000_000)
+    ap.add_argument("--train-epochs", type=int, default=8)
+    ap.add_argument("--weights", default="", help="load band MLP weights instead of training")
+    ap.add_argument("--audit-period", type=int, default=1024)
+    ap.add_argument("--oracle-sample", type=int, default=20000)
+    ap.add_argument("--edge-threshold", type=float, default=1e-3)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
         return
+    form = args.form or ("band" if args.workload in ("config4", "config1") else "plain")
 
     world, rank, local, pg = dist_setup(args)
     from biovoltron_b200.native import load
     from biovoltron_b200.pairhmm import PairHMMEngine
     import ctypes as C
 
+    t_gen = time.perf_counter()
     batch = make_workload(args.workload, args.seed + 1000 * rank, args.regions)
-    log(f"[rank {rank}] workload: {batch.name}: {batch.n_pairs} pairs, {batch.n_cells():.3e} cells")
-    eng = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp)
+    t_gen = time.perf_counter() - t_gen
+    log(f"[rank {rank}] workload: {batch.name}: {batch.n_pairs} pairs, {batch.n_cells():.3e} cells "
+        f"(generated in {t_gen:.1f} s)")
     lib = load()
     peak = C.c_double(0)
     st = lib.bv_phmm_measure_fp32_peak(local, C.byref(peak))
     fp32_peak = peak.value if st == 0 else None
 
-    # ---- device-resident throughput -------------------------------------
-    n = eng.stage(batch)
-    for _ in range(args.warmup):
-        eng.run()
-    barrier(pg)
-    clocks = ClockSampler(local)
+    plain = band = None
+    train_rep = None
+    clocks = ClockSampler(local)  # sampled over every timed section below
     clocks.start()
-    dev_ms, fp32_ms, fp64_ms = [], [], []
-    stats = None
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        stats = eng.run()
-        fp32_ms.append(stats["ms_fp32"])
-        fp64_ms.append(stats["ms_fp64"])
-        dev_ms.append(stats["ms_fp32"] + stats["ms_fp64"])
-    wall = time.perf_counter() - t0
-    clk = clocks.stop()
-    barrier(pg)
-    t_dev = allreduce(pg, float(np.sum(dev_ms)), "max")
-    total_pairs = allreduce(pg, float(n * args.steps), "sum")
-    value = total_pairs / (t_dev / 1e3)
-    cells = stats["cells"]
-    gcups = allreduce(pg, float(cells * args.steps), "sum") / (t_dev / 1e3) / 1e9
-    results = eng.fetch(n)
+    # ---- plain full DP, device-resident --------------------------------------
+    if form == "plain" or not args.no_plain:
+        with PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp) as ep:
+            n, steps, wall, res = time_form(ep, batch, args, pg, band=False)
+        plain = {"n": n, "steps": steps, "wall": wall, "res": res}
+    # ---- learned band, device-resident --------------------------------------
+    eb = None
+    if form == "band":
+        eb = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp)
+        train_rep = train_band(eb, args, rank)
+        eb.set_band_options(use_mlp=True, margin=2, edge_threshold=args.edge_threshold,
+                            audit_period=args.audit_period)
+        n, steps, wall, res = time_form(eb, batch, args, pg, band=True)
+        band = {"n": n, "steps": steps, "wall": wall, "res": res}
+    main_run = band if band else plain
+    n = main_run["n"]
 
-    # ---- end to end through the public API --------------------------------
+    def device_ms(run):
+        return [s_["ms_fp32"] + s_["ms_fp64"] for s_ in run["steps"]]
+
+    # ---- end to end through the public API (host buffers) ---------------------
+    e2e_eng = eb if eb is not None else PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp)
     arrays = [batch.read_bases, batch.read_q, batch.read_i, batch.read_d, batch.read_c, batch.hap_bases]
     for a in arrays:
-        eng.host_register(a)
+        e2e_eng.host_register(a)
     out = np.empty(max(n, 1), np.float64)
-    eng.host_register(out)
-    for _ in range(max(1, args.warmup)):
-        eng.compute_regions(batch, out=out)
+    e2e_eng.host_register(out)
+    for _ in range(max(1, min(args.warmup, 2))):
+        e2e_eng.compute_regions(batch, out=out)
     barrier(pg)
     e2e_t = []
     for _ in range(args.steps):
         t1 = time.perf_counter()
-        eng.compute_regions(batch, out=out)
+        e2e_eng.compute_regions(batch, out=out)
         e2e_t.append(time.perf_counter() - t1)
+    clk = clocks.stop()
     barrier(pg)
     for a in arrays + [out]:
-        eng.host_unregister(a)
+        e2e_eng.host_unregister(a)
+    same = bool(np.array_equal(out[:n], main_run["res"], equal_nan=True))
+    e2e_eng.close()
+
+    # ---- aggregate over ranks --------------------------------------------------
+    t_dev = allreduce(pg, float(np.sum(device_ms(main_run))), "max")
+    total_pairs = allreduce(pg, float(n * args.steps), "sum")
+    total_cells = allreduce(pg, float(batch.n_cells() * args.steps), "sum")
+    value = total_pairs / (t_dev / 1e3)
     e2e_time = allreduce(pg, float(np.sum(e2e_t)), "max")
     e2e = total_pairs / e2e_time
-    same = bool(np.array_equal(out[:n], results))
+    plain_pps = None
+    if plain is not None:
+        t_plain = allreduce(pg, float(np.sum(device_ms(plain))), "max")
+        plain_pps = total_pairs / (t_plain / 1e3)
 
-    # ---- CPU baseline (rank 0, one GPU only) ------------------------------
+    acc = None
     cpu = None
+    if rank == 0 and args.oracle_sample > 0:
+        acc = accuracy(batch, band["res"] if band else None, plain["res"] if plain else None, args.oracle_sample,
+                       seed=99)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(batch, target_s=args.ref_seconds)
 
     if rank == 0:
-        fp32_mean = float(np.mean(fp32_ms))
-        achieved = FLOPS_PER_CELL * cells / (fp32_mean / 1e3) / 1e12
+        def mean(run, key):
+            return float(np.mean([s_[key] for s_ in run["steps"]]))
+
+        last = main_run["steps"][-1]
+        ms_step = t_dev / args.steps
         line = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_dev / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
-            "gcups": gcups,
-            "config": {"workload": batch.name, "form": "plain full DP, batched (persistent length-binned launches)",
-                       "pairs_per_gpu": n, "cells_per_gpu": cells, "rescued_per_step": stats["rescued"],
-                       "l2": "inputs 274 MB > 126 MB L2, no flush", "parallelism": f"dp{world} (independent regions)"},
-            "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(batch.nbytes()),
-                    "d2h_bytes_per_step": int(8 * n), "results_identical_to_device_run": same},
-            "roofline": {"bound": "fp32", "kernel": "k_forward<float> (all rows-per-lane variants)",
-                         "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": (achieved / fp32_peak) if fp32_peak else None, "traffic": None,
-                         "peak_source": "measured: FP32 FMA probe kernel in this run (bv_phmm_measure_fp32_peak)",
-                         "flops_per_cell": FLOPS_PER_CELL},
-            "kernel_ms": {"fp32": fp32_mean, "fp64_rescue": float(np.mean(fp64_ms))},
-            "gpu_launches": int(stats["kernel_launches"]) * args.steps,
-            "clocks": clk,
-            "wall_s_timed": wall,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+            "gcups_effective": total_cells / (t_dev / 1e3) / 1e9,
+            "config": {"workload": batch.name,
+                       "form": ("learned band + batched (persistent length-binned launches, graph replay) + "
+                                "FP32 with FP64 rescue") if band else "plain full DP, batched, FP32 with FP64 rescue",
+                       "pairs_per_gpu": n, "cells_per_gpu": batch.n_cells(),
+                       "l2": f"inputs {batch.nbytes() / 1e9:.2f} GB > 126 MB L2, no flush",
+                       "parallelism": f"dp{world} (independent regions, one replica per GPU)",
+                       "generate_s": round(t_gen, 1)},
         }
+        if plain is not None:
+            pl = plain["steps"][-1]
+            ms_plain = float(np.mean(device_ms(plain)))
+            ach = FLOPS_PER_CELL * batch.n_cells() / (mean(plain, "ms_full") / 1e3) / 1e12
+            line["plain"] = {"value": plain_pps, "unit": "pairs/s", "ms_per_step": ms_plain,
+                             "gcups": batch.n_cells() / (ms_plain / 1e3) / 1e9,
+                             "rescued_per_step": pl["rescued"], "kernel_ms": {
+                                 "fp32": mean(plain, "ms_full"), "fp64_rescue": mean(plain, "ms_fp64")}}
+            line["roofline_plain"] = {"bound": "fp32", "kernel": "k_forward<float> (full DP, all variants)",
+                                      "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
+                                      "frac": (ach / fp32_peak) if fp32_peak else None,
+                                      "flops_per_cell": FLOPS_PER_CELL, "traffic": None}
+            if band is not None:
+                line["speedup_vs_plain"] = value / plain_pps
+        if band is not None:
+            ms_band = mean(band, "ms_band")
+            band_cells = int(last["band_cells"])
+            ach = FLOPS_PER_CELL * band_cells / (ms_band / 1e3) / 1e12 if ms_band > 0 else 0.0
+            line["band"] = {
+                "kernel_ms": {"seed_features_mlp_route": mean(band, "ms_seed"), "banded_fwd_bwd": ms_band,
+                              "fallback_full_dp": mean(band, "ms_full"), "fp64_rescue": mean(band, "ms_fp64")},
+                "band_pairs": int(last["band_pairs"]), "routed_full": int(last["band_routed_full"]),
+                "edge_fallback": int(last["band_fallback"]), "promoted": int(last["band_promoted"]),
+                "fallback_rate": (int(last["band_routed_full"]) + int(last["band_fallback"])) / max(n, 1),
+                "band_cell_updates": band_cells, "rescued": int(last["rescued"]),
+                "audit_pairs": int(last["audit_pairs"]), "audit_max_err": float(last["audit_max_err"]),
+                "audit_p99_err": float(last["audit_p99_err"]), "train": train_rep}
+            line["roofline"] = {"bound": "fp32", "kernel": "k_band_f32<W> (banded forward-backward, W = 8/16/32)",
+                                "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
+                                "frac": (ach / fp32_peak) if fp32_peak else None,
+                                "flops_per_cell_update": FLOPS_PER_CELL, "traffic": None}
+        else:
+            line["roofline"] = line.get("roofline_plain")
+        line["peak_source"] = "measured: FP32 FMA probe kernel in this run (bv_phmm_measure_fp32_peak)"
+        line["accuracy"] = acc
+        line["e2e"] = {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(batch.nbytes()),
+                       "d2h_bytes_per_step": int(8 * n), "results_identical_to_device_run": same}
+        line["gpu_launches"] = int(last["kernel_launches"]) * args.steps
+        line["clocks"] = clk
+        line["wall_s_timed"] = main_run["wall"]
         if cpu:
             line["cpu_baseline"] = {"value": cpu["pairs_per_s"], "unit": "pairs/s", "cores": cpu["cores"],
                                     "kind": cpu["kind"], "sample": cpu["sample"], "gcups": cpu["gcups"]}
         print(json.dumps(line), flush=True)
-    eng.close()
     if pg is not None:
         pg.destroy_process_group()
 

@@ -469,6 +469,17 @@ bv_status Engine::run(bv_phmm_stats* stats) {
                                  : (int64_t)plans_.size() + 1;
     stats->ms_fp32 = ms32;
     stats->ms_fp64 = ms64;
+    if (band_enabled()) {
+      float seed = 0, band = 0, full = 0;
+      cudaEventElapsedTime(&seed, ev_[2], ev_[5]);
+      cudaEventElapsedTime(&band, ev_[5], ev_[6]);
+      cudaEventElapsedTime(&full, ev_[6], ev_[3]);
+      stats->ms_seed = seed;
+      stats->ms_band = band;
+      stats->ms_full = full;
+    } else {
+      stats->ms_full = ms32;
+    }
     stats->ms_h2d = ms_h2d_;
     stats->ms_total =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

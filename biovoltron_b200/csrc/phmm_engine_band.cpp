@@ -124,7 +124,9 @@ bv_status Engine::band_prepare() {
 }
 
 bv_status Engine::enqueue_band(bool capturing, KernelParams& kp) {
-  (void)capturing;
+  auto rec = [&](cudaEvent_t ev) {
+    return capturing ? cudaEventRecordWithFlags(ev, stream_, cudaEventRecordExternal) : cudaEventRecord(ev, stream_);
+  };
   BandParams p = band_params();
   BV_CUDA(cudaMemsetAsync(d_bctr_.get(), 0, sizeof(BandCounters), stream_), "memset band counters");
   BV_CUDA(launch_hap_table(p.batch.hap_bases, p.batch.hap_off, n_haps_, d_hap_table_.as<uint32_t>(), sms_, stream_), "hap tables");
@@ -134,7 +136,9 @@ bv_status Engine::enqueue_band(bool capturing, KernelParams& kp) {
   BV_CUDA(launch_band_route(p, 0, sms_, stream_), "route");
   BV_CUDA(launch_band_scan(p.bctr, stream_), "scan");
   BV_CUDA(launch_band_route(p, 1, sms_, stream_), "route");
+  BV_CUDA(rec(ev_[5]), "event");
   for (int cls = 0; cls < kBandWidths; ++cls) BV_CUDA(launch_band_dp(p, cls, sms_, stream_), "band dp");
+  BV_CUDA(rec(ev_[6]), "event");
   // full DP for everything the band path handed back
   for (int v = 0; v < 9; ++v) {
     const LaunchPlan& lp = full_plans_[v];

@@ -46,7 +46,8 @@ class Stats(C.Structure):
         ("ms_h2d", C.c_double), ("ms_fp32", C.c_double), ("ms_fp64", C.c_double), ("ms_band", C.c_double),
         ("ms_d2h", C.c_double), ("ms_total", C.c_double),
         ("band_routed_full", C.c_int64), ("audit_pairs", C.c_int64), ("audit_max_err", C.c_double),
-        ("audit_p99_err", C.c_double), ("band_promoted", C.c_int64),
+        ("audit_p99_err", C.c_double), ("band_promoted", C.c_int64), ("ms_seed", C.c_double),
+        ("ms_full", C.c_double),
     ]
 
     def as_dict(self):

@@ -288,67 +288,112 @@ def config2(seed: int = 2, n_pairs: int = 2000, max_read: int = 10000, max_hap: 
 
 
 def config4(seed: int = 4, n_regions: int = 200_000, region_len: int = 300, coverage: float = 30.0,
-            read_len: int = 150, pad: int = 75) -> RegionBatch:
-    """Whole-genome-shaped batch; vectorised so 200k regions build in tens of seconds."""
+            read_len: int = 150, pad: int = 75, read_chunk: int = 1 << 20) -> RegionBatch:
+    """Whole-genome-shaped batch.  Random draws are made in bulk and reads are
+    built in chunks of ``read_chunk``, so 200k regions build in seconds with
+    temporaries of a few hundred MB."""
     rng = np.random.default_rng(seed)
     genome_len = n_regions * region_len + 2 * pad + read_len
     genome = _random_seq(rng, genome_len)
+    next_base = np.zeros(256, np.uint8)
+    next_base[ACGT] = np.roll(ACGT, -1)  # SNV allele: the next base in ACGT order
+    base_index = np.zeros(256, np.int64)
+    base_index[ACGT] = np.arange(4)
     # haplotypes: span [start - pad, end + pad) of each region with allele edits
     span = region_len + 2 * pad
     nh = rng.integers(2, 17, size=n_regions)
-    hap_parts: List[np.ndarray] = []
-    for g in range(n_regions):
-        s = g * region_len  # genome has `pad` bases of lead-in
-        base = genome[s:s + span]
-        n_var = max(1, int(rng.poisson(span / 1000.0)) + 1)
-        vpos = rng.integers(5, span - 15, size=n_var)
-        vkind = rng.integers(0, 3, size=n_var)  # 0 SNV, 1 ins, 2 del
-        vlen = rng.integers(1, 6, size=n_var)
-        alt_bases = _random_seq(rng, 8 * n_var)
-        for h in range(int(nh[g])):
-            carry = rng.random(n_var) < 0.5 if h else np.zeros(n_var, bool)
-            hp = base
-            for k in np.nonzero(carry)[0][::-1]:
-                p = int(vpos[k])
-                if vkind[k] == 0:
-                    hp = hp.copy()
-                    hp[p] = ACGT[(np.searchsorted(ACGT, hp[p]) + 1) % 4]
-                elif vkind[k] == 1:
-                    hp = np.concatenate([hp[:p], alt_bases[8 * k:8 * k + vlen[k]], hp[p:]])
-                else:
-                    hp = np.concatenate([hp[:p], hp[p + vlen[k]:]])
-            hap_parts.append(hp)
-    hap_bases, hap_off = _concat(hap_parts)
-    # reads: starts uniform; each read is assigned to the region whose hap span contains it
+    n_var = np.maximum(1, rng.poisson(span / 1000.0, size=n_regions) + 1)
+    v_off = np.concatenate([[0], np.cumsum(n_var)])
+    tot_v = int(v_off[-1])
+    vpos = rng.integers(5, span - 15, size=tot_v)
+    vkind = rng.integers(0, 3, size=tot_v)  # 0 SNV, 1 insertion, 2 deletion
+    vlen = rng.integers(1, 6, size=tot_v)
+    alt = _random_seq(rng, 8 * tot_v)
+    h_off = np.concatenate([[0], np.cumsum(nh)])
+    n_haps = int(h_off[-1])
+    # carry[h, k]: haplotype h carries its region's variant k; each region's first haplotype is the reference
+    kmax = int(n_var.max())
+    carry = rng.random((n_haps, kmax)) < 0.5
+    carry[h_off[:-1]] = False
+    carry &= np.arange(kmax)[None, :] < n_var[np.repeat(np.arange(n_regions), nh)][:, None]
+    # Haplotypes are built in region chunks on a (haplotype, position) grid: each cell emits the
+    # bases inserted before the position (0-5) and then its base, substituted or deleted.
+    hap_chunks, len_chunks = [], []
+    reg_of_hap = np.repeat(np.arange(n_regions), nh)
+    hap_windows = np.lib.stride_tricks.sliding_window_view(genome, span)
+    for g0 in range(0, n_regions, 16384):
+        g1 = min(n_regions, g0 + 16384)
+        h0, h1 = int(h_off[g0]), int(h_off[g1])
+        rg = reg_of_hap[h0:h1]
+        base2d = hap_windows[rg * region_len]
+        keep = np.ones(base2d.shape, bool)
+        ins_len = np.zeros(base2d.shape, np.int8)
+        ins_k = np.zeros(base2d.shape, np.int32)
+        for kk in range(kmax):
+            hh = np.nonzero(carry[h0:h1, kk])[0]
+            if hh.size == 0:
+                continue
+            k = v_off[rg[hh]] + kk
+            p, kind, ln = vpos[k], vkind[k], vlen[k]
+            snv, dl, il = kind == 0, kind == 2, kind == 1
+            base2d[hh[snv], p[snv]] = next_base[base2d[hh[snv], p[snv]]]
+            for t in range(5):
+                m = dl & (t < ln)
+                keep[hh[m], p[m] + t] = False
+            ins_len[hh[il], p[il]] = ln[il]
+            ins_k[hh[il], p[il]] = k[il]
+        cnt = (ins_len + keep).reshape(-1)
+        hl = cnt.reshape(base2d.shape).sum(axis=1, dtype=np.int64)
+        start = np.cumsum(cnt, dtype=np.int32) - cnt  # exclusive prefix over the grid
+        out = np.empty(int(hl.sum()), np.uint8)
+        kf, lf, sf = keep.reshape(-1), ins_len.reshape(-1), start
+        out[sf[kf] + lf[kf]] = base2d.reshape(-1)[kf]
+        ic = np.nonzero(lf)[0]
+        for t in range(5):
+            m = ic[lf[ic] > t]
+            out[sf[m] + t] = alt[8 * ins_k.reshape(-1)[m] + t]
+        hap_chunks.append(out)
+        len_chunks.append(hl)
+    hap_bases = np.concatenate(hap_chunks)
+    hap_off = np.concatenate([[0], np.cumsum(np.concatenate(len_chunks))]).astype(np.int64)
+    # reads: starts uniform; each read belongs to the region whose haplotype span contains it
     n_reads_total = int(round(n_regions * region_len * coverage / read_len))
     starts = np.sort(rng.integers(0, n_regions * region_len, size=n_reads_total))
     region_of = np.minimum(starts // region_len, n_regions - 1)
-    offs = starts - region_of * region_len  # offset inside the hap span, <= region_len - 1
-    offs = np.minimum(offs, span - read_len - 4)
-    src_idx = (region_of * region_len)[:, None] + offs[:, None] + np.arange(read_len)[None, :]
-    bases = genome[src_idx]
-    # 0.1% indels: at most one per read, applied by index shifting
-    ind = rng.random(n_reads_total) < (0.001 * read_len)
-    n_ind = int(ind.sum())
-    if n_ind:
-        rows = np.nonzero(ind)[0]
-        p = rng.integers(10, read_len - 10, size=n_ind)
-        ln = rng.integers(1, 4, size=n_ind)
-        is_ins = rng.random(n_ind) < 0.5
-        k = np.arange(read_len)[None, :]
-        base_idx = src_idx[rows]
-        shift = np.where(k >= p[:, None], np.where(is_ins[:, None], -ln[:, None], ln[:, None]), 0)
-        new_idx = np.clip(base_idx + shift, 0, genome_len - 1)
-        nb = genome[new_idx]
-        ins_mask = is_ins[:, None] & (k >= p[:, None]) & (k < (p + ln)[:, None])
-        nb = np.where(ins_mask, ACGT[rng.integers(0, 4, size=nb.shape)], nb)
-        bases[rows] = nb
-    # 1% substitutions
-    sub = rng.random(bases.shape) < 0.01
-    bases = np.where(sub, ACGT[(np.searchsorted(ACGT, bases) + rng.integers(1, 4, size=bases.shape)) % 4], bases)
-    flat = bases.reshape(-1).astype(np.uint8)
+    offs = np.minimum(starts - region_of * region_len, span - read_len - 4)
+    bases = np.empty((n_reads_total, read_len), np.uint8)
+    k = np.arange(read_len)[None, :]
+    windows = np.lib.stride_tricks.sliding_window_view(genome, read_len)
+    for a in range(0, n_reads_total, read_chunk):
+        b = min(n_reads_total, a + read_chunk)
+        first = region_of[a:b] * region_len + offs[a:b]
+        blk = windows[first]
+        # 0.1% indels: at most one per read, applied by shifting the source index
+        ind = np.nonzero(rng.random(b - a) < 0.001 * read_len)[0]
+        if ind.size:
+            p = rng.integers(10, read_len - 10, size=ind.size)[:, None]
+            ln = rng.integers(1, 4, size=ind.size)[:, None]
+            is_ins = (rng.random(ind.size) < 0.5)[:, None]
+            shift = np.where(k >= p, np.where(is_ins, -ln, ln), 0)
+            nb = genome[np.clip(first[ind][:, None] + k + shift, 0, genome_len - 1)]
+            ins_mask = is_ins & (k >= p) & (k < p + ln)
+            blk[ind] = np.where(ins_mask, ACGT[rng.integers(0, 4, size=nb.shape)], nb)
+        # 1% substitutions (to one of the three other bases)
+        n_sub = int(rng.binomial(blk.size, 0.01))
+        flat_i = rng.integers(0, blk.size, size=n_sub)
+        fb = blk.reshape(-1)
+        fb[flat_i] = ACGT[(base_index[fb[flat_i]] + rng.integers(1, 4, size=n_sub)) % 4]
+        bases[a:b] = blk
+    flat = bases.reshape(-1)
     n = flat.size
-    q = rng.integers(10, 41, size=n).astype(np.uint8)
+    # base qualities U(10, 40): random bytes below 248 = 8 * 31, divided by 8
+    q = np.frombuffer(rng.bytes(n), np.uint8).copy()
+    bad = np.flatnonzero(q >= 248)
+    while bad.size:
+        q[bad] = np.frombuffer(rng.bytes(bad.size), np.uint8)
+        bad = bad[q[bad] >= 248]
+    q >>= 3
+    q += 10
     counts = np.bincount(region_of, minlength=n_regions)
     return RegionBatch(
         read_bases=flat, read_q=q, read_i=np.full(n, 45, np.uint8), read_d=np.full(n, 45, np.uint8),

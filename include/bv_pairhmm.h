@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define BV_PHMM_ABI_VERSION 1
+#define BV_PHMM_ABI_VERSION 2
 
 typedef enum bv_status {
   BV_OK = 0,
@@ -83,9 +83,9 @@ typedef struct bv_phmm_stats {
   int64_t band_cells;     /* cells the banded kernel computed */
   int64_t kernel_launches;
   double ms_h2d;          /* host->device copies (events on the context stream) */
-  double ms_fp32;         /* FP32 forward kernels */
+  double ms_fp32;         /* all FP32 kernels (band mode: seeding, banded DP and fallback full DP) */
   double ms_fp64;         /* FP64 rescue kernel */
-  double ms_band;         /* featurise + band MLP + banded DP kernels */
+  double ms_band;         /* banded forward-backward kernels */
   double ms_d2h;          /* device->host copy of the results */
   double ms_total;        /* whole call, host wall clock */
   int64_t band_routed_full; /* pairs the router sent to the full DP (no seed, too wide, too long) */
@@ -93,6 +93,8 @@ typedef struct bv_phmm_stats {
   double audit_max_err;     /* max |log10 band - log10 full| over the audit pairs */
   double audit_p99_err;     /* 99th percentile of the same */
   int64_t band_promoted;    /* banded pairs retried on the next wider band after the edge check */
+  double ms_seed;           /* band mode: k-mer tables, featuriser, band MLP and routing kernels */
+  double ms_full;           /* full-DP FP32 kernels (band mode: the fallback pairs) */
 } bv_phmm_stats;
 
 typedef struct bv_phmm_ctx bv_phmm_ctx;
