@@ -305,9 +305,11 @@ def main():
     ap.add_argument("--train-pairs", type=int, default=1_000_000)
     ap.add_argument("--train-epochs", type=int, default=8)
     ap.add_argument("--weights", default="", help="load band MLP weights instead of training")
+    ap.add_argument("--save-weights", default="", help="write the trained band MLP weights here")
     ap.add_argument("--audit-period", type=int, default=1024)
     ap.add_argument("--oracle-sample", type=int, default=20000)
     ap.add_argument("--edge-threshold", type=float, default=1e-3)
+    ap.add_argument("--margin", type=int, default=2, help="diagonals added on both sides of the predicted band")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -343,7 +345,9 @@ def main():
     if form == "band":
         eb = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp)
         train_rep = train_band(eb, args, rank)
-        eb.set_band_options(use_mlp=True, margin=2, edge_threshold=args.edge_threshold,
+        if args.save_weights and rank == 0:
+            eb.band_save(args.save_weights)
+        eb.set_band_options(use_mlp=True, margin=args.margin, edge_threshold=args.edge_threshold,
                             audit_period=args.audit_period)
         n, steps, wall, res = time_form(eb, batch, args, pg, band=True)
         band = {"n": n, "steps": steps, "wall": wall, "res": res}
