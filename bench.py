@@ -308,7 +308,7 @@ def main():
     ap.add_argument("--save-weights", default="", help="write the trained band MLP weights here")
     ap.add_argument("--audit-period", type=int, default=1024)
     ap.add_argument("--oracle-sample", type=int, default=20000)
-    ap.add_argument("--edge-threshold", type=float, default=1e-3)
+    ap.add_argument("--edge-threshold", type=float, default=3e-3)
     ap.add_argument("--margin", type=int, default=2, help="diagonals added on both sides of the predicted band")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -135,7 +135,7 @@ __global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n
 // t read bases uncovered (t <= kEndRows, or any t for the read's last hit)
 // the band reaches t diagonals down, and likewise up from a diagonal whose
 // first hit starts h bases into the read.
-constexpr int kFeatWarps = 8;
+constexpr int kFeatWarps = kFeatWarpsPerBlock;
 constexpr int kHitCap = 256;
 constexpr int kEndRows = 24;   // horizon of the per-diagonal end triangles
 constexpr int kUnitChunk = 32;
@@ -403,8 +403,10 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
   Unit* su = reinterpret_cast<Unit*>(smem + (size_t)(2 * kBandMaxHap + 4) * 4);
   // [0] chunk, [1] max nh, [2] groups, [3..3+33) group starts, [36..68) group max nh
   int* sctl = reinterpret_cast<int*>(su + kUnitChunk);
-  uint32_t* hist = reinterpret_cast<uint32_t*>(sctl + kCtlInts) + (size_t)wib * kHistSlots;
-  int* hits = reinterpret_cast<int*>(sctl + kCtlInts) + (size_t)kFeatWarps * kHistSlots + (size_t)wib * (kHitCap + 1);
+  // the repeated-11-mer histogram of each warp lives in global scratch (rarely touched), which
+  // leaves the block ~17 KB of shared memory and five blocks per SM
+  uint32_t* hist = p.feat_hist + ((size_t)blockIdx.x * kFeatWarps + wib) * kHistSlots;
+  int* hits = reinterpret_cast<int*>(sctl + kCtlInts) + (size_t)wib * (kHitCap + 1);
   int* nhit = hits + kHitCap;
   for (int x = lane; x < kHistSlots; x += 32) hist[x] = 0u;
   const long long nchunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
@@ -1377,7 +1379,7 @@ cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, l
 }
 
 constexpr int kFeatSmem = (2 * kBandMaxHap + 4) * 4 + kUnitChunk * (int)sizeof(Unit) + kCtlInts * 4 +
-                          kFeatWarps * (kHistSlots + kHitCap + 1) * 4;
+                          kFeatWarps * (kHitCap + 1) * 4;
 
 cudaError_t prepare_band_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_featurize, cudaFuncAttributeMaxDynamicSharedMemorySize, kFeatSmem);
@@ -1388,7 +1390,7 @@ cudaError_t prepare_band_kernels() {
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
   if (p.n_units <= 0) return cudaSuccess;
   const long long chunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
-  const long long blocks = std::min<long long>(chunks, (long long)sms * 3);
+  const long long blocks = std::min<long long>(chunks, (long long)feat_blocks(sms));
   k_featurize<<<(int)blocks, kFeatWarps * 32, kFeatSmem, st>>>(p);
   return cudaGetLastError();
 }

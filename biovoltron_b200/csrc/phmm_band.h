@@ -104,6 +104,7 @@ struct BandParams {
   const Unit* units;          // work units (featuriser order)
   long long n_units;
   const uint32_t* read_kmers; // 11-mer code per read position
+  uint32_t* feat_hist;        // featuriser scratch: one histogram of kBandMaxRead + kBandMaxHap slots per warp
   int32_t* dstar;             // [n_pairs] seed diagonal (INT32_MIN: no seed)
   int32_t* kmin;              // [n_pairs] lowest / highest diagonal of a shared 11-mer
   int32_t* kmax;
@@ -143,6 +144,10 @@ cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream
 cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st);
 cudaError_t launch_band_dp(const BandParams& p, int width_class, int sms, cudaStream_t st);
 inline int band_dp_blocks(int sms) { return sms * 4; }
+// featuriser grid and its per-warp scratch histograms (words)
+constexpr int kFeatWarpsPerBlock = 8;
+inline int feat_blocks(int sms) { return sms * 5; }
+inline long long feat_hist_words(int sms) { return (long long)feat_blocks(sms) * kFeatWarpsPerBlock * (kBandMaxRead + kBandMaxHap); }
 // Sets the dynamic shared-memory limits of the band kernels (before any capture).
 cudaError_t prepare_band_kernels();
 // audit: full-DP units for the sampled pairs (out = audit slot), then the differences

@@ -46,6 +46,7 @@ BandParams Engine::band_params() const {
   p.units = d_units_.as<Unit>();
   p.n_units = (long long)units_.size();
   p.read_kmers = d_read_kmers_.as<uint32_t>();
+  p.feat_hist = d_feat_hist_.as<uint32_t>();
   p.dstar = d_dstar_.as<int32_t>();
   p.kmin = d_kmin_.as<int32_t>();
   p.kmax = d_kmax_.as<int32_t>();
@@ -82,6 +83,7 @@ bv_status Engine::band_prepare() {
   BV_CUDA(d_pair_hap_.reserve(sizeof(int32_t) * n), "alloc pairs");
   BV_CUDA(d_hap_table_.reserve(sizeof(uint32_t) * (2 * std::max<int64_t>(n_hap_bytes_, 1) + 4 * n_haps_)), "alloc hap tables");
   BV_CUDA(d_read_kmers_.reserve(sizeof(uint32_t) * std::max<int64_t>(n_read_bytes_, 1)), "alloc kmers");
+  BV_CUDA(d_feat_hist_.reserve(sizeof(uint32_t) * (size_t)feat_hist_words(sms_)), "alloc featuriser scratch");
   BV_CUDA(d_dstar_.reserve(sizeof(int32_t) * n), "alloc seeds");
   BV_CUDA(d_kmin_.reserve(sizeof(int32_t) * n), "alloc seeds");
   BV_CUDA(d_kmax_.reserve(sizeof(int32_t) * n), "alloc seeds");
