@@ -445,7 +445,7 @@ def main():
                 "band_cell_updates": band_cells, "rescued": int(last["rescued"]),
                 "audit_pairs": int(last["audit_pairs"]), "audit_max_err": float(last["audit_max_err"]),
                 "audit_p99_err": float(last["audit_p99_err"]), "train": train_rep}
-            line["roofline"] = {"bound": "fp32", "kernel": "k_band_f32<W> (banded forward-backward, W = 8/16/32)",
+            line["roofline"] = {"bound": "fp32", "kernel": "k_band_f32<W> / k_band_pair_f32<8> (banded forward-backward, W = 8/16/24/32)",
                                 "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
                                 "frac": (ach / fp32_peak) if fp32_peak else None,
                                 "flops_per_cell_update": FLOPS_PER_CELL, "traffic": None}

@@ -101,16 +101,35 @@ __global__ void __launch_bounds__(256) k_hap_table(const uint8_t* __restrict__ h
 constexpr uint32_t kNoCode = 0xffffffffu;
 
 __global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n_bytes, uint32_t* __restrict__ codes) {
-  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n_bytes;
-       x += (long long)gridDim.x * blockDim.x) {
-    uint32_t code = 0;
-    bool ok = x + kK <= n_bytes;
-    for (int t = 0; t < kK && ok; ++t) {
-      const int c = kmer_code(read_bases[x + t]);
-      ok &= c >= 0;
-      code = (code << 2) | (uint32_t)(c & 3);
+  // Four positions per thread from four aligned 32-bit loads (bytes x0 .. x0+15;
+  // the buffer carries 16 bytes of tail padding): each base is converted once.
+  const long long n4 = (n_bytes + 3) / 4;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4; t += (long long)gridDim.x * blockDim.x) {
+    const long long x0 = 4 * t;
+    uint32_t code16 = 0, bad = 0;  // bases x0 .. x0+15: 2-bit codes (first base highest), invalid-base mask
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t w = x0 + 4 * j < n_bytes ? *reinterpret_cast<const uint32_t*>(read_bases + x0 + 4 * j) : 0u;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const long long x = x0 + 4 * j + b;
+        const int c = x < n_bytes ? kmer_code((uint8_t)(w >> (8 * b))) : -1;
+        code16 = (code16 << 2) | (uint32_t)(c & 3);
+        bad |= (c < 0 ? 1u : 0u) << (4 * j + b);
+      }
     }
-    codes[x] = ok ? code : kNoCode;  // positions too close to a read's end are masked by the caller
+    uint32_t out[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const bool ok = x0 + q + kK <= n_bytes && ((bad >> q) & 0x7ffu) == 0u;
+      out[q] = ok ? (code16 >> (2 * (16 - kK - q))) & ((1u << (2 * kK)) - 1u) : kNoCode;
+    }
+    // positions too close to a read's end are masked by the caller
+    if (x0 + 4 <= n_bytes) {
+      *reinterpret_cast<uint4*>(codes + x0) = make_uint4(out[0], out[1], out[2], out[3]);
+    } else {
+      for (int q = 0; q < 4 && x0 + q < n_bytes; ++q) codes[x0 + q] = out[q];
+    }
   }
 }
 
@@ -216,15 +235,14 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
       if (head <= kEndRows) tri_hi = d + head;
     }
     total = __popc(vmask);
-    for (int o = 16; o > 0; o >>= 1) {
-      best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-      fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
-      lkey = max(lkey, __shfl_xor_sync(0xffffffffu, lkey, o));
-      smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
-      smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
-      tri_lo = min(tri_lo, __shfl_xor_sync(0xffffffffu, tri_lo, o));
-      tri_hi = max(tri_hi, __shfl_xor_sync(0xffffffffu, tri_hi, o));
-    }
+    // warp reductions (one REDUX each)
+    best = __reduce_max_sync(0xffffffffu, best);
+    fkey = __reduce_min_sync(0xffffffffu, fkey);
+    lkey = __reduce_max_sync(0xffffffffu, lkey);
+    smin = __reduce_min_sync(0xffffffffu, smin);
+    smax = __reduce_max_sync(0xffffffffu, smax);
+    tri_lo = __reduce_min_sync(0xffffffffu, tri_lo);
+    tri_hi = __reduce_max_sync(0xffffffffu, tri_hi);
     wbin[lane] = 0;
     wbin[lane + 32] = 0;
     __syncwarp();
@@ -295,16 +313,14 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
       if (head <= kEndRows) tri_hi = max(tri_hi, d + head);
       total += (int)c;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
-      fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
-      lkey = max(lkey, __shfl_xor_sync(0xffffffffu, lkey, o));
-      smin = min(smin, __shfl_xor_sync(0xffffffffu, smin, o));
-      smax = max(smax, __shfl_xor_sync(0xffffffffu, smax, o));
-      tri_lo = min(tri_lo, __shfl_xor_sync(0xffffffffu, tri_lo, o));
-      tri_hi = max(tri_hi, __shfl_xor_sync(0xffffffffu, tri_hi, o));
-      total += __shfl_xor_sync(0xffffffffu, total, o);
-    }
+    best = __reduce_max_sync(0xffffffffu, best);
+    fkey = __reduce_min_sync(0xffffffffu, fkey);
+    lkey = __reduce_max_sync(0xffffffffu, lkey);
+    smin = __reduce_min_sync(0xffffffffu, smin);
+    smax = __reduce_max_sync(0xffffffffu, smax);
+    tri_lo = __reduce_min_sync(0xffffffffu, tri_lo);
+    tri_hi = __reduce_max_sync(0xffffffffu, tri_hi);
+    total = __reduce_add_sync(0xffffffffu, total);
   }
   if (best == 0u) {
     no_seed(p, pi, lane);
@@ -342,11 +358,9 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
       peak = max(peak, cb[t]);
     }
     *reinterpret_cast<__nv_bfloat162*>(f + 2 * lane) = __floats2bfloat162_rn((float)cb[0] * inv, (float)cb[1] * inv);
-    for (int o = 16; o > 0; o >>= 1) {
-      win += __shfl_xor_sync(0xffffffffu, win, o);
-      nonzero += __shfl_xor_sync(0xffffffffu, nonzero, o);
-      peak = max(peak, __shfl_xor_sync(0xffffffffu, peak, o));
-    }
+    win = __reduce_add_sync(0xffffffffu, win);
+    nonzero = __reduce_add_sync(0xffffffffu, nonzero);
+    peak = __reduce_max_sync(0xffffffffu, peak);
     if (overflow) total = max(total, win);
     if (lane == 0) {
       // 16 scalars, written as two 16-byte stores
@@ -562,16 +576,31 @@ __global__ void __launch_bounds__(kMlpWarps * 32) k_mlp_forward(BandParams p) {
   __syncthreads();
   __nv_bfloat16* act = s.act[wib];
   const long long ntiles = (p.n_pairs + 15) / 16;
-  for (long long tile = blockIdx.x * (long long)kMlpWarps + wib; tile < ntiles; tile += (long long)gridDim.x * kMlpWarps) {
+  const long long tstride = (long long)gridDim.x * kMlpWarps;
+  // input tiles (16 pairs x kFeat, zero rows past the end) are loaded one tile ahead into registers
+  constexpr int kVec = 16 * kFeat / 8 / 32;  // 16-byte vectors per lane
+  static_assert(kVec * 32 * 8 == 16 * kFeat, "tile split");
+  uint4 pre[kVec];
+  auto load_tile = [&](long long tile) {
+#pragma unroll
+    for (int u = 0; u < kVec; ++u) {
+      const int x = lane + 32 * u, rr = x / (kFeat / 8), cc = (x % (kFeat / 8)) * 8;
+      const long long row = tile * 16 + rr;
+      pre[u] = (tile < ntiles && row < p.n_pairs) ? *reinterpret_cast<const uint4*>(p.feat + row * kFeat + cc)
+                                                  : make_uint4(0, 0, 0, 0);
+    }
+  };
+  long long tile = blockIdx.x * (long long)kMlpWarps + wib;
+  load_tile(tile);
+  for (; tile < ntiles; tile += tstride) {
     const long long row0 = tile * 16;
-    // input tile: 16 pairs x kFeat, zero rows past the end
-    for (int x = lane; x < 16 * kFeat / 8; x += 32) {
-      const int rr = x / (kFeat / 8), cc = (x % (kFeat / 8)) * 8;
-      uint4 v = make_uint4(0, 0, 0, 0);
-      if (row0 + rr < p.n_pairs) v = *reinterpret_cast<const uint4*>(p.feat + (row0 + rr) * kFeat + cc);
-      *reinterpret_cast<uint4*>(act + rr * kLdH + cc) = v;
+#pragma unroll
+    for (int u = 0; u < kVec; ++u) {
+      const int x = lane + 32 * u, rr = x / (kFeat / 8), cc = (x % (kFeat / 8)) * 8;
+      *reinterpret_cast<uint4*>(act + rr * kLdH + cc) = pre[u];
     }
     __syncwarp();
+    load_tile(tile + tstride);
     float acc[16][4];
 #pragma unroll
     for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
@@ -631,7 +660,7 @@ __device__ __forceinline__ bool route_band(const BandParams& p, long long pi, in
   const int blo = min(ds + (int)floorf(lo) - p.margin, km), bhi = max(ds + (int)ceilf(hi) + p.margin, kx);
   const int width = bhi - blo + 1;
   if (width > band_width(kBandWidths - 1) || width < 1) return false;
-  cls = width <= band_width(0) ? 0 : width <= band_width(1) ? 1 : 2;
+  cls = (width - 1) / 8;  // band_width(cls) = 8 (cls + 1) >= width
   d_lo = blo - (band_width(cls) - width) / 2;
   return true;
 }
@@ -1329,7 +1358,10 @@ __global__ void k_audit_units(BandParams p, Unit* units) {
     const long long pi = p.audit_pairs[a];
     Unit u{};
     u.read = p.pair_read[pi]; u.hap0 = p.pair_hap[pi]; u.nh = 1; u.out0 = (long long)a;
-    units[a] = u;
+    const int R = (int)(p.batch.read_off[u.read + 1] - p.batch.read_off[u.read]);
+    const int v = full_variant(R);
+    const unsigned long long q = atomicAdd(&p.bctr->audit_var[v], 1ull);
+    units[(size_t)v * p.audit_cap + q] = u;  // q < n <= audit_cap
   }
 }
 
@@ -1365,7 +1397,7 @@ cudaError_t launch_pairs_from_units(const Unit* units, long long n_units, int32_
 
 cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint32_t* codes, int sms, cudaStream_t st) {
   if (n_bytes <= 0) return cudaSuccess;
-  const long long blocks = std::min<long long>((n_bytes + 255) / 256, (long long)sms * 16);
+  const long long blocks = std::min<long long>(((n_bytes + 3) / 4 + 255) / 256, (long long)sms * 16);
   k_read_kmers<<<(int)blocks, 256, 0, st>>>(read_bases, n_bytes, codes);
   return cudaGetLastError();
 }
@@ -1425,8 +1457,10 @@ cudaError_t launch_band_dp(const BandParams& p, int cls, int sms, cudaStream_t s
     k_band_f32<8><<<blocks, 128, 0, st>>>(p, 0);
   } else if (cls == 1) {
     k_band_f32<16><<<blocks, 128, 0, st>>>(p, 1);
+  } else if (cls == 2) {
+    k_band_f32<24><<<blocks, 128, 0, st>>>(p, 2);
   } else {
-    k_band_f32<32><<<blocks, 128, 0, st>>>(p, 2);
+    k_band_f32<32><<<blocks, 128, 0, st>>>(p, 3);
   }
   return cudaGetLastError();
 }

@@ -14,8 +14,8 @@
 //   k_band_pair_f32<W>  banded forward-backward, one thread per two pairs of a
 //                       read that route to the same class (W = 8), packed
 //                       FP32x2 arithmetic, edge-mass check per pair
-//   k_band_f32<W>       the same for single pairs (and every W = 32 pair);
-//                       classes W = 8, 16, 32 run in that order, and a pair
+//   k_band_f32<W>       the same for single pairs (and every W >= 16 pair);
+//                       classes W = 8, 16, 24, 32 run in that order, and a pair
 //                       that fails the check is promoted, as a single item, to
 //                       the next wider band
 // Pairs that leave the band path (routed out, or failing at W = 32) go to the
@@ -38,11 +38,11 @@ constexpr int kOut = 2;                // outputs: lower and upper band edge (di
 constexpr int kHistBins = 64;          // histogram window: d* - 32 .. d* + 31
 constexpr int kBandMaxSpan = 2048;     // read_len + hap_len limit of the featuriser (per-warp histogram)
 constexpr int kBandMaxHap = 1024;      // haplotype limit of the k-mer sort and the featuriser's staging
-constexpr int kBandWidths = 3;         // width classes of the banded kernel
+constexpr int kBandWidths = 4;         // width classes of the banded kernel
 #if defined(__CUDACC__)
 __host__ __device__
 #endif
-constexpr int band_width(int cls) { return cls == 0 ? 8 : cls == 1 ? 16 : 32; }
+constexpr int band_width(int cls) { return 8 * (cls + 1); }  // 8, 16, 24, 32 diagonals
 constexpr int kRBuckets = 64;          // read-length buckets (8 rows each) for warp-uniform band launches
 constexpr int kRBucketRows = 8;
 constexpr int kBandMaxRead = kRBuckets * kRBucketRows - 1;
@@ -88,6 +88,7 @@ struct BandCounters {
   unsigned long long promoted[kBandWidths];               // items promoted from the next narrower class
   unsigned long long full_count[16];                      // fallback items per full-DP variant
   unsigned long long audit_count;
+  unsigned long long audit_var[16];                       // audit units per full-DP variant
   unsigned long long fallback_edge;                       // pairs sent back by the edge check
   unsigned long long fallback_route;                      // pairs routed to the full DP up front
   unsigned long long band_cells;
@@ -150,7 +151,8 @@ inline int feat_blocks(int sms) { return sms * 5; }
 inline long long feat_hist_words(int sms) { return (long long)feat_blocks(sms) * kFeatWarpsPerBlock * (kBandMaxRead + kBandMaxHap); }
 // Sets the dynamic shared-memory limits of the band kernels (before any capture).
 cudaError_t prepare_band_kernels();
-// audit: full-DP units for the sampled pairs (out = audit slot), then the differences
+// audit: full-DP units for the sampled pairs (out = audit slot), listed per full-DP
+// variant ([9][audit_cap]), then the differences
 cudaError_t launch_audit_units(const BandParams& p, Unit* units, cudaStream_t st);
 cudaError_t launch_audit_compare(const BandParams& p, double* err, cudaStream_t st);
 

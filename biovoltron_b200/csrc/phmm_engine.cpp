@@ -272,7 +272,7 @@ bv_status Engine::upload(const bv_region_batch& b) {
   n_read_bytes_ = b.num_reads > 0 ? b.read_offsets[b.num_reads] : 0;
   n_hap_bytes_ = b.num_haps > 0 ? b.hap_offsets[b.num_haps] : 0;
   const size_t rb = (size_t)std::max<int64_t>(n_read_bytes_, 1);
-  BV_CUDA(d_read_bases_.reserve(rb), "alloc reads");
+  BV_CUDA(d_read_bases_.reserve(rb + 16), "alloc reads");  // tail padding for the k-mer kernel's word loads
   BV_CUDA(d_q_.reserve(rb), "alloc q");
   BV_CUDA(d_i_.reserve(rb), "alloc i");
   BV_CUDA(d_d_.reserve(rb), "alloc d");
@@ -465,7 +465,7 @@ bv_status Engine::run(bv_phmm_stats* stats) {
     stats->underflow = (int64_t)c.underflow_count;
     stats->kernel_launches = band_enabled()
                                  ? 6 + (band_opt_.use_mlp ? 1 : 0) + kBandWidths + kPairedClasses + 9 +
-                                       (band_opt_.audit_period > 0 ? 3 : 0) + 1
+                                       (band_opt_.audit_period > 0 ? 11 : 0) + 1
                                  : (int64_t)plans_.size() + 1;
     stats->ms_fp32 = ms32;
     stats->ms_fp64 = ms64;

@@ -102,7 +102,7 @@ bv_status Engine::band_prepare() {
   BV_CUDA(d_band_items2_.reserve(sizeof(BandItem2) * kPairedClasses * item2_cap_), "alloc paired band items");
   BV_CUDA(d_full_items_.reserve(sizeof(Unit) * 9 * full_cap_), "alloc fallback units");
   BV_CUDA(d_audit_pairs_.reserve(sizeof(int64_t) * audit_cap_), "alloc audit");
-  BV_CUDA(d_audit_units_.reserve(sizeof(Unit) * audit_cap_), "alloc audit");
+  BV_CUDA(d_audit_units_.reserve(sizeof(Unit) * 9 * audit_cap_), "alloc audit");
   BV_CUDA(d_audit_out_.reserve(sizeof(double) * audit_cap_), "alloc audit");
   BV_CUDA(d_audit_err_.reserve(sizeof(double) * audit_cap_), "alloc audit");
   // Fallback launches: one persistent launch per full-DP variant, sized for the
@@ -165,18 +165,21 @@ bv_status Engine::enqueue_band(bool capturing, KernelParams& kp) {
   }
   if (band_opt_.audit_period > 0) {
     BV_CUDA(launch_audit_units(p, d_audit_units_.as<Unit>(), stream_), "audit units");
-    KernelParams ak = kp;
-    const LaunchPlan& lp = full_plans_[8];
-    ak.units = d_audit_units_.as<Unit>();
-    ak.n_units_dev = &d_bctr_.as<BandCounters>()->audit_count;
-    ak.slot = 14;
-    ak.hap_bytes = lp.hap_bytes;
-    ak.warp_smem_bytes = lp.warp_smem;
-    ak.bnd = d_bnd32_.get();
-    ak.bnd_cols = lp.bnd_cols;
-    ak.out = d_audit_out_.as<double>();
-    ak.rescue = nullptr;  // audit pairs that need FP64 are left out of the comparison
-    BV_CUDA(launch_forward(8, ak, lp.grid, stream_), "audit full DP");
+    // the audit pairs' full DP, on the variant each read length takes
+    for (int v = 0; v < 9; ++v) {
+      KernelParams ak = kp;
+      const LaunchPlan& lp = full_plans_[v];
+      ak.units = d_audit_units_.as<Unit>() + (size_t)v * audit_cap_;
+      ak.n_units_dev = &d_bctr_.as<BandCounters>()->audit_var[v];
+      ak.slot = 16 + v;
+      ak.hap_bytes = lp.hap_bytes;
+      ak.warp_smem_bytes = lp.warp_smem;
+      ak.bnd = lp.multi ? d_bnd32_.get() : nullptr;
+      ak.bnd_cols = lp.bnd_cols;
+      ak.out = d_audit_out_.as<double>();
+      ak.rescue = nullptr;  // audit pairs that need FP64 are left out of the comparison
+      BV_CUDA(launch_forward(v, ak, lp.grid, stream_), "audit full DP");
+    }
   }
   kp.n_units_dev = nullptr;
   return BV_OK;

@@ -47,7 +47,7 @@ constexpr int kRT = 4;
 constexpr int kMaxHap = BV_PHMM_NOALLOC_MAX_HAP_LEN;
 constexpr long long kBndCols = ((kMaxHap + kWarp - 1 + 31) / 32) * 32 + 128;  // as the allocating path sizes them
 constexpr int kHapBytes = ((kMaxHap + (kWarp - 1) + 32 + kHapLead + 16 + 15) / 16) * 16;
-constexpr size_t kCountersBytes = 256;
+constexpr size_t kCountersBytes = 512;
 constexpr size_t kTablesBytes = (sizeof(Tables) + 255) / 256 * 256;
 constexpr size_t kBndBytes = (size_t)kWarps * kBndCols * 4 * sizeof(double);
 constexpr size_t kScratchBytes = kCountersBytes + kTablesBytes + kBndBytes;
@@ -69,7 +69,7 @@ unsigned long long g_status_host[kMaxDevices];
 
 __global__ void k_noalloc_reset(Counters* c) {
   if (threadIdx.x == 0) {
-    for (int k = 0; k < 16; ++k) c->unit_next[k] = 0;
+    for (int k = 0; k < (int)(sizeof(c->unit_next) / sizeof(c->unit_next[0])); ++k) c->unit_next[k] = 0;
     c->rescue_count = 0;
     c->rescue_next = 0;
     c->underflow_count = 0;

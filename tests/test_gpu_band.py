@@ -43,7 +43,7 @@ def test_fixed_band_matches_oracle_band(oracle):
         width = bhi - blo + 1
         if width > 32:
             continue
-        W_cls = 8 if width <= 8 else 16 if width <= 16 else 32
+        W_cls = 8 * ((width - 1) // 8 + 1)  # classes of 8, 16, 24 and 32 diagonals
         d_lo.append(blo - (W_cls - width) // 2)
         wcls.append(W_cls)
         sel.append(k)
