@@ -669,6 +669,7 @@ __device__ __forceinline__ bool route_band(const BandParams& p, long long pi, in
 // (counter, block); pass 1 reserves each bucket's range for the block at once.
 // A thread routes the result slots 2t and 2t+1: when both are banded in the
 // same paired class and belong to the same read they become one paired item.
+constexpr bool kPairRouting = false;  // the ring kernels take single pairs
 constexpr int kSlotPair = kBandWidths * kRBuckets;
 constexpr int kSlotFull = kSlotPair + kPairedClasses * kRBuckets;
 constexpr int kRouteSlots = kSlotFull + 9;
@@ -698,7 +699,7 @@ __global__ void __launch_bounds__(256) k_band_route(BandParams p, int pass) {
         const int H = (int)(p.batch.hap_off[hp[q] + 1] - p.batch.hap_off[hp[q]]);
         band[q] = route_band(p, pi, R[q], H, cls[q], d_lo[q]);
       }
-      paired = band[0] && band[1] && cls[0] == cls[1] && cls[0] < kPairedClasses && rd[0] == rd[1];
+      paired = kPairRouting && band[0] && band[1] && cls[0] == cls[1] && cls[0] < kPairedClasses && rd[0] == rd[1];
       if (paired) {
         slot[0] = kSlotPair + cls[0] * kRBuckets + min(R[0] / kRBucketRows, kRBuckets - 1);
         local[0] = atomicAdd(&cnt[slot[0]], 1u);
@@ -919,6 +920,161 @@ __device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb
   for (int x = threadIdx.x; x < 128; x += blockDim.x) sm.qp[x] = tb->qp[x];
   for (int x = threadIdx.x; x < kMMEntries; x += blockDim.x) sm.mm[x] = tb->mm_f[x];
   __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Ring test.  A pair banded on [d_lo, d_lo + W) is also scored on the band
+// widened by a ring of four diagonals on each side (eight for W >= 16); the
+// wider band's likelihood is the result, and the pair is promoted to the next
+// class (whose band is centred on this one) when the ring adds more than
+// edge_threshold of it.  Unlike a posterior test on the band's edge
+// diagonals, the ring also sees mass that enters the band from outside (an
+// alignment start or end on a diagonal next to the band), which a banded
+// model cannot represent.  W = 8 runs both bands in one row sweep (shared row
+// constants and emissions); the wider classes run them one after the other.
+// ---------------------------------------------------------------------------
+template <int WB, int WI>
+__device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Tables* tb, const uchar4* __restrict__ quals,
+                                               const uint8_t* __restrict__ rbase, const uint8_t* __restrict__ hap,
+                                               int R, int H, int d) {
+  constexpr int NW = WB / 8;
+  constexpr int OFF = (WB - WI) / 2;  // inner band = outer diagonals OFF .. OFF + WI - 1
+  constexpr int WIN = WI > 0 ? WI : 1;
+  float M[WB], X[WB], Y[WB], Mi[WIN], Xi[WIN], Yi[WIN];
+  const float init_y = tb->init_f / (float)H;
+#pragma unroll
+  for (int k = 0; k < WB; ++k) {
+    const int c = d + k;
+    M[k] = 0.f; X[k] = 0.f;
+    Y[k] = (c >= 0 && c <= H) ? init_y : 0.f;
+  }
+#pragma unroll
+  for (int k = 0; k < WIN; ++k) {
+    const int c = d + OFF + k;
+    Mi[k] = 0.f; Xi[k] = 0.f;
+    Yi[k] = (WI > 0 && c >= 0 && c <= H) ? init_y : 0.f;
+  }
+  uint32_t win[NW];  // row 1: columns d + 1 + k
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int c = d + 1 + w * 8 + t;
+      v |= ((c >= 1 && c <= H) ? onehot(hap[c - 1]) : 0u) << (4 * t);
+    }
+    win[w] = v;
+  }
+  float pmx_last = 1.f;
+  FwdRow cur = fwd_row(sm.qp, sm.mm, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
+  uchar4 qn = quals[min(1, R - 1)];
+  uint8_t bn = rbase[min(1, R - 1)];
+  for (int r = 1; r <= R; ++r) {
+    const FwdRow nxt = fwd_row(sm.qp, sm.mm, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
+    {
+      const int rn = min(r + 1, R - 1);  // row r + 2
+      qn = quals[rn];
+      bn = rbase[rn];
+    }
+    const int cn = r + 1 + d + WB - 1;  // next row's window: shift, append column cn
+    const uint8_t hb = (cn >= 1 && cn <= H) ? hap[cn - 1] : (uint8_t)0;
+    float lm = 0.f, ly = 0.f, lmi = 0.f, lyi = 0.f;
+#pragma unroll
+    for (int k = 0; k < WB; ++k) {
+      const bool match = (win[k >> 3] & cur.rb & (0xFu << (4 * (k & 7)))) != 0u;
+      const float e = match ? cur.em : cur.ex;
+      {
+        const float upm = (k + 1 < WB) ? M[k + 1] : 0.f;
+        const float upx = (k + 1 < WB) ? X[k + 1] : 0.f;
+        const float mn = e * __fmaf_rn(cur.mm, M[k], __fmaf_rn(cur.cx, X[k], cur.cy * Y[k]));
+        const float xn = __fmaf_rn(cur.kap, upx, upm);
+        const float yn = __fmaf_rn(cur.g, ly, lm);
+        M[k] = mn; X[k] = xn; Y[k] = yn;
+        lm = mn; ly = yn;
+      }
+      if constexpr (WI > 0) {
+        if (k >= OFF && k < OFF + WI) {
+          const int ki = k - OFF;
+          const float upm = (ki + 1 < WI) ? Mi[ki + 1] : 0.f;
+          const float upx = (ki + 1 < WI) ? Xi[ki + 1] : 0.f;
+          const float mn = e * __fmaf_rn(cur.mm, Mi[ki], __fmaf_rn(cur.cx, Xi[ki], cur.cy * Yi[ki]));
+          const float xn = __fmaf_rn(cur.kap, upx, upm);
+          const float yn = __fmaf_rn(cur.g, lyi, lmi);
+          Mi[ki] = mn; Xi[ki] = xn; Yi[ki] = yn;
+          lmi = mn; lyi = yn;
+        }
+      }
+    }
+    const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
+#pragma unroll
+    for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
+    win[NW - 1] = (win[NW - 1] >> 4) | (nib << 28);
+    pmx_last = cur.pmx;
+    cur = nxt;
+  }
+  float tot = 0.f, toti = 0.f;
+#pragma unroll
+  for (int k = 0; k < WB; ++k) {
+    const int c = R + d + k;
+    tot += (c >= 1 && c <= H) ? M[k] + pmx_last * X[k] : 0.f;
+  }
+#pragma unroll
+  for (int k = 0; k < WIN; ++k) {
+    const int c = R + d + OFF + k;
+    toti += (WI > 0 && c >= 1 && c <= H) ? Mi[k] + pmx_last * Xi[k] : 0.f;
+  }
+  return make_float2(tot, toti);
+}
+
+// One band alone, not inlined: the two passes of the wider classes then hold
+// one band's state at a time.
+template <int WB>
+__device__ __noinline__ float band_forward_pass(const BandSmem& sm, const Tables* tb, const uchar4* quals,
+                                                const uint8_t* rbase, const uint8_t* hap, int R, int H, int d) {
+  return band_forward_body<WB, 0>(sm, tb, quals, rbase, hap, R, H, d).x;
+}
+
+template <int W>
+__global__ void __launch_bounds__(128) k_band_ring_f32(BandParams p, int cls) {
+  constexpr bool kDual = W <= 8;  // both bands in one sweep
+  // ring width on each side: pairs routed to wider bands have indel-rich alignments whose
+  // alternatives lie farther out, so W >= 16 test eight diagonals
+  constexpr int kRing = W >= 16 ? 8 : 4;
+  const Tables* tb = p.tables;
+  __shared__ BandSmem sm;
+  stage_band_tables(sm, tb);
+  // routed items (bucketed by read length), then items promoted from the next narrower class
+  const unsigned long long total =
+      p.bctr->band_total[cls] + min(p.bctr->promoted[cls], (unsigned long long)p.item_cap - p.bctr->band_total[cls]);
+  const BandItem* items = p.items + (size_t)cls * p.item_cap;
+  const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  unsigned long long cells = 0;
+  for (unsigned long long ii = tid; ii < total; ii += nthreads) {
+    const BandItem it = items[ii];
+    const int64_t ro = p.batch.read_off[it.read], ho = p.batch.hap_off[it.hap];
+    const int R = (int)(p.batch.read_off[it.read + 1] - ro), H = (int)(p.batch.hap_off[it.hap + 1] - ho);
+    const uchar4* quals = p.batch.read_quals + ro;
+    const uint8_t* rbase = p.batch.read_bases + ro;
+    const uint8_t* hap = p.batch.hap_bases + ho;
+    float lin, lout;
+    if constexpr (kDual) {
+      const float2 t = band_forward_body<W + 2 * kRing, W>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
+      lout = t.x;
+      lin = t.y;
+    } else {
+      lin = band_forward_pass<W>(sm, tb, quals, rbase, hap, R, H, it.d_lo);
+      lout = band_forward_pass<W + 2 * kRing>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
+    }
+    cells += (unsigned long long)R * (2 * W + 2 * kRing);
+    bool fall_back = !(lout > 0.f);
+    const bool rescue = !fall_back && (!(lout >= (float)kMinAccepted) || isinf(lout));
+    // the ring's share of the outer likelihood (NaN or a negative share fall back too)
+    if (!fall_back && !rescue) fall_back = !(lout - lin <= p.edge_threshold * lout && lin >= 0.f);
+    band_outcome(p, cls, it, R, lout, fall_back, rescue);
+  }
+  for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
+  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(&p.bctr->band_cells, cells);
 }
 
 template <int W>
@@ -1451,16 +1607,14 @@ cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st) {
 
 cudaError_t launch_band_dp(const BandParams& p, int cls, int sms, cudaStream_t st) {
   const int blocks = band_dp_blocks(sms);
-  // paired items of the class first, then its single items (routed and promoted)
   if (cls == 0) {
-    k_band_pair_f32<8><<<blocks, 128, 0, st>>>(p, 0);
-    k_band_f32<8><<<blocks, 128, 0, st>>>(p, 0);
+    k_band_ring_f32<8><<<blocks, 128, 0, st>>>(p, 0);
   } else if (cls == 1) {
-    k_band_f32<16><<<blocks, 128, 0, st>>>(p, 1);
+    k_band_ring_f32<16><<<blocks, 128, 0, st>>>(p, 1);
   } else if (cls == 2) {
-    k_band_f32<24><<<blocks, 128, 0, st>>>(p, 2);
+    k_band_ring_f32<24><<<blocks, 128, 0, st>>>(p, 2);
   } else {
-    k_band_f32<32><<<blocks, 128, 0, st>>>(p, 3);
+    k_band_ring_f32<32><<<blocks, 128, 0, st>>>(p, 3);
   }
   return cudaGetLastError();
 }
