@@ -11,8 +11,10 @@ region +-75 bp with SNV/indel alleles at 1/1000 bp; q ~ U(10, 40), i = d =
 The full chosen form runs: the band MLP is first trained on the GPU (labels
 from the full DP's posterior spreads, 1M pairs drawn from config 1's
 distribution, its own seed); then every step scores the whole batch with the
-learned band (featuriser, BF16 MLP, banded forward-backward with edge-mass
-fallback to the full DP, sampled audit) and FP32 with FP64 rescue.  The plain
+learned band (featuriser, BF16 MLP, banded forward pass with the ring test
+-- the band widened by 4 or 8 diagonals per side is the result, a ring share
+above the threshold widens the band, after 32 diagonals the full DP takes the
+pair -- and a sampled audit against the full DP) and FP32 with FP64 rescue.  The plain
 full-DP kernels score the same batch in the same run for the comparison.
 
 * value        pairs/s of the full chosen form with the batch resident in HBM
@@ -25,9 +27,9 @@ full-DP kernels score the same batch in the same run for the comparison.
 * accuracy     max / p99 |dlog10L| of both forms against the FP64 oracle on a
                seeded sample of pairs, and of the band against the full DP on
                every pair.
-* roofline     the dominant kernel (the banded forward-backward) against the
-               measured FP32 FMA peak, 12 algorithmic flops per band-cell
-               update; roofline_plain the full-DP kernels, 12 flops per cell
+* roofline     the dominant kernels (the banded forward passes) against the
+               measured FP32 FMA peak, 12 algorithmic flops per band cell;
+               roofline_plain the full-DP kernels, 12 flops per cell
                (the reference's computeMXY count).
 * cpu_baseline Biovoltron's own AVX PairHMM kernel (oracle/_ref, compiled from
                the reference sources) on all host cores, on a seeded sample of
@@ -308,7 +310,7 @@ def main():
     ap.add_argument("--save-weights", default="", help="write the trained band MLP weights here")
     ap.add_argument("--audit-period", type=int, default=1024)
     ap.add_argument("--oracle-sample", type=int, default=20000)
-    ap.add_argument("--edge-threshold", type=float, default=3e-3)
+    ap.add_argument("--edge-threshold", type=float, default=1e-3)
     ap.add_argument("--margin", type=int, default=2, help="diagonals added on both sides of the predicted band")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -437,18 +439,18 @@ def main():
             band_cells = int(last["band_cells"])
             ach = FLOPS_PER_CELL * band_cells / (ms_band / 1e3) / 1e12 if ms_band > 0 else 0.0
             line["band"] = {
-                "kernel_ms": {"seed_features_mlp_route": mean(band, "ms_seed"), "banded_fwd_bwd": ms_band,
+                "kernel_ms": {"seed_features_mlp_route": mean(band, "ms_seed"), "banded_dp": ms_band,
                               "fallback_full_dp": mean(band, "ms_full"), "fp64_rescue": mean(band, "ms_fp64")},
                 "band_pairs": int(last["band_pairs"]), "routed_full": int(last["band_routed_full"]),
                 "edge_fallback": int(last["band_fallback"]), "promoted": int(last["band_promoted"]),
                 "fallback_rate": (int(last["band_routed_full"]) + int(last["band_fallback"])) / max(n, 1),
-                "band_cell_updates": band_cells, "rescued": int(last["rescued"]),
+                "band_cells": band_cells, "rescued": int(last["rescued"]),
                 "audit_pairs": int(last["audit_pairs"]), "audit_max_err": float(last["audit_max_err"]),
                 "audit_p99_err": float(last["audit_p99_err"]), "train": train_rep}
-            line["roofline"] = {"bound": "fp32", "kernel": "k_band_f32<W> / k_band_pair_f32<8> (banded forward-backward, W = 8/16/24/32)",
+            line["roofline"] = {"bound": "fp32", "kernel": "k_band_ring_f32<W> (banded forward, band and ring, W = 8/16/24/32)",
                                 "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
                                 "frac": (ach / fp32_peak) if fp32_peak else None,
-                                "flops_per_cell_update": FLOPS_PER_CELL, "traffic": None}
+                                "flops_per_cell": FLOPS_PER_CELL, "traffic": None}
         else:
             line["roofline"] = line.get("roofline_plain")
         line["peak_source"] = "measured: FP32 FMA probe kernel in this run (bv_phmm_measure_fp32_peak)"

@@ -667,119 +667,70 @@ __device__ __forceinline__ bool route_band(const BandParams& p, long long pi, in
 
 // Block-aggregated: per-block shared counters, one global atomic per
 // (counter, block); pass 1 reserves each bucket's range for the block at once.
-// A thread routes the result slots 2t and 2t+1: when both are banded in the
-// same paired class and belong to the same read they become one paired item.
-constexpr bool kPairRouting = false;  // the ring kernels take single pairs
-constexpr int kSlotPair = kBandWidths * kRBuckets;
-constexpr int kSlotFull = kSlotPair + kPairedClasses * kRBuckets;
+constexpr int kSlotFull = kBandWidths * kRBuckets;
 constexpr int kRouteSlots = kSlotFull + 9;
 
 __global__ void __launch_bounds__(256) k_band_route(BandParams p, int pass) {
   __shared__ unsigned int cnt[kRouteSlots];
   __shared__ unsigned long long base[kRouteSlots];
-  const long long n2 = (p.n_pairs + 1) / 2;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long t0 = blockIdx.x * (long long)blockDim.x; t0 < n2; t0 += stride) {
+  for (long long pi0 = blockIdx.x * (long long)blockDim.x; pi0 < p.n_pairs; pi0 += stride) {
     for (int x = threadIdx.x; x < kRouteSlots; x += blockDim.x) cnt[x] = 0;
     __syncthreads();
-    const long long t = t0 + threadIdx.x;
-    int slot[2] = {-1, -1};
-    unsigned local[2] = {0u, 0u};
-    int rd[2] = {0, 0}, hp[2] = {0, 0}, d_lo[2] = {0, 0}, cls[2] = {0, 0}, R[2] = {0, 0};
-    bool band[2] = {false, false}, live[2] = {false, false}, paired = false;
-    if (t < n2) {
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const long long pi = 2 * t + q;
-        if (pi >= p.n_pairs) continue;
-        live[q] = true;
-        rd[q] = p.pair_read[pi];
-        hp[q] = p.pair_hap[pi];
-        R[q] = (int)(p.batch.read_off[rd[q] + 1] - p.batch.read_off[rd[q]]);
-        const int H = (int)(p.batch.hap_off[hp[q] + 1] - p.batch.hap_off[hp[q]]);
-        band[q] = route_band(p, pi, R[q], H, cls[q], d_lo[q]);
-      }
-      paired = kPairRouting && band[0] && band[1] && cls[0] == cls[1] && cls[0] < kPairedClasses && rd[0] == rd[1];
-      if (paired) {
-        slot[0] = kSlotPair + cls[0] * kRBuckets + min(R[0] / kRBucketRows, kRBuckets - 1);
-        local[0] = atomicAdd(&cnt[slot[0]], 1u);
-      } else {
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          if (!live[q]) continue;
-          slot[q] = band[q] ? cls[q] * kRBuckets + min(R[q] / kRBucketRows, kRBuckets - 1)
-                            : kSlotFull + full_variant(R[q]);
-          if (pass == 0 || band[q]) local[q] = atomicAdd(&cnt[slot[q]], 1u);
-        }
-      }
+    const long long pi = pi0 + threadIdx.x;
+    int slot = -1;
+    unsigned local = 0;
+    int r = 0, h = 0, d_lo = 0, R = 0, cls = 0;
+    bool band = false;
+    if (pi < p.n_pairs) {
+      r = p.pair_read[pi];
+      h = p.pair_hap[pi];
+      R = (int)(p.batch.read_off[r + 1] - p.batch.read_off[r]);
+      const int H = (int)(p.batch.hap_off[h + 1] - p.batch.hap_off[h]);
+      band = route_band(p, pi, R, H, cls, d_lo);
+      slot = band ? cls * kRBuckets + min(R / kRBucketRows, kRBuckets - 1) : kSlotFull + full_variant(R);
+      if (pass == 0 || band) local = atomicAdd(&cnt[slot], 1u);
     }
     __syncthreads();
     for (int x = threadIdx.x; x < kRouteSlots; x += blockDim.x) {
       const unsigned c = cnt[x];
       if (c == 0) continue;
-      if (x < kSlotPair) {
+      if (x < kSlotFull) {
         const int cl = x / kRBuckets, bucket = x % kRBuckets;
         if (pass == 0) atomicAdd(&p.bctr->band_count[cl][bucket], (unsigned long long)c);
         else base[x] = atomicAdd(&p.bctr->band_fill[cl][bucket], (unsigned long long)c);
-      } else if (x < kSlotFull) {
-        const int cl = (x - kSlotPair) / kRBuckets, bucket = (x - kSlotPair) % kRBuckets;
-        if (pass == 0) atomicAdd(&p.bctr->band2_count[cl][bucket], (unsigned long long)c);
-        else base[x] = atomicAdd(&p.bctr->band2_fill[cl][bucket], (unsigned long long)c);
       } else if (pass == 0) {
         base[x] = atomicAdd(&p.bctr->full_count[x - kSlotFull], (unsigned long long)c);
         atomicAdd(&p.bctr->fallback_route, (unsigned long long)c);
       }
     }
     __syncthreads();
-    if (t < n2) {
-      if (paired) {
-        if (pass == 1) {
-          BandItem2 it;
-          it.read = rd[0];
-          it.hap[0] = hp[0]; it.hap[1] = hp[1];
-          it.d_lo[0] = d_lo[0]; it.d_lo[1] = d_lo[1];
-          it.pad_ = 0;
-          it.out[0] = 2 * t; it.out[1] = 2 * t + 1;
-          p.items2[(size_t)cls[0] * p.item2_cap + base[slot[0]] + local[0]] = it;
-        }
-      } else {
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          if (!live[q]) continue;
-          const long long pi = 2 * t + q;
-          if (band[q] && pass == 1) {
-            BandItem it;
-            it.read = rd[q]; it.hap = hp[q]; it.out = pi; it.d_lo = d_lo[q]; it.pad_ = 0;
-            p.items[(size_t)cls[q] * p.item_cap + base[slot[q]] + local[q]] = it;
-          } else if (!band[q] && pass == 0) {
-            const int v = slot[q] - kSlotFull;
-            const unsigned long long qq = base[slot[q]] + local[q];
-            if (qq < (unsigned long long)p.full_cap) {
-              Unit u{};
-              u.read = rd[q]; u.hap0 = hp[q]; u.nh = 1; u.out0 = pi;
-              p.full_items[(size_t)v * p.full_cap + qq] = u;
-            } else {
-              atomicOr(&p.ctr->status, 4ull);
-            }
-          }
+    if (pi < p.n_pairs) {
+      if (band && pass == 1) {
+        BandItem it;
+        it.read = r; it.hap = h; it.out = pi; it.d_lo = d_lo; it.pad_ = 0;
+        p.items[(size_t)cls * p.item_cap + base[slot] + local] = it;
+      } else if (!band && pass == 0) {
+        const int v = slot - kSlotFull;
+        const unsigned long long q = base[slot] + local;
+        if (q < (unsigned long long)p.full_cap) {
+          Unit u{};
+          u.read = r; u.hap0 = h; u.nh = 1; u.out0 = pi;
+          p.full_items[(size_t)v * p.full_cap + q] = u;
+        } else {
+          atomicOr(&p.ctr->status, 4ull);
         }
       }
-      if (pass == 0 && p.audit_period > 0) {
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const long long pi = 2 * t + q;
-          if (band[q] && pi % p.audit_period == 0) {
-            const unsigned long long a = atomicAdd(&p.bctr->audit_count, 1ull);
-            if (a < (unsigned long long)p.audit_cap) p.audit_pairs[a] = pi;
-          }
-        }
+      if (band && pass == 0 && p.audit_period > 0 && pi % p.audit_period == 0) {
+        const unsigned long long a = atomicAdd(&p.bctr->audit_count, 1ull);
+        if (a < (unsigned long long)p.audit_cap) p.audit_pairs[a] = pi;
       }
     }
     __syncthreads();
   }
 }
 
-// exclusive prefix over buckets, per width class (single and paired items)
+// exclusive prefix over buckets, per width class
 __global__ void k_band_scan(BandCounters* c) {
   if (threadIdx.x < kBandWidths) {
     unsigned long long acc = 0;
@@ -788,39 +739,7 @@ __global__ void k_band_scan(BandCounters* c) {
       acc += c->band_count[threadIdx.x][b];
     }
     c->band_total[threadIdx.x] = acc;
-  } else if (threadIdx.x >= 8 && threadIdx.x < 8 + kPairedClasses) {
-    const int cl = threadIdx.x - 8;
-    unsigned long long acc = 0;
-    for (int b = 0; b < kRBuckets; ++b) {
-      c->band2_fill[cl][b] = acc;
-      acc += c->band2_count[cl][b];
-    }
-    c->band2_total[cl] = acc;
   }
-}
-
-// ---------------------------------------------------------------------------
-// Banded forward-backward: one thread per pair, the band's state in
-// registers, rows swept top to bottom (forward) then bottom to top
-// (backward).  In band coordinates k = d - d_lo,
-//   forward   M(r,k) <- (r-1,k)   X(r,k) <- (r-1,k+1)   Y(r,k) <- (r,k-1)
-//   backward  B(r,k) <- B(r+1,k) via M, B(r+1,k-1) via X, B(r,k+1) via Y
-// with the FP32 scaled forward recurrence of the full kernel.  Cells left of
-// column 1 stay exactly zero in the forward (their inputs are zero); cells
-// right of column H never feed a cell inside the matrix in the forward and
-// are exactly zero in the backward (their successors lie right of H too).
-// The haplotype window is W one-hot nibbles, shifted one column per row; a
-// match is one AND against the read base's replicated nibble.
-//
-// Fallback test: the posterior mass on the band's two edge diagonals,
-//   sum_r [A(r,0) Bmax(r,0) + A(r,W-1) Bmax(r,W-1)] / L_band,
-// with A = M + X + Y forward and Bmax = max(B_M, B_X, B_Y) -- an upper bound on
-// sum_s F_s B_s at the cell.  The forward keeps A at the two edge cells per
-// row as a pair of BF16 in a per-thread slab (row r at slab[r * nthreads]).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ int mm_index(int qi, int qd) {
-  const int mx = max(qi, qd), mn = min(qi, qd);
-  return ((mx * (mx + 1)) >> 1) + mn;
 }
 
 // A banded pair's outcome: promotion to the next wider class (a single item
@@ -864,10 +783,15 @@ __device__ __forceinline__ void band_outcome(const BandParams& p, int cls, const
   }
 }
 
-// Row constants of the banded recurrences, from the row's quality bytes and
-// the row above's pMX / pMY (forward) or the next row's bytes (backward).
-// The kernels compute them one row ahead, with the quality bytes loaded two
-// rows ahead, so the table lookups overlap the previous row's cells.
+// Row constants of the banded recurrence, from the row's quality bytes and
+// the row above's pMX / pMY.  The kernels compute them one row ahead, with the
+// quality bytes loaded two rows ahead, so the table lookups overlap the
+// previous row's cells.
+__device__ __forceinline__ int mm_index(int qi, int qd) {
+  const int mx = max(qi, qd), mn = min(qi, qd);
+  return ((mx * (mx + 1)) >> 1) + mn;
+}
+
 struct FwdRow {
   float mm, cx, cy, kap, g, pmx, pmy, em, ex;
   uint32_t rb;  // the read base's one-hot nibble, replicated 8 times
@@ -890,27 +814,6 @@ __device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, uch
   c.rb = onehot(base) * 0x11111111u;
   return c;
 }
-struct BwdRow {
-  float mm1, mx1, g1, gp1, em1, ex1, my0, g0;
-  uint32_t rb1;
-};
-// q1, base1: row r+1; q0: row r
-__device__ __forceinline__ BwdRow bwd_row(const QProb* qp, const float* mmt, uchar4 q1, uint8_t base1, uchar4 q0) {
-  BwdRow c;
-  const int qi1 = q1.y & kQualMask, qd1 = q1.z & kQualMask;
-  c.mm1 = mmt[mm_index(qi1, qd1)];
-  c.mx1 = qp[qi1].p;
-  const QProb qg1 = qp[q1.w & kQualMask], qb1 = qp[q1.x & kQualMask];
-  c.g1 = qg1.p;
-  c.gp1 = qg1.q;
-  c.em1 = qb1.q;
-  c.ex1 = qb1.third;
-  c.my0 = qp[q0.z & kQualMask].p;
-  c.g0 = qp[q0.w & kQualMask].p;
-  c.rb1 = onehot(base1) * 0x11111111u;
-  return c;
-}
-
 // Stages the probability tables the band kernels read per row into shared memory.
 struct BandSmem {
   QProb qp[128];
@@ -1077,436 +980,6 @@ __global__ void __launch_bounds__(128) k_band_ring_f32(BandParams p, int cls) {
   if ((threadIdx.x & 31) == 0 && cells) atomicAdd(&p.bctr->band_cells, cells);
 }
 
-template <int W>
-__global__ void __launch_bounds__(128) k_band_f32(BandParams p, int cls) {
-  constexpr int NW = W / 8;
-  const Tables* tb = p.tables;
-  __shared__ BandSmem sm;
-  stage_band_tables(sm, tb);
-  const QProb* qp = sm.qp;
-  // routed items (bucketed by read length), then items promoted from the next narrower class
-  const unsigned long long total =
-      p.bctr->band_total[cls] + min(p.bctr->promoted[cls], (unsigned long long)p.item_cap - p.bctr->band_total[cls]);
-  const BandItem* items = p.items + (size_t)cls * p.item_cap;
-  const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
-  const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
-  uint32_t* slab = p.edge_slab + tid;
-  unsigned long long cells = 0;
-  for (unsigned long long ii = tid; ii < total; ii += nthreads) {
-    const BandItem it = items[ii];
-    const int64_t ro = p.batch.read_off[it.read], ho = p.batch.hap_off[it.hap];
-    const int R = (int)(p.batch.read_off[it.read + 1] - ro), H = (int)(p.batch.hap_off[it.hap + 1] - ho);
-    const uchar4* quals = p.batch.read_quals + ro;
-    const uint8_t* rbase = p.batch.read_bases + ro;
-    const uint8_t* hap = p.batch.hap_bases + ho;
-    const int d_lo = it.d_lo;
-    float M[W], X[W], Y[W];
-    const float init_y = tb->init_f / (float)H;
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-      const int c = d_lo + k;
-      M[k] = 0.f; X[k] = 0.f;
-      Y[k] = (c >= 0 && c <= H) ? init_y : 0.f;
-    }
-    uint32_t win[NW];  // row 1: columns d_lo + 1 + k
-#pragma unroll
-    for (int w = 0; w < NW; ++w) {
-      uint32_t v = 0;
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const int c = d_lo + 1 + w * 8 + t;
-        v |= ((c >= 1 && c <= H) ? onehot(hap[c - 1]) : 0u) << (4 * t);
-      }
-      win[w] = v;
-    }
-    float pmx_last = 1.f;
-    FwdRow cur = fwd_row(qp, sm.mm, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
-    uchar4 qn = quals[min(1, R - 1)];
-    uint8_t bn = rbase[min(1, R - 1)];
-    for (int r = 1; r <= R; ++r) {
-      const FwdRow nxt = fwd_row(qp, sm.mm, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
-      {
-        const int rn = min(r + 1, R - 1);  // row r + 2
-        qn = quals[rn];
-        bn = rbase[rn];
-      }
-      const int cn = r + 1 + d_lo + W - 1;  // next row's window: shift, append column cn
-      const uint8_t hb = (cn >= 1 && cn <= H) ? hap[cn - 1] : (uint8_t)0;
-      float lm = 0.f, ly = 0.f;
-#pragma unroll
-      for (int k = 0; k < W; ++k) {
-        const bool match = (win[k >> 3] & cur.rb & (0xFu << (4 * (k & 7)))) != 0u;
-        const float e = match ? cur.em : cur.ex;
-        const float upm = (k + 1 < W) ? M[k + 1] : 0.f;
-        const float upx = (k + 1 < W) ? X[k + 1] : 0.f;
-        const float mn = e * __fmaf_rn(cur.mm, M[k], __fmaf_rn(cur.cx, X[k], cur.cy * Y[k]));
-        const float xn = __fmaf_rn(cur.kap, upx, upm);
-        const float yn = __fmaf_rn(cur.g, ly, lm);
-        M[k] = mn; X[k] = xn; Y[k] = yn;
-        lm = mn; ly = yn;
-      }
-      // edge cells' A = M + X + Y (true X, Y) for the backward's posterior test
-      const float a0 = M[0] + cur.pmx * X[0] + cur.pmy * Y[0];
-      const float a1 = M[W - 1] + cur.pmx * X[W - 1] + cur.pmy * Y[W - 1];
-      const __nv_bfloat162 pk = __floats2bfloat162_rn(a0, a1);
-      slab[(size_t)r * nthreads] = *reinterpret_cast<const uint32_t*>(&pk);
-      const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
-#pragma unroll
-      for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
-      win[NW - 1] = (win[NW - 1] >> 4) | (nib << 28);
-      pmx_last = cur.pmx;
-      cur = nxt;
-    }
-    float tot = 0.f;
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-      const int c = R + d_lo + k;
-      tot += (c >= 1 && c <= H) ? M[k] + pmx_last * X[k] : 0.f;
-    }
-    cells += (unsigned long long)R * W;
-    bool fall_back = !(tot > 0.f);
-    const bool rescue = !fall_back && (!(tot >= (float)kMinAccepted) || isinf(tot));
-    if (!fall_back && !rescue) {
-      // ---- backward: B in registers, renormalised by powers of two ----
-      float BM[W], BX[W], BY[W];
-#pragma unroll
-      for (int k = 0; k < W; ++k) {
-        const int c = R + d_lo + k;
-        const float v = (c >= 1 && c <= H) ? 1.f : 0.f;
-        BM[k] = v; BX[k] = v; BY[k] = 0.f;
-      }
-      double acc = 0.0;
-      double bscale = 1.0;  // true B = stored B * bscale (a power of two)
-      {
-        const __nv_bfloat162 pk = *reinterpret_cast<const __nv_bfloat162*>(&slab[(size_t)R * nthreads]);
-        acc += (double)__low2float(pk) * fmaxf(BM[0], BX[0]) + (double)__high2float(pk) * fmaxf(BM[W - 1], BX[W - 1]);
-      }
-      // window to row R's columns (R + d_lo + k): shift back one column
-      {
-        const int c0 = R + d_lo;
-        const uint32_t nib = (c0 >= 1 && c0 <= H) ? onehot(hap[c0 - 1]) : 0u;
-#pragma unroll
-        for (int w = NW - 1; w > 0; --w) win[w] = __funnelshift_l(win[w - 1], win[w], 4);
-        win[0] = (win[0] << 4) | nib;
-      }
-      // row r's constants use row r+1's bytes (q1) and row r's (q0); both are one row ahead
-      BwdRow cb = bwd_row(qp, sm.mm, quals[R - 1], rbase[R - 1], quals[max(R - 2, 0)]);
-      uchar4 qa = quals[max(R - 2, 0)], qb = quals[max(R - 3, 0)];
-      for (int r = R - 1; r >= 1; --r) {
-        const BwdRow nb = bwd_row(qp, sm.mm, qa, rbase[r - 1], qb);  // row r - 1 (unused after row 1)
-        qa = qb;
-        qb = quals[max(r - 3, 0)];
-        const int c0 = r + d_lo;
-        const uint8_t hb = (c0 >= 1 && c0 <= H) ? hap[c0 - 1] : (uint8_t)0;
-        float byn = 0.f;  // B_Y(r, k+1)
-#pragma unroll
-        for (int k = W - 1; k >= 0; --k) {
-          const bool match = (win[k >> 3] & cb.rb1 & (0xFu << (4 * (k & 7)))) != 0u;
-          const float e = match ? cb.em1 : cb.ex1;
-          const float emb = e * BM[k];
-          const float bxk = (k > 0) ? BX[k - 1] : 0.f;
-          const float nbm = __fmaf_rn(cb.mm1, emb, __fmaf_rn(cb.mx1, bxk, cb.my0 * byn));
-          const float nbx = __fmaf_rn(cb.gp1, emb, cb.g1 * bxk);
-          const float nby = __fmaf_rn(cb.gp1, emb, cb.g0 * byn);
-          BM[k] = nbm; BX[k] = nbx; BY[k] = nby;
-          byn = nby;
-        }
-        const __nv_bfloat162 pk = *reinterpret_cast<const __nv_bfloat162*>(&slab[(size_t)r * nthreads]);
-        const float b0 = fmaxf(BM[0], fmaxf(BX[0], BY[0])), b1 = fmaxf(BM[W - 1], fmaxf(BX[W - 1], BY[W - 1]));
-        acc += (double)(__low2float(pk) * b0 + __high2float(pk) * b1) * bscale;
-        if ((r & 7) == 0) {
-          float m = 0.f;
-#pragma unroll
-          for (int k = 0; k < W; ++k) m = fmaxf(m, fmaxf(BM[k], BX[k]));
-          if (m > 0.f && (m < 0x1p-60f || m > 0x1p60f)) {
-            int e2;
-            frexpf(m, &e2);
-            const float sc = ldexpf(1.f, -e2);
-#pragma unroll
-            for (int k = 0; k < W; ++k) { BM[k] *= sc; BX[k] *= sc; BY[k] *= sc; }
-            bscale = ldexp(bscale, e2);
-          }
-        }
-        // window to row r's columns: shift back one column, new k = 0 is column r + d_lo
-        const uint32_t nib = (c0 >= 1 && c0 <= H) ? onehot(hb) : 0u;
-#pragma unroll
-        for (int w = NW - 1; w > 0; --w) win[w] = __funnelshift_l(win[w - 1], win[w], 4);
-        win[0] = (win[0] << 4) | nib;
-        cb = nb;
-      }
-      cells += (unsigned long long)R * W;
-      const double edge = acc / (double)tot;
-      fall_back = !(edge <= (double)p.edge_threshold);
-    }
-    band_outcome(p, cls, it, R, tot, fall_back, rescue);
-  }
-  for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
-  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(&p.bctr->band_cells, cells);
-}
-
-// ---------------------------------------------------------------------------
-// Paired banded forward-backward: one thread scores two pairs of one read in
-// the same width class.  The read's row constants are computed once per row
-// and both pairs' band states are the halves of float2 values, so each
-// transition is one packed FP32x2 instruction; every half follows
-// k_band_f32's operation order, so a paired pair's result, edge statistics and
-// outcome equal the single kernel's.
-// ---------------------------------------------------------------------------
-template <int W>
-__global__ void __launch_bounds__(128) k_band_pair_f32(BandParams p, int cls) {
-  constexpr int NW = W / 8;
-  const Tables* tb = p.tables;
-  __shared__ BandSmem sm;
-  stage_band_tables(sm, tb);
-  const QProb* qp = sm.qp;
-  const unsigned long long total = p.bctr->band2_total[cls];
-  const BandItem2* items = p.items2 + (size_t)cls * p.item2_cap;
-  const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
-  const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
-  uint2* slab = reinterpret_cast<uint2*>(p.edge_slab) + tid;
-  unsigned long long cells = 0;
-  for (unsigned long long ii = tid; ii < total; ii += nthreads) {
-    const BandItem2 it = items[ii];
-    const int64_t ro = p.batch.read_off[it.read];
-    const int R = (int)(p.batch.read_off[it.read + 1] - ro);
-    const uchar4* quals = p.batch.read_quals + ro;
-    const uint8_t* rbase = p.batch.read_bases + ro;
-    int H[2], d_lo[2];
-    const uint8_t* hap[2];
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int64_t ho = p.batch.hap_off[it.hap[q]];
-      H[q] = (int)(p.batch.hap_off[it.hap[q] + 1] - ho);
-      hap[q] = p.batch.hap_bases + ho;
-      d_lo[q] = it.d_lo[q];
-    }
-    float2 M[W], X[W], Y[W];
-    const float init_y0 = tb->init_f / (float)H[0], init_y1 = tb->init_f / (float)H[1];
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-      const int c0 = d_lo[0] + k, c1 = d_lo[1] + k;
-      M[k] = make_float2(0.f, 0.f);
-      X[k] = make_float2(0.f, 0.f);
-      Y[k] = make_float2((c0 >= 0 && c0 <= H[0]) ? init_y0 : 0.f, (c1 >= 0 && c1 <= H[1]) ? init_y1 : 0.f);
-    }
-    uint32_t win[2][NW];  // row 1: columns d_lo + 1 + k
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-#pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        uint32_t v = 0;
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-          const int c = d_lo[q] + 1 + w * 8 + t;
-          v |= ((c >= 1 && c <= H[q]) ? onehot(hap[q][c - 1]) : 0u) << (4 * t);
-        }
-        win[q][w] = v;
-      }
-    }
-    float pmx_last = 1.f;
-    FwdRow cur = fwd_row(qp, sm.mm, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
-    uchar4 qn = quals[min(1, R - 1)];
-    uint8_t bn = rbase[min(1, R - 1)];
-    for (int r = 1; r <= R; ++r) {
-      const FwdRow nxt = fwd_row(qp, sm.mm, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
-      {
-        const int rn = min(r + 1, R - 1);  // row r + 2
-        qn = quals[rn];
-        bn = rbase[rn];
-      }
-      uint8_t hb[2];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int cn = r + 1 + d_lo[q] + W - 1;  // next row's window: append column cn
-        hb[q] = (cn >= 1 && cn <= H[q]) ? hap[q][cn - 1] : (uint8_t)0;
-      }
-      const float pmx = cur.pmx, pmy = cur.pmy, em = cur.em, ex = cur.ex;
-      const uint32_t rb = cur.rb;
-      const float2 mm2 = make_float2(cur.mm, cur.mm), cx2 = make_float2(cur.cx, cur.cx);
-      const float2 cy2 = make_float2(cur.cy, cur.cy), kap2 = make_float2(cur.kap, cur.kap);
-      const float2 g2 = make_float2(cur.g, cur.g);
-      float2 lm = make_float2(0.f, 0.f), ly = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int k = 0; k < W; ++k) {
-        const uint32_t bit = 0xFu << (4 * (k & 7));
-        const float e0 = (win[0][k >> 3] & rb & bit) != 0u ? em : ex;
-        const float e1 = (win[1][k >> 3] & rb & bit) != 0u ? em : ex;
-        const float2 upm = (k + 1 < W) ? M[k + 1] : make_float2(0.f, 0.f);
-        const float2 upx = (k + 1 < W) ? X[k + 1] : make_float2(0.f, 0.f);
-        float2 t = __fmul2_rn(cy2, Y[k]);
-        t = __ffma2_rn(cx2, X[k], t);
-        t = __ffma2_rn(mm2, M[k], t);
-        const float2 mn = make_float2(e0 * t.x, e1 * t.y);
-        const float2 xn = __ffma2_rn(kap2, upx, upm);
-        const float2 yn = __ffma2_rn(g2, ly, lm);
-        M[k] = mn; X[k] = xn; Y[k] = yn;
-        lm = mn; ly = yn;
-      }
-      // edge cells' A = M + X + Y (true X, Y) for the backward's posterior test
-      const float a00 = M[0].x + pmx * X[0].x + pmy * Y[0].x;
-      const float a01 = M[W - 1].x + pmx * X[W - 1].x + pmy * Y[W - 1].x;
-      const float a10 = M[0].y + pmx * X[0].y + pmy * Y[0].y;
-      const float a11 = M[W - 1].y + pmx * X[W - 1].y + pmy * Y[W - 1].y;
-      const __nv_bfloat162 pk0 = __floats2bfloat162_rn(a00, a01), pk1 = __floats2bfloat162_rn(a10, a11);
-      slab[(size_t)r * nthreads] =
-          make_uint2(*reinterpret_cast<const uint32_t*>(&pk0), *reinterpret_cast<const uint32_t*>(&pk1));
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int cn = r + 1 + d_lo[q] + W - 1;
-        const uint32_t nib = (cn >= 1 && cn <= H[q]) ? onehot(hb[q]) : 0u;
-#pragma unroll
-        for (int w = 0; w < NW - 1; ++w) win[q][w] = __funnelshift_r(win[q][w], win[q][w + 1], 4);
-        win[q][NW - 1] = (win[q][NW - 1] >> 4) | (nib << 28);
-      }
-      pmx_last = pmx;
-      cur = nxt;
-    }
-    float tot[2] = {0.f, 0.f};
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-      const int c0 = R + d_lo[0] + k, c1 = R + d_lo[1] + k;
-      tot[0] += (c0 >= 1 && c0 <= H[0]) ? M[k].x + pmx_last * X[k].x : 0.f;
-      tot[1] += (c1 >= 1 && c1 <= H[1]) ? M[k].y + pmx_last * X[k].y : 0.f;
-    }
-    cells += 2ull * (unsigned long long)R * W;
-    bool fall_back[2], rescue[2], need[2];
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      fall_back[q] = !(tot[q] > 0.f);
-      rescue[q] = !fall_back[q] && (!(tot[q] >= (float)kMinAccepted) || isinf(tot[q]));
-      need[q] = !fall_back[q] && !rescue[q];
-    }
-    if (need[0] || need[1]) {
-      // ---- backward: B in registers, renormalised by powers of two per pair ----
-      float2 BM[W], BX[W], BY[W];
-#pragma unroll
-      for (int k = 0; k < W; ++k) {
-        const int c0 = R + d_lo[0] + k, c1 = R + d_lo[1] + k;
-        const float v0 = (c0 >= 1 && c0 <= H[0]) ? 1.f : 0.f, v1 = (c1 >= 1 && c1 <= H[1]) ? 1.f : 0.f;
-        BM[k] = make_float2(v0, v1); BX[k] = make_float2(v0, v1); BY[k] = make_float2(0.f, 0.f);
-      }
-      double acc[2] = {0.0, 0.0};
-      double bscale[2] = {1.0, 1.0};  // true B = stored B * bscale (a power of two)
-      {
-        const uint2 pk = slab[(size_t)R * nthreads];
-        const __nv_bfloat162 p0 = *reinterpret_cast<const __nv_bfloat162*>(&pk.x);
-        const __nv_bfloat162 p1 = *reinterpret_cast<const __nv_bfloat162*>(&pk.y);
-        acc[0] += (double)__low2float(p0) * fmaxf(BM[0].x, BX[0].x) +
-                  (double)__high2float(p0) * fmaxf(BM[W - 1].x, BX[W - 1].x);
-        acc[1] += (double)__low2float(p1) * fmaxf(BM[0].y, BX[0].y) +
-                  (double)__high2float(p1) * fmaxf(BM[W - 1].y, BX[W - 1].y);
-      }
-      // windows to row R's columns (R + d_lo + k): shift back one column
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int c0 = R + d_lo[q];
-        const uint32_t nib = (c0 >= 1 && c0 <= H[q]) ? onehot(hap[q][c0 - 1]) : 0u;
-#pragma unroll
-        for (int w = NW - 1; w > 0; --w) win[q][w] = __funnelshift_l(win[q][w - 1], win[q][w], 4);
-        win[q][0] = (win[q][0] << 4) | nib;
-      }
-      BwdRow cb = bwd_row(qp, sm.mm, quals[R - 1], rbase[R - 1], quals[max(R - 2, 0)]);
-      uchar4 qa = quals[max(R - 2, 0)], qb = quals[max(R - 3, 0)];
-      for (int r = R - 1; r >= 1; --r) {
-        const BwdRow nb = bwd_row(qp, sm.mm, qa, rbase[r - 1], qb);  // row r - 1 (unused after row 1)
-        qa = qb;
-        qb = quals[max(r - 3, 0)];
-        uint8_t hb[2];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int c0 = r + d_lo[q];
-          hb[q] = (c0 >= 1 && c0 <= H[q]) ? hap[q][c0 - 1] : (uint8_t)0;
-        }
-        const float mm1 = cb.mm1, mx1 = cb.mx1, g1 = cb.g1, gp1 = cb.gp1, em1 = cb.em1, ex1 = cb.ex1;
-        const float my0 = cb.my0, g0 = cb.g0;
-        const float2 mm12 = make_float2(mm1, mm1), mx12 = make_float2(mx1, mx1), my02 = make_float2(my0, my0);
-        const float2 gp12 = make_float2(gp1, gp1), g12 = make_float2(g1, g1), g02 = make_float2(g0, g0);
-        const uint32_t rb1 = cb.rb1;
-        float2 byn = make_float2(0.f, 0.f);  // B_Y(r, k+1)
-#pragma unroll
-        for (int k = W - 1; k >= 0; --k) {
-          const uint32_t bit = 0xFu << (4 * (k & 7));
-          const float e0 = (win[0][k >> 3] & rb1 & bit) != 0u ? em1 : ex1;
-          const float e1 = (win[1][k >> 3] & rb1 & bit) != 0u ? em1 : ex1;
-          const float2 emb = make_float2(e0 * BM[k].x, e1 * BM[k].y);
-          const float2 bxk = (k > 0) ? BX[k - 1] : make_float2(0.f, 0.f);
-          const float2 nbm = __ffma2_rn(mm12, emb, __ffma2_rn(mx12, bxk, __fmul2_rn(my02, byn)));
-          const float2 nbx = __ffma2_rn(gp12, emb, __fmul2_rn(g12, bxk));
-          const float2 nby = __ffma2_rn(gp12, emb, __fmul2_rn(g02, byn));
-          BM[k] = nbm; BX[k] = nbx; BY[k] = nby;
-          byn = nby;
-        }
-        const uint2 pk = slab[(size_t)r * nthreads];
-        const __nv_bfloat162 p0 = *reinterpret_cast<const __nv_bfloat162*>(&pk.x);
-        const __nv_bfloat162 p1 = *reinterpret_cast<const __nv_bfloat162*>(&pk.y);
-        {
-          const float b0 = fmaxf(BM[0].x, fmaxf(BX[0].x, BY[0].x));
-          const float b1 = fmaxf(BM[W - 1].x, fmaxf(BX[W - 1].x, BY[W - 1].x));
-          acc[0] += (double)(__low2float(p0) * b0 + __high2float(p0) * b1) * bscale[0];
-        }
-        {
-          const float b0 = fmaxf(BM[0].y, fmaxf(BX[0].y, BY[0].y));
-          const float b1 = fmaxf(BM[W - 1].y, fmaxf(BX[W - 1].y, BY[W - 1].y));
-          acc[1] += (double)(__low2float(p1) * b0 + __high2float(p1) * b1) * bscale[1];
-        }
-        if ((r & 7) == 0) {
-          float m0 = 0.f, m1 = 0.f;
-#pragma unroll
-          for (int k = 0; k < W; ++k) {
-            m0 = fmaxf(m0, fmaxf(BM[k].x, BX[k].x));
-            m1 = fmaxf(m1, fmaxf(BM[k].y, BX[k].y));
-          }
-          float sc0 = 1.f, sc1 = 1.f;
-          if (m0 > 0.f && (m0 < 0x1p-60f || m0 > 0x1p60f)) {
-            int e2;
-            frexpf(m0, &e2);
-            sc0 = ldexpf(1.f, -e2);
-            bscale[0] = ldexp(bscale[0], e2);
-          }
-          if (m1 > 0.f && (m1 < 0x1p-60f || m1 > 0x1p60f)) {
-            int e2;
-            frexpf(m1, &e2);
-            sc1 = ldexpf(1.f, -e2);
-            bscale[1] = ldexp(bscale[1], e2);
-          }
-          if (sc0 != 1.f || sc1 != 1.f) {
-            const float2 sc = make_float2(sc0, sc1);
-#pragma unroll
-            for (int k = 0; k < W; ++k) {
-              BM[k] = __fmul2_rn(BM[k], sc); BX[k] = __fmul2_rn(BX[k], sc); BY[k] = __fmul2_rn(BY[k], sc);
-            }
-          }
-        }
-        // windows to row r's columns: shift back one column, new k = 0 is column r + d_lo
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int c0 = r + d_lo[q];
-          const uint32_t nib = (c0 >= 1 && c0 <= H[q]) ? onehot(hb[q]) : 0u;
-#pragma unroll
-          for (int w = NW - 1; w > 0; --w) win[q][w] = __funnelshift_l(win[q][w - 1], win[q][w], 4);
-          win[q][0] = (win[q][0] << 4) | nib;
-        }
-        cb = nb;
-      }
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        if (!need[q]) continue;
-        cells += (unsigned long long)R * W;
-        const double edge = acc[q] / (double)tot[q];
-        fall_back[q] = !(edge <= (double)p.edge_threshold);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      BandItem bi;
-      bi.read = it.read; bi.hap = it.hap[q]; bi.out = it.out[q]; bi.d_lo = d_lo[q]; bi.pad_ = 0;
-      band_outcome(p, cls, bi, R, tot[q], fall_back[q], rescue[q]);
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
-  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(&p.bctr->band_cells, cells);
-}
-
 __global__ void k_audit_units(BandParams p, Unit* units) {
   const unsigned long long n = min(p.bctr->audit_count, (unsigned long long)p.audit_cap);
   for (unsigned long long a = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; a < n;
@@ -1594,8 +1067,7 @@ cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st) {
 
 cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st) {
   if (p.n_pairs <= 0) return cudaSuccess;
-  const long long n2 = (p.n_pairs + 1) / 2;  // one thread per two result slots
-  const long long blocks = std::min<long long>((n2 + 255) / 256, (long long)sms * 8);
+  const long long blocks = std::min<long long>((p.n_pairs + 255) / 256, (long long)sms * 8);
   k_band_route<<<(int)blocks, 256, 0, st>>>(p, pass);
   return cudaGetLastError();
 }

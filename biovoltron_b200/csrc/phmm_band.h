@@ -11,13 +11,11 @@
 //   k_mlp_forward       per pair: BF16 MLP 80-128-128-2 (FP32 accumulation) ->
 //                       lower and upper band edge relative to d*
 //   k_band_route        band (by width class and read-length bucket) or full DP
-//   k_band_pair_f32<W>  banded forward-backward, one thread per two pairs of a
-//                       read that route to the same class (W = 8), packed
-//                       FP32x2 arithmetic, edge-mass check per pair
-//   k_band_f32<W>       the same for single pairs (and every W >= 16 pair);
-//                       classes W = 8, 16, 24, 32 run in that order, and a pair
-//                       that fails the check is promoted, as a single item, to
-//                       the next wider band
+//   k_band_ring_f32<W>  banded forward pass, one thread per pair, on the band
+//                       and on the band widened by a ring of 4 (W = 8) or 8
+//                       diagonals per side; the wider band is the result and a
+//                       ring share above the threshold promotes the pair to the
+//                       next class; classes W = 8, 16, 24, 32 run in that order
 // Pairs that leave the band path (routed out, or failing at W = 32) go to the
 // full-DP kernels through per-variant device lists; FP32 results below 1e-28
 // go to the FP64 list as before.
@@ -66,23 +64,9 @@ struct BandItem {
   int32_t pad_;
 };
 
-// Two pairs of one read routed to the same width class, banded together by
-// one thread (packed FP32x2 arithmetic, shared row constants).
-struct BandItem2 {
-  int32_t read;
-  int32_t hap[2];
-  int32_t d_lo[2];
-  int32_t pad_;
-  int64_t out[2];
-};
-constexpr int kPairedClasses = 1;      // W = 8 has a paired kernel (W = 16 paired needs 168 registers)
-
 struct BandCounters {
   unsigned long long band_count[kBandWidths][kRBuckets];  // items per (width, bucket)
   unsigned long long band_fill[kBandWidths][kRBuckets];
-  unsigned long long band2_count[kPairedClasses][kRBuckets];  // paired items per (width, bucket)
-  unsigned long long band2_fill[kPairedClasses][kRBuckets];
-  unsigned long long band2_total[kPairedClasses];
   unsigned long long band_next[kBandWidths];              // work-queue heads of the band launches
   unsigned long long band_total[kBandWidths];             // routed items per width class
   unsigned long long promoted[kBandWidths];               // items promoted from the next narrower class
@@ -115,15 +99,12 @@ struct BandParams {
   int use_mlp;                // 0: fixed band half-width `fixed_half` around d*
   int fixed_half;
   int margin;                 // diagonals added on both sides of the predicted band
-  float edge_threshold;       // fallback when the posterior band-edge mass exceeds it
-  uint32_t* edge_slab;        // [kBandMaxRead + 1][band_dp_blocks * 128] forward edge cells (BF16 pairs)
+  float edge_threshold;       // promotion when the ring adds more than this share of the likelihood
   int audit_period;           // every audit_period-th pair is also scored by the full DP (0: off)
   BandCounters* bctr;
   Counters* ctr;
   BandItem* items;            // [kBandWidths][capacity]
   long long item_cap;
-  BandItem2* items2;          // [kPairedClasses][capacity2]
-  long long item2_cap;
   Unit* full_items;           // [16][capacity] fallback units (nh = 1), per full-DP variant
   long long full_cap;
   int64_t* audit_pairs;       // [audit capacity]

@@ -464,7 +464,7 @@ bv_status Engine::run(bv_phmm_stats* stats) {
     stats->rescued = (int64_t)c.rescue_count;
     stats->underflow = (int64_t)c.underflow_count;
     stats->kernel_launches = band_enabled()
-                                 ? 6 + (band_opt_.use_mlp ? 1 : 0) + kBandWidths + kPairedClasses + 9 +
+                                 ? 6 + (band_opt_.use_mlp ? 1 : 0) + kBandWidths + 9 +
                                        (band_opt_.audit_period > 0 ? 11 : 0) + 1
                                  : (int64_t)plans_.size() + 1;
     stats->ms_fp32 = ms32;

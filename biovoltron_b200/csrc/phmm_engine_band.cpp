@@ -50,7 +50,6 @@ BandParams Engine::band_params() const {
   p.dstar = d_dstar_.as<int32_t>();
   p.kmin = d_kmin_.as<int32_t>();
   p.kmax = d_kmax_.as<int32_t>();
-  p.edge_slab = d_edge_slab_.as<uint32_t>();
   p.feat = d_feat_.as<__nv_bfloat16>();
   p.mlp_out = d_mlp_out_.as<float>();
   p.mlp = d_mlp_.as<MlpParams>();
@@ -63,8 +62,6 @@ BandParams Engine::band_params() const {
   p.ctr = d_counters_.as<Counters>();
   p.items = d_band_items_.as<BandItem>();
   p.item_cap = item_cap_;
-  p.items2 = d_band_items2_.as<BandItem2>();
-  p.item2_cap = item2_cap_;
   p.full_items = d_full_items_.as<Unit>();
   p.full_cap = full_cap_;
   p.audit_pairs = d_audit_pairs_.as<int64_t>();
@@ -87,19 +84,14 @@ bv_status Engine::band_prepare() {
   BV_CUDA(d_dstar_.reserve(sizeof(int32_t) * n), "alloc seeds");
   BV_CUDA(d_kmin_.reserve(sizeof(int32_t) * n), "alloc seeds");
   BV_CUDA(d_kmax_.reserve(sizeof(int32_t) * n), "alloc seeds");
-  // two BF16 pairs per row and thread (the paired kernels store both pairs' edges)
-  BV_CUDA(d_edge_slab_.reserve(sizeof(uint2) * (size_t)(kBandMaxRead + 1) * band_dp_blocks(sms_) * 128),
-          "alloc edge slab");
   BV_CUDA(d_feat_.reserve(sizeof(__nv_bfloat16) * kFeat * n), "alloc features");
   BV_CUDA(d_mlp_out_.reserve(sizeof(float) * kOut * n), "alloc mlp out");
   BV_CUDA(d_mlp_.reserve(sizeof(MlpParams)), "alloc mlp");
   BV_CUDA(d_bctr_.reserve(sizeof(BandCounters)), "alloc band counters");
   item_cap_ = n;
-  item2_cap_ = n / 2 + 1;
   full_cap_ = n;
   audit_cap_ = band_opt_.audit_period > 0 ? n / band_opt_.audit_period + 1 : 1;
   BV_CUDA(d_band_items_.reserve(sizeof(BandItem) * kBandWidths * item_cap_), "alloc band items");
-  BV_CUDA(d_band_items2_.reserve(sizeof(BandItem2) * kPairedClasses * item2_cap_), "alloc paired band items");
   BV_CUDA(d_full_items_.reserve(sizeof(Unit) * 9 * full_cap_), "alloc fallback units");
   BV_CUDA(d_audit_pairs_.reserve(sizeof(int64_t) * audit_cap_), "alloc audit");
   BV_CUDA(d_audit_units_.reserve(sizeof(Unit) * 9 * audit_cap_), "alloc audit");
@@ -191,8 +183,6 @@ bv_status Engine::band_stats(bv_phmm_stats* st) {
   long long banded = 0;
   for (int c = 0; c < kBandWidths; ++c)
     for (int b = 0; b < kRBuckets; ++b) banded += (long long)bc.band_count[c][b];
-  for (int c = 0; c < kPairedClasses; ++c)
-    for (int b = 0; b < kRBuckets; ++b) banded += 2 * (long long)bc.band2_count[c][b];
   st->band_pairs = banded;
   st->band_fallback = (int64_t)bc.fallback_edge;
   st->band_routed_full = (int64_t)bc.fallback_route;
@@ -242,19 +232,6 @@ bv_status Engine::band_routes(int64_t n, int32_t* d_lo, int32_t* width, int32_t*
       width[x.out] = band_width(c);
       route[x.out] = 0;
     }
-  }
-  for (int c = 0; c < kPairedClasses; ++c) {
-    const unsigned long long cnt = std::min<unsigned long long>(bc.band2_total[c], (unsigned long long)item2_cap_);
-    std::vector<BandItem2> it(cnt);
-    if (cnt) BV_CUDA(cudaMemcpy(it.data(), d_band_items2_.as<BandItem2>() + (size_t)c * item2_cap_,
-                                sizeof(BandItem2) * cnt, cudaMemcpyDeviceToHost), "paired band items");
-    for (const auto& x : it)
-      for (int q = 0; q < 2; ++q) {
-        if (x.out[q] < 0 || x.out[q] >= n || route[x.out[q]] == 0) continue;  // a promoted copy is already recorded
-        d_lo[x.out[q]] = x.d_lo[q];
-        width[x.out[q]] = band_width(c);
-        route[x.out[q]] = 0;
-      }
   }
   for (int v = 0; v < 9; ++v) {
     const unsigned long long cnt = std::min<unsigned long long>(bc.full_count[v], (unsigned long long)full_cap_);

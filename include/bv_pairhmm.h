@@ -115,9 +115,14 @@ const char* bv_phmm_last_error(const bv_phmm_ctx* ctx);
  * With `enabled`, every pair is first scored on a diagonal band around its
  * 11-mer seed diagonal: [seed + lo - margin, seed + hi + margin], where lo/hi
  * come from the band MLP (use_mlp, weights from bv_phmm_band_train or
- * bv_phmm_band_load) or are -fixed_half/+fixed_half.  Pairs without a seed,
- * with a band wider than 32 diagonals or reads longer than 511 bases, and
- * pairs whose band-edge mass exceeds edge_threshold are scored by the full DP.
+ * bv_phmm_band_load) or are -fixed_half/+fixed_half, widened to hold every
+ * diagonal a shared 11-mer votes for and rounded up to a width class of 8,
+ * 16, 24 or 32 diagonals.  A banded pair is also scored on its band widened by
+ * a ring of 4 (class 8) or 8 diagonals on each side; that wider band's value
+ * is the result, and when the ring adds more than edge_threshold of it the
+ * pair moves to the next class (after class 32: the full DP).  Pairs without
+ * a seed, with a band wider than 32 diagonals or reads longer than 511 bases
+ * are scored by the full DP.
  * Every audit_period-th banded pair is also scored by the full DP and the
  * differences are reported in bv_phmm_stats.  No counterpart in the reference
  * (its PairHMM always computes the full matrix). */
@@ -128,7 +133,7 @@ typedef struct bv_band_options {
   int32_t fixed_half;
   int32_t margin;
   int32_t audit_period;
-  double edge_threshold;
+  double edge_threshold;   /* largest share of the likelihood the ring may add (default 1e-3) */
   int32_t reserved[6];
 } bv_band_options;
 
