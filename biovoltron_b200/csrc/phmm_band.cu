@@ -833,8 +833,8 @@ __device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb
 // edge_threshold of it.  Unlike a posterior test on the band's edge
 // diagonals, the ring also sees mass that enters the band from outside (an
 // alignment start or end on a diagonal next to the band), which a banded
-// model cannot represent.  W = 8 runs both bands in one row sweep (shared row
-// constants and emissions); the wider classes run them one after the other.
+// model cannot represent.  W = 8, 16 run both bands in one row sweep (shared
+// row constants and emissions); W = 24, 32 run them one after the other.
 // ---------------------------------------------------------------------------
 template <int WB, int WI>
 __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Tables* tb, const uchar4* __restrict__ quals,
@@ -937,9 +937,10 @@ __device__ __noinline__ float band_forward_pass(const BandSmem& sm, const Tables
   return band_forward_body<WB, 0>(sm, tb, quals, rbase, hap, R, H, d).x;
 }
 
+// W = 8 keeps four blocks per SM (128 registers); the wider classes two.
 template <int W>
-__global__ void __launch_bounds__(128) k_band_ring_f32(BandParams p, int cls) {
-  constexpr bool kDual = W <= 8;  // both bands in one sweep
+__global__ void __launch_bounds__(128, W <= 8 ? 4 : 2) k_band_ring_f32(BandParams p, int cls) {
+  constexpr bool kDual = W <= 16;  // both bands in one sweep
   // ring width on each side: pairs routed to wider bands have indel-rich alignments whose
   // alternatives lie farther out, so W >= 16 test eight diagonals
   constexpr int kRing = W >= 16 ? 8 : 4;
