@@ -312,6 +312,8 @@ def main():
     ap.add_argument("--oracle-sample", type=int, default=20000)
     ap.add_argument("--edge-threshold", type=float, default=1e-3)
     ap.add_argument("--margin", type=int, default=2, help="diagonals added on both sides of the predicted band")
+    ap.add_argument("--tune-regions", type=int, default=500,
+                    help="regions of the workload the launch-shape autotuner times (0: default shapes)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -335,17 +337,28 @@ def main():
 
     plain = band = None
     train_rep = None
+    tuning = None
+    if args.tune_regions > 0 and args.haps_per_warp == 0:
+        # launch shapes per rows-per-lane bin, timed on a seeded sample of the workload's regions
+        picks = np.random.default_rng(5).choice(batch.n_regions, size=min(args.tune_regions, batch.n_regions),
+                                                replace=False)
+        with PairHMMEngine(device=local) as et:
+            tuning = et.autotune(W.subsample_regions(batch, sorted(picks.tolist())), repeats=3)
     clocks = ClockSampler(local)  # sampled over every timed section below
     clocks.start()
     # ---- plain full DP, device-resident --------------------------------------
     if form == "plain" or not args.no_plain:
         with PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp) as ep:
+            if tuning:
+                ep.set_tuning(tuning)
             n, steps, wall, res = time_form(ep, batch, args, pg, band=False)
         plain = {"n": n, "steps": steps, "wall": wall, "res": res}
     # ---- learned band, device-resident --------------------------------------
     eb = None
     if form == "band":
         eb = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp)
+        if tuning:
+            eb.set_tuning(tuning)
         train_rep = train_band(eb, args, rank)
         if args.save_weights and rank == 0:
             eb.band_save(args.save_weights)
@@ -418,7 +431,8 @@ def main():
                        "pairs_per_gpu": n, "cells_per_gpu": batch.n_cells(),
                        "l2": f"inputs {batch.nbytes() / 1e9:.2f} GB > 126 MB L2, no flush",
                        "parallelism": f"dp{world} (independent regions, one replica per GPU)",
-                       "generate_s": round(t_gen, 1)},
+                       "generate_s": round(t_gen, 1),
+                       "launch_shapes": tuning or "engine defaults (2 haplotypes per warp, 4 warps per block)"},
         }
         if plain is not None:
             pl = plain["steps"][-1]

@@ -309,6 +309,22 @@ bv_status bv_phmm_band_mlp_eval(bv_phmm_ctx* ctx, const float* w, const float* x
   return guard(ctx, [&] { return ctx->engine.band_mlp_eval(w, x, targets, n, alpha, out, loss, grad); });
 }
 
+bv_status bv_phmm_autotune(bv_phmm_ctx* ctx, const bv_region_batch* sample, int32_t repeats, bv_phmm_tune_entry* out,
+                           int32_t* num_out) {
+  if (!ctx || !sample || !out || !num_out) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.autotune(*sample, repeats, out, num_out); });
+}
+
+bv_status bv_phmm_set_tuning(bv_phmm_ctx* ctx, const bv_phmm_tune_entry* entries, int32_t num) {
+  if (!ctx) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.set_tuning(entries, num); });
+}
+
+bv_status bv_phmm_get_tuning(bv_phmm_ctx* ctx, bv_phmm_tune_entry* out, int32_t* num_out) {
+  if (!ctx || !out || !num_out) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.get_tuning(out, num_out); });
+}
+
 bv_status bv_phmm_host_register(bv_phmm_ctx* ctx, void* ptr, size_t bytes) {
   if (!ctx || !ptr || bytes == 0) return BV_ERR_INVALID_ARG;
   cudaError_t e = cudaSetDevice(ctx->engine.device());

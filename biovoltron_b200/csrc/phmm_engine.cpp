@@ -74,6 +74,8 @@ Engine::~Engine() {
     cudaStreamSynchronize(stream_);
     for (auto& e : ev_)
       if (e) cudaEventDestroy(e);
+    for (auto& e : tune_ev_)
+      if (e) cudaEventDestroy(e);
     cudaStreamDestroy(stream_);
   }
 }
@@ -174,8 +176,11 @@ bv_status Engine::plan(const bv_region_batch& b) {
     region_max_hap[g] = mh;
     max_hap_ = std::max(max_hap_, mh);
   }
-  // two haplotypes per warp (paired variants) unless the options ask for one
-  auto pair_rows = [&](int64_t rt) { return opt_.haps_per_warp != 1 && rt >= 1 && per_unit >= 2; };
+  // two haplotypes per warp (paired variants) unless the options or the bin's tuning ask for one
+  auto pair_rows = [&](int64_t rt) {
+    if (opt_.haps_per_warp == 1 || per_unit < 2 || rt < 1 || rt > kTuneBins) return false;
+    return opt_.haps_per_warp == 2 || tune_[rt].haps_per_warp == 2;
+  };
   auto variant_of = [&](int64_t rlen) {
     // rows of the single-strip FP32 kernel: row 0, the read, the summing row
     // and one padding row on top (phmm_device.cuh, rows_needed)
@@ -239,11 +244,19 @@ bv_status Engine::plan(const bv_region_batch& b) {
     // a paired variant stages one 32-bit entry (both haplotypes' table offsets) per column
     lp.hap_bytes = variant_paired(v) ? 4 * lp.code_row_bytes : lp.code_row_bytes;
     lp.warp_smem = warp_smem_bytes(v, lp.hap_bytes);
-    const int smem_block = lp.warp_smem * (kThreadsPerBlock / kWarp);
-    if (smem_block > 227 * 1024) return fail(BV_ERR_INVALID_ARG, "haplotype too long for shared-memory staging");
-    BV_CUDA(prepare_variant(v, smem_block), "kernel attribute");
-    const int bps = std::max(1, blocks_per_sm(v, smem_block));
-    const int64_t need = (count[v] + (kThreadsPerBlock / kWarp) - 1) / (kThreadsPerBlock / kWarp);
+    {
+      // the bin's block size (rows per lane of a single-strip FP32 variant)
+      int rt = 0;
+      for (int t = 1; t <= kTuneBins; ++t)
+        if (v == variant_index(false, t, false, false) || v == variant_index(false, t, false, true)) rt = t;
+      lp.warps_per_block = rt ? tune_[rt].warps_per_block : kThreadsPerBlock / kWarp;
+    }
+    const int smem_block = lp.warp_smem * lp.warps_per_block;
+    if (lp.warp_smem * (kThreadsPerBlock / kWarp) > 227 * 1024)
+      return fail(BV_ERR_INVALID_ARG, "haplotype too long for shared-memory staging");
+    BV_CUDA(prepare_variant(v, lp.warp_smem * (kThreadsPerBlock / kWarp)), "kernel attribute");
+    const int bps = std::max(1, blocks_per_sm(v, smem_block, lp.warps_per_block * kWarp));
+    const int64_t need = (count[v] + lp.warps_per_block - 1) / lp.warps_per_block;
     lp.grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms_ * bps));
     lp.bnd_cols = lp.multi ? bnd_cols_for(var_max_hap[v]) : 0;
     plans_.push_back(lp);
@@ -287,7 +300,7 @@ bv_status Engine::upload(const bv_region_batch& b) {
   // strip-boundary buffers for the multi-strip launches
   size_t need32 = 0;
   for (const auto& lp : plans_)
-    if (lp.multi) need32 = std::max<size_t>(need32, (size_t)lp.grid * (kThreadsPerBlock / kWarp) * (size_t)lp.bnd_cols * 4 * sizeof(float));
+    if (lp.multi) need32 = std::max<size_t>(need32, (size_t)lp.grid * lp.warps_per_block * (size_t)lp.bnd_cols * 4 * sizeof(float));
   if (need32) BV_CUDA(d_bnd32_.reserve(need32), "alloc boundary buffers");
   const size_t need64 = (size_t)rescue_plan_.grid * (kThreadsPerBlock / kWarp) * (size_t)rescue_plan_.bnd_cols * 4 * sizeof(double);
   BV_CUDA(d_bnd64_.reserve(need64), "alloc FP64 boundary buffers");
@@ -368,25 +381,38 @@ bv_status Engine::enqueue_kernels(bool capturing) {
   p.out = d_out_.as<double>();
   p.rescue = d_rescue_.as<PairRef>();
   p.rescue_cap = std::max<int64_t>(n_results_, 1);
+  p.warps_per_block = kThreadsPerBlock / kWarp;  // band-path fallback and audit launches
   BV_CUDA(rec(ev_[2]), "event");
   if (band_enabled()) {
     bv_status bs = enqueue_band(capturing, p);
     if (bs != BV_OK) return bs;
   }
-  for (const auto& lp : plans_) {
+  if (tune_timing_ && !capturing) {
+    while (tune_ev_.size() < 2 * plans_.size()) {
+      cudaEvent_t e;
+      BV_CUDA(cudaEventCreate(&e), "event");
+      tune_ev_.push_back(e);
+    }
+  }
+  for (size_t pi = 0; pi < plans_.size(); ++pi) {
+    const LaunchPlan& lp = plans_[pi];
     if (band_enabled()) break;
+    const bool timed = tune_timing_ && !capturing;
+    if (timed) BV_CUDA(cudaEventRecord(tune_ev_[2 * pi], stream_), "event");
     p.unit_base = lp.unit_base;
     p.n_units = lp.n_units;
     p.slot = lp.slot;
     p.from_rescue = 0;
     p.hap_bytes = lp.hap_bytes;
     p.code_row_bytes = lp.code_row_bytes;
+    p.warps_per_block = lp.warps_per_block;
     p.warp_smem_bytes = lp.warp_smem;
     p.bnd = lp.multi ? d_bnd32_.get() : nullptr;
     p.bnd_cols = lp.bnd_cols;
     p.rescale = 0;
     p.rescale_target = 0;
     BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP32 forward launch");
+    if (timed) BV_CUDA(cudaEventRecord(tune_ev_[2 * pi + 1], stream_), "event");
   }
   BV_CUDA(rec(ev_[3]), "event");
   {
@@ -397,6 +423,7 @@ bv_status Engine::enqueue_kernels(bool capturing) {
     p.from_rescue = 1;
     p.hap_bytes = lp.hap_bytes;
     p.code_row_bytes = 0;
+    p.warps_per_block = kThreadsPerBlock / kWarp;
     p.warp_smem_bytes = lp.warp_smem;
     p.bnd = d_bnd64_.get();
     p.bnd_cols = lp.bnd_cols;

@@ -31,11 +31,20 @@ class DevBuf {
   size_t cap_ = 0;
 };
 
+// Launch parameters of one rows-per-lane bin (single-strip FP32 full DP),
+// chosen by the autotuner or set by the caller.
+struct BinTune {
+  int haps_per_warp = 2;    // 1: one haplotype per warp; 2: two (packed FP32x2)
+  int warps_per_block = 4;  // 1..4
+};
+constexpr int kTuneBins = 8;  // rows per lane 1..8
+
 struct LaunchPlan {
   int variant = -1;
   int slot = 0;
   long long unit_base = 0;
   long long n_units = 0;
+  int warps_per_block = kThreadsPerBlock / kWarp;
   int hap_bytes = 0;
   int code_row_bytes = 0;
   int warp_smem = 0;
@@ -74,6 +83,9 @@ class Engine {
   bv_status band_load(const char* path);
   bv_status band_mlp_eval(const float* w, const float* x, const float* t, int64_t n, float alpha, float* out,
                           float* loss, float* grad);
+  bv_status autotune(const bv_region_batch& sample, int repeats, bv_phmm_tune_entry* out, int32_t* n_out);
+  bv_status set_tuning(const bv_phmm_tune_entry* entries, int32_t n);
+  bv_status get_tuning(bv_phmm_tune_entry* out, int32_t* n_out);
 
  private:
   bv_status validate(const bv_region_batch& b);
@@ -124,6 +136,11 @@ class Engine {
   bv_status install_weights(const float* w_host);
   std::vector<float> mlp_w_;  // FP32 master weights of the installed MLP
   DevBuf d_lab_lo_, d_lab_hi_, d_lab_fbuf_, d_mlp_w_;
+
+  // per-bin launch parameters; per-launch timing while tuning
+  BinTune tune_[kTuneBins + 1];
+  bool tune_timing_ = false;
+  std::vector<cudaEvent_t> tune_ev_;
 
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & (kWarp - 1);
   const int wib = threadIdx.x >> 5;
-  const int warp_global = blockIdx.x * (kThreadsPerBlock / kWarp) + wib;
+  const int warp_global = blockIdx.x * p.warps_per_block + wib;
   unsigned char* wsm = smem + (size_t)wib * p.warp_smem_bytes;
   T* bnd = MULTI ? reinterpret_cast<T*>(p.bnd) + (size_t)warp_global * p.bnd_cols * 4 : nullptr;
   const unsigned long long n = p.from_rescue ? p.ctr->rescue_count
@@ -106,8 +106,8 @@ int warp_smem_bytes_for(int hap_bytes) {
 
 template <typename T, int RT, bool MULTI, bool PAIR>
 static cudaError_t launch_one(const KernelParams& p, int grid, cudaStream_t st) {
-  const int smem = (kThreadsPerBlock / kWarp) * p.warp_smem_bytes;
-  k_forward<T, RT, MULTI, PAIR><<<grid, kThreadsPerBlock, smem, st>>>(p);
+  const int smem = p.warps_per_block * p.warp_smem_bytes;
+  k_forward<T, RT, MULTI, PAIR><<<grid, p.warps_per_block * kWarp, smem, st>>>(p);
   return cudaGetLastError();
 }
 
@@ -118,11 +118,11 @@ static cudaError_t prepare_one(int smem_per_block) {
 }
 
 template <typename T, int RT, bool MULTI, bool PAIR>
-static int occupancy_one(int smem_per_block) {
+static int occupancy_one(int smem_per_block, int threads) {
   int nb = 0;
   auto k = &k_forward<T, RT, MULTI, PAIR>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kThreadsPerBlock, smem_per_block) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem_per_block) != cudaSuccess) return 0;
   return nb;
 }
 
@@ -182,10 +182,10 @@ cudaError_t launch_forward(int variant, const KernelParams& p, int grid, cudaStr
   return cudaErrorInvalidValue;
 }
 
-int blocks_per_sm(int variant, int smem_per_block) {
+int blocks_per_sm(int variant, int smem_per_block, int threads) {
   int idx = 0;
 #define BV_OCC(T, RT, MULTI, PAIR) \
-  if (idx++ == variant) return occupancy_one<T, RT, MULTI, PAIR>(smem_per_block);
+  if (idx++ == variant) return occupancy_one<T, RT, MULTI, PAIR>(smem_per_block, threads);
   BV_VARIANTS(BV_OCC)
 #undef BV_OCC
   return 0;

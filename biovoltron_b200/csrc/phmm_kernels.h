@@ -22,6 +22,7 @@ struct KernelParams {
   double* out;            // log10 likelihoods, one per result slot
   PairRef* rescue;        // null: pairs below the FP32 threshold get NaN (audit runs)
   long long rescue_cap;
+  int warps_per_block;    // block size of the launch / 32 (1..4)
   int hap_bytes;          // per-warp bytes for staged haplotype codes
   int code_row_bytes;     // entries of a staged code row (paired variants stage 4-byte entries)
   int warp_smem_bytes;    // per-warp dynamic shared memory
@@ -36,7 +37,7 @@ struct KernelParams {
 int variant_index(bool f64, int rows_per_lane, bool multi, bool paired = false);
 bool variant_paired(int variant);
 int warp_smem_bytes(int variant, int hap_bytes);
-int blocks_per_sm(int variant, int smem_per_block);
+int blocks_per_sm(int variant, int smem_per_block, int threads = kThreadsPerBlock);
 // Sets the variant's dynamic shared-memory limit; call before launching or capturing it.
 cudaError_t prepare_variant(int variant, int smem_per_block);
 cudaError_t launch_forward(int variant, const KernelParams& p, int grid, cudaStream_t st);

@@ -75,6 +75,15 @@ class BandTrainReport(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("rows_per_lane", C.c_int32), ("haps_per_warp", C.c_int32), ("warps_per_block", C.c_int32),
+                ("reserved", C.c_int32), ("ms", C.c_double)]
+
+    def as_dict(self):
+        return {"rows_per_lane": self.rows_per_lane, "haps_per_warp": self.haps_per_warp,
+                "warps_per_block": self.warps_per_block, "ms": self.ms}
+
+
 class TestcaseC(C.Structure):
     _fields_ = [
         ("rslen", C.c_int), ("haplen", C.c_int),
@@ -155,6 +164,9 @@ def load() -> C.CDLL:
         "bv_phmm_band_save": (C.c_int, [V, C.c_char_p]),
         "bv_phmm_band_load": (C.c_int, [V, C.c_char_p]),
         "bv_phmm_band_mlp_eval": (C.c_int, [V, V, V, V, C.c_int64, C.c_float, V, V, V]),
+        "bv_phmm_autotune": (C.c_int, [V, P(RegionBatchC), C.c_int32, P(TuneEntry), P(C.c_int32)]),
+        "bv_phmm_set_tuning": (C.c_int, [V, P(TuneEntry), C.c_int32]),
+        "bv_phmm_get_tuning": (C.c_int, [V, P(TuneEntry), P(C.c_int32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

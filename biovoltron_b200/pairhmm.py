@@ -211,6 +211,30 @@ class PairHMMEngine:
                                                    _ptr(loss), _ptr(g) if grad else None))
         return out, float(loss[0]), g
 
+    # --- launch-shape autotuning -------------------------------------------
+    def autotune(self, sample: RegionBatch, repeats: int = 3) -> List[dict]:
+        """Times every launch shape per rows-per-lane bin on `sample` and keeps
+        the fastest (bv_phmm_autotune); returns the chosen shape per bin."""
+        v = _BatchView(sample)
+        out = (N.TuneEntry * 8)()
+        n = C.c_int32(0)
+        self._check(self.lib.bv_phmm_autotune(self.h, C.byref(v.c), repeats, out, C.byref(n)))
+        self._staged = None
+        return [out[k].as_dict() for k in range(n.value)]
+
+    def tuning(self) -> List[dict]:
+        out = (N.TuneEntry * 8)()
+        n = C.c_int32(0)
+        self._check(self.lib.bv_phmm_get_tuning(self.h, out, C.byref(n)))
+        return [out[k].as_dict() for k in range(n.value)]
+
+    def set_tuning(self, entries: Sequence[dict]):
+        arr = (N.TuneEntry * max(len(entries), 1))()
+        for k, e in enumerate(entries):
+            arr[k] = N.TuneEntry(e["rows_per_lane"], e["haps_per_warp"], e["warps_per_block"], 0, 0.0)
+        self._check(self.lib.bv_phmm_set_tuning(self.h, arr, len(entries)))
+        self._staged = None
+
     def host_register(self, arr: np.ndarray):
         self._check(self.lib.bv_phmm_host_register(self.h, _ptr(arr), arr.nbytes))
 

@@ -341,6 +341,30 @@ typedef struct bv_phmm_device_pairs {
 bv_status bv_phmm_forward_f64_noalloc(int device, const bv_phmm_device_pairs* pairs, double* out_log10,
                                       int64_t num_out, void* stream);
 
+/* --- autotuning ------------------------------------------------------------
+ * The full-DP kernels run one launch per bin of reads with the same rows per
+ * lane (ceil((read_len + 3) / 32), 1..8; longer reads use the multi-strip
+ * kernel).  Per bin a warp scores one or two haplotypes of a read at a time
+ * (haps_per_warp) and a block holds 1..4 warps (warps_per_block).
+ * bv_phmm_autotune times every combination on `sample` (repeats timed runs
+ * each, device time per bin launch), installs the fastest per bin in the
+ * context and writes one entry per bin the sample exercises (at most 8).
+ * No counterpart in the reference (its AVX kernels have no launch shape). */
+typedef struct bv_phmm_tune_entry {
+  int32_t rows_per_lane;    /* bin: 1..8 */
+  int32_t haps_per_warp;    /* 1 or 2 */
+  int32_t warps_per_block;  /* 1..4 */
+  int32_t reserved;
+  double ms;                /* the bin's best time on the sample (autotune output) */
+} bv_phmm_tune_entry;
+
+bv_status bv_phmm_autotune(bv_phmm_ctx* ctx, const bv_region_batch* sample, int32_t repeats, bv_phmm_tune_entry* out,
+                           int32_t* num_out);
+/* Installs (set) or reads (get) per-bin launch parameters; entries for bins
+ * not listed keep their values (defaults: two haplotypes per warp, 4 warps). */
+bv_status bv_phmm_set_tuning(bv_phmm_ctx* ctx, const bv_phmm_tune_entry* entries, int32_t num);
+bv_status bv_phmm_get_tuning(bv_phmm_ctx* ctx, bv_phmm_tune_entry* out, int32_t* num_out);
+
 /* Diagnostics: writes the probability tables a context uploads (ph2pr for
  * quals 0..127 and the match-to-match triangle for quals <= 127, both
  * precisions; Context.h:42-175).  Host-only, needs no device.  Returns 0, or

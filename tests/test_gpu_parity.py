@@ -183,3 +183,27 @@ def test_paired_haplotypes_bit_identical_to_single(seed):
         two, st2 = e2.compute_regions(b, with_stats=True)
     assert st1["rescued"] == st2["rescued"]
     assert np.array_equal(one, two)
+
+
+def test_autotune_picks_shapes_and_keeps_results():
+    """The launch-shape autotuner times every shape per rows-per-lane bin; any
+    shape gives the same results (each pair's arithmetic does not depend on
+    the launch shape)."""
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    b = W.config1(seed=9, n_regions=24)
+    with PairHMMEngine() as e:
+        ref = e.compute_regions(b)
+        chosen = e.autotune(b, repeats=2)
+        assert chosen
+        for c in chosen:
+            assert 1 <= c["rows_per_lane"] <= 8 and c["haps_per_warp"] in (1, 2)
+            assert 1 <= c["warps_per_block"] <= 4 and c["ms"] > 0
+        assert {(c["rows_per_lane"], c["haps_per_warp"], c["warps_per_block"]) for c in chosen} <= \
+            {(t["rows_per_lane"], t["haps_per_warp"], t["warps_per_block"]) for t in e.tuning()}
+        assert np.array_equal(e.compute_regions(b), ref)
+        e.set_tuning([{"rows_per_lane": rt, "haps_per_warp": 1, "warps_per_block": 1} for rt in range(1, 9)])
+        assert np.array_equal(e.compute_regions(b), ref)
+        with pytest.raises(RuntimeError):
+            e.set_tuning([{"rows_per_lane": 9, "haps_per_warp": 1, "warps_per_block": 1}])
+        with pytest.raises(RuntimeError):
+            e.set_tuning([{"rows_per_lane": 3, "haps_per_warp": 3, "warps_per_block": 1}])
