@@ -54,6 +54,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from biovoltron_b200 import replicas  # noqa: E402
 from biovoltron_b200 import workloads as W  # noqa: E402
 
 METRIC = "PairHMM GCUPS & pairs/s on 1 B200: learned-band+batched vs plain DP, <=1e-3 log10L err"
@@ -175,40 +176,8 @@ def cpu_reference_rate(batch: W.RegionBatch, target_s: float, seed: int = 0):
     }
 
 
-def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-        pg = dist
-    return world, rank, local, pg
-
-
-def allreduce(pg, x: float, op: str) -> float:
-    if pg is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op={"max": pg.ReduceOp.MAX, "sum": pg.ReduceOp.SUM}[op])
-    return float(t.item())
-
-
-def barrier(pg):
-    if pg is not None:
-        pg.barrier()
-
-
 def run_reference(args):
-    world, rank, local, pg = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
-    if rank != 0:
+    if int(os.environ.get("RANK", "0")) != 0:  # rank 0 alone times the host kernel
         return
     batch = make_workload(args.workload, args.seed, args.regions)
     per_step = []
@@ -248,18 +217,18 @@ def train_band(eng, args, local_seed: int) -> dict:
     return rep
 
 
-def time_form(eng, batch, args, pg, band: bool):
+def time_form(eng, batch, args, rep, band: bool):
     """Stages the batch once; returns per-step stats, device ms and results."""
     n = eng.stage(batch)
     for _ in range(args.warmup):
         eng.run()
-    barrier(pg)
+    rep.barrier()
     steps = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
         steps.append(eng.run())
     wall = time.perf_counter() - t0
-    barrier(pg)
+    rep.barrier()
     res = eng.fetch(n)
     return n, steps, wall, res
 
@@ -320,13 +289,14 @@ def main():
         return
     form = args.form or ("band" if args.workload in ("config4", "config1") else "plain")
 
-    world, rank, local, pg = dist_setup(args)
+    rep = replicas.setup("nccl")
+    world, rank, local = rep.world, rep.rank, rep.local
     from biovoltron_b200.native import load
     from biovoltron_b200.pairhmm import PairHMMEngine
     import ctypes as C
 
     t_gen = time.perf_counter()
-    batch = make_workload(args.workload, args.seed + 1000 * rank, args.regions)
+    batch = make_workload(args.workload, rep.shard_seed(args.seed), args.regions)
     t_gen = time.perf_counter() - t_gen
     log(f"[rank {rank}] workload: {batch.name}: {batch.n_pairs} pairs, {batch.n_cells():.3e} cells "
         f"(generated in {t_gen:.1f} s)")
@@ -351,7 +321,7 @@ def main():
         with PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp) as ep:
             if tuning:
                 ep.set_tuning(tuning)
-            n, steps, wall, res = time_form(ep, batch, args, pg, band=False)
+            n, steps, wall, res = time_form(ep, batch, args, rep, band=False)
         plain = {"n": n, "steps": steps, "wall": wall, "res": res}
     # ---- learned band, device-resident --------------------------------------
     eb = None
@@ -364,7 +334,7 @@ def main():
             eb.band_save(args.save_weights)
         eb.set_band_options(use_mlp=True, margin=args.margin, edge_threshold=args.edge_threshold,
                             audit_period=args.audit_period)
-        n, steps, wall, res = time_form(eb, batch, args, pg, band=True)
+        n, steps, wall, res = time_form(eb, batch, args, rep, band=True)
         band = {"n": n, "steps": steps, "wall": wall, "res": res}
     main_run = band if band else plain
     n = main_run["n"]
@@ -381,30 +351,29 @@ def main():
     e2e_eng.host_register(out)
     for _ in range(max(1, min(args.warmup, 2))):
         e2e_eng.compute_regions(batch, out=out)
-    barrier(pg)
+    rep.barrier()
     e2e_t = []
     for _ in range(args.steps):
         t1 = time.perf_counter()
         e2e_eng.compute_regions(batch, out=out)
         e2e_t.append(time.perf_counter() - t1)
     clk = clocks.stop()
-    barrier(pg)
+    rep.barrier()
     for a in arrays + [out]:
         e2e_eng.host_unregister(a)
     same = bool(np.array_equal(out[:n], main_run["res"], equal_nan=True))
     e2e_eng.close()
 
     # ---- aggregate over ranks --------------------------------------------------
-    t_dev = allreduce(pg, float(np.sum(device_ms(main_run))), "max")
-    total_pairs = allreduce(pg, float(n * args.steps), "sum")
-    total_cells = allreduce(pg, float(batch.n_cells() * args.steps), "sum")
-    value = total_pairs / (t_dev / 1e3)
-    e2e_time = allreduce(pg, float(np.sum(e2e_t)), "max")
-    e2e = total_pairs / e2e_time
+    agg = replicas.aggregate(rep, float(n * args.steps), [m / 1e3 for m in device_ms(main_run)])
+    t_dev = agg["seconds"] * 1e3
+    total_pairs = agg["pairs"]
+    total_cells = rep.allreduce(float(batch.n_cells() * args.steps), "sum")
+    value = agg["pairs_per_s"]
+    e2e = replicas.aggregate(rep, float(n * args.steps), e2e_t)["pairs_per_s"]
     plain_pps = None
     if plain is not None:
-        t_plain = allreduce(pg, float(np.sum(device_ms(plain))), "max")
-        plain_pps = total_pairs / (t_plain / 1e3)
+        plain_pps = replicas.aggregate(rep, float(n * args.steps), [m / 1e3 for m in device_ms(plain)])["pairs_per_s"]
 
     acc = None
     cpu = None
@@ -478,8 +447,7 @@ def main():
             line["cpu_baseline"] = {"value": cpu["pairs_per_s"], "unit": "pairs/s", "cores": cpu["cores"],
                                     "kind": cpu["kind"], "sample": cpu["sample"], "gcups": cpu["gcups"]}
         print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
