@@ -744,7 +744,8 @@ __global__ void k_band_scan(BandCounters* c) {
 
 // A banded pair's outcome: promotion to the next wider class (a single item
 // centred on this band), the full DP (edge check failed at W = 32, or the
-// banded sum is not positive), the FP64 list, or its log10 result.
+// banded sum is not positive -- NaN included), the FP64 list, or its log10
+// result.
 __device__ __forceinline__ void band_outcome(const BandParams& p, int cls, const BandItem& it, int R, float tot,
                                              bool fall_back, bool rescue) {
   if (fall_back && cls + 1 < kBandWidths) {
@@ -792,12 +793,18 @@ __device__ __forceinline__ int mm_index(int qi, int qd) {
   return ((mx * (mx + 1)) >> 1) + mn;
 }
 
+// Folded form (as the full-DP kernels): pMM(r) is folded into the row's
+// emissions and cx, cy carry 1/pMM, so an M update is two FMAs and a
+// multiply.  A row whose pMM is below kFoldMin cannot be folded: its 1/pMM
+// table entry is NaN, which makes the banded sums NaN, and such pairs end in
+// the full DP (which keeps the plain form for them) like any pair whose
+// banded sum is not positive.
 struct FwdRow {
-  float mm, cx, cy, kap, g, pmx, pmy, em, ex;
+  float cx, cy, kap, g, pmx, pmy, em, ex;
   uint32_t rb;  // the read base's one-hot nibble, replicated 8 times
 };
-__device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, uchar4 qv, uint8_t base, float ap,
-                                          float bp) {
+__device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, const float* __restrict__ minv,
+                                          uchar4 qv, uint8_t base, float ap, float bp) {
   FwdRow c;
   const int qi = qv.y & kQualMask, qd = qv.z & kQualMask;
   const QProb qpi = qp[qi], qpg = qp[qv.w & kQualMask], qpb = qp[qv.x & kQualMask];
@@ -805,12 +812,13 @@ __device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, uch
   c.pmy = qp[qd].p;
   c.g = qpg.p;
   const float gp = qpg.q;
-  c.mm = mmt[mm_index(qi, qd)];
-  c.cx = gp * ap;
-  c.cy = gp * bp;
+  const int mi = mm_index(qi, qd);
+  const float mm = mmt[mi], inv = __ldg(minv + mi);
+  c.cx = gp * ap * inv;
+  c.cy = gp * bp * inv;
   c.kap = c.g * ap * qpi.inv;
-  c.em = qpb.q;
-  c.ex = qpb.third;
+  c.em = qpb.q * mm;
+  c.ex = qpb.third * mm;
   c.rb = onehot(base) * 0x11111111u;
   return c;
 }
@@ -869,11 +877,11 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
     win[w] = v;
   }
   float pmx_last = 1.f;
-  FwdRow cur = fwd_row(sm.qp, sm.mm, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
+  FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm.qp, sm.mm, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
+    const FwdRow nxt = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
     {
       const int rn = min(r + 1, R - 1);  // row r + 2
       qn = quals[rn];
@@ -889,7 +897,7 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
       {
         const float upm = (k + 1 < WB) ? M[k + 1] : 0.f;
         const float upx = (k + 1 < WB) ? X[k + 1] : 0.f;
-        const float mn = e * __fmaf_rn(cur.mm, M[k], __fmaf_rn(cur.cx, X[k], cur.cy * Y[k]));
+        const float mn = e * __fmaf_rn(cur.cy, Y[k], __fmaf_rn(cur.cx, X[k], M[k]));
         const float xn = __fmaf_rn(cur.kap, upx, upm);
         const float yn = __fmaf_rn(cur.g, ly, lm);
         M[k] = mn; X[k] = xn; Y[k] = yn;
@@ -900,7 +908,7 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
           const int ki = k - OFF;
           const float upm = (ki + 1 < WI) ? Mi[ki + 1] : 0.f;
           const float upx = (ki + 1 < WI) ? Xi[ki + 1] : 0.f;
-          const float mn = e * __fmaf_rn(cur.mm, Mi[ki], __fmaf_rn(cur.cx, Xi[ki], cur.cy * Yi[ki]));
+          const float mn = e * __fmaf_rn(cur.cy, Yi[ki], __fmaf_rn(cur.cx, Xi[ki], Mi[ki]));
           const float xn = __fmaf_rn(cur.kap, upx, upm);
           const float yn = __fmaf_rn(cur.g, lyi, lmi);
           Mi[ki] = mn; Xi[ki] = xn; Yi[ki] = yn;

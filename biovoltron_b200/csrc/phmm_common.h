@@ -26,6 +26,11 @@ constexpr int kHapTail = 48;
 // Reference constants (Context.h:104-110, 144-150; pairhmm_common.h:16).
 constexpr double kMinAccepted = 1e-28;
 
+// The FP32 kernels fold pMM(r) into row r's emissions (five operations per
+// cell instead of six) when every row involved has pMM >= kFoldMin; pMM is
+// that small only for indel qualities of a few units.
+constexpr float kFoldMin = 0.5f;
+
 // Per-quality FP32 probabilities for the banded kernel: p = 10^(-q/10),
 // 1 - p, p / 3 and 1 / p, one 16-byte load per quality byte.
 struct alignas(16) QProb {
@@ -36,6 +41,7 @@ struct Tables {
   QProb qp[128];
   float ph2pr_f[128];
   float mm_f[kMMEntries];
+  float mm_inv_f[kMMEntries];  // 1 / mm_f where mm_f >= kFoldMin, else NaN
   double ph2pr_d[128];
   double mm_d[kMMEntries];
   float init_f;          // 2^120

@@ -168,6 +168,15 @@ template <typename T> struct ScaledXY { static constexpr bool value = sizeof(T) 
 // Per-lane row constants for one strip.  Scaled form: mm = pMM, cx = pGAPM *
 // pMX(r-1), cy = pGAPM * pMY(r-1), kap = pXX pMX(r-1)/pMX(r), g = pYY.
 // Unscaled form: mm = pMM, cx = pGAPM, kap = pMX, my = pMY, g = pXX = pYY.
+//
+// Folded form (FP32, every real row of the strip with pMM >= kFoldMin): pMM(r)
+// moves into row r's emissions and out of the M coefficient, cx and cy are
+// multiplied by 1/pMM (Tables::mm_inv_f), so
+//   M(r,c) = [e(r,c) pMM(r)] (M(r-1,c-1) + cx/pMM Xh(r-1,c-1) + cy/pMM Yh(r-1,c-1))
+// takes two FMAs and a multiply: five operations per cell instead of six.
+// The states keep their meaning (M, X/pMX, Y/pMY), so strips of one read may
+// differ in form.  Rows with a small pMM (indel qualities of a few units)
+// would need large coefficients; a strip holding one keeps the plain form.
 template <typename T, int RT>
 struct Rows {
   T mm[RT], cx[RT], cy[RT], kap[RT], my[RT], g[RT], y0[RT];
@@ -177,17 +186,21 @@ struct Rows {
 // numbers, row 0 = initial row, negative = padding) and writes the lane's
 // emission-table column.  initializeVectors (avx-pairhmm-template.h:108-127)
 // and stripeINITIALIZATION (:150-158) give the per-row probabilities.
+// Returns whether the strip uses the folded form (warp-uniform; FP32 only).
 template <typename T, int RT>
-__device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const uchar4* __restrict__ quals,
+__device__ __forceinline__ bool setup_rows(const Tables* __restrict__ tb, const uchar4* __restrict__ quals,
                                            const uint8_t* __restrict__ bases, int R, int rbase, T init_y,
                                            Rows<T, RT>& rw, unsigned char* etab, int lane) {
   const T* ph = ph2pr_tab<T>(tb);
   const T* mmt = mm_tab<T>(tb);
   T em[RT], ex[RT];
+  float minv[RT];  // 1/pMM of the row (NaN: too small to fold)
   uint32_t rc[RT];
   bool valid[RT], sumrow[RT];
 #pragma unroll
-  for (int j = 0; j < RT; ++j) { em[j] = T(0); ex[j] = T(0); rc[j] = 0; valid[j] = false; sumrow[j] = false; }
+  for (int j = 0; j < RT; ++j) {
+    em[j] = T(0); ex[j] = T(0); minv[j] = 1.f; rc[j] = 0; valid[j] = false; sumrow[j] = false;
+  }
 #pragma unroll
   for (int j = 0; j < RT; ++j) {
     const int r = rbase + j;
@@ -210,6 +223,7 @@ __device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const 
         bp = ph[pv.z & kQualMask];
       }
       rw.mm[j] = mmt[mm_index(qi, qd)];
+      minv[j] = tb->mm_inv_f[mm_index(qi, qd)];
       if constexpr (ScaledXY<T>::value) {
         rw.cx[j] = gp * ap;
         rw.cy[j] = gp * bp;
@@ -235,8 +249,27 @@ __device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const 
       rw.y0[j] = (r == 0) ? init_y : T(0);
     }
   }
+  bool fold = false;
+  if constexpr (ScaledXY<T>::value) {
+    bool small = false;
+#pragma unroll
+    for (int j = 0; j < RT; ++j) small |= valid[j] && !(minv[j] > 0.f);
+    fold = !__any_sync(0xffffffffu, small);
+    if (fold) {
+#pragma unroll
+      for (int j = 0; j < RT; ++j) {
+        if (valid[j]) {
+          rw.cx[j] = rw.cx[j] * minv[j];
+          rw.cy[j] = rw.cy[j] * minv[j];
+          em[j] = em[j] * rw.mm[j];
+          ex[j] = ex[j] * rw.mm[j];
+        }
+      }
+    }
+  }
   // Emission table: for haplotype code h, row j: 1-eps on a match, eps/3 on a
-  // mismatch (a read or haplotype N matches everything), 0 for padding.
+  // mismatch (a read or haplotype N matches everything), 0 for padding; times
+  // pMM in the folded form.
 #pragma unroll
   for (int h = 0; h < kCodes; ++h) {
     T v[RT];
@@ -247,6 +280,7 @@ __device__ __forceinline__ void setup_rows(const Tables* __restrict__ tb, const 
     }
     store_emissions<T, RT>(etab, lane, h, v);
   }
+  return fold;
 }
 
 // Stages a haplotype as column codes: code[kHapLead + c - 1] for c = 1..H,
@@ -282,7 +316,7 @@ __device__ __forceinline__ void stage_hap_pair(const uint8_t* __restrict__ ha, i
 // result for FP32), the per-step sums of M and X over the bottom row (FP64,
 // which has no summing row) and the largest bottom-row value (FP64, for
 // renormalisation between strips).
-template <typename T, int RT, bool MULTI, int CH>
+template <typename T, int RT, bool MULTI, int CH, bool FOLD = false>
 __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
                                           const unsigned char* __restrict__ hc_lane, int nsteps, int lane,
                                           T* __restrict__ bnd, unsigned char* ring, T in_scale, T& lastM,
@@ -347,7 +381,11 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
 #pragma unroll
       for (int j = 0; j < RT; ++j) {
         T mn, xn, yn;
-        if constexpr (ScaledXY<T>::value) {
+        if constexpr (ScaledXY<T>::value && FOLD) {
+          mn = e[j] * fma_(rw.cy[j], dy, fma_(rw.cx[j], dx, dm));
+          xn = fma_(rw.kap[j], ux, um);
+          yn = fma_(rw.g[j], Y[j], M[j]);
+        } else if constexpr (ScaledXY<T>::value) {
           mn = e[j] * fma_(rw.mm[j], dm, fma_(rw.cx[j], dx, rw.cy[j] * dy));
           xn = fma_(rw.kap[j], ux, um);
           yn = fma_(rw.g[j], Y[j], M[j]);
@@ -422,7 +460,7 @@ __device__ __forceinline__ float2 shfl_up2(float2 v) {
 // kapN), with the operations and operands of the top row's own update.
 // Lane 0 receives its own sums: its top row is padding (e = 0) and the row
 // below has zero X coefficient, so they reach no real row.
-template <int RT>
+template <int RT, bool FOLD>
 __device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const float* __restrict__ y0a,
                                                const float* __restrict__ y0b, const ELane el,
                                                const uint32_t* __restrict__ hcp_lane, int nsteps,
@@ -447,8 +485,13 @@ __device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const 
   const float2 mmN = make_float2(mmN1, mmN1), cxN = make_float2(cxN1, cxN1);
   const float2 cyN = make_float2(cyN1, cyN1), kapN = make_float2(kapN1, kapN1);
   // sums for step 0 from the column-0 boundary state (M = X = 0, Y = y0)
+  // (the folded form drops pMM: mmN is 1 there and unused)
+  auto msum = [&](float2 m, float2 x, float2 y) {
+    if constexpr (FOLD) return __ffma2_rn(cyN, y, __ffma2_rn(cxN, x, m));
+    else return __ffma2_rn(mmN, m, __ffma2_rn(cxN, x, __fmul2_rn(cyN, y)));
+  };
   float2 zx = shfl_up2(__ffma2_rn(kapN, X[RT - 1], M[RT - 1]));
-  float2 zm = shfl_up2(__ffma2_rn(mmN, M[RT - 1], __ffma2_rn(cxN, X[RT - 1], __fmul2_rn(cyN, Y[RT - 1]))));
+  float2 zm = shfl_up2(msum(M[RT - 1], X[RT - 1], Y[RT - 1]));
   for (int s0 = 0; s0 < nsteps; s0 += CH) {
 #pragma unroll
     for (int u = 0; u < CH; ++u) {
@@ -465,9 +508,15 @@ __device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const 
       M[0] = mn0; X[0] = zx; Y[0] = yn0;
 #pragma unroll
       for (int j = 1; j < RT; ++j) {
-        float2 t = __fmul2_rn(cy[j], dy);
-        t = __ffma2_rn(cx[j], dx, t);
-        t = __ffma2_rn(mm[j], dm, t);
+        float2 t;
+        if constexpr (FOLD) {
+          t = __ffma2_rn(cx[j], dx, dm);
+          t = __ffma2_rn(cy[j], dy, t);
+        } else {
+          t = __fmul2_rn(cy[j], dy);
+          t = __ffma2_rn(cx[j], dx, t);
+          t = __ffma2_rn(mm[j], dm, t);
+        }
         const float2 mn = make_float2(ea[j] * t.x, eb[j] * t.y);
         const float2 xn = __ffma2_rn(kap[j], ux, um);
         const float2 yn = __ffma2_rn(g[j], Y[j], M[j]);
@@ -477,7 +526,7 @@ __device__ __forceinline__ void run_strip_pair(const Rows<float, RT>& rw, const 
       }
       // dm/dx/dy: the bottom row at column c-1; M/X/Y[RT-1]: at column c
       zx = shfl_up2(__ffma2_rn(kapN, X[RT - 1], M[RT - 1]));
-      zm = shfl_up2(__ffma2_rn(mmN, dm, __ffma2_rn(cxN, dx, __fmul2_rn(cyN, dy))));
+      zm = shfl_up2(msum(dm, dx, dy));
     }
   }
   lastM = M[RT - 1];
@@ -550,9 +599,10 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
   unsigned char* ring = etab + S::kEtabBytes;
   const bool is_f64 = sizeof(T) == 8;
   Rows<T, RT> rw;
+  bool fold = false;
   if (!MULTI) {
     // single strip: rows and emission table are shared by all haplotypes
-    setup_rows<T, RT>(p.tables, quals, bases, R, lane * RT - pad, T(0), rw, etab, lane);
+    fold = setup_rows<T, RT>(p.tables, quals, bases, R, lane * RT - pad, T(0), rw, etab, lane);
   }
   for (int k = 0; k < it.nh; ++k) {
     const int h = it.hap0 + k;
@@ -578,7 +628,8 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
           }
           __syncwarp();
           float2 lastM, lastY;
-          run_strip_pair<RT>(rw, y0a, y0b, el, hcp + kHapLead - lane, nsteps, lastM, lastY);
+          if (fold) run_strip_pair<RT, true>(rw, y0a, y0b, el, hcp + kHapLead - lane, nsteps, lastM, lastY);
+          else run_strip_pair<RT, false>(rw, y0a, y0b, el, hcp + kHapLead - lane, nsteps, lastM, lastY);
           if (lane == kWarp - 1) {
             write_result<float>(p, it.read, h, it.out0 + k, lastY.x + lastM.x, 0);
             write_result<float>(p, it.read, h + 1, it.out0 + k + 1, lastY.y + lastM.y, 0);
@@ -618,10 +669,14 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
       T in_scale = T(1);
       for (int st = 0; st < nstrips; ++st) {
         __syncwarp();
-        setup_rows<T, RT>(p.tables, quals, bases, R, st * strip_rows + lane * RT - pad, init_y, rw, etab, lane);
+        fold = setup_rows<T, RT>(p.tables, quals, bases, R, st * strip_rows + lane * RT - pad, init_y, rw, etab, lane);
         __syncwarp();
-        run_strip<T, RT, true, 32>(rw, el, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
-                                   lastY, sumM, sumX, bmax);
+        if (fold)
+          run_strip<T, RT, true, 32, true>(rw, el, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
+                                           lastY, sumM, sumX, bmax);
+        else
+          run_strip<T, RT, true, 32>(rw, el, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
+                                     lastY, sumM, sumX, bmax);
         __syncwarp();
         in_scale = T(1);
         if (p.rescale && st + 1 < nstrips) {
@@ -637,8 +692,12 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
         }
       }
     } else {
-      run_strip<T, RT, false, 8>(rw, el, hc + kHapLead - lane, nsteps, lane, nullptr, nullptr, T(1), lastM,
-                                 lastY, sumM, sumX, bmax);
+      if (fold)
+        run_strip<T, RT, false, 8, true>(rw, el, hc + kHapLead - lane, nsteps, lane, nullptr, nullptr, T(1), lastM,
+                                         lastY, sumM, sumX, bmax);
+      else
+        run_strip<T, RT, false, 8>(rw, el, hc + kHapLead - lane, nsteps, lane, nullptr, nullptr, T(1), lastM,
+                                   lastY, sumM, sumX, bmax);
     }
     if (lane == kWarp - 1) {
       // FP32: the summing row's Y + M; FP64: the accumulated last-row sums.

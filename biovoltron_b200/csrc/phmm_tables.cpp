@@ -12,6 +12,7 @@
 // The kernels read these tables unchanged, so per-row probabilities equal the
 // reference's bit for bit.
 #include <cmath>
+#include <limits>
 #include <algorithm>
 #include <vector>
 
@@ -73,6 +74,7 @@ void build_tables(Tables* t) {
   }
   fill_mm<float>(t->mm_f);
   fill_mm<double>(t->mm_d);
+  for (int x = 0; x < kMMEntries; ++x) t->mm_inv_f[x] = t->mm_f[x] >= kFoldMin ? 1.f / t->mm_f[x] : std::numeric_limits<float>::quiet_NaN();
   t->init_f = std::ldexp(1.f, 120);
   t->log10_init_f = log10f(t->init_f);
   t->init_d = std::ldexp(1.0, 1020);
