@@ -212,7 +212,8 @@ def train_band(eng, args, local_seed: int) -> dict:
     per_region = 5_388_348 / 4096
     n_reg = max(8, int(round(args.train_pairs / per_region)))
     tb = W.config1(seed=7000 + local_seed, n_regions=n_reg)
-    rep = eng.band_train(tb, epochs=args.train_epochs, seed=1234 + local_seed)
+    rep = eng.band_train(tb, epochs=args.train_epochs, alpha=args.train_alpha, tau=args.train_tau,
+                         seed=1234 + local_seed)
     rep["train_workload"] = tb.name
     return rep
 
@@ -275,11 +276,15 @@ def main():
     ap.add_argument("--haps-per-warp", type=int, default=0, help="0: engine default, 1 or 2")
     ap.add_argument("--train-pairs", type=int, default=1_000_000)
     ap.add_argument("--train-epochs", type=int, default=8)
+    ap.add_argument("--train-alpha", type=float, default=16.0, help="MLP loss weight of a too-narrow band")
+    ap.add_argument("--train-tau", type=float, default=1e-4, help="posterior threshold of the training labels")
     ap.add_argument("--weights", default="", help="load band MLP weights instead of training")
     ap.add_argument("--save-weights", default="", help="write the trained band MLP weights here")
     ap.add_argument("--audit-period", type=int, default=1024)
     ap.add_argument("--oracle-sample", type=int, default=20000)
     ap.add_argument("--edge-threshold", type=float, default=1e-3)
+    ap.add_argument("--fixed-half", type=int, default=-1,
+                    help=">= 0: band of seed diagonal +- this many diagonals (and the 11-mer extent), no MLP")
     ap.add_argument("--margin", type=int, default=2, help="diagonals added on both sides of the predicted band")
     ap.add_argument("--tune-regions", type=int, default=500,
                     help="regions of the workload the launch-shape autotuner times (0: default shapes)")
@@ -332,8 +337,12 @@ def main():
         train_rep = train_band(eb, args, rank)
         if args.save_weights and rank == 0:
             eb.band_save(args.save_weights)
-        eb.set_band_options(use_mlp=True, margin=args.margin, edge_threshold=args.edge_threshold,
-                            audit_period=args.audit_period)
+        if args.fixed_half >= 0:  # seed-centred band of +-fixed_half diagonals instead of the MLP's
+            eb.set_band_options(use_mlp=False, fixed_half=args.fixed_half, margin=args.margin,
+                                edge_threshold=args.edge_threshold, audit_period=args.audit_period)
+        else:
+            eb.set_band_options(use_mlp=True, margin=args.margin, edge_threshold=args.edge_threshold,
+                                audit_period=args.audit_period)
         n, steps, wall, res = time_form(eb, batch, args, rep, band=True)
         band = {"n": n, "steps": steps, "wall": wall, "res": res}
     main_run = band if band else plain
@@ -353,9 +362,10 @@ def main():
         e2e_eng.compute_regions(batch, out=out)
     rep.barrier()
     e2e_t = []
+    e2e_st = None
     for _ in range(args.steps):
         t1 = time.perf_counter()
-        e2e_eng.compute_regions(batch, out=out)
+        _, e2e_st = e2e_eng.compute_regions(batch, out=out, with_stats=True)
         e2e_t.append(time.perf_counter() - t1)
     clk = clocks.stop()
     rep.barrier()
@@ -440,6 +450,12 @@ def main():
         line["accuracy"] = acc
         line["e2e"] = {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(batch.nbytes()),
                        "d2h_bytes_per_step": int(8 * n), "results_identical_to_device_run": same}
+        if e2e_st is not None:
+            # last step: copies (first H2D to packed qualities, events; they overlap the host's
+            # planning), kernels (events), result D2H and the whole call (host clock)
+            line["e2e"]["last_step_ms"] = {"h2d_and_pack": e2e_st["ms_h2d"],
+                                           "kernels": e2e_st["ms_fp32"] + e2e_st["ms_fp64"],
+                                           "d2h": e2e_st["ms_d2h"], "call": e2e_st["ms_total"]}
         line["gpu_launches"] = int(last["kernel_launches"]) * args.steps
         line["clocks"] = clk
         line["wall_s_timed"] = main_run["wall"]

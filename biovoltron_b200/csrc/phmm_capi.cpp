@@ -14,6 +14,7 @@
 
 struct bv_phmm_ctx {
   bvphmm::Engine engine;
+  std::unique_ptr<bvphmm::Engine> second;  // the chunked compute's other context, made on first use
   explicit bv_phmm_ctx(const bv_phmm_options& o) : engine(o) {}
 };
 
@@ -113,6 +114,7 @@ bv_status bv_phmm_create(const bv_phmm_options* opts, bv_phmm_ctx** out) {
   if (o.mode != BV_MODE_FULL && o.mode != BV_MODE_BAND) return BV_ERR_INVALID_ARG;
   if (o.rescue_threshold != bvphmm::kMinAccepted) return BV_ERR_UNSUPPORTED;
   if (o.haps_per_warp < 0 || o.haps_per_warp > 2) return BV_ERR_INVALID_ARG;
+  if (o.pipeline_chunks < 0 || o.pipeline_chunks > 64 || o.pipeline_min_pairs < 0) return BV_ERR_INVALID_ARG;
   bv_phmm_ctx* c = new (std::nothrow) bv_phmm_ctx(o);
   if (!c) return BV_ERR_OOM;
   bv_status s = guard(c, [&] { return c->engine.init(); });
@@ -138,7 +140,25 @@ int64_t bv_phmm_region_results(const bv_region_batch* b) {
 
 bv_status bv_phmm_compute_regions(bv_phmm_ctx* ctx, const bv_region_batch* batch, double* out, bv_phmm_stats* stats) {
   if (!ctx || !batch) return BV_ERR_INVALID_ARG;
-  return guard(ctx, [&] { return ctx->engine.compute(*batch, out, stats); });
+  return guard(ctx, [&] {
+    bvphmm::Engine& a = ctx->engine;
+    const bv_phmm_options& o = a.options();
+    const int chunks = o.pipeline_chunks > 0 ? o.pipeline_chunks : 4;
+    const int64_t min_pairs = o.pipeline_min_pairs > 0 ? o.pipeline_min_pairs : (int64_t)1 << 22;
+    if (chunks < 2 || bv_phmm_region_results(batch) < min_pairs) return a.compute(*batch, out, stats);
+    if (!ctx->second) {
+      auto e = std::make_unique<bvphmm::Engine>(o);
+      const bv_status s = e->init();
+      if (s != BV_OK) return a.fail(s, std::string("second context: ") + e->last_error());
+      ctx->second = std::move(e);
+    }
+    bvphmm::Engine& b = *ctx->second;
+    if (b.mirrored_version() != a.config_version()) {
+      const bv_status s = b.mirror_config(a);
+      if (s != BV_OK) return a.fail(s, std::string("second context: ") + b.last_error());
+    }
+    return a.compute_chunked(b, *batch, out, stats, chunks);
+  });
 }
 
 bv_status bv_phmm_stage_regions(bv_phmm_ctx* ctx, const bv_region_batch* batch) {

@@ -72,6 +72,7 @@ Engine::~Engine() {
   destroy_graph();
   if (stream_) {
     cudaStreamSynchronize(stream_);
+    if (h_counters_) cudaFreeHost(h_counters_);
     for (auto& e : ev_)
       if (e) cudaEventDestroy(e);
     for (auto& e : tune_ev_)
@@ -208,9 +209,10 @@ bv_status Engine::plan(const bv_region_batch& b) {
   for (int64_t g = 0; g < b.num_regions; ++g) {
     const int64_t h0 = b.region_haps[g], nh = b.region_haps[g + 1] - h0;
     const int64_t r0 = b.region_reads[g], nr = b.region_reads[g + 1] - r0;
+    const int64_t hap_bases = nh > 0 ? b.hap_offsets[h0 + nh] - b.hap_offsets[h0] : 0;  // haplotypes are contiguous
     for (int64_t r = r0; r < r0 + nr; ++r) {
       const int64_t rl = b.read_offsets[r + 1] - b.read_offsets[r];
-      for (int64_t h = h0; h < h0 + nh; ++h) n_cells_ += rl * (b.hap_offsets[h + 1] - b.hap_offsets[h]);
+      n_cells_ += rl * hap_bases;
       if (all_f64) {
         for (int64_t k = 0; k < nh; ++k)
           f64_items_.push_back(PairRef{(int32_t)r, (int32_t)(h0 + k), res + (r - r0) * nh + k});
@@ -279,7 +281,9 @@ bv_status Engine::plan(const bv_region_batch& b) {
   return BV_OK;
 }
 
-bv_status Engine::upload(const bv_region_batch& b) {
+// Inputs: the byte arrays and offsets go to the device as soon as the batch
+// is validated, so the copies run while the host plans the launches.
+bv_status Engine::upload_inputs(const bv_region_batch& b) {
   n_reads_ = b.num_reads;
   n_haps_ = b.num_haps;
   n_read_bytes_ = b.num_reads > 0 ? b.read_offsets[b.num_reads] : 0;
@@ -294,22 +298,9 @@ bv_status Engine::upload(const bv_region_batch& b) {
   BV_CUDA(d_read_off_.reserve(sizeof(int64_t) * (n_reads_ + 1)), "alloc read offsets");
   BV_CUDA(d_hap_bases_.reserve((size_t)std::max<int64_t>(n_hap_bytes_, 1)), "alloc haps");
   BV_CUDA(d_hap_off_.reserve(sizeof(int64_t) * (n_haps_ + 1)), "alloc hap offsets");
-  BV_CUDA(d_units_.reserve(sizeof(Unit) * std::max<size_t>(units_.size(), 1)), "alloc units");
-  BV_CUDA(d_out_.reserve(sizeof(double) * (size_t)std::max<int64_t>(n_results_, 1)), "alloc results");
-  BV_CUDA(d_rescue_.reserve(sizeof(PairRef) * (size_t)std::max<int64_t>(n_results_, 1)), "alloc rescue list");
-  // strip-boundary buffers for the multi-strip launches
-  size_t need32 = 0;
-  for (const auto& lp : plans_)
-    if (lp.multi) need32 = std::max<size_t>(need32, (size_t)lp.grid * lp.warps_per_block * (size_t)lp.bnd_cols * 4 * sizeof(float));
-  if (need32) BV_CUDA(d_bnd32_.reserve(need32), "alloc boundary buffers");
-  const size_t need64 = (size_t)rescue_plan_.grid * (kThreadsPerBlock / kWarp) * (size_t)rescue_plan_.bnd_cols * 4 * sizeof(double);
-  BV_CUDA(d_bnd64_.reserve(need64), "alloc FP64 boundary buffers");
-
   BV_CUDA(cudaEventRecord(ev_[0], stream_), "event");
-  const int64_t r0 = b.num_reads > 0 ? b.read_offsets[0] : 0;
   // Offsets are copied verbatim; the byte arrays are copied from index 0 so
   // offsets index them directly.
-  (void)r0;
   if (n_read_bytes_ > 0) {
     BV_CUDA(cudaMemcpyAsync(d_read_bases_.get(), b.read_bases, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
     BV_CUDA(cudaMemcpyAsync(d_q_.get(), b.read_q, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
@@ -325,6 +316,23 @@ bv_status Engine::upload(const bv_region_batch& b) {
   if (n_haps_ > 0)
     BV_CUDA(cudaMemcpyAsync(d_hap_off_.get(), b.hap_offsets, sizeof(int64_t) * (n_haps_ + 1), cudaMemcpyHostToDevice,
                             stream_), "H2D");
+  return BV_OK;
+}
+
+// The plan's device side: work units, result and list buffers, and the packed
+// qualities.  Nothing here waits for the copies; run() reads the copy time
+// once its own synchronisation has passed.
+bv_status Engine::upload_plan() {
+  BV_CUDA(d_units_.reserve(sizeof(Unit) * std::max<size_t>(units_.size(), 1)), "alloc units");
+  BV_CUDA(d_out_.reserve(sizeof(double) * (size_t)std::max<int64_t>(n_results_, 1)), "alloc results");
+  BV_CUDA(d_rescue_.reserve(sizeof(PairRef) * (size_t)std::max<int64_t>(n_results_, 1)), "alloc rescue list");
+  // strip-boundary buffers for the multi-strip launches
+  size_t need32 = 0;
+  for (const auto& lp : plans_)
+    if (lp.multi) need32 = std::max<size_t>(need32, (size_t)lp.grid * lp.warps_per_block * (size_t)lp.bnd_cols * 4 * sizeof(float));
+  if (need32) BV_CUDA(d_bnd32_.reserve(need32), "alloc boundary buffers");
+  const size_t need64 = (size_t)rescue_plan_.grid * (kThreadsPerBlock / kWarp) * (size_t)rescue_plan_.bnd_cols * 4 * sizeof(double);
+  BV_CUDA(d_bnd64_.reserve(need64), "alloc FP64 boundary buffers");
   if (!units_.empty())
     BV_CUDA(cudaMemcpyAsync(d_units_.get(), units_.data(), sizeof(Unit) * units_.size(), cudaMemcpyHostToDevice,
                             stream_), "H2D");
@@ -334,25 +342,28 @@ bv_status Engine::upload(const bv_region_batch& b) {
   BV_CUDA(launch_pack_quals(d_q_.as<uint8_t>(), d_i_.as<uint8_t>(), d_d_.as<uint8_t>(), d_c_.as<uint8_t>(),
                             d_quals4_.as<uchar4>(), n_read_bytes_, sms_, stream_), "pack quals");
   BV_CUDA(cudaEventRecord(ev_[1], stream_), "event");
-  BV_CUDA(cudaStreamSynchronize(stream_), "stage sync");
-  BV_CUDA(cudaEventElapsedTime(&ms_h2d_, ev_[0], ev_[1]), "event time");
+  h2d_time_pending_ = true;
   return BV_OK;
 }
 
-bv_status Engine::stage(const bv_region_batch& b) {
+// The caller's host arrays are borrowed for the call: unless the caller runs
+// the batch before returning (compute, whose run synchronises), stage waits
+// for the copies, and every error path after the first copy waits for them too.
+bv_status Engine::stage(const bv_region_batch& b, bool wait) {
   staged_ = false;
   destroy_graph();
   BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");
   bv_status s = validate(b);
   if (s != BV_OK) return s;
-  s = plan(b);
-  if (s != BV_OK) return s;
-  s = upload(b);
-  if (s != BV_OK) return s;
-  if (band_enabled()) {
-    s = band_prepare();
-    if (s != BV_OK) return s;
+  s = upload_inputs(b);
+  if (s == BV_OK) s = plan(b);
+  if (s == BV_OK) s = upload_plan();
+  if (s == BV_OK && band_enabled()) s = band_prepare();
+  if (s != BV_OK) {
+    cudaStreamSynchronize(stream_);
+    return s;
   }
+  if (wait) BV_CUDA(cudaStreamSynchronize(stream_), "stage sync");
   staged_ = true;
   runs_since_stage_ = 0;
   return BV_OK;
@@ -446,9 +457,16 @@ void Engine::destroy_graph() {
 }
 
 bv_status Engine::run(bv_phmm_stats* stats) {
+  bv_status s = launch();
+  if (s != BV_OK) return s;
+  return finish(stats);
+}
+
+bv_status Engine::launch() {
   if (!staged_) return fail(BV_ERR_INVALID_ARG, "no staged batch");
   BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");
-  const auto t0 = std::chrono::steady_clock::now();
+  run_t0_ = std::chrono::steady_clock::now();
+  if (!h_counters_) BV_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_counters_), sizeof(Counters)), "pinned counters");
   // The first run of a staged batch launches directly; later runs replay a
   // captured graph of the same launch sequence.
   if (runs_since_stage_ == 0 || !graph_exec_) {
@@ -473,9 +491,19 @@ bv_status Engine::run(bv_phmm_stats* stats) {
     BV_CUDA(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
   }
   ++runs_since_stage_;
-  Counters c{};
-  BV_CUDA(cudaMemcpyAsync(&c, d_counters_.get(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_), "counters D2H");
+  // page-locked destination: the copy is queued, the host goes on
+  BV_CUDA(cudaMemcpyAsync(h_counters_, d_counters_.get(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_),
+          "counters D2H");
+  return BV_OK;
+}
+
+bv_status Engine::finish(bv_phmm_stats* stats) {
   BV_CUDA(cudaStreamSynchronize(stream_), "run sync");
+  if (h2d_time_pending_) {
+    BV_CUDA(cudaEventElapsedTime(&ms_h2d_, ev_[0], ev_[1]), "event time");
+    h2d_time_pending_ = false;
+  }
+  const Counters c = *h_counters_;
   if (c.status != 0) return fail(BV_ERR_INTERNAL, "kernel reported an inconsistent state");
   if (stats) *stats = bv_phmm_stats{};
   if (stats && band_enabled()) {
@@ -509,7 +537,7 @@ bv_status Engine::run(bv_phmm_stats* stats) {
     }
     stats->ms_h2d = ms_h2d_;
     stats->ms_total =
-        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - run_t0_).count();
   }
   return BV_OK;
 }
@@ -524,13 +552,33 @@ bv_status Engine::fetch(double* out, int64_t n) {
   return BV_OK;
 }
 
+bv_status Engine::fetch_async(double* out, int64_t n) {
+  if (!staged_) return fail(BV_ERR_INVALID_ARG, "no staged batch");
+  if (n < 0 || n > n_results_) return fail(BV_ERR_INVALID_ARG, "fetch size exceeds staged results");
+  if (n == 0) return BV_OK;
+  if (!out) return fail(BV_ERR_INVALID_ARG, "null output");
+  BV_CUDA(cudaMemcpyAsync(out, d_out_.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, stream_), "results D2H");
+  return BV_OK;
+}
+
 bv_status Engine::compute(const bv_region_batch& b, double* out, bv_phmm_stats* stats) {
   const auto t0 = std::chrono::steady_clock::now();
-  bv_status s = stage(b);
+  if (!out && b.num_regions > 0) {
+    // checked before any copy starts (a batch with results needs an output)
+    bv_status v = validate(b);
+    if (v != BV_OK) return v;
+    int64_t res = 0;
+    for (int64_t g = 0; g < b.num_regions; ++g)
+      res += (b.region_reads[g + 1] - b.region_reads[g]) * (b.region_haps[g + 1] - b.region_haps[g]);
+    if (res > 0) return fail(BV_ERR_INVALID_ARG, "null output");
+  }
+  bv_status s = stage(b, false);  // run() synchronises before this call returns
   if (s != BV_OK) return s;
-  if (n_results_ > 0 && !out) return fail(BV_ERR_INVALID_ARG, "null output");
   s = run(stats);
-  if (s != BV_OK) return s;
+  if (s != BV_OK) {
+    cudaStreamSynchronize(stream_);  // no copy from the caller's arrays outlives the call
+    return s;
+  }
   const auto t1 = std::chrono::steady_clock::now();
   s = fetch(out, n_results_);
   if (s != BV_OK) return s;

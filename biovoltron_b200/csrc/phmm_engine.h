@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <string>
+#include <chrono>
 #include <vector>
 
 #include "bv_pairhmm.h"
@@ -60,9 +61,24 @@ class Engine {
   ~Engine();
   bv_status init();
 
-  bv_status stage(const bv_region_batch& b);
-  bv_status run(bv_phmm_stats* stats);
+  bv_status stage(const bv_region_batch& b, bool wait = true);
+  bv_status run(bv_phmm_stats* stats);  // launch + finish
+  bv_status launch();                    // queue one run of the staged batch; does not wait
+  bv_status finish(bv_phmm_stats* stats);  // wait for the queued run, check it, fill stats
   bv_status fetch(double* out, int64_t n);
+  bv_status fetch_async(double* out, int64_t n);  // queued behind the run; finish() or a sync waits for it
+  const bv_phmm_options& options() const { return opt_; }
+  const bv_band_options& band_options() const { return band_opt_; }
+  bool mlp_ready() const { return mlp_ready_; }
+  uint64_t config_version() const { return config_version_; }
+  // Copies band options, MLP weights and launch shapes from `src` (a context
+  // with the same options); the chunked compute keeps its second context in step.
+  bv_status mirror_config(Engine& src);
+  uint64_t mirrored_version() const { return mirrored_version_; }
+  // One batch split into `chunks` region chunks that alternate between this
+  // context and `other`: a chunk's copies and the host's planning overlap the
+  // previous chunk's kernels.  Results and stats as compute().
+  bv_status compute_chunked(Engine& other, const bv_region_batch& b, double* out, bv_phmm_stats* stats, int chunks);
   bv_status compute(const bv_region_batch& b, double* out, bv_phmm_stats* stats);
 
   const char* last_error() const { return err_.c_str(); }
@@ -90,7 +106,8 @@ class Engine {
  private:
   bv_status validate(const bv_region_batch& b);
   bv_status plan(const bv_region_batch& b);
-  bv_status upload(const bv_region_batch& b);
+  bv_status upload_inputs(const bv_region_batch& b);
+  bv_status upload_plan();
   bv_status enqueue_kernels(bool capturing);
   bv_status band_prepare();
   bv_status enqueue_band(bool capturing, KernelParams& p);
@@ -120,6 +137,11 @@ class Engine {
   int max_hap_ = 0;
   bool staged_ = false;
   float ms_h2d_ = 0;
+  bool h2d_time_pending_ = false;  // ms_h2d_ is read after the next synchronisation
+  Counters* h_counters_ = nullptr;  // page-locked copy of the device counters
+  std::chrono::steady_clock::time_point run_t0_{};
+  uint64_t config_version_ = 0;     // bumped by every change a second context must mirror
+  uint64_t mirrored_version_ = ~0ull;  // the source's config_version_ this context last mirrored
 
   // learned band
   bv_band_options band_opt_{};

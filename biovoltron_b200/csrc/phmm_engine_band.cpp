@@ -26,6 +26,7 @@ bv_status Engine::set_band_options(const bv_band_options& o) {
     return fail(BV_ERR_INVALID_ARG, "band option out of range");
   if (o.enabled && o.use_mlp && !mlp_ready_) return fail(BV_ERR_INVALID_ARG, "no band MLP weights (train or load)");
   band_opt_ = o;
+  ++config_version_;
   staged_ = false;  // buffers and launch sequence depend on the mode: stage again
   destroy_graph();
   return BV_OK;
@@ -118,7 +119,6 @@ bv_status Engine::band_prepare() {
   if (need32 > d_bnd32_.capacity()) BV_CUDA(d_bnd32_.reserve(need32), "alloc boundary buffers");
   BV_CUDA(launch_pairs_from_units(d_units_.as<Unit>(), (long long)units_.size(), d_pair_read_.as<int32_t>(),
                                   d_pair_hap_.as<int32_t>(), sms_, stream_), "pairs");
-  BV_CUDA(cudaStreamSynchronize(stream_), "band prepare sync");
   return BV_OK;
 }
 

@@ -75,9 +75,11 @@ bv_status Engine::stage_for_labels(const bv_region_batch& b) {
   BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");
   bv_status s = validate(b);
   if (s != BV_OK) return s;
+  s = upload_inputs(b);
+  if (s != BV_OK) return s;
   s = plan(b);
   if (s != BV_OK) return s;
-  s = upload(b);
+  s = upload_plan();
   if (s != BV_OK) return s;
   s = band_prepare();
   if (s != BV_OK) return s;
@@ -152,6 +154,7 @@ bv_status Engine::install_weights(const float* w) {
   BV_CUDA(cudaStreamSynchronize(stream_), "weights sync");
   mlp_w_.assign(w, w + kMlpParamCount);
   mlp_ready_ = true;
+  ++config_version_;
   destroy_graph();  // a captured launch sequence may read the old weights only through d_mlp_ (same address)
   return BV_OK;
 }

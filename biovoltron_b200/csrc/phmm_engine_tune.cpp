@@ -30,6 +30,7 @@ bv_status Engine::set_tuning(const bv_phmm_tune_entry* e, int32_t n) {
     tune_[e[i].rows_per_lane].haps_per_warp = e[i].haps_per_warp;
     tune_[e[i].rows_per_lane].warps_per_block = e[i].warps_per_block;
   }
+  ++config_version_;
   staged_ = false;  // the launch plan depends on it: stage again
   destroy_graph();
   return BV_OK;
@@ -140,6 +141,7 @@ bv_status Engine::autotune(const bv_region_batch& sample, int repeats, bv_phmm_t
     out[n++] = t;
   }
   *n_out = n;
+  ++config_version_;
   return BV_OK;
 }
 

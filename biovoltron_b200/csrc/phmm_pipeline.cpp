@@ -1,0 +1,167 @@
+// phmm_pipeline.cpp -- region-chunked compute over two contexts of one GPU.
+//
+// compute() copies the whole batch to the device, runs it, and copies the
+// results back, one after the other.  For large batches the copies (and the
+// host's planning) cost about as much as the kernels, so compute_chunked
+// splits the regions into chunks and alternates them between two contexts
+// (two streams, two sets of buffers): chunk k's copies and planning run
+// while chunk k-1's kernels run.  Every pair is scored exactly as in
+// compute(); only the sampled band audit sees different samples.
+#include <algorithm>
+#include <chrono>
+#include <vector>
+
+#include "phmm_engine.h"
+
+namespace bvphmm {
+
+bv_status Engine::mirror_config(Engine& src) {
+  if (src.mlp_ready_) {
+    bv_status s = install_weights(src.mlp_w_.data());
+    if (s != BV_OK) return s;
+  }
+  band_opt_ = src.band_opt_;
+  std::copy(src.tune_, src.tune_ + kTuneBins + 1, tune_);
+  staged_ = false;
+  destroy_graph();
+  mirrored_version_ = src.config_version_;
+  return BV_OK;
+}
+
+namespace {
+
+// A chunk of regions [g0, g1) as a batch of its own: offsets rebased to the
+// chunk's first read / haplotype, byte pointers moved to match.
+struct Chunk {
+  int64_t g0 = 0, g1 = 0, out0 = 0, n_out = 0;
+  std::vector<int64_t> region_reads, region_haps, read_off, hap_off;
+  bv_region_batch view{};
+
+  void build(const bv_region_batch& b) {
+    const int64_t r0 = b.region_reads[g0], r1 = b.region_reads[g1];
+    const int64_t h0 = b.region_haps[g0], h1 = b.region_haps[g1];
+    region_reads.resize(g1 - g0 + 1);
+    region_haps.resize(g1 - g0 + 1);
+    for (int64_t g = g0; g <= g1; ++g) {
+      region_reads[g - g0] = b.region_reads[g] - r0;
+      region_haps[g - g0] = b.region_haps[g] - h0;
+    }
+    read_off.resize(r1 - r0 + 1);
+    const int64_t rb0 = r1 > r0 ? b.read_offsets[r0] : 0;
+    for (int64_t r = r0; r <= r1 && r1 > r0; ++r) read_off[r - r0] = b.read_offsets[r] - rb0;
+    if (r1 == r0) read_off[0] = 0;
+    hap_off.resize(h1 - h0 + 1);
+    const int64_t hb0 = h1 > h0 ? b.hap_offsets[h0] : 0;
+    for (int64_t h = h0; h <= h1 && h1 > h0; ++h) hap_off[h - h0] = b.hap_offsets[h] - hb0;
+    if (h1 == h0) hap_off[0] = 0;
+    view = b;
+    view.num_regions = g1 - g0;
+    view.region_reads = region_reads.data();
+    view.region_haps = region_haps.data();
+    view.num_reads = r1 - r0;
+    view.read_offsets = read_off.data();
+    view.num_haps = h1 - h0;
+    view.hap_offsets = hap_off.data();
+    auto shift = [](const uint8_t* p, int64_t o) { return p ? p + o : p; };
+    view.read_bases = shift(b.read_bases, rb0);
+    view.read_q = shift(b.read_q, rb0);
+    view.read_i = shift(b.read_i, rb0);
+    view.read_d = shift(b.read_d, rb0);
+    view.read_c = shift(b.read_c, rb0);
+    view.hap_bases = shift(b.hap_bases, hb0);
+  }
+};
+
+void add_stats(bv_phmm_stats& t, const bv_phmm_stats& s) {
+  t.pairs += s.pairs;
+  t.cells += s.cells;
+  t.rescued += s.rescued;
+  t.underflow += s.underflow;
+  t.band_pairs += s.band_pairs;
+  t.band_fallback += s.band_fallback;
+  t.band_cells += s.band_cells;
+  t.kernel_launches += s.kernel_launches;
+  t.ms_h2d += s.ms_h2d;
+  t.ms_fp32 += s.ms_fp32;
+  t.ms_fp64 += s.ms_fp64;
+  t.ms_band += s.ms_band;
+  t.band_routed_full += s.band_routed_full;
+  t.audit_pairs += s.audit_pairs;
+  t.audit_max_err = std::max(t.audit_max_err, s.audit_max_err);
+  t.audit_p99_err = std::max(t.audit_p99_err, s.audit_p99_err);  // the largest chunk p99
+  t.band_promoted += s.band_promoted;
+  t.ms_seed += s.ms_seed;
+  t.ms_full += s.ms_full;
+}
+
+}  // namespace
+
+bv_status Engine::compute_chunked(Engine& other, const bv_region_batch& b, double* out, bv_phmm_stats* stats,
+                                  int chunks) {
+  const auto t0 = std::chrono::steady_clock::now();
+  bv_status s = validate(b);
+  if (s != BV_OK) return s;
+  // results per region and the chunk cuts (about equal numbers of pairs)
+  int64_t total = 0;
+  for (int64_t g = 0; g < b.num_regions; ++g)
+    total += (b.region_reads[g + 1] - b.region_reads[g]) * (b.region_haps[g + 1] - b.region_haps[g]);
+  if (total > 0 && !out) return fail(BV_ERR_INVALID_ARG, "null output");
+  std::vector<Chunk> ck;
+  {
+    const int64_t target = (total + chunks - 1) / std::max(chunks, 1);
+    int64_t g0 = 0, acc = 0, out0 = 0;
+    for (int64_t g = 0; g < b.num_regions; ++g) {
+      acc += (b.region_reads[g + 1] - b.region_reads[g]) * (b.region_haps[g + 1] - b.region_haps[g]);
+      if (acc >= target || g + 1 == b.num_regions) {
+        Chunk c;
+        c.g0 = g0;
+        c.g1 = g + 1;
+        c.out0 = out0;
+        c.n_out = acc;
+        ck.push_back(std::move(c));
+        out0 += acc;
+        acc = 0;
+        g0 = g + 1;
+      }
+    }
+  }
+  for (auto& c : ck) c.build(b);
+  Engine* eng[2] = {this, &other};
+  std::vector<bv_phmm_stats> cs(ck.size());
+  auto drain = [&](size_t k) -> bv_status {  // results and stats of chunk k
+    Engine& e = *eng[k % 2];
+    bv_status r = e.fetch(out + ck[k].out0, ck[k].n_out);
+    if (r != BV_OK) return fail(r, e.last_error());
+    r = e.finish(&cs[k]);
+    return r == BV_OK ? r : fail(r, e.last_error());
+  };
+  auto abort = [&](bv_status r) {
+    // no copy from the caller's arrays may outlive the call
+    cudaStreamSynchronize(stream_);
+    cudaStreamSynchronize(other.stream_);
+    return r;
+  };
+  for (size_t k = 0; k < ck.size(); ++k) {
+    Engine& e = *eng[k % 2];
+    s = e.stage(ck[k].view, false);
+    if (s == BV_OK) s = e.launch();
+    if (s != BV_OK) return abort(fail(s, e.last_error()));
+    if (k >= 1) {
+      s = drain(k - 1);
+      if (s != BV_OK) return abort(s);
+    }
+  }
+  if (!ck.empty()) {
+    s = drain(ck.size() - 1);
+    if (s != BV_OK) return abort(s);
+  }
+  if (stats) {
+    *stats = bv_phmm_stats{};
+    for (const auto& c : cs) add_stats(*stats, c);
+    stats->ms_d2h = 0;  // the result copies overlap the next chunk's work
+    stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return BV_OK;
+}
+
+}  // namespace bvphmm

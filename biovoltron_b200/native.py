@@ -34,7 +34,7 @@ class Options(C.Structure):
     _fields_ = [
         ("struct_size", C.c_int32), ("device", C.c_int32), ("precision", C.c_int32), ("mode", C.c_int32),
         ("rescue_threshold", C.c_double), ("haps_per_unit", C.c_int32), ("haps_per_warp", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("pipeline_chunks", C.c_int32), ("pipeline_min_pairs", C.c_int32), ("reserved", C.c_int32 * 4),
     ]
 
 

@@ -62,7 +62,7 @@ class PairHMMEngine:
     """One ``bv_phmm_ctx`` (a CUDA stream and its device buffers on one GPU)."""
 
     def __init__(self, device: int = 0, precision: str = "auto", mode: str = "full", haps_per_unit: int = 8,
-                 haps_per_warp: int = 0):
+                 haps_per_warp: int = 0, pipeline_chunks: int = 0, pipeline_min_pairs: int = 0):
         self.lib = N.load()
         o = N.Options()
         self.lib.bv_phmm_default_options(C.byref(o))
@@ -71,6 +71,8 @@ class PairHMMEngine:
         o.mode = {"full": N.BV_MODE_FULL, "band": N.BV_MODE_BAND}[mode]
         o.haps_per_unit = haps_per_unit
         o.haps_per_warp = haps_per_warp
+        o.pipeline_chunks = pipeline_chunks
+        o.pipeline_min_pairs = pipeline_min_pairs
         h = C.c_void_p()
         st = self.lib.bv_phmm_create(C.byref(o), C.byref(h))
         if st != N.BV_OK:

@@ -70,7 +70,12 @@ typedef struct bv_phmm_options {
   int32_t haps_per_unit;    /* haplotypes one warp scores against a read before taking new work; default 8 */
   int32_t haps_per_warp;    /* 2: a warp scores two haplotypes of a read at once (packed FP32x2), 1: one;
                                0 (default): 2 */
-  int32_t reserved[6];
+  int32_t pipeline_chunks;  /* bv_phmm_compute_regions on a batch of at least pipeline_min_pairs pairs:
+                               region chunks scored by two alternating contexts on the device, one
+                               chunk's copies overlapping the previous chunk's kernels; 0 (default): 4,
+                               1: no chunking */
+  int32_t pipeline_min_pairs; /* 0 (default): 4,194,304 */
+  int32_t reserved[4];
 } bv_phmm_options;
 
 typedef struct bv_phmm_stats {

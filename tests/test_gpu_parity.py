@@ -207,3 +207,38 @@ def test_autotune_picks_shapes_and_keeps_results():
             e.set_tuning([{"rows_per_lane": 9, "haps_per_warp": 1, "warps_per_block": 1}])
         with pytest.raises(RuntimeError):
             e.set_tuning([{"rows_per_lane": 3, "haps_per_warp": 3, "warps_per_block": 1}])
+
+
+@pytest.mark.parametrize("chunks", [2, 3, 5])
+def test_chunked_compute_matches_single_pass(chunks):
+    """bv_phmm_compute_regions on a batch at or above the chunking threshold
+    splits the regions into chunks that alternate between two contexts; every
+    result equals the single-pass device-resident run, in full-DP and band
+    mode, and the stats add up over the chunks."""
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    b = W.config1(seed=41, n_regions=40)
+    with PairHMMEngine() as ref:
+        n = ref.stage(b)
+        ref.run()
+        want = ref.fetch(n)
+    with PairHMMEngine(pipeline_chunks=chunks, pipeline_min_pairs=1) as e:
+        got, st = e.compute_regions(b, with_stats=True)
+        assert np.array_equal(got, want)
+        assert st["pairs"] == n and st["cells"] == b.n_cells()
+        # again: the second context is reused
+        assert np.array_equal(e.compute_regions(b), want)
+        # band mode is mirrored into the second context
+        e.set_band_options(fixed_half=8, margin=2)
+        band, bst = e.compute_regions(b, with_stats=True)
+    with PairHMMEngine() as one:
+        one.set_band_options(fixed_half=8, margin=2)
+        assert np.array_equal(band, one.compute_regions(b))
+    assert bst["band_pairs"] > 0
+
+
+def test_chunked_compute_rejects_bad_options():
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    with pytest.raises(RuntimeError):
+        PairHMMEngine(pipeline_chunks=-1)
+    with pytest.raises(RuntimeError):
+        PairHMMEngine(pipeline_chunks=65)
