@@ -286,6 +286,8 @@ def main():
     ap.add_argument("--fixed-half", type=int, default=-1,
                     help=">= 0: band of seed diagonal +- this many diagonals (and the 11-mer extent), no MLP")
     ap.add_argument("--margin", type=int, default=2, help="diagonals added on both sides of the predicted band")
+    ap.add_argument("--pipeline-chunks", type=int, default=0,
+                    help="region chunks of the end-to-end call (0: the library default, one per 4M pairs; 1: one pass)")
     ap.add_argument("--tune-regions", type=int, default=500,
                     help="regions of the workload the launch-shape autotuner times (0: default shapes)")
     args = ap.parse_args()
@@ -331,7 +333,7 @@ def main():
     # ---- learned band, device-resident --------------------------------------
     eb = None
     if form == "band":
-        eb = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp)
+        eb = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp, pipeline_chunks=args.pipeline_chunks)
         if tuning:
             eb.set_tuning(tuning)
         train_rep = train_band(eb, args, rank)
@@ -352,7 +354,8 @@ def main():
         return [s_["ms_fp32"] + s_["ms_fp64"] for s_ in run["steps"]]
 
     # ---- end to end through the public API (host buffers) ---------------------
-    e2e_eng = eb if eb is not None else PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp)
+    e2e_eng = eb if eb is not None else PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp,
+                                                      pipeline_chunks=args.pipeline_chunks)
     arrays = [batch.read_bases, batch.read_q, batch.read_i, batch.read_d, batch.read_c, batch.hap_bases]
     for a in arrays:
         e2e_eng.host_register(a)

@@ -2,6 +2,7 @@
 //
 // Nothing crosses the C boundary as an exception: every entry point catches
 // and maps failures to a bv_status.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -143,9 +144,12 @@ bv_status bv_phmm_compute_regions(bv_phmm_ctx* ctx, const bv_region_batch* batch
   return guard(ctx, [&] {
     bvphmm::Engine& a = ctx->engine;
     const bv_phmm_options& o = a.options();
-    const int chunks = o.pipeline_chunks > 0 ? o.pipeline_chunks : 4;
     const int64_t min_pairs = o.pipeline_min_pairs > 0 ? o.pipeline_min_pairs : (int64_t)1 << 22;
-    if (chunks < 2 || bv_phmm_region_results(batch) < min_pairs) return a.compute(*batch, out, stats);
+    const int64_t pairs = bv_phmm_region_results(batch);
+    // default: one chunk per min_pairs pairs, 2 to 64 chunks
+    const int chunks = o.pipeline_chunks > 0 ? o.pipeline_chunks
+                                             : (int)std::min<int64_t>(64, std::max<int64_t>(2, pairs / min_pairs));
+    if (chunks < 2 || pairs < min_pairs) return a.compute(*batch, out, stats);
     if (!ctx->second) {
       auto e = std::make_unique<bvphmm::Engine>(o);
       const bv_status s = e->init();

@@ -72,8 +72,8 @@ typedef struct bv_phmm_options {
                                0 (default): 2 */
   int32_t pipeline_chunks;  /* bv_phmm_compute_regions on a batch of at least pipeline_min_pairs pairs:
                                region chunks scored by two alternating contexts on the device, one
-                               chunk's copies overlapping the previous chunk's kernels; 0 (default): 4,
-                               1: no chunking */
+                               chunk's copies and planning overlapping the previous chunk's kernels;
+                               0 (default): one chunk per pipeline_min_pairs pairs, 2 to 64; 1: one pass */
   int32_t pipeline_min_pairs; /* 0 (default): 4,194,304 */
   int32_t reserved[4];
 } bv_phmm_options;
