@@ -317,6 +317,16 @@ bv_status bv_phmm_band_set_weights(bv_phmm_ctx* ctx, const float* w, int64_t n) 
   return guard(ctx, [&] { return ctx->engine.band_set_weights(w, n); });
 }
 
+bv_status bv_phmm_set_transitions(bv_phmm_ctx* ctx, const double* trans7) {
+  if (!ctx) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.set_transitions(trans7); });
+}
+
+int bv_phmm_get_transitions(const bv_phmm_ctx* ctx, double* trans7) {
+  if (!ctx) return 0;
+  return ctx->engine.constant_transitions(trans7) ? 1 : 0;
+}
+
 bv_status bv_phmm_band_save(bv_phmm_ctx* ctx, const char* path) {
   if (!ctx || !path) return BV_ERR_INVALID_ARG;
   return guard(ctx, [&] { return ctx->engine.band_save(path); });

@@ -44,6 +44,14 @@ struct Tables {
   float mm_inv_f[kMMEntries];  // 1 / mm_f where mm_f >= kFoldMin, else NaN
   double ph2pr_d[128];
   double mm_d[kMMEntries];
+  // Constant transitions (the scalar PairHMM model, pairhmm.hpp:32-33, 56-80):
+  // const_mode = 1 takes every row's transitions from cf / cd instead of the
+  // quality bytes: [0] M->M, [1] M->I, [2] M->D, [3] I->M, [4] I->I, [5] D->M,
+  // [6] D->D (PairHMM::TrasMatrx order); cf[7] = 1 / cf[0] when the folded form
+  // applies, else NaN.  Only the base qualities are read then.
+  int32_t const_mode;
+  float cf[8];
+  double cd[8];
   float init_f;          // 2^120
   float log10_init_f;    // log10f(2^120), evaluated on the host as the reference does
   double init_d;         // 2^1020

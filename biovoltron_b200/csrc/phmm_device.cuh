@@ -167,7 +167,10 @@ template <typename T> struct ScaledXY { static constexpr bool value = sizeof(T) 
 
 // Per-lane row constants for one strip.  Scaled form: mm = pMM, cx = pGAPM *
 // pMX(r-1), cy = pGAPM * pMY(r-1), kap = pXX pMX(r-1)/pMX(r), g = pYY.
-// Unscaled form: mm = pMM, cx = pGAPM, kap = pMX, my = pMY, g = pXX = pYY.
+// Unscaled form: mm = pMM, cx = pGAPM (X->M), cy = pGAPM (Y->M), kap = pMX,
+// my = pMY, gx = pXX, g = pYY.  With constant transitions (Tables::const_mode,
+// the scalar model) X->M / Y->M and X->X / Y->Y may differ; both forms take
+// them from the table instead of the quality bytes.
 //
 // Folded form (FP32, every real row of the strip with pMM >= kFoldMin): pMM(r)
 // moves into row r's emissions and out of the M coefficient, cx and cy are
@@ -179,8 +182,12 @@ template <typename T> struct ScaledXY { static constexpr bool value = sizeof(T) 
 // would need large coefficients; a strip holding one keeps the plain form.
 template <typename T, int RT>
 struct Rows {
-  T mm[RT], cx[RT], cy[RT], kap[RT], my[RT], g[RT], y0[RT];
+  T mm[RT], cx[RT], cy[RT], kap[RT], my[RT], g[RT], gx[RT], y0[RT];
 };
+
+template <typename T> __device__ __forceinline__ const T* const_tab(const Tables* t);
+template <> __device__ __forceinline__ const float* const_tab<float>(const Tables* t) { return t->cf; }
+template <> __device__ __forceinline__ const double* const_tab<double>(const Tables* t) { return t->cd; }
 
 // Computes the lane's row constants for the rows [rbase, rbase+RT) (real row
 // numbers, row 0 = initial row, negative = padding) and writes the lane's
@@ -206,36 +213,49 @@ __device__ __forceinline__ bool setup_rows(const Tables* __restrict__ tb, const 
     const int r = rbase + j;
     if (SumRow<T>::value && r == R + 1 && R >= 1) {
       rw.mm[j] = T(1);
-      rw.cx[j] = ph[quals[R - 1].y & kQualMask];  // pMX(R): Xh(R) * pMX(R) = X(R)
+      // pMX(R): Xh(R) * pMX(R) = X(R)
+      rw.cx[j] = tb->const_mode ? const_tab<T>(tb)[1] : ph[quals[R - 1].y & kQualMask];
       rw.cy[j] = T(0); rw.kap[j] = T(0); rw.my[j] = T(0);
-      rw.g[j] = T(1);
+      rw.g[j] = T(1); rw.gx[j] = T(1);
       rw.y0[j] = T(0);
       sumrow[j] = true;
     } else if (r >= 1 && r <= R) {
       const uchar4 qv = quals[r - 1];
-      const int qq = qv.x & kQualMask, qi = qv.y & kQualMask, qd = qv.z & kQualMask, qc = qv.w & kQualMask;
-      const T pmx = ph[qi], pmy = ph[qd], g = ph[qc];
-      const T gp = T(1) - g;
+      const int qq = qv.x & kQualMask;
+      // transitions into row r: M->M, M->X, M->Y, X->M, X->X, Y->M, Y->Y
+      T mmv, pmx, pmy, gpx, gx, gpy, gy;
       T ap = T(1), bp = T(1);  // scale of the row above: pMX/pMY, or 1 for row 0
-      if (ScaledXY<T>::value && r >= 2) {
-        const uchar4 pv = quals[r - 2];
-        ap = ph[pv.y & kQualMask];
-        bp = ph[pv.z & kQualMask];
+      if (tb->const_mode) {
+        const T* c = const_tab<T>(tb);
+        mmv = c[0]; pmx = c[1]; pmy = c[2]; gpx = c[3]; gx = c[4]; gpy = c[5]; gy = c[6];
+        minv[j] = tb->cf[7];
+        if (ScaledXY<T>::value && r >= 2) { ap = pmx; bp = pmy; }
+      } else {
+        const int qi = qv.y & kQualMask, qd = qv.z & kQualMask, qc = qv.w & kQualMask;
+        pmx = ph[qi]; pmy = ph[qd]; gx = ph[qc]; gy = gx;
+        gpx = T(1) - gx; gpy = gpx;
+        mmv = mmt[mm_index(qi, qd)];
+        minv[j] = tb->mm_inv_f[mm_index(qi, qd)];
+        if (ScaledXY<T>::value && r >= 2) {
+          const uchar4 pv = quals[r - 2];
+          ap = ph[pv.y & kQualMask];
+          bp = ph[pv.z & kQualMask];
+        }
       }
-      rw.mm[j] = mmt[mm_index(qi, qd)];
-      minv[j] = tb->mm_inv_f[mm_index(qi, qd)];
+      rw.mm[j] = mmv;
       if constexpr (ScaledXY<T>::value) {
-        rw.cx[j] = gp * ap;
-        rw.cy[j] = gp * bp;
-        rw.kap[j] = g * ap / pmx;
+        rw.cx[j] = gpx * ap;
+        rw.cy[j] = gpy * bp;
+        rw.kap[j] = gx * ap / pmx;
         rw.my[j] = T(0);
       } else {
-        rw.cx[j] = gp;
-        rw.cy[j] = T(0);
+        rw.cx[j] = gpx;
+        rw.cy[j] = gpy;
         rw.kap[j] = pmx;
         rw.my[j] = pmy;
       }
-      rw.g[j] = g;
+      rw.g[j] = gy;
+      rw.gx[j] = gx;
       rw.y0[j] = T(0);
       const T eps = ph[qq];
       em[j] = T(1) - eps;
@@ -245,7 +265,7 @@ __device__ __forceinline__ bool setup_rows(const Tables* __restrict__ tb, const 
     } else {
       // padding rows and row 0: M = 0, X = 0, Y carried unchanged
       rw.mm[j] = T(0); rw.cx[j] = T(0); rw.cy[j] = T(0); rw.kap[j] = T(0); rw.my[j] = T(0);
-      rw.g[j] = T(1);
+      rw.g[j] = T(1); rw.gx[j] = T(0);
       rw.y0[j] = (r == 0) ? init_y : T(0);
     }
   }
@@ -390,8 +410,8 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
           xn = fma_(rw.kap[j], ux, um);
           yn = fma_(rw.g[j], Y[j], M[j]);
         } else {
-          mn = e[j] * fma_(rw.mm[j], dm, rw.cx[j] * (dx + dy));
-          xn = fma_(rw.g[j], ux, rw.kap[j] * um);
+          mn = e[j] * fma_(rw.mm[j], dm, fma_(rw.cx[j], dx, rw.cy[j] * dy));
+          xn = fma_(rw.gx[j], ux, rw.kap[j] * um);
           yn = fma_(rw.g[j], Y[j], rw.my[j] * M[j]);
         }
         dm = M[j]; dx = X[j]; dy = Y[j];

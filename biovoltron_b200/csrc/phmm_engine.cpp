@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <memory>
 #include <cstring>
 #include <string>
 
@@ -99,6 +100,29 @@ bv_status Engine::cuda_fail(cudaError_t e, const char* what) {
     if (e__ != cudaSuccess) return cuda_fail(e__, what); \
   } while (0)
 
+bv_status Engine::set_transitions(const double* trans) {
+  if (trans) {
+    for (int k = 0; k < 7; ++k)
+      if (!(trans[k] >= 0.0 && trans[k] <= 1.0)) return fail(BV_ERR_INVALID_ARG, "transition outside [0, 1]");
+    if (band_enabled()) return fail(BV_ERR_UNSUPPORTED, "constant transitions run the full-DP path: disable the band");
+  }
+  BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");
+  BV_CUDA(cudaStreamSynchronize(stream_), "sync before table update");
+  set_constant_transitions(h_tables_.get(), trans);
+  BV_CUDA(cudaMemcpy(d_tables_.get(), h_tables_.get(), sizeof(Tables), cudaMemcpyHostToDevice), "tables copy");
+  ++config_version_;
+  staged_ = false;
+  destroy_graph();
+  return BV_OK;
+}
+
+bool Engine::constant_transitions(double* trans) const {
+  if (!h_tables_ || !h_tables_->const_mode) return false;
+  if (trans)
+    for (int k = 0; k < 7; ++k) trans[k] = h_tables_->cd[k];
+  return true;
+}
+
 bv_status Engine::init() {
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -108,10 +132,11 @@ bv_status Engine::init() {
   BV_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, opt_.device), "SM count");
   BV_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
   for (auto& ev : ev_) BV_CUDA(cudaEventCreate(&ev), "event");
-  Tables host{};
-  build_tables(&host);
+  h_tables_ = std::make_unique<Tables>();
+  build_tables(h_tables_.get());
   BV_CUDA(d_tables_.reserve(sizeof(Tables)), "tables alloc");
-  BV_CUDA(cudaMemcpyAsync(d_tables_.get(), &host, sizeof(Tables), cudaMemcpyHostToDevice, stream_), "tables copy");
+  BV_CUDA(cudaMemcpyAsync(d_tables_.get(), h_tables_.get(), sizeof(Tables), cudaMemcpyHostToDevice, stream_),
+          "tables copy");
   BV_CUDA(d_counters_.reserve(sizeof(Counters)), "counters alloc");
   BV_CUDA(cudaStreamSynchronize(stream_), "init sync");
   return BV_OK;

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <string>
 #include <chrono>
+#include <memory>
 #include <vector>
 
 #include "bv_pairhmm.h"
@@ -74,6 +75,10 @@ class Engine {
   // Copies band options, MLP weights and launch shapes from `src` (a context
   // with the same options); the chunked compute keeps its second context in step.
   bv_status mirror_config(Engine& src);
+  // Constant transitions for every row (the scalar PairHMM model; 7 entries in
+  // PairHMM::TrasMatrx order), or the quality-derived ones again (nullptr).
+  bv_status set_transitions(const double* trans);
+  bool constant_transitions(double* trans) const;
   uint64_t mirrored_version() const { return mirrored_version_; }
   // One batch split into `chunks` region chunks that alternate between this
   // context and `other`: a chunk's copies and the host's planning overlap the
@@ -120,6 +125,7 @@ class Engine {
   cudaEvent_t ev_[8] = {};
   std::string err_;
 
+  std::unique_ptr<Tables> h_tables_;  // host copy of d_tables_
   DevBuf d_tables_, d_read_bases_, d_q_, d_i_, d_d_, d_c_, d_quals4_, d_read_off_, d_hap_bases_, d_hap_off_;
   DevBuf d_units_, d_out_, d_rescue_, d_counters_, d_bnd32_, d_bnd64_, d_f64_items_;
 

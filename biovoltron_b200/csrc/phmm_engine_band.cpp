@@ -25,6 +25,8 @@ bv_status Engine::set_band_options(const bv_band_options& o) {
       !(o.edge_threshold > 0))
     return fail(BV_ERR_INVALID_ARG, "band option out of range");
   if (o.enabled && o.use_mlp && !mlp_ready_) return fail(BV_ERR_INVALID_ARG, "no band MLP weights (train or load)");
+  if (o.enabled && constant_transitions(nullptr))
+    return fail(BV_ERR_UNSUPPORTED, "the band path takes its transitions from the quality bytes");
   band_opt_ = o;
   ++config_version_;
   staged_ = false;  // buffers and launch sequence depend on the mode: stage again

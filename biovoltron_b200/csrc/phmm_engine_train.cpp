@@ -70,6 +70,8 @@ float bf16_to_float(uint16_t h) {
 }  // namespace
 
 bv_status Engine::stage_for_labels(const bv_region_batch& b) {
+  if (constant_transitions(nullptr))
+    return fail(BV_ERR_UNSUPPORTED, "band labels take their transitions from the quality bytes");
   staged_ = false;
   destroy_graph();
   BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");

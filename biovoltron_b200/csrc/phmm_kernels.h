@@ -49,5 +49,8 @@ cudaError_t launch_set_u64(unsigned long long* dst, unsigned long long v, cudaSt
 
 // Host-side construction of the reference's probability tables (Context.h).
 void build_tables(Tables* t);
+// Constant transitions for every row (7 entries, PairHMM::TrasMatrx order), or
+// back to the quality-derived ones (nullptr).
+void set_constant_transitions(Tables* t, const double* trans);
 
 }  // namespace bvphmm

@@ -16,6 +16,11 @@
 namespace bvphmm {
 
 bv_status Engine::mirror_config(Engine& src) {
+  double tr[7];
+  const bool ct = src.constant_transitions(tr);
+  band_opt_.enabled = 0;  // the transitions first: they refuse a band context
+  bv_status st = set_transitions(ct ? tr : nullptr);
+  if (st != BV_OK) return st;
   if (src.mlp_ready_) {
     bv_status s = install_weights(src.mlp_w_.data());
     if (s != BV_OK) return s;

@@ -75,10 +75,33 @@ void build_tables(Tables* t) {
   fill_mm<float>(t->mm_f);
   fill_mm<double>(t->mm_d);
   for (int x = 0; x < kMMEntries; ++x) t->mm_inv_f[x] = t->mm_f[x] >= kFoldMin ? 1.f / t->mm_f[x] : std::numeric_limits<float>::quiet_NaN();
+  t->const_mode = 0;
+  for (int k = 0; k < 8; ++k) {
+    t->cf[k] = 0.f;
+    t->cd[k] = 0.0;
+  }
   t->init_f = std::ldexp(1.f, 120);
   t->log10_init_f = log10f(t->init_f);
   t->init_d = std::ldexp(1.0, 1020);
   t->log10_init_d = std::log10(t->init_d);
+}
+
+}  // namespace bvphmm
+
+namespace bvphmm {
+
+void set_constant_transitions(Tables* t, const double* trans) {
+  if (!trans) {
+    t->const_mode = 0;
+    return;
+  }
+  t->const_mode = 1;
+  for (int k = 0; k < 7; ++k) {
+    t->cd[k] = trans[k];
+    t->cf[k] = (float)trans[k];
+  }
+  t->cd[7] = 0.0;
+  t->cf[7] = t->cf[0] >= kFoldMin ? 1.f / t->cf[0] : std::numeric_limits<float>::quiet_NaN();
 }
 
 }  // namespace bvphmm

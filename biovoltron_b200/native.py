@@ -167,6 +167,8 @@ def load() -> C.CDLL:
         "bv_phmm_autotune": (C.c_int, [V, P(RegionBatchC), C.c_int32, P(TuneEntry), P(C.c_int32)]),
         "bv_phmm_set_tuning": (C.c_int, [V, P(TuneEntry), C.c_int32]),
         "bv_phmm_get_tuning": (C.c_int, [V, P(TuneEntry), P(C.c_int32)]),
+        "bv_phmm_set_transitions": (C.c_int, [V, P(C.c_double)]),
+        "bv_phmm_get_transitions": (C.c_int, [V, P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

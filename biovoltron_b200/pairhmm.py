@@ -134,6 +134,17 @@ class PairHMMEngine:
         self._check(self.lib.bv_phmm_fetch_results(self.h, _ptr(out), n))
         return out[:n]
 
+    def set_transitions(self, trans: Optional[Sequence[float]]):
+        """Constant transitions for every row (the scalar PairHMM model, seven
+        values in PairHMM::TrasMatrx order), or None for the quality-derived ones
+        (bv_phmm_set_transitions)."""
+        arr = None if trans is None else (C.c_double * 7)(*[float(x) for x in trans])
+        self._check(self.lib.bv_phmm_set_transitions(self.h, arr))
+
+    def transitions(self) -> Optional[List[float]]:
+        arr = (C.c_double * 7)()
+        return list(arr) if self.lib.bv_phmm_get_transitions(self.h, arr) else None
+
     def set_band_options(self, enabled: bool = True, use_mlp: bool = False, fixed_half: int = 8, margin: int = 2,
                          audit_period: int = 0, edge_threshold: float = 1e-3):
         """Routes pairs through the banded kernel (see bv_band_options)."""
@@ -342,6 +353,36 @@ def filter_poorly_modeled_reads(reads: list, ll: List[List[float]]) -> None:
             kept_l.append(row)
     reads[:] = kept_r
     ll[:] = kept_l
+
+
+ORIGINAL_DEFAULT = (0.9998, 0.0001, 0.0001, 0.9, 0.1, 0.9, 0.1)  # pairhmm.hpp:32-33
+
+
+class GpuScalarPairHMM:
+    """Drop-in for the scalar ``biovoltron::PairHMM`` (pairhmm.hpp:14-141) on
+    one GPU: constant transitions, the base qualities' emission prior, then
+    normalize_likelihoods and filter_poorly_modeled_reads as PairHMM does."""
+
+    def __init__(self, device: int = 0, engine: Optional[PairHMMEngine] = None):
+        self.engine = engine or PairHMMEngine(device=device)
+
+    def compute_likelihoods(self, haplotypes: Sequence[Haplotype], reads: list,
+                            trans: Sequence[float] = ORIGINAL_DEFAULT) -> List[List[float]]:
+        nr, nh = len(reads), len(haplotypes)
+        if nr == 0:
+            return []
+        self.engine.set_transitions(trans)
+        try:
+            tcs = [(r.seq, r.qual, r.qual, r.qual, r.qual, h.seq) for r in reads for h in haplotypes]
+            flat = self.engine.compute_testcases(tcs) if tcs else np.zeros(0)
+        finally:
+            self.engine.set_transitions(None)
+        ll = [list(map(float, flat[k * nh:(k + 1) * nh])) for k in range(nr)]
+        if nh == 0:
+            return ll
+        normalize_likelihoods(ll)
+        filter_poorly_modeled_reads(reads, ll)
+        return ll
 
 
 class GpuPairHMM:

@@ -23,6 +23,7 @@
 #pragma once
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <stdexcept>
 #include <string>
@@ -55,31 +56,7 @@ class GpuPairHMM {
     const size_t nr = reads.size(), nh = haplotypes.size();
     std::vector<std::vector<double>> ll(nr, std::vector<double>(nh, 0.0));
     if (nr == 0 || nh == 0) return ll;
-    std::vector<bv_testcase> tcs;
-    tcs.reserve(nr * nh);
-    for (const auto& r : reads) {
-      const int len = static_cast<int>(r.seq.size());
-      const char* ins = r.insertion_gop().data();
-      const char* del = r.deletion_gop().data();
-      const char* gcp = r.overall_gcp().data();
-      for (const auto& h : haplotypes) {
-        bv_testcase t{};
-        t.rslen = len;
-        t.haplen = static_cast<int>(h.seq.size());
-        t.q = r.qual.data();
-        t.i = ins;
-        t.d = del;
-        t.c = gcp;
-        t.hap = h.seq.data();
-        t.rs = r.seq.data();
-        tcs.push_back(t);
-      }
-    }
-    std::vector<double> flat(nr * nh);
-    check(bv_phmm_compute_testcases(ctx_, tcs.data(), static_cast<int64_t>(tcs.size()), flat.data(), nullptr),
-          "bv_phmm_compute_testcases");
-    for (size_t r = 0; r < nr; ++r)
-      std::copy(flat.begin() + r * nh, flat.begin() + (r + 1) * nh, ll[r].begin());
+    score(haplotypes, reads, false, ll);
     normalize_likelihoods(ll);
     filter_poorly_modeled_reads(reads, ll);
     return ll;
@@ -114,6 +91,40 @@ class GpuPairHMM {
 
   bv_phmm_ctx* context() const { return ctx_; }
 
+ protected:
+  // Scores every read against every haplotype into ll (no normalising or
+  // filtering); `scalar` takes only the base qualities (constant transitions).
+  template <class HapVec, class ReadVec>
+  void score(const HapVec& haplotypes, const ReadVec& reads, bool scalar, std::vector<std::vector<double>>& ll) {
+    const size_t nr = reads.size(), nh = haplotypes.size();
+    std::vector<bv_testcase> tcs;
+    tcs.reserve(nr * nh);
+    for (const auto& r : reads) {
+      const int len = static_cast<int>(r.seq.size());
+      const char* q = r.qual.data();
+      const char* ins = scalar ? q : r.insertion_gop().data();
+      const char* del = scalar ? q : r.deletion_gop().data();
+      const char* gcp = scalar ? q : r.overall_gcp().data();
+      for (const auto& h : haplotypes) {
+        bv_testcase t{};
+        t.rslen = len;
+        t.haplen = static_cast<int>(h.seq.size());
+        t.q = q;
+        t.i = ins;
+        t.d = del;
+        t.c = gcp;
+        t.hap = h.seq.data();
+        t.rs = r.seq.data();
+        tcs.push_back(t);
+      }
+    }
+    std::vector<double> flat(nr * nh);
+    check(bv_phmm_compute_testcases(ctx_, tcs.data(), static_cast<int64_t>(tcs.size()), flat.data(), nullptr),
+          "bv_phmm_compute_testcases");
+    for (size_t r = 0; r < nr; ++r)
+      std::copy(flat.begin() + r * nh, flat.begin() + (r + 1) * nh, ll[r].begin());
+  }
+
  private:
   void check(bv_status s, const char* what) {
     if (s != BV_OK) {
@@ -123,6 +134,41 @@ class GpuPairHMM {
     }
   }
   bv_phmm_ctx* ctx_ = nullptr;
+};
+
+// Drop-in for the scalar biovoltron::PairHMM (include/biovoltron/algo/align/
+// inexact_match/pairhmm.hpp): compute_likelihoods(haplotypes, reads, trans)
+// scores with seven constant transition probabilities (ORIGINAL_DEFAULT
+// unless given, :32-33) and the base qualities' emission prior (:39-54), then
+// normalises and filters as PairHMM does (:83-114).  Bases compare as
+// A/C/G/T with N matching everything, which is the scalar model's raw-byte
+// comparison for upper-case ACGTN sequences.
+class GpuScalarPairHMM : public GpuPairHMM {
+ public:
+  using TransMatrix = std::array<double, 7>;  // M->M, M->I, M->D, I->M, I->I, D->M, D->D
+  static constexpr TransMatrix kOriginalDefault = {0.9998, 0.0001, 0.0001, 0.9, 0.1, 0.9, 0.1};
+
+  explicit GpuScalarPairHMM(int device = 0) : GpuPairHMM(device, false) {}
+
+  template <class HapVec, class ReadVec>
+  std::vector<std::vector<double>> compute_likelihoods(const HapVec& haplotypes, ReadVec& reads,
+                                                       const TransMatrix& trans = kOriginalDefault) {
+    const size_t nr = reads.size(), nh = haplotypes.size();
+    std::vector<std::vector<double>> ll(nr, std::vector<double>(nh, 0.0));
+    if (nr == 0 || nh == 0) return ll;
+    check_status(bv_phmm_set_transitions(context(), trans.data()), "bv_phmm_set_transitions");
+    score(haplotypes, reads, true, ll);
+    normalize_likelihoods(ll);
+    filter_poorly_modeled_reads(reads, ll);
+    return ll;
+  }
+
+ private:
+  void check_status(bv_status s, const char* what) {
+    if (s != BV_OK)
+      throw std::runtime_error(std::string(what) + ": " + bv_phmm_status_string(s) + " (" +
+                               bv_phmm_last_error(context()) + ")");
+  }
 };
 
 }  // namespace biovoltron_b200

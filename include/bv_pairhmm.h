@@ -370,6 +370,23 @@ bv_status bv_phmm_autotune(bv_phmm_ctx* ctx, const bv_region_batch* sample, int3
 bv_status bv_phmm_set_tuning(bv_phmm_ctx* ctx, const bv_phmm_tune_entry* entries, int32_t num);
 bv_status bv_phmm_get_tuning(bv_phmm_ctx* ctx, bv_phmm_tune_entry* out, int32_t* num_out);
 
+/* --- the scalar PairHMM model ----------------------------------------------
+ * Replaces PairHMM::compute_likelihoods(haplotypes, reads, trans)
+ * (include/biovoltron/algo/align/inexact_match/pairhmm.hpp:116-141; the model
+ * :56-80): every row uses the same seven transition probabilities, in
+ * PairHMM::TrasMatrx order {M->M, M->I, M->D, I->M, I->I, D->M, D->D}
+ * (ORIGINAL_DEFAULT = {0.9998, 1e-4, 1e-4, 0.9, 0.1, 0.9, 0.1}, :32-33), and the
+ * emission prior comes from the base quality byte (& 127) alone: the insertion,
+ * deletion and gap-continuation arrays of a batch are not read (they must still
+ * be valid pointers).  Bases compare as A/C/G/T with N matching everything (the
+ * scalar model compares raw bytes: equal for upper-case ACGTN input).  NULL
+ * goes back to the quality-derived transitions.  The band path needs the
+ * quality-derived ones (BV_ERR_UNSUPPORTED while the band is on).  Values
+ * outside [0, 1]: BV_ERR_INVALID_ARG. */
+bv_status bv_phmm_set_transitions(bv_phmm_ctx* ctx, const double* trans7);
+/* 1 and the seven values when constant transitions are set, else 0. */
+int bv_phmm_get_transitions(const bv_phmm_ctx* ctx, double* trans7);
+
 /* Diagnostics: writes the probability tables a context uploads (ph2pr for
  * quals 0..127 and the match-to-match triangle for quals <= 127, both
  * precisions; Context.h:42-175).  Host-only, needs no device.  Returns 0, or

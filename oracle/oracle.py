@@ -186,6 +186,29 @@ class Oracle:
         }
 
 
+REF_SCALAR_SO = os.path.join(HERE, "_ref", "libref_scalar.so")
+
+
+class ReferenceScalar:
+    """Biovoltron's scalar PairHMM (pairhmm.hpp), one pair at a time through
+    its per-pair step (oracle/ref_scalar_shim.cpp)."""
+
+    def __init__(self, path: str = REF_SCALAR_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference scalar model not built: {path}")
+        self.lib = C.CDLL(path)
+        self._f = _bind(self.lib, "ref_scalar_log10", C.c_double,
+                        [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_void_p])
+
+    @staticmethod
+    def available(path: str = REF_SCALAR_SO) -> bool:
+        return os.path.exists(path)
+
+    def log10(self, read: bytes, qual: bytes, hap: bytes, trans: Optional[Sequence[float]] = None) -> float:
+        t = None if trans is None else (C.c_double * 7)(*trans)
+        return self._f(read, qual, len(read), hap, len(hap), C.cast(t, C.c_void_p) if t is not None else None)
+
+
 class Reference:
     """Biovoltron's own PairHMM kernel, called as AvxPairHMM calls it."""
 

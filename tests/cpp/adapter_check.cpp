@@ -1,5 +1,6 @@
 // adapter_check.cpp -- drives include/biovoltron_b200/gpu_pairhmm.hpp with
 // record types shaped like Biovoltron's SamRecord<> / Haplotype.
+// With the argument "scalar" it drives GpuScalarPairHMM (the scalar model).
 // Input (stdin): lines "H <bases>" and "R <bases> <quals>"; quals are raw
 // bytes given as printable characters.  Output: the kept reads' indices and
 // the [read][hap] log10 matrix after normalize/filter, one row per line.
@@ -25,7 +26,8 @@ struct SamRecord {
   std::string_view overall_gcp() const { return gcp; }
 };
 
-int main() {
+int main(int argc, char** argv) {
+  const bool scalar = argc > 1 && std::string(argv[1]) == "scalar";
   std::vector<Haplotype> haps;
   std::vector<SamRecord> reads;
   std::string line;
@@ -46,8 +48,14 @@ int main() {
       reads.push_back(r);
     }
   }
-  biovoltron_b200::GpuPairHMM hmm(0);
-  auto ll = hmm.compute_likelihoods(haps, reads);
+  std::vector<std::vector<double>> ll;
+  if (scalar) {
+    biovoltron_b200::GpuScalarPairHMM hmm(0);
+    ll = hmm.compute_likelihoods(haps, reads);
+  } else {
+    biovoltron_b200::GpuPairHMM hmm(0);
+    ll = hmm.compute_likelihoods(haps, reads);
+  }
   std::printf("kept");
   for (const auto& r : reads) std::printf(" %d", r.id);
   std::printf("\n");

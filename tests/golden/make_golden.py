@@ -22,6 +22,10 @@ Fixtures:
                   reference's FP64 underflows on most, so the expected values
                   are the rescaled FP64 oracle, cross-checked against the
                   reference wherever the reference is finite
+  scalar.npz      the scalar PairHMM model (pairhmm.hpp, compiled by
+                  oracle/Makefile into oracle/_ref/libref_scalar.so): a small
+                  region and edge pairs, expected log10 values with
+                  ORIGINAL_DEFAULT and with one custom transition matrix
 """
 from __future__ import annotations
 
@@ -35,7 +39,7 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
 sys.path.insert(0, ROOT)
 
 from biovoltron_b200 import workloads as W  # noqa: E402
-from oracle.oracle import Oracle, Reference, TestcaseArray  # noqa: E402
+from oracle.oracle import Oracle, Reference, ReferenceScalar, TestcaseArray  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_TEST = "/root/reference/tests/algo/align/inexact_match/pairhmm_avx.cpp"
@@ -135,6 +139,58 @@ def ref_test_batch() -> W.RegionBatch:
     return W._build(regions, "reference AvxPairHMM test sequences")
 
 
+SCALAR_CUSTOM = (0.995, 0.003, 0.002, 0.85, 0.15, 0.7, 0.3)
+
+
+def scalar_batch() -> W.RegionBatch:
+    """A config-0-shaped region (16 reads x 4 haplotypes) and edge pairs,
+    upper-case A/C/G/T/N only (the scalar model compares raw bytes)."""
+    rng = np.random.default_rng(21)
+    base = W._random_seq(rng, 300)
+    haps = [W._apply_indels(rng, W._substitute(rng, base, 0.01), int(rng.integers(0, 3)), 1, 10) for _ in range(4)]
+    reads = []
+    for _ in range(16):
+        src = haps[int(rng.integers(0, 4))]
+        st = int(rng.integers(0, len(src) - 150 + 1))
+        b = W._substitute(rng, src[st:st + 150].copy(), 0.01)
+        q = rng.integers(10, 41, size=150).astype(np.uint8)
+        reads.append((b, q, q, q, q))
+    regions = [(reads, haps)]
+
+    def arr(x):
+        return np.frombuffer(x, np.uint8).copy()
+
+    def pair(read, qual, hap):
+        r, q = arr(read), np.full(len(read), qual, np.uint8) if isinstance(qual, int) else arr(qual)
+        return ([(r, q, q, q, q)], [arr(hap)])
+
+    regions += [pair(b"A", 30, b"A"), pair(b"A", 30, b"C"), pair(b"N" * 20, 30, b"ACGTACGTACGTACGTACGTACGT"),
+                pair(b"ACGTACGTAC", 30, b"NNNNNNNNNNNN"), pair(b"ACGTACGTACGT", 0, b"ACGTACGTACGT"),
+                pair(b"ACGTACGTACGT", 127, b"ACGTACGTACGT"),
+                pair(b"ACGTAAAAACGTTT", 35, b"ACGTACGTTT"),        # insertion in the read
+                pair(b"ACGTACGTTT", 35, b"ACGTAAAAACGTTT"),        # deletion from the read
+                pair(b"GATTACA", bytes([5, 15, 25, 35, 45, 55, 65]), b"TTGATTACATT"),
+                pair(b"ACGTTGCA" * 4, 25, b"A")]
+    return W._build(regions, "scalar model cases")
+
+
+def save_scalar(name, batch, ref_scalar):
+    r, h = batch.pair_index()
+    ro, ho = batch.read_offsets, batch.hap_offsets
+    exp_d, exp_c = [], []
+    for k in range(len(r)):
+        rd = bytes(batch.read_bases[ro[r[k]]:ro[r[k] + 1]])
+        q = bytes(batch.read_q[ro[r[k]]:ro[r[k] + 1]])
+        hp = bytes(batch.hap_bases[ho[h[k]]:ho[h[k] + 1]])
+        exp_d.append(ref_scalar.log10(rd, q, hp))
+        exp_c.append(ref_scalar.log10(rd, q, hp, SCALAR_CUSTOM))
+    d = {k: getattr(batch, k) for k in BATCH_FIELDS}
+    d.update(ref_scalar_default=np.array(exp_d), ref_scalar_custom=np.array(exp_c),
+             custom_trans=np.array(SCALAR_CUSTOM))
+    np.savez_compressed(os.path.join(HERE, name), **d)
+    print(f"{name}: {batch.n_pairs} pairs")
+
+
 def main():
     ref = Reference()
     oracle = Oracle()
@@ -143,6 +199,7 @@ def main():
     if os.path.exists(REF_TEST):
         save("ref_test.npz", ref_test_batch(), ref, oracle)
     save("long_pairs.npz", W.config2(seed=11, n_pairs=6, max_read=2000, max_hap=2600), ref, oracle)
+    save_scalar("scalar.npz", scalar_batch(), ReferenceScalar())
 
 
 if __name__ == "__main__":

@@ -45,3 +45,24 @@ def test_adapter_matches_python_mirror(engine):
     ll = GpuPairHMM(engine=engine).compute_likelihoods([Haplotype(h) for h in haps], py_reads)
     assert kept == [ids[id(r)] for r in py_reads]
     assert np.allclose(np.array(mat), np.array(ll), rtol=0, atol=1e-8)
+
+
+@pytest.mark.gpu
+def test_scalar_adapter_matches_python_mirror():
+    from biovoltron_b200 import workloads as W
+    from biovoltron_b200.pairhmm import GpuScalarPairHMM, Haplotype, SamRecord
+    _build()
+    rng = np.random.default_rng(13)
+    base = bytes(W._random_seq(rng, 400))
+    haps = [base, base[:200] + b"A" + base[201:]]
+    reads = [(base[50:200], bytes(rng.integers(43, 74, size=150).astype(np.uint8))),
+             (bytes(W._random_seq(rng, 70)), b"+" * 70), (base[100:180], b"5" * 80)]
+    txt = "".join(f"H {h.decode()}\n" for h in haps) + "".join(f"R {s.decode()} {q.decode()}\n" for s, q in reads)
+    out = subprocess.run([EXE, "scalar"], input=txt, capture_output=True, text=True, check=True).stdout.splitlines()
+    kept = [int(x) for x in out[0].split()[1:]]
+    mat = [[float(x) for x in l.split()] for l in out[1:]]
+    py_reads = [SamRecord(s, q) for s, q in reads]
+    ids = {id(r): k for k, r in enumerate(py_reads)}
+    ll = GpuScalarPairHMM().compute_likelihoods([Haplotype(h) for h in haps], py_reads)
+    assert kept == [ids[id(r)] for r in py_reads]
+    assert np.allclose(np.array(mat), np.array(ll), rtol=0, atol=1e-8)

@@ -242,3 +242,64 @@ def test_chunked_compute_rejects_bad_options():
         PairHMMEngine(pipeline_chunks=-1)
     with pytest.raises(RuntimeError):
         PairHMMEngine(pipeline_chunks=65)
+
+
+def test_scalar_model_matches_reference_scalar_pairhmm():
+    """Constant transitions (the scalar PairHMM model): the GPU result for the
+    golden scalar cases is within FP32 tolerance of Biovoltron's scalar
+    PairHMM (FP64), with the default and a custom transition matrix; turning
+    the constants off gives the quality-derived results again."""
+    from biovoltron_b200.pairhmm import ORIGINAL_DEFAULT, PairHMMEngine
+    b, exp = load_golden("scalar")
+    with PairHMMEngine() as e:
+        plain = e.compute_regions(b)
+        e.set_transitions(ORIGINAL_DEFAULT)
+        assert e.transitions() == list(ORIGINAL_DEFAULT)
+        got = e.compute_regions(b)
+        want = exp["ref_scalar_default"]
+        fin = np.isfinite(want)
+        assert np.all(np.isneginf(got[~fin]))
+        assert np.max(np.abs(got[fin] - want[fin])) <= TOL_FP32
+        e.set_transitions([float(x) for x in exp["custom_trans"]])
+        got = e.compute_regions(b)
+        want = exp["ref_scalar_custom"]
+        fin = np.isfinite(want)
+        assert np.max(np.abs(got[fin] - want[fin])) <= TOL_FP32
+        # the FP64 path with constants (precision f64 context)
+        e.set_transitions(None)
+        assert e.transitions() is None
+        assert np.array_equal(e.compute_regions(b), plain)
+        # the band path takes its transitions from the quality bytes
+        e.set_band_options(fixed_half=8, margin=2)
+        with pytest.raises(RuntimeError):
+            e.set_transitions(ORIGINAL_DEFAULT)
+    with PairHMMEngine(precision="f64") as e:
+        e.set_transitions(ORIGINAL_DEFAULT)
+        got = e.compute_regions(b)
+        want = exp["ref_scalar_default"]
+        fin = np.isfinite(want)
+        assert np.max(np.abs(got[fin] - want[fin])) <= 1e-9
+        with pytest.raises(RuntimeError):
+            e.set_transitions([0.9998, 0.0001, 0.0001, 0.9, 0.1, 0.9, 1.5])
+
+
+def test_scalar_drop_in_normalises_and_filters():
+    """GpuScalarPairHMM mirrors PairHMM::compute_likelihoods: scalar-model
+    likelihoods, normalised and filtered like the reference."""
+    from biovoltron_b200.pairhmm import GpuScalarPairHMM, Haplotype, SamRecord
+    from oracle.oracle import Oracle
+    rng = np.random.default_rng(8)
+    base = bytes(W._random_seq(rng, 300))
+    haps = [Haplotype(base), Haplotype(base[:150] + b"T" + base[151:])]
+    reads = [SamRecord(base[20:120], bytes(rng.integers(20, 41, 100).astype(np.uint8))),
+             SamRecord(bytes(W._random_seq(rng, 80)), bytes([30] * 80))]
+    raw = [[Oracle().scalar_log10(r.seq, r.qual, h.seq) for h in haps] for r in reads]
+    keep = list(reads)
+    ll = GpuScalarPairHMM().compute_likelihoods(haps, keep)
+    exp = [list(row) for row in raw]
+    from biovoltron_b200.pairhmm import filter_poorly_modeled_reads, normalize_likelihoods
+    exp_reads = list(reads)
+    normalize_likelihoods(exp)
+    filter_poorly_modeled_reads(exp_reads, exp)
+    assert [id(r) for r in keep] == [id(r) for r in exp_reads]
+    assert np.allclose(np.array(ll), np.array(exp), rtol=0, atol=TOL_FP32)

@@ -4,6 +4,8 @@
   tests/golden/make_golden.py): the oracle's FP32 and FP64 probabilities are
   bit-identical and its log10 under the rescue rule is identical.
 * Against the reference kernel itself, live, where oracle/_ref is built.
+* The scalar PairHMM model's restatement against Biovoltron's scalar
+  PairHMM (golden vectors and, where built, live).
 * The rescaled FP64 variant agrees with the plain FP64 wherever that is finite.
 * Hand-computable cases.
 """
@@ -119,3 +121,38 @@ def test_identical_read_scores_near_uniform_start(oracle):
     pmm = float(tab["mm_f64"][45 * 46 // 2 + 45])
     approx = n * math.log10(1 - eps) + (n - 1) * math.log10(pmm) + math.log10(0.9 / 300)
     assert abs(got - approx) < 1e-3
+
+
+def _scalar_pairs(b):
+    r, h = b.pair_index()
+    ro, ho = b.read_offsets, b.hap_offsets
+    for k in range(len(r)):
+        yield (bytes(b.read_bases[ro[r[k]]:ro[r[k] + 1]]), bytes(b.read_q[ro[r[k]]:ro[r[k] + 1]]),
+               bytes(b.hap_bases[ho[h[k]]:ho[h[k] + 1]]))
+
+
+def test_scalar_oracle_bit_exact_vs_golden(oracle):
+    """The scalar model's restatement equals Biovoltron's scalar PairHMM
+    (pairhmm.hpp:56-80, compiled from the reference) bit for bit, with the
+    default and with a custom transition matrix."""
+    b, exp = load_golden("scalar")
+    trans = [float(x) for x in exp["custom_trans"]]
+    got_d = [oracle.scalar_log10(rd, q, hp) for rd, q, hp in _scalar_pairs(b)]
+    got_c = [oracle.scalar_log10(rd, q, hp, trans) for rd, q, hp in _scalar_pairs(b)]
+    assert _same(got_d, exp["ref_scalar_default"])
+    assert _same(got_c, exp["ref_scalar_custom"])
+
+
+def test_scalar_oracle_bit_exact_vs_live_reference(oracle):
+    from oracle.oracle import ReferenceScalar
+    if not ReferenceScalar.available():
+        pytest.skip("reference scalar model not built (oracle/_ref)")
+    ref = ReferenceScalar()
+    rng = np.random.default_rng(3)
+    for k in range(200):
+        rl, hl = int(rng.integers(1, 120)), int(rng.integers(1, 200))
+        rd = bytes(rng.choice(list(b"ACGTN"), rl, p=[.24, .24, .24, .24, .04]).astype(np.uint8))
+        hp = bytes(rng.choice(list(b"ACGTN"), hl, p=[.24, .24, .24, .24, .04]).astype(np.uint8))
+        q = bytes(rng.integers(0, 128, rl).astype(np.uint8))
+        tr = None if k % 2 else [0.99, 0.005, 0.005, 0.8, 0.2, 0.7, 0.3]
+        assert _same(oracle.scalar_log10(rd, q, hp, tr), ref.log10(rd, q, hp, tr))
