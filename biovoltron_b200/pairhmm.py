@@ -407,3 +407,87 @@ class GpuPairHMM:
         normalize_likelihoods(ll)
         filter_poorly_modeled_reads(reads, ll)
         return ll
+
+
+class RegionBatcher:
+    """Queues many active regions and scores them in one GPU call.
+
+    ``HaplotypeCaller::run`` calls the PairHMM once per window, one window
+    after another (haplotypecaller.hpp:126-151; the call at :90).  Here a
+    caller adds each window's haplotypes and reads, runs the queue once
+    (``bv_phmm_compute_regions`` over all of them: one batch, one set of
+    launches) and reads each window's matrix back, normalised and filtered
+    exactly as ``compute_likelihoods`` would have done for that window alone
+    (the filter removes reads from the window's own list).  ``model="scalar"``
+    scores with the scalar PairHMM's constant transitions instead.
+    """
+
+    def __init__(self, engine: Optional[PairHMMEngine] = None, device: int = 0, model: str = "avx",
+                 trans: Sequence[float] = ORIGINAL_DEFAULT):
+        if model not in ("avx", "scalar"):
+            raise ValueError("model is 'avx' or 'scalar'")
+        self.engine = engine or PairHMMEngine(device=device)
+        self.model, self.trans = model, tuple(trans)
+        self._queue: List[tuple] = []
+        self._results: List[Optional[List[List[float]]]] = []
+
+    def add(self, haplotypes: Sequence[Haplotype], reads: list) -> int:
+        """Queues one window; returns its handle for ``result``."""
+        self._queue.append((list(haplotypes), reads))
+        self._results.append(None)
+        return len(self._results) - 1
+
+    def run(self) -> None:
+        """Scores every queued window in one call and stores the results."""
+        if not self._queue:
+            return
+        scalar = self.model == "scalar"
+        rb, rq, ri, rd, rc, hb = [], [], [], [], [], []
+        nreads, nhaps = [], []
+        for haps, reads in self._queue:
+            for r in reads:
+                q = np.frombuffer(r.qual, np.uint8)
+                rb.append(np.frombuffer(r.seq, np.uint8))
+                rq.append(q)
+                ri.append(q if scalar else np.frombuffer(r.insertion_gop(), np.uint8))
+                rd.append(q if scalar else np.frombuffer(r.deletion_gop(), np.uint8))
+                rc.append(q if scalar else np.frombuffer(r.overall_gcp(), np.uint8))
+            hb.extend(np.frombuffer(h.seq, np.uint8) for h in haps)
+            nreads.append(len(reads))
+            nhaps.append(len(haps))
+
+        def cat(parts):
+            if not parts:
+                return np.zeros(0, np.uint8), np.zeros(1, np.int64)
+            lens = np.array([len(p) for p in parts], np.int64)
+            return np.concatenate(parts).astype(np.uint8), np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+
+        read_bases, read_off = cat(rb)
+        batch = RegionBatch(read_bases=read_bases, read_q=cat(rq)[0], read_i=cat(ri)[0], read_d=cat(rd)[0],
+                            read_c=cat(rc)[0], read_offsets=read_off, hap_bases=cat(hb)[0], hap_offsets=cat(hb)[1],
+                            region_reads=np.concatenate([[0], np.cumsum(nreads)]).astype(np.int64),
+                            region_haps=np.concatenate([[0], np.cumsum(nhaps)]).astype(np.int64),
+                            name="queued windows")
+        if scalar:
+            self.engine.set_transitions(self.trans)
+        try:
+            flat = self.engine.compute_regions(batch)
+        finally:
+            if scalar:
+                self.engine.set_transitions(None)
+        pos = 0
+        for k, (haps, reads) in enumerate(self._queue):
+            nr, nh = len(reads), len(haps)
+            ll = [list(map(float, flat[pos + i * nh: pos + (i + 1) * nh])) for i in range(nr)]
+            pos += nr * nh
+            if nh and nr:
+                normalize_likelihoods(ll)
+                filter_poorly_modeled_reads(reads, ll)
+            self._results[k] = ll
+        self._queue = []
+
+    def result(self, handle: int) -> List[List[float]]:
+        r = self._results[handle]
+        if r is None:
+            raise RuntimeError("window not scored yet: call run()")
+        return r

@@ -171,4 +171,115 @@ class GpuScalarPairHMM : public GpuPairHMM {
   }
 };
 
+// Queues many windows (a window = the haplotypes and reads one
+// compute_likelihoods call would take) and scores them in one
+// bv_phmm_compute_regions call.  HaplotypeCaller::run calls the PairHMM once
+// per window, one after another (haplotypecaller.hpp:126-151, the call at
+// :90); with a batcher the caller adds the windows, runs once, and reads each
+// window's [read][hap] matrix back, normalised and filtered exactly as a
+// per-window compute_likelihoods call would (the filter edits that window's
+// read vector, which must outlive run()).  scalar = true uses the scalar
+// PairHMM's constant transitions.
+template <class HapVec, class ReadVec>
+class RegionBatcher {
+ public:
+  explicit RegionBatcher(GpuPairHMM& hmm, bool scalar = false,
+                         const GpuScalarPairHMM::TransMatrix& trans = GpuScalarPairHMM::kOriginalDefault)
+      : hmm_(hmm), scalar_(scalar), trans_(trans) {}
+
+  size_t add(const HapVec& haplotypes, ReadVec& reads) {
+    queue_.push_back({&haplotypes, &reads});
+    results_.emplace_back();
+    done_.push_back(false);
+    return results_.size() - 1;
+  }
+
+  void run() {
+    if (queue_.empty()) return;
+    std::vector<int64_t> region_reads{0}, region_haps{0}, read_off{0}, hap_off{0};
+    std::string rb, rq, ri, rd, rc, hb;
+    for (const auto& w : queue_) {
+      for (const auto& r : *w.reads) {
+        rb.append(r.seq.data(), r.seq.size());
+        rq.append(r.qual.data(), r.qual.size());
+        if (scalar_) {
+          ri.append(r.qual.data(), r.qual.size());
+          rd.append(r.qual.data(), r.qual.size());
+          rc.append(r.qual.data(), r.qual.size());
+        } else {
+          ri.append(r.insertion_gop().data(), r.seq.size());
+          rd.append(r.deletion_gop().data(), r.seq.size());
+          rc.append(r.overall_gcp().data(), r.seq.size());
+        }
+        read_off.push_back(static_cast<int64_t>(rb.size()));
+      }
+      for (const auto& h : *w.haps) {
+        hb.append(h.seq.data(), h.seq.size());
+        hap_off.push_back(static_cast<int64_t>(hb.size()));
+      }
+      region_reads.push_back(static_cast<int64_t>(read_off.size() - 1));
+      region_haps.push_back(static_cast<int64_t>(hap_off.size() - 1));
+    }
+    auto u8 = [](const std::string& x) { return reinterpret_cast<const uint8_t*>(x.data()); };
+    bv_region_batch b{};
+    b.num_regions = static_cast<int64_t>(queue_.size());
+    b.region_reads = region_reads.data();
+    b.region_haps = region_haps.data();
+    b.num_reads = static_cast<int64_t>(read_off.size() - 1);
+    b.read_offsets = read_off.data();
+    b.read_bases = u8(rb);
+    b.read_q = u8(rq);
+    b.read_i = u8(ri);
+    b.read_d = u8(rd);
+    b.read_c = u8(rc);
+    b.num_haps = static_cast<int64_t>(hap_off.size() - 1);
+    b.hap_offsets = hap_off.data();
+    b.hap_bases = u8(hb);
+    std::vector<double> flat(static_cast<size_t>(std::max<int64_t>(bv_phmm_region_results(&b), 1)));
+    bv_phmm_ctx* ctx = hmm_.context();
+    if (scalar_) throw_if(bv_phmm_set_transitions(ctx, trans_.data()), "bv_phmm_set_transitions");
+    const bv_status st = bv_phmm_compute_regions(ctx, &b, flat.data(), nullptr);
+    if (scalar_) bv_phmm_set_transitions(ctx, nullptr);
+    throw_if(st, "bv_phmm_compute_regions");
+    size_t pos = 0, k0 = results_.size() - queue_.size();
+    for (size_t k = 0; k < queue_.size(); ++k) {
+      auto& w = queue_[k];
+      const size_t nr = w.reads->size(), nh = w.haps->size();
+      std::vector<std::vector<double>> ll(nr, std::vector<double>(nh, 0.0));
+      for (size_t i = 0; i < nr; ++i)
+        std::copy(flat.begin() + pos + i * nh, flat.begin() + pos + (i + 1) * nh, ll[i].begin());
+      pos += nr * nh;
+      if (nr && nh) {
+        GpuPairHMM::normalize_likelihoods(ll);
+        GpuPairHMM::filter_poorly_modeled_reads(*w.reads, ll);
+      }
+      results_[k0 + k] = std::move(ll);
+      done_[k0 + k] = true;
+    }
+    queue_.clear();
+  }
+
+  const std::vector<std::vector<double>>& result(size_t handle) const {
+    if (handle >= results_.size() || !done_[handle]) throw std::runtime_error("window not scored yet: call run()");
+    return results_[handle];
+  }
+
+ private:
+  struct Window {
+    const HapVec* haps;
+    ReadVec* reads;
+  };
+  void throw_if(bv_status s, const char* what) {
+    if (s != BV_OK)
+      throw std::runtime_error(std::string(what) + ": " + bv_phmm_status_string(s) + " (" +
+                               bv_phmm_last_error(hmm_.context()) + ")");
+  }
+  GpuPairHMM& hmm_;
+  bool scalar_;
+  GpuScalarPairHMM::TransMatrix trans_;
+  std::vector<Window> queue_;
+  std::vector<std::vector<std::vector<double>>> results_;
+  std::vector<bool> done_;
+};
+
 }  // namespace biovoltron_b200

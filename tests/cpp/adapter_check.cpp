@@ -1,6 +1,8 @@
 // adapter_check.cpp -- drives include/biovoltron_b200/gpu_pairhmm.hpp with
 // record types shaped like Biovoltron's SamRecord<> / Haplotype.
-// With the argument "scalar" it drives GpuScalarPairHMM (the scalar model).
+// With the argument "scalar" it drives GpuScalarPairHMM (the scalar model);
+// with "batch" it scores the window twice through RegionBatcher and prints
+// both results one after the other.
 // Input (stdin): lines "H <bases>" and "R <bases> <quals>"; quals are raw
 // bytes given as printable characters.  Output: the kept reads' indices and
 // the [read][hap] log10 matrix after normalize/filter, one row per line.
@@ -49,6 +51,25 @@ int main(int argc, char** argv) {
     }
   }
   std::vector<std::vector<double>> ll;
+  if (argc > 1 && std::string(argv[1]) == "batch") {
+    // two copies of the window through the region batcher: both must equal one call
+    biovoltron_b200::GpuPairHMM hmm(0);
+    std::vector<SamRecord> copy = reads;
+    biovoltron_b200::RegionBatcher<std::vector<Haplotype>, std::vector<SamRecord>> batcher(hmm);
+    const size_t a = batcher.add(haps, reads), b = batcher.add(haps, copy);
+    batcher.run();
+    for (size_t w : {a, b}) {
+      const auto& rr = w == a ? reads : copy;
+      std::printf("kept");
+      for (const auto& r : rr) std::printf(" %d", r.id);
+      std::printf("\n");
+      for (const auto& row : batcher.result(w)) {
+        for (size_t j = 0; j < row.size(); ++j) std::printf(j ? " %.9f" : "%.9f", row[j]);
+        std::printf("\n");
+      }
+    }
+    return 0;
+  }
   if (scalar) {
     biovoltron_b200::GpuScalarPairHMM hmm(0);
     ll = hmm.compute_likelihoods(haps, reads);

@@ -66,3 +66,20 @@ def test_scalar_adapter_matches_python_mirror():
     ll = GpuScalarPairHMM().compute_likelihoods([Haplotype(h) for h in haps], py_reads)
     assert kept == [ids[id(r)] for r in py_reads]
     assert np.allclose(np.array(mat), np.array(ll), rtol=0, atol=1e-8)
+
+
+@pytest.mark.gpu
+def test_region_batcher_adapter_matches_one_call():
+    from biovoltron_b200 import workloads as W
+    _build()
+    rng = np.random.default_rng(14)
+    base = bytes(W._random_seq(rng, 400))
+    haps = [base, base[:220] + b"C" + base[221:], bytes(W._random_seq(rng, 350))]
+    reads = [(base[30:180], bytes(rng.integers(43, 74, size=150).astype(np.uint8))),
+             (bytes(W._random_seq(rng, 70)), b"+" * 70), (base[150:250], b"5" * 100)]
+    txt = "".join(f"H {h.decode()}\n" for h in haps) + "".join(f"R {s.decode()} {q.decode()}\n" for s, q in reads)
+    one = subprocess.run([EXE], input=txt, capture_output=True, text=True, check=True).stdout.splitlines()
+    two = subprocess.run([EXE, "batch"], input=txt, capture_output=True, text=True, check=True).stdout.splitlines()
+    n = len(one)
+    assert len(two) == 2 * n
+    assert two[:n] == one and two[n:] == one

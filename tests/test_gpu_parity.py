@@ -303,3 +303,40 @@ def test_scalar_drop_in_normalises_and_filters():
     filter_poorly_modeled_reads(exp_reads, exp)
     assert [id(r) for r in keep] == [id(r) for r in exp_reads]
     assert np.allclose(np.array(ll), np.array(exp), rtol=0, atol=TOL_FP32)
+
+
+@pytest.mark.parametrize("model", ["avx", "scalar"])
+def test_region_batcher_equals_per_window_calls(model):
+    """Windows queued in a RegionBatcher and scored in one call give the same
+    normalised, filtered matrices (and the same kept reads) as one
+    compute_likelihoods call per window."""
+    from biovoltron_b200.pairhmm import GpuPairHMM, GpuScalarPairHMM, Haplotype, PairHMMEngine, RegionBatcher, SamRecord
+    rng = np.random.default_rng(17)
+    windows = []
+    for w in range(6):
+        base = bytes(W._random_seq(rng, int(rng.integers(200, 400))))
+        haps = [Haplotype(base)] + [Haplotype(bytes(W._substitute(rng, np.frombuffer(base, np.uint8).copy(), 0.02)))
+                                    for _ in range(int(rng.integers(0, 4)))]
+        reads = []
+        for _ in range(int(rng.integers(0, 12))):
+            st = int(rng.integers(0, len(base) - 100))
+            reads.append(SamRecord(base[st:st + 100], bytes(rng.integers(15, 41, 100).astype(np.uint8))))
+        if w == 2:
+            reads.append(SamRecord(bytes(W._random_seq(rng, 90)), bytes([30] * 90)))  # poorly modelled: kept
+        windows.append((haps, reads))
+    with PairHMMEngine() as e:
+        one = GpuScalarPairHMM(engine=e) if model == "scalar" else GpuPairHMM(engine=e)
+        want = []
+        for haps, reads in windows:
+            rr = list(reads)
+            want.append((one.compute_likelihoods(haps, rr), [id(r) for r in rr]))
+        bt = RegionBatcher(engine=e, model=model)
+        lists = [list(reads) for _, reads in windows]
+        hs = [bt.add(haps, lists[k]) for k, (haps, _) in enumerate(windows)]
+        with pytest.raises(RuntimeError):
+            bt.result(hs[0])
+        bt.run()
+        for k, h in enumerate(hs):
+            ll, ids = want[k]
+            assert [id(r) for r in lists[k]] == ids
+            assert bt.result(h) == ll
