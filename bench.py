@@ -59,6 +59,13 @@ from biovoltron_b200 import workloads as W  # noqa: E402
 
 METRIC = "PairHMM GCUPS & pairs/s on 1 B200: learned-band+batched vs plain DP, <=1e-3 log10L err"
 FLOPS_PER_CELL = 12  # computeMXY: 8 mul + 4 add (avx-pairhmm-template.h:183-198)
+# DRAM bytes (read + write) per pair from one ncu capture of a config-4-shaped
+# batch of 2,000 regions (profiles/kernels_ncu_full.md): the full-size step is
+# too large to capture, and both kernels' traffic grows with the pairs.
+DRAM_BYTES_PER_PAIR_PLAIN = 103.3  # k_forward<float, 5, 0, 1>: 113 MB per launch, 1.094e6 pairs
+DRAM_BYTES_PER_BAND_PAIR = 179.4   # k_band_ring_f32<8..32>: 194.8 MB per step, 1.086e6 banded pairs
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum on 2,000 config-4 regions, "
+                  "scaled by the step's pairs (profiles/kernels_ncu_full.md)")
 
 
 def log(*a):
@@ -427,7 +434,9 @@ def main():
             line["roofline_plain"] = {"bound": "fp32", "kernel": "k_forward<float> (full DP, all variants)",
                                       "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
                                       "frac": (ach / fp32_peak) if fp32_peak else None,
-                                      "flops_per_cell": FLOPS_PER_CELL, "traffic": None}
+                                      "flops_per_cell": FLOPS_PER_CELL,
+                                      "traffic": DRAM_BYTES_PER_PAIR_PLAIN * n if args.workload == "config4" else None,
+                                      "traffic_source": TRAFFIC_SOURCE if args.workload == "config4" else None}
             if band is not None:
                 line["speedup_vs_plain"] = value / plain_pps
         if band is not None:
@@ -446,7 +455,10 @@ def main():
             line["roofline"] = {"bound": "fp32", "kernel": "k_band_ring_f32<W> (banded forward, band and ring, W = 8/16/24/32)",
                                 "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
                                 "frac": (ach / fp32_peak) if fp32_peak else None,
-                                "flops_per_cell": FLOPS_PER_CELL, "traffic": None}
+                                "flops_per_cell": FLOPS_PER_CELL,
+                                "traffic": DRAM_BYTES_PER_BAND_PAIR * int(last["band_pairs"])
+                                if args.workload == "config4" else None,
+                                "traffic_source": TRAFFIC_SOURCE if args.workload == "config4" else None}
         else:
             line["roofline"] = line.get("roofline_plain")
         line["peak_source"] = "measured: FP32 FMA probe kernel in this run (bv_phmm_measure_fp32_peak)"
