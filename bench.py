@@ -241,6 +241,26 @@ def time_form(eng, batch, args, rep, band: bool):
     return n, steps, wall, res
 
 
+def genotype_staged_timing(eng, batch) -> dict:
+    """The device genotyper on the staged batch (the step after the PairHMM in
+    HaplotypeCaller): two alleles per region, the first haplotype carrying the
+    reference allele and the others the alternate, 90 % of reads overlapping
+    the site (seeded)."""
+    rng = np.random.default_rng(77)
+    A = np.full(batch.n_regions, 2, np.int32)
+    nh = np.diff(batch.region_haps)
+    hap_allele = np.ones(batch.n_haps, np.int32)
+    hap_allele[batch.region_haps[:-1][nh > 0]] = 0
+    overlap = (rng.random(batch.n_reads) < 0.9).astype(np.uint8)
+    eng.genotype_staged(batch, A, hap_allele, overlap)  # warm-up (table upload)
+    t0 = time.perf_counter()
+    out = eng.genotype_staged(batch, A, hap_allele, overlap)
+    call = time.perf_counter() - t0
+    return {"regions": int(batch.n_regions), "alleles_per_region": 2, "kernel_ms": out["kernel_ms"],
+            "call_ms_with_d2h": call * 1e3, "kept_reads": int(out["kept_count"].sum()),
+            "regions_per_s": batch.n_regions / (out["kernel_ms"] / 1e3) if out["kernel_ms"] > 0 else None}
+
+
 def accuracy(batch, got_band, got_plain, n_sample: int, seed: int):
     """max / p99 |dlog10| against the FP64 oracle on a seeded sample of pairs."""
     from oracle.oracle import Oracle, TestcaseArray
@@ -339,6 +359,7 @@ def main():
         plain = {"n": n, "steps": steps, "wall": wall, "res": res}
     # ---- learned band, device-resident --------------------------------------
     eb = None
+    geno = None
     if form == "band":
         eb = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp, pipeline_chunks=args.pipeline_chunks)
         if tuning:
@@ -354,6 +375,7 @@ def main():
                                 audit_period=args.audit_period)
         n, steps, wall, res = time_form(eb, batch, args, rep, band=True)
         band = {"n": n, "steps": steps, "wall": wall, "res": res}
+        geno = genotype_staged_timing(eb, batch)
     main_run = band if band else plain
     n = main_run["n"]
 
@@ -463,6 +485,8 @@ def main():
             line["roofline"] = line.get("roofline_plain")
         line["peak_source"] = "measured: FP32 FMA probe kernel in this run (bv_phmm_measure_fp32_peak)"
         line["accuracy"] = acc
+        if geno is not None:
+            line["genotype"] = geno
         line["e2e"] = {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(batch.nbytes()),
                        "d2h_bytes_per_step": int(8 * n), "results_identical_to_device_run": same}
         if e2e_st is not None:

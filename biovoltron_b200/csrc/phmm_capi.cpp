@@ -12,6 +12,7 @@
 #include "bv_pairhmm.h"
 #include "phmm_engine.h"
 #include "phmm_mlp.h"
+#include "phmm_genotype.h"
 
 struct bv_phmm_ctx {
   bvphmm::Engine engine;
@@ -325,6 +326,22 @@ bv_status bv_phmm_set_transitions(bv_phmm_ctx* ctx, const double* trans7) {
 int bv_phmm_get_transitions(const bv_phmm_ctx* ctx, double* trans7) {
   if (!ctx) return 0;
   return ctx->engine.constant_transitions(trans7) ? 1 : 0;
+}
+
+int bv_phmm_debug_jacobian_table(double* out, int n) {
+  std::vector<double> t(bvphmm::kJacobianEntries);
+  bvphmm::build_jacobian_table(t.data());
+  for (int k = 0; out && k < n && k < bvphmm::kJacobianEntries; ++k) out[k] = t[k];
+  return bvphmm::kJacobianEntries;
+}
+
+bv_status bv_phmm_genotype_staged(bv_phmm_ctx* ctx, const bv_region_batch* staged, const bv_genotype_batch* gt,
+                                  int32_t* kept_count, int32_t* kept_reads, double* allele_lik,
+                                  double* genotype_lik, double* kernel_ms) {
+  if (!ctx || !staged || !gt) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] {
+    return ctx->engine.genotype_staged(*staged, *gt, kept_count, kept_reads, allele_lik, genotype_lik, kernel_ms);
+  });
 }
 
 bv_status bv_phmm_band_save(bv_phmm_ctx* ctx, const char* path) {

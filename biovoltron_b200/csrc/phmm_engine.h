@@ -79,6 +79,8 @@ class Engine {
   // PairHMM::TrasMatrx order), or the quality-derived ones again (nullptr).
   bv_status set_transitions(const double* trans);
   bool constant_transitions(double* trans) const;
+  bv_status genotype_staged(const bv_region_batch& b, const bv_genotype_batch& g, int32_t* kept_count,
+                            int32_t* kept_reads, double* allele_lik, double* genotype_lik, double* kernel_ms);
   uint64_t mirrored_version() const { return mirrored_version_; }
   // One batch split into `chunks` region chunks that alternate between this
   // context and `other`: a chunk's copies and the host's planning overlap the
@@ -126,6 +128,9 @@ class Engine {
   std::string err_;
 
   std::unique_ptr<Tables> h_tables_;  // host copy of d_tables_
+  DevBuf d_jacobian_, d_gt_regions_, d_gt_offsets_, d_gt_alleles_, d_gt_hap_allele_, d_gt_overlap_;
+  DevBuf d_gt_kept_count_, d_gt_kept_reads_, d_gt_allele_lik_, d_gt_geno_lik_;
+  bool jacobian_ready_ = false;
   DevBuf d_tables_, d_read_bases_, d_q_, d_i_, d_d_, d_c_, d_quals4_, d_read_off_, d_hap_bases_, d_hap_off_;
   DevBuf d_units_, d_out_, d_rescue_, d_counters_, d_bnd32_, d_bnd64_, d_f64_items_;
 

@@ -12,12 +12,14 @@
 // The kernels read these tables unchanged, so per-row probabilities equal the
 // reference's bit for bit.
 #include <cmath>
+#include <quadmath.h>
 #include <limits>
 #include <algorithm>
 #include <vector>
 
 #include "phmm_common.h"
 #include "phmm_kernels.h"
+#include "phmm_genotype.h"
 
 namespace bvphmm {
 namespace {
@@ -102,6 +104,24 @@ void set_constant_transitions(Tables* t, const double* trans) {
   }
   t->cd[7] = 0.0;
   t->cf[7] = t->cf[0] >= kFoldMin ? 1.f / t->cf[0] : std::numeric_limits<float>::quiet_NaN();
+}
+
+}  // namespace bvphmm
+
+namespace bvphmm {
+
+void build_jacobian_table(double* out) {
+  // MathUtils::JacobianLogTable (math_utils.hpp:122-139): entry i is
+  // log10(1 + 10^(-1e-4 i)); each step is rounded once to double from
+  // 113-bit arithmetic, which gives the correctly rounded values the
+  // reference's compile-time table holds.
+  constexpr double kStep = 0.0001;
+  for (int i = 0; i < kJacobianEntries; ++i) {
+    const double x = -kStep * i;
+    const double pw = (double)powq((__float128)10, (__float128)x);
+    const double s = 1.0 + pw;
+    out[i] = (double)log10q((__float128)s);
+  }
 }
 
 }  // namespace bvphmm

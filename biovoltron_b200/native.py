@@ -116,6 +116,10 @@ class RegionBatchC(C.Structure):
     ]
 
 
+class GenotypeBatch(C.Structure):
+    _fields_ = [("allele_count", C.c_void_p), ("hap_allele", C.c_void_p), ("read_overlaps", C.c_void_p)]
+
+
 class NativeError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"bv_pairhmm status {status}: {msg}")
@@ -168,6 +172,8 @@ def load() -> C.CDLL:
         "bv_phmm_set_tuning": (C.c_int, [V, P(TuneEntry), C.c_int32]),
         "bv_phmm_get_tuning": (C.c_int, [V, P(TuneEntry), P(C.c_int32)]),
         "bv_phmm_set_transitions": (C.c_int, [V, P(C.c_double)]),
+        "bv_phmm_genotype_staged": (C.c_int, [V, P(RegionBatchC), P(GenotypeBatch), V, V, V, V, P(C.c_double)]),
+        "bv_phmm_debug_jacobian_table": (C.c_int, [V, C.c_int]),
         "bv_phmm_get_transitions": (C.c_int, [V, P(C.c_double)]),
     }
     for name, (res, args) in sig.items():

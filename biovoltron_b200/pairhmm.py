@@ -134,6 +134,28 @@ class PairHMMEngine:
         self._check(self.lib.bv_phmm_fetch_results(self.h, _ptr(out), n))
         return out[:n]
 
+    def genotype_staged(self, batch: RegionBatch, allele_count, hap_allele, read_overlaps) -> dict:
+        """Device genotyping of the staged, run batch (bv_phmm_genotype_staged):
+        per region the kept reads, allele likelihoods [kept][A] and diploid
+        genotype likelihoods, as numpy arrays."""
+        v = _BatchView(batch)
+        ac = np.ascontiguousarray(allele_count, np.int32)
+        ha = np.ascontiguousarray(hap_allele, np.int32)
+        ov = np.ascontiguousarray(read_overlaps, np.uint8)
+        g = N.GenotypeBatch(allele_count=_ptr(ac), hap_allele=_ptr(ha), read_overlaps=_ptr(ov))
+        nr = np.diff(batch.region_reads)
+        n_al = int(np.sum(nr * ac)) if len(ac) else 0
+        n_ge = int(np.sum(ac * (ac + 1) // 2)) if len(ac) else 0
+        kept = np.zeros(max(batch.n_regions, 1), np.int32)
+        kept_reads = np.full(max(batch.n_reads, 1), -1, np.int32)
+        al = np.zeros(max(n_al, 1), np.float64)
+        ge = np.zeros(max(n_ge, 1), np.float64)
+        ms = C.c_double(0)
+        self._check(self.lib.bv_phmm_genotype_staged(self.h, C.byref(v.c), C.byref(g), _ptr(kept), _ptr(kept_reads),
+                                                     _ptr(al), _ptr(ge), C.byref(ms)))
+        return {"kept_count": kept[:batch.n_regions], "kept_reads": kept_reads[:batch.n_reads],
+                "allele_lik": al[:n_al], "genotype_lik": ge[:n_ge], "kernel_ms": ms.value}
+
     def set_transitions(self, trans: Optional[Sequence[float]]):
         """Constant transitions for every row (the scalar PairHMM model, seven
         values in PairHMM::TrasMatrx order), or None for the quality-derived ones

@@ -387,11 +387,44 @@ bv_status bv_phmm_set_transitions(bv_phmm_ctx* ctx, const double* trans7);
 /* 1 and the seven values when constant transitions are set, else 0. */
 int bv_phmm_get_transitions(const bv_phmm_ctx* ctx, double* trans7);
 
+/* --- genotyping on the device -------------------------------------------
+ * After bv_phmm_run_staged, runs on the staged batch's [read][hap] log10
+ * matrix (it stays on the device) what HaplotypeCaller does with each
+ * region's matrix next: PairHMM::normalize_likelihoods and
+ * filter_poorly_modeled_reads (pairhmm.hpp:83-114), the genotyper's read
+ * selection by site overlap, Genotyper::marginal_likelihoods and the diploid
+ * genotype likelihoods with MathUtils::approximate_log10_sum_log10
+ * (genotyper.hpp:223-240, 254-326; math_utils.hpp:112-139).  Results equal
+ * the reference's bit for bit.  `staged` is the batch that was staged (its
+ * region and read structure is read again).  Outputs, per region g with nr_g
+ * reads, nh_g haplotypes and A_g alleles, in region order:
+ *   kept_count[g]                     reads kept (filter and overlap);
+ *   kept_reads[first read of g + k]   their batch read indices, k < kept;
+ *   allele_lik[sum of nr * A before g + k * A_g + a]  max over the region's
+ *                                     haplotypes of allele a (normalised);
+ *   genotype_lik[sum of A (A + 1) / 2 before g + i]  genotype i = (a1, a2),
+ *                                     a1 <= a2, in the reference's order.
+ * Slots beyond kept_count are left unwritten. */
+typedef struct bv_genotype_batch {
+  const int32_t* allele_count;  /* [num_regions]: alleles at the region's site, 1..64 */
+  const int32_t* hap_allele;    /* [num_haps]: allele (0..A-1) each haplotype carries; others are ignored */
+  const uint8_t* read_overlaps; /* [num_reads]: nonzero when the read overlaps its region's site */
+} bv_genotype_batch;
+
+bv_status bv_phmm_genotype_staged(bv_phmm_ctx* ctx, const bv_region_batch* staged, const bv_genotype_batch* gt,
+                                  int32_t* kept_count, int32_t* kept_reads, double* allele_lik,
+                                  double* genotype_lik, double* kernel_ms);
+
 /* Diagnostics: writes the probability tables a context uploads (ph2pr for
  * quals 0..127 and the match-to-match triangle for quals <= 127, both
  * precisions; Context.h:42-175).  Host-only, needs no device.  Returns 0, or
  * -1 if mm_entries is not 127*128/2 + 128. */
 int bv_phmm_debug_tables(float* ph2pr_f32, double* ph2pr_f64, float* mm_f32, double* mm_f64, int mm_entries);
+
+/* Diagnostics: writes up to n entries of the genotyper's Jacobian log table
+ * (math_utils.hpp:122-139) as this library builds it; returns the table size.
+ * Host-only. */
+int bv_phmm_debug_jacobian_table(double* out, int n);
 
 /* Diagnostics: measures the device's achievable FP32 FMA throughput (TFLOP/s,
  * 2 flops per FMA), the roofline denominator of the forward kernels, which

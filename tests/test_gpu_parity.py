@@ -340,3 +340,42 @@ def test_region_batcher_equals_per_window_calls(model):
             ll, ids = want[k]
             assert [id(r) for r in lists[k]] == ids
             assert bt.result(h) == ll
+
+
+@pytest.mark.parametrize("band", [False, True])
+def test_device_genotyper_equals_reference_steps(band):
+    """bv_phmm_genotype_staged on the staged batch's matrix equals, region by
+    region, the reference's normalise / filter / overlap / marginalise /
+    genotype-likelihood steps (restated in oracle/genotyper.py, pinned to
+    the reference) applied to the same matrix, bit for bit."""
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    from oracle import genotyper as OG
+    b = W.config1(seed=23, n_regions=30)
+    rng = np.random.default_rng(5)
+    nr, nh = np.diff(b.region_reads), np.diff(b.region_haps)
+    A = rng.integers(1, 5, b.n_regions).astype(np.int32)
+    hap_allele = np.concatenate([rng.integers(0, A[g], nh[g]) for g in range(b.n_regions)]).astype(np.int32)
+    overlap = (rng.random(b.n_reads) < 0.85).astype(np.uint8)
+    with PairHMMEngine() as e:
+        if band:
+            e.set_band_options(fixed_half=8, margin=2)
+        n = e.stage(b)
+        e.run()
+        ll = e.fetch(n)
+        out = e.genotype_staged(b, A, hap_allele, overlap)
+    rl = np.diff(b.read_offsets)
+    res = al_off = ge_off = 0
+    for g in range(b.n_regions):
+        r0, h0 = int(b.region_reads[g]), int(b.region_haps[g])
+        m = ll[res:res + nr[g] * nh[g]].reshape(nr[g], nh[g])
+        kept, al, ge = OG.genotype_window(m.tolist(), rl[r0:r0 + nr[g]].tolist(), overlap[r0:r0 + nr[g]].tolist(),
+                                          int(A[g]), (hap_allele[h0:h0 + nh[g]]).tolist())
+        k = int(out["kept_count"][g])
+        assert k == len(kept)
+        assert out["kept_reads"][r0:r0 + k].tolist() == [r0 + x for x in kept]
+        assert np.array_equal(out["allele_lik"][al_off:al_off + k * A[g]], np.array(al).reshape(-1))
+        assert np.array_equal(out["genotype_lik"][ge_off:ge_off + A[g] * (A[g] + 1) // 2], np.array(ge))
+        res += nr[g] * nh[g]
+        al_off += nr[g] * A[g]
+        ge_off += A[g] * (A[g] + 1) // 2
+    assert out["kernel_ms"] > 0
