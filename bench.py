@@ -23,7 +23,12 @@ full-DP kernels score the same batch in the same run for the comparison.
 * plain        the same for the plain full DP (FP32 + FP64 rescue).
 * e2e          pairs/s through bv_phmm_compute_regions in band mode with
                page-locked host buffers: validation, planning, host->device
-               copies, all kernels and the device->host copy of the results.
+               copies, all kernels and the device->host copy of the results
+               (the call splits the batch into region chunks over two
+               contexts so copies overlap kernels).
+* genotype     the device genotyper on the staged batch's matrix (normalise,
+               filter, marginalise, diploid genotype likelihoods), outside
+               the timed region.
 * accuracy     max / p99 |dlog10L| of both forms against the FP64 oracle on a
                seeded sample of pairs, and of the band against the full DP on
                every pair.

@@ -32,6 +32,12 @@
 //       Yh(r,c) = Y(r,c)/pMY(r) = Yh(r,c-1) * pYY(r) + M(r,c-1)
 //   so each costs one FMA, and M costs FMUL + 2 FMA + FMUL: six FP32
 //   instructions per cell instead of the reference's twelve flops.
+// * Folded form (the default): pMM(r) is folded into row r's emission table
+//   and cx, cy carry 1/pMM, so M costs 2 FMA + FMUL: five instructions per
+//   cell.  A strip with a row whose pMM is below kFoldMin keeps the six-
+//   instruction form (phmm_device.cuh, setup_rows).
+// * Constant transitions (the scalar PairHMM model) take the seven
+//   probabilities from the table instead of the quality bytes.
 // * The emission e(r,c) is read from a per-lane shared-memory table indexed by
 //   the haplotype code of the column: one 16-byte load yields four rows' e.
 //   Columns outside the haplotype have code 5 and e = 0, which makes the
