@@ -130,7 +130,6 @@ bv_status Engine::compute_chunked(Engine& other, const bv_region_batch& b, doubl
       }
     }
   }
-  for (auto& c : ck) c.build(b);
   Engine* eng[2] = {this, &other};
   std::vector<bv_phmm_stats> cs(ck.size());
   auto drain = [&](size_t k) -> bv_status {  // results and stats of chunk k
@@ -148,6 +147,7 @@ bv_status Engine::compute_chunked(Engine& other, const bv_region_batch& b, doubl
   };
   for (size_t k = 0; k < ck.size(); ++k) {
     Engine& e = *eng[k % 2];
+    ck[k].build(b);  // here rather than up front: the host rebases chunk k while chunk k-1 runs
     s = e.stage(ck[k].view, false);
     if (s == BV_OK) s = e.launch();
     if (s != BV_OK) return abort(fail(s, e.last_error()));
