@@ -124,8 +124,7 @@ __global__ void __launch_bounds__(kLabelWarps * 32) k_posterior_spread(DeviceBat
     const int stride = H + 2;
     for (int r = 1; r <= R; ++r) {
       const RowC k = row_consts(tb, quals, bases, r);
-      // M, X from the previous row; local Y pass with carry-in 0
-      float yl = 0.f, ml = 0.f;  // Y and M of the column left of the chunk (carry-in applied later)
+      // M, X from the previous row; the Y pass with its carry-in follows
       for (int c = c0; c <= c1; ++c) {
         const float e = emis(k, hcode[c]);
         curM[c] = e * (k.mm * prevM[c - 1] + k.gp * (prevX[c - 1] + prevY[c - 1]));
