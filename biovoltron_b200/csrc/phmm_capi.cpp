@@ -328,6 +328,20 @@ int bv_phmm_get_transitions(const bv_phmm_ctx* ctx, double* trans7) {
   return ctx->engine.constant_transitions(trans7) ? 1 : 0;
 }
 
+int64_t bv_phmm_debug_chunks(const bv_region_batch* batch, int32_t chunks, int64_t* out, int64_t max) {
+  if (!batch || chunks < 1 || batch->num_regions < 0 || (batch->num_regions > 0 && (!batch->region_reads ||
+                                                                                  !batch->region_haps)))
+    return -1;
+  const auto cuts = bvphmm::plan_chunks(*batch, chunks);
+  for (int64_t k = 0; out && k < (int64_t)cuts.size() && k < max; ++k) {
+    out[4 * k] = cuts[k].g0;
+    out[4 * k + 1] = cuts[k].g1;
+    out[4 * k + 2] = cuts[k].out0;
+    out[4 * k + 3] = cuts[k].n_out;
+  }
+  return (int64_t)cuts.size();
+}
+
 int bv_phmm_debug_jacobian_table(double* out, int n) {
   std::vector<double> t(bvphmm::kJacobianEntries);
   bvphmm::build_jacobian_table(t.data());

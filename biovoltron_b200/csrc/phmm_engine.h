@@ -56,6 +56,15 @@ struct LaunchPlan {
   bool f64 = false;
 };
 
+// A chunk of regions [g0, g1) of a batch and its result slots [out0, out0 + n_out).
+struct ChunkCut {
+  int64_t g0, g1, out0, n_out;
+};
+// Cuts a batch's regions into consecutive chunks of about total / chunks
+// pairs each (a chunk ends at the region that reaches the target; the last
+// chunk takes the rest).
+std::vector<ChunkCut> plan_chunks(const bv_region_batch& b, int chunks);
+
 class Engine {
  public:
   explicit Engine(const bv_phmm_options& opt);

@@ -101,6 +101,25 @@ void add_stats(bv_phmm_stats& t, const bv_phmm_stats& s) {
 
 }  // namespace
 
+std::vector<ChunkCut> plan_chunks(const bv_region_batch& b, int chunks) {
+  int64_t total = 0;
+  for (int64_t g = 0; g < b.num_regions; ++g)
+    total += (b.region_reads[g + 1] - b.region_reads[g]) * (b.region_haps[g + 1] - b.region_haps[g]);
+  std::vector<ChunkCut> cuts;
+  const int64_t target = std::max<int64_t>(1, (total + chunks - 1) / std::max(chunks, 1));
+  int64_t g0 = 0, acc = 0, out0 = 0;
+  for (int64_t g = 0; g < b.num_regions; ++g) {
+    acc += (b.region_reads[g + 1] - b.region_reads[g]) * (b.region_haps[g + 1] - b.region_haps[g]);
+    if (acc >= target || g + 1 == b.num_regions) {
+      cuts.push_back(ChunkCut{g0, g + 1, out0, acc});
+      out0 += acc;
+      acc = 0;
+      g0 = g + 1;
+    }
+  }
+  return cuts;
+}
+
 bv_status Engine::compute_chunked(Engine& other, const bv_region_batch& b, double* out, bv_phmm_stats* stats,
                                   int chunks) {
   const auto t0 = std::chrono::steady_clock::now();
@@ -112,23 +131,13 @@ bv_status Engine::compute_chunked(Engine& other, const bv_region_batch& b, doubl
     total += (b.region_reads[g + 1] - b.region_reads[g]) * (b.region_haps[g + 1] - b.region_haps[g]);
   if (total > 0 && !out) return fail(BV_ERR_INVALID_ARG, "null output");
   std::vector<Chunk> ck;
-  {
-    const int64_t target = (total + chunks - 1) / std::max(chunks, 1);
-    int64_t g0 = 0, acc = 0, out0 = 0;
-    for (int64_t g = 0; g < b.num_regions; ++g) {
-      acc += (b.region_reads[g + 1] - b.region_reads[g]) * (b.region_haps[g + 1] - b.region_haps[g]);
-      if (acc >= target || g + 1 == b.num_regions) {
-        Chunk c;
-        c.g0 = g0;
-        c.g1 = g + 1;
-        c.out0 = out0;
-        c.n_out = acc;
-        ck.push_back(std::move(c));
-        out0 += acc;
-        acc = 0;
-        g0 = g + 1;
-      }
-    }
+  for (const ChunkCut& cut : plan_chunks(b, chunks)) {
+    Chunk c;
+    c.g0 = cut.g0;
+    c.g1 = cut.g1;
+    c.out0 = cut.out0;
+    c.n_out = cut.n_out;
+    ck.push_back(std::move(c));
   }
   Engine* eng[2] = {this, &other};
   std::vector<bv_phmm_stats> cs(ck.size());

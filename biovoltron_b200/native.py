@@ -174,6 +174,7 @@ def load() -> C.CDLL:
         "bv_phmm_set_transitions": (C.c_int, [V, P(C.c_double)]),
         "bv_phmm_genotype_staged": (C.c_int, [V, P(RegionBatchC), P(GenotypeBatch), V, V, V, V, P(C.c_double)]),
         "bv_phmm_debug_jacobian_table": (C.c_int, [V, C.c_int]),
+        "bv_phmm_debug_chunks": (C.c_int64, [P(RegionBatchC), C.c_int32, V, C.c_int64]),
         "bv_phmm_get_transitions": (C.c_int, [V, P(C.c_double)]),
     }
     for name, (res, args) in sig.items():

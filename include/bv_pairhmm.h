@@ -421,6 +421,11 @@ bv_status bv_phmm_genotype_staged(bv_phmm_ctx* ctx, const bv_region_batch* stage
  * -1 if mm_entries is not 127*128/2 + 128. */
 int bv_phmm_debug_tables(float* ph2pr_f32, double* ph2pr_f64, float* mm_f32, double* mm_f64, int mm_entries);
 
+/* Diagnostics: the region chunks bv_phmm_compute_regions would use for
+ * `chunks` chunks: writes up to `max` (first region, end region, first result,
+ * results) quadruples and returns the number of chunks.  Host-only. */
+int64_t bv_phmm_debug_chunks(const bv_region_batch* batch, int32_t chunks, int64_t* out, int64_t max);
+
 /* Diagnostics: writes up to n entries of the genotyper's Jacobian log table
  * (math_utils.hpp:122-139) as this library builds it; returns the table size.
  * Host-only. */

@@ -4,6 +4,7 @@ stand-in engine, no GPU), and the workload generators."""
 import math
 
 import numpy as np
+import pytest
 
 from biovoltron_b200 import workloads as W
 from biovoltron_b200.pairhmm import (GpuPairHMM, Haplotype, SamRecord, filter_poorly_modeled_reads,
@@ -107,3 +108,49 @@ def test_config2_shape():
 def test_generators_are_seeded():
     a, b = W.config1(seed=4, n_regions=3), W.config1(seed=4, n_regions=3)
     assert np.array_equal(a.read_bases, b.read_bases) and np.array_equal(a.hap_bases, b.hap_bases)
+
+
+def _chunks(b, k):
+    import ctypes as C
+    from biovoltron_b200.native import load
+    from biovoltron_b200.pairhmm import _BatchView
+    lib = load()
+    v = _BatchView(b)
+    n = lib.bv_phmm_debug_chunks(C.byref(v.c), k, None, 0)
+    out = np.zeros(max(4 * n, 1), np.int64)
+    assert lib.bv_phmm_debug_chunks(C.byref(v.c), k, out.ctypes.data, n) == n
+    return out[:4 * n].reshape(n, 4)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 7, 64])
+def test_chunk_plan_covers_regions_in_order(k):
+    """The chunked call's region cuts: consecutive, covering every region and
+    result slot once, each chunk but the last holding at least total / k pairs."""
+    b = W.config1(seed=3, n_regions=50)
+    nr, nh = np.diff(b.region_reads), np.diff(b.region_haps)
+    per = nr * nh
+    c = _chunks(b, k)
+    assert c[0, 0] == 0 and c[-1, 1] == b.n_regions
+    assert np.all(c[1:, 0] == c[:-1, 1]) and np.all(c[:, 1] > c[:, 0])
+    assert np.all(c[:, 2] == np.concatenate([[0], np.cumsum(c[:-1, 3])]))
+    for g0, g1, o0, n in c:
+        assert n == per[g0:g1].sum()
+    target = -(-per.sum() // k)
+    assert np.all(c[:-1, 3] >= target)
+    assert len(c) <= k
+
+
+def test_chunk_plan_with_empty_regions():
+    b = W.config1(seed=4, n_regions=12)
+    # drop the haplotypes of a few regions: zero-pair regions must still be covered
+    keep = np.ones(b.n_regions, bool)
+    keep[[0, 5, 11]] = False
+    rh = b.region_haps.copy()
+    nh = np.diff(rh)
+    nh[~keep] = 0
+    b2 = W.RegionBatch(read_bases=b.read_bases, read_q=b.read_q, read_i=b.read_i, read_d=b.read_d, read_c=b.read_c,
+                       read_offsets=b.read_offsets, hap_bases=b.hap_bases, hap_offsets=b.hap_offsets,
+                       region_reads=b.region_reads, region_haps=np.concatenate([[0], np.cumsum(nh)]).astype(np.int64),
+                       name="holes")
+    c = _chunks(b2, 4)
+    assert c[0, 0] == 0 and c[-1, 1] == b2.n_regions and c[:, 3].sum() == b2.n_pairs
