@@ -154,3 +154,77 @@ def test_chunk_plan_with_empty_regions():
                        name="holes")
     c = _chunks(b2, 4)
     assert c[0, 0] == 0 and c[-1, 1] == b2.n_regions and c[:, 3].sum() == b2.n_pairs
+
+
+class _OracleRegionEngine:
+    """Stands in for PairHMMEngine on the CPU: compute_regions scores a region
+    batch with the oracle (AVX model, or the scalar model while constant
+    transitions are set), so the host logic around the engine can be tested
+    without a device."""
+
+    def __init__(self):
+        from oracle.oracle import Oracle
+        self.oracle = Oracle()
+        self.trans = None
+        self.calls = 0
+
+    def set_transitions(self, trans):
+        self.trans = None if trans is None else list(trans)
+
+    def compute_regions(self, batch):
+        self.calls += 1
+        if self.trans is None:
+            return self.oracle.log10_rescaled(TestcaseArray.for_batch(batch))
+        r, h = batch.pair_index()
+        ro, ho = batch.read_offsets, batch.hap_offsets
+        return np.array([self.oracle.scalar_log10(bytes(batch.read_bases[ro[a]:ro[a + 1]]),
+                                                  bytes(batch.read_q[ro[a]:ro[a + 1]]),
+                                                  bytes(batch.hap_bases[ho[c]:ho[c + 1]]), self.trans)
+                         for a, c in zip(r, h)])
+
+
+@pytest.mark.parametrize("model", ["avx", "scalar"])
+def test_region_batcher_assembles_slices_and_filters(model):
+    """RegionBatcher packs the queued windows into one region batch (one
+    engine call), slices the flat results back per window and normalises and
+    filters each window as a per-window compute_likelihoods would."""
+    from biovoltron_b200.pairhmm import ORIGINAL_DEFAULT, RegionBatcher
+    from oracle.oracle import Oracle
+    rng = np.random.default_rng(31)
+    windows = []
+    for w in range(5):
+        base = bytes(W._random_seq(rng, int(rng.integers(150, 260))))
+        haps = [Haplotype(base)] + [Haplotype(bytes(W._substitute(rng, np.frombuffer(base, np.uint8).copy(), 0.03)))
+                                    for _ in range(int(rng.integers(0, 3)))]
+        reads = []
+        for _ in range(int(rng.integers(0, 6))):
+            st = int(rng.integers(0, len(base) - 80))
+            reads.append(SamRecord(base[st:st + 80], bytes(rng.integers(15, 41, 80).astype(np.uint8))))
+        reads.append(SamRecord(bytes(W._random_seq(rng, 60)), bytes([30] * 60)))
+        windows.append((haps, reads))
+    eng = _OracleRegionEngine()
+    bt = RegionBatcher(engine=eng, model=model)
+    lists = [list(r) for _, r in windows]
+    hs = [bt.add(haps, lists[k]) for k, (haps, _) in enumerate(windows)]
+    bt.run()
+    assert eng.calls == 1 and eng.trans is None
+    o = Oracle()
+    for k, (haps, reads) in enumerate(windows):
+        if model == "scalar":
+            ll = [[o.scalar_log10(r.seq, r.qual, h.seq, ORIGINAL_DEFAULT) for h in haps] for r in reads]
+        else:
+            tcs = [(r.seq, r.qual, r.insertion_gop(), r.deletion_gop(), r.overall_gcp(), h.seq)
+                   for r in reads for h in haps]
+            flat = [o.log10_rescaled(_tcs_array(t))[0] for t in tcs]
+            ll = [flat[i * len(haps):(i + 1) * len(haps)] for i in range(len(reads))]
+        rr = list(reads)
+        normalize_likelihoods(ll)
+        filter_poorly_modeled_reads(rr, ll)
+        assert [id(r) for r in lists[k]] == [id(r) for r in rr]
+        assert bt.result(hs[k]) == ll
+
+
+def _tcs_array(t):
+    rs, q, i, d, c, hap = t
+    b = W.from_pairs([(rs, q, i, d, c, hap)])
+    return TestcaseArray.for_batch(b)
