@@ -171,6 +171,11 @@ class _OracleRegionEngine:
     def set_transitions(self, trans):
         self.trans = None if trans is None else list(trans)
 
+    def compute_testcases(self, tcs):
+        return np.array([self.oracle.scalar_log10(rs, q, hap, self.trans) if self.trans is not None else
+                         self.oracle.log10_rescaled(_tcs_array((rs, q, i, d, c, hap)))[0]
+                         for rs, q, i, d, c, hap in tcs])
+
     def compute_regions(self, batch):
         self.calls += 1
         if self.trans is None:
@@ -228,3 +233,27 @@ def _tcs_array(t):
     rs, q, i, d, c, hap = t
     b = W.from_pairs([(rs, q, i, d, c, hap)])
     return TestcaseArray.for_batch(b)
+
+
+def test_scalar_drop_in_host_logic():
+    """GpuScalarPairHMM sets the constant transitions for its call only,
+    scores [read][hap] in order, then normalises and filters."""
+    from biovoltron_b200.pairhmm import ORIGINAL_DEFAULT, GpuScalarPairHMM
+    from oracle.oracle import Oracle
+    rng = np.random.default_rng(9)
+    base = bytes(W._random_seq(rng, 200))
+    haps = [Haplotype(base), Haplotype(base[:90] + b"G" + base[91:])]
+    reads = [SamRecord(base[10:90], bytes(rng.integers(20, 41, 80).astype(np.uint8))),
+             SamRecord(bytes(W._random_seq(rng, 70)), bytes([30] * 70))]
+    eng = _OracleRegionEngine()
+    rr = list(reads)
+    trans = (0.999, 0.0005, 0.0005, 0.8, 0.2, 0.85, 0.15)
+    ll = GpuScalarPairHMM(engine=eng).compute_likelihoods(haps, rr, trans)
+    assert eng.trans is None
+    o = Oracle()
+    exp = [[o.scalar_log10(r.seq, r.qual, h.seq, trans) for h in haps] for r in reads]
+    er = list(reads)
+    normalize_likelihoods(exp)
+    filter_poorly_modeled_reads(er, exp)
+    assert ll == exp and [id(r) for r in rr] == [id(r) for r in er]
+    assert tuple(ORIGINAL_DEFAULT) == (0.9998, 0.0001, 0.0001, 0.9, 0.1, 0.9, 0.1)
