@@ -476,7 +476,10 @@ def main():
                 "band_pairs": int(last["band_pairs"]), "routed_full": int(last["band_routed_full"]),
                 "edge_fallback": int(last["band_fallback"]), "promoted": int(last["band_promoted"]),
                 "fallback_rate": (int(last["band_routed_full"]) + int(last["band_fallback"])) / max(n, 1),
-                "band_cells": band_cells, "rescued": int(last["rescued"]),
+                "band_cells": band_cells,
+                # computed cells per second of the banded kernels (band + ring + inner band)
+                "gcups_computed_banded_dp": band_cells / (ms_band / 1e3) / 1e9 if ms_band > 0 else None,
+                "rescued": int(last["rescued"]),
                 "audit_pairs": int(last["audit_pairs"]), "audit_max_err": float(last["audit_max_err"]),
                 "audit_p99_err": float(last["audit_p99_err"]), "train": train_rep}
             line["roofline"] = {"bound": "fp32", "kernel": "k_band_ring_f32<W> (banded forward, band and ring, W = 8/16/24/32)",
