@@ -11,7 +11,7 @@ if ROOT not in sys.path:
 from biovoltron_b200 import workloads as W  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-FIXTURES = ("config0", "edge_cases", "ref_test", "long_pairs")
+FIXTURES = ("config0", "edge_cases", "ref_test", "long_pairs", "config4_small")
 BATCH_FIELDS = ("read_bases", "read_q", "read_i", "read_d", "read_c", "read_offsets", "hap_bases", "hap_offsets",
                 "region_reads", "region_haps")
 

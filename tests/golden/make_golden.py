@@ -22,6 +22,8 @@ Fixtures:
                   reference's FP64 underflows on most, so the expected values
                   are the rescaled FP64 oracle, cross-checked against the
                   reference wherever the reference is finite
+  config4_small.npz  two regions of the headline workload's shape (config 4:
+                  150 bp reads at 30x, 2-16 haplotypes of ~450 bp, seed 44)
   scalar.npz      the scalar PairHMM model (pairhmm.hpp, compiled by
                   oracle/Makefile into oracle/_ref/libref_scalar.so): a small
                   region and edge pairs, expected log10 values with
@@ -199,6 +201,7 @@ def main():
     if os.path.exists(REF_TEST):
         save("ref_test.npz", ref_test_batch(), ref, oracle)
     save("long_pairs.npz", W.config2(seed=11, n_pairs=6, max_read=2000, max_hap=2600), ref, oracle)
+    save("config4_small.npz", W.config4(seed=44, n_regions=2), ref, oracle)
     save_scalar("scalar.npz", scalar_batch(), ReferenceScalar())
 
 
