@@ -127,8 +127,8 @@ cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st);
 cudaError_t launch_band_dp(const BandParams& p, int width_class, int sms, cudaStream_t st);
 inline int band_dp_blocks(int sms) { return sms * 4; }
 // featuriser grid and its per-warp scratch histograms (words)
-constexpr int kFeatWarpsPerBlock = 8;
-inline int feat_blocks(int sms) { return sms * 5; }
+constexpr int kFeatWarpsPerBlock = 4;
+inline int feat_blocks(int sms) { return sms * 10; }
 inline long long feat_hist_words(int sms) { return (long long)feat_blocks(sms) * kFeatWarpsPerBlock * (kBandMaxRead + kBandMaxHap); }
 // Sets the dynamic shared-memory limits of the band kernels (before any capture).
 cudaError_t prepare_band_kernels();
