@@ -83,3 +83,19 @@ def test_create_without_gpu_reports_no_device():
     h = C.c_void_p()
     assert lib.bv_phmm_create(None, C.byref(h)) == N.BV_ERR_NO_DEVICE
     assert not h.value
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_device():
+    lib = N.load()
+    h = C.c_void_p()
+    o = N.Options()
+    for field, value in (("pipeline_chunks", -1), ("pipeline_chunks", 65), ("pipeline_min_pairs", -5)):
+        lib.bv_phmm_default_options(C.byref(o))
+        setattr(o, field, value)
+        assert lib.bv_phmm_create(C.byref(o), C.byref(h)) == N.BV_ERR_INVALID_ARG
+    assert lib.bv_phmm_set_transitions(None, None) == N.BV_ERR_INVALID_ARG
+    assert lib.bv_phmm_get_transitions(None, None) == 0
+    assert lib.bv_phmm_genotype_staged(None, None, None, None, None, None, None, None) == N.BV_ERR_INVALID_ARG
+    assert lib.bv_phmm_debug_chunks(None, 4, None, 0) == -1
+    lib.bv_phmm_default_options(C.byref(o))
+    assert o.pipeline_chunks == 0 and o.pipeline_min_pairs == 0
