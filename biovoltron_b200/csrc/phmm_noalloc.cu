@@ -28,6 +28,13 @@
 //   * the first call on a device sets that device up (looks up the array's
 //     device address with cudaGetSymbolAddress and copies the tables into
 //     it, synchronously); make that first call before any stream capture.
+//     With lazy module loading (the CUDA default since 12.2) that first call
+//     is also when the driver loads this library's device code on the device
+//     and reserves the array, so a caller whose framework will later take
+//     nearly all of HBM makes its first call at start-up, before the
+//     framework's allocator reserves memory (or runs with
+//     CUDA_MODULE_LOADING=EAGER, which loads every module when the context is
+//     created).  After that first call, calls reserve no device memory.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -45,13 +52,21 @@ constexpr int kWarps = 64;
 constexpr int kBlocks = kWarps / (kThreadsPerBlock / kWarp);
 constexpr int kRT = 4;
 constexpr int kMaxHap = BV_PHMM_NOALLOC_MAX_HAP_LEN;
-constexpr long long kBndCols = ((kMaxHap + kWarp - 1 + 31) / 32) * 32 + 128;  // as the allocating path sizes them
+// boundary columns per warp: the haplotype rounded up to the warp, plus 128 of
+// headroom; the kernel's largest index is nsteps + 96 (2,176 at 2,048 bases),
+// below these 2,208 (the allocating path keeps 160 columns of headroom)
+constexpr long long kBndCols = ((kMaxHap + kWarp - 1 + 31) / 32) * 32 + 128;
 constexpr int kHapBytes = ((kMaxHap + (kWarp - 1) + 32 + kHapLead + 16 + 15) / 16) * 16;
 constexpr size_t kCountersBytes = 512;
 constexpr size_t kTablesBytes = (sizeof(Tables) + 255) / 256 * 256;
 constexpr size_t kBndBytes = (size_t)kWarps * kBndCols * 4 * sizeof(double);
 constexpr size_t kScratchBytes = kCountersBytes + kTablesBytes + kBndBytes;
 static_assert(sizeof(Counters) <= kCountersBytes, "counters do not fit");
+// The launch sets no dynamic shared-memory attribute, so a block must stay
+// within the 48 KB every kernel may use without one.
+static_assert((size_t)(kHapBytes + WarpSmem<double, kRT>::kEtabBytes + WarpSmem<double, kRT>::kRingBytes) *
+                      (kThreadsPerBlock / kWarp) <= 48 * 1024,
+              "no-allocation kernel needs more than 48 KB of shared memory per block");
 constexpr int kMaxDevices = 64;
 
 // The scratch.  Host code only ever uses the address cudaGetSymbolAddress

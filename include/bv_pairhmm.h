@@ -325,7 +325,11 @@ bv_status bv_phmm_band_mlp_eval(bv_phmm_ctx* ctx, const float* w, const float* x
  * and returns after the stream has finished it.  The first call on a device
  * sets that device up (finds the scratch array's device address, copies the
  * probability tables into it, synchronously): make it before any stream
- * capture.  All calls share the one scratch array and it keeps the last
+ * capture.  Under lazy module loading (the CUDA default since 12.2) that
+ * first call is also when the driver loads this library's device code on the
+ * device and reserves the 4.6 MB array: make it at start-up, before the
+ * framework's allocator reserves its memory, or set CUDA_MODULE_LOADING=EAGER.
+ * Later calls reserve no device memory.  All calls share the one scratch array and it keeps the last
  * call's contents (the call clears what must start at zero); calls that
  * overlap on the GPU -- from two host threads or on two streams -- race. */
 #define BV_PHMM_NOALLOC_MAX_HAP_LEN 2048

@@ -1,8 +1,10 @@
 """Generates the golden PairHMM fixtures in this directory.
 
-Run from the repository root where the reference tree is present:
+Run from the repository root, naming the reference tree (the directory
+that holds Biovoltron's include/, lib/ and tests/):
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference tree> &&
+    python tests/golden/make_golden.py --ref <reference tree>
 
 Every expected value is produced by Biovoltron's own PairHMM kernel
 (lib/intel_native/pairhmm, compiled by oracle/Makefile into
@@ -44,7 +46,7 @@ from biovoltron_b200 import workloads as W  # noqa: E402
 from oracle.oracle import Oracle, Reference, ReferenceScalar, TestcaseArray  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_TEST = "/root/reference/tests/algo/align/inexact_match/pairhmm_avx.cpp"
+REF_TEST_REL = os.path.join("tests", "algo", "align", "inexact_match", "pairhmm_avx.cpp")
 
 BATCH_FIELDS = ("read_bases", "read_q", "read_i", "read_d", "read_c", "read_offsets", "hap_bases", "hap_offsets",
                 "region_reads", "region_haps")
@@ -116,8 +118,8 @@ def edge_batch() -> W.RegionBatch:
     return W.from_pairs(P, "edge cases")
 
 
-def ref_test_batch() -> W.RegionBatch:
-    src = open(REF_TEST).read()
+def ref_test_batch(ref_test: str) -> W.RegionBatch:
+    src = open(ref_test).read()
     strings = re.findall(r'"([ACGTN]{500,})"', src)
     ref_seq = strings[0]
     haps = strings[1:9]
@@ -194,12 +196,18 @@ def save_scalar(name, batch, ref_scalar):
 
 
 def main():
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", required=True, help="the reference tree (holds include/, lib/ and tests/)")
+    args = ap.parse_args()
+    ref_test = os.path.join(args.ref, REF_TEST_REL)
     ref = Reference()
     oracle = Oracle()
     save("config0.npz", W.config0(0), ref, oracle)
     save("edge_cases.npz", edge_batch(), ref, oracle)
-    if os.path.exists(REF_TEST):
-        save("ref_test.npz", ref_test_batch(), ref, oracle)
+    if os.path.exists(ref_test):
+        save("ref_test.npz", ref_test_batch(ref_test), ref, oracle)
     save("long_pairs.npz", W.config2(seed=11, n_pairs=6, max_read=2000, max_hap=2600), ref, oracle)
     save("config4_small.npz", W.config4(seed=44, n_regions=2), ref, oracle)
     save_scalar("scalar.npz", scalar_batch(), ReferenceScalar())

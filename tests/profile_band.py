@@ -1,6 +1,6 @@
 """Runs the band path on a seeded batch (timing and profiling case).
 
-    python -m biovoltron_b200.profile_band --workload config1 --regions 512 \
+    python tests/profile_band.py --workload config1 --regions 512 \
         --weights band.bvw --threshold 1e-3 --runs 3
 
 With --weights the learned band is used (--train-regions > 0 trains and
@@ -11,9 +11,11 @@ same batch as JSON lines; used under ncu to list the band pipeline's kernels.
 import argparse
 import json
 import os
+import sys
 
-from . import workloads as W
-from .pairhmm import PairHMMEngine
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from biovoltron_b200 import workloads as W  # noqa: E402
+from biovoltron_b200.pairhmm import PairHMMEngine  # noqa: E402
 
 
 def _batch(workload: str, regions: int, seed: int):
