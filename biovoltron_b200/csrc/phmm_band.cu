@@ -56,7 +56,11 @@ __global__ void k_pairs_from_units(const Unit* __restrict__ units, long long n_u
 // slot.  Built in shared memory, written out coalesced.  Haplotypes longer
 // than kBandMaxHap get no table (the featuriser routes their pairs to the
 // full DP).
-__device__ __forceinline__ int64_t tbl_base(int64_t hap_off, long long h) { return 2 * hap_off + 4 * h; }
+// A table starts on a 16-byte boundary (its buckets are read as uint4 from
+// global memory): word 2 hap_off + 8 h rounded up to a multiple of 4.  Table
+// h spans at most 2 H + 2 words, which ends before table h + 1 starts; the
+// buffer holds 2 n_hap_bytes + 8 n_haps + 4 words (kHapTableWords).
+__device__ __forceinline__ int64_t tbl_base(int64_t hap_off, long long h) { return (2 * hap_off + 8 * h + 3) & ~3ll; }
 __device__ __forceinline__ uint32_t tbl_bucket(uint32_t code, uint32_t nb) {
   return (uint32_t)(((uint64_t)(code * 0x9E3779B1u) * nb) >> 32);
 }
@@ -133,32 +137,28 @@ __global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n
   }
 }
 
-// One block per chunk of kUnitChunk consecutive work units (a read and up
-// to haps_per_unit haplotypes of its region), chunks taken from a device
-// counter.  The chunk's pairs run haplotype by haplotype (units sorted by
-// first haplotype): the block stages the haplotype's 11-mer hash table into
-// shared memory once and its warps share out the reads that meet it, one
-// warp per pair.  The read's
-// 11-mers at positions 0, kSeedStride, 2 kSeedStride, ... and R - 11 are
-// looked up there, and every shared occurrence votes for diagonal d = j - i
-// in a per-warp histogram whose slot also keeps the first and last sampled
-// read position voting for it.  d* is the most
-// voted diagonal (smallest on ties); the features are the 64 bins
-// d* - 32 .. d* + 31 divided by the number of read 11-mers, and 16 scalars:
-// vote totals, lengths, d*'s position, the uncovered read ends (t_pre, t_suf),
-// the diagonals of the first and last hit relative to d*, the mismatches of
-// the first and last 16 read bases along those diagonals, and the voted
-// extent relative to d*.  kmin/kmax are the extreme voted diagonals widened
-// by the read ends' triangles: an insertion run in a read end moves the
-// alignment one diagonal per row, so below a diagonal whose last hit leaves
-// t read bases uncovered (t <= kEndRows, or any t for the read's last hit)
-// the band reaches t diagonals down, and likewise up from a diagonal whose
-// first hit starts h bases into the read.
+// Features of a pair.  The read's 11-mers at positions 0, kSeedStride,
+// 2 kSeedStride, ... and R - 11 are looked up in the haplotype's table, and
+// every shared occurrence votes for diagonal d = j - i; per voted diagonal
+// the votes and the first and last sampled read position voting for it are
+// kept.  d* is the most voted diagonal (smallest on ties); the features are
+// the 64 bins d* - 32 .. d* + 31 divided by the number of read 11-mers, and 16
+// scalars: vote totals, lengths, d*'s position, the uncovered read ends
+// (t_pre, t_suf), the diagonals of the first and last hit relative to d*, the
+// mismatches of the first and last 16 read bases along those diagonals, and
+// the voted extent relative to d*.  kmin/kmax are the extreme voted diagonals
+// widened by the read ends' triangles: an insertion run in a read end moves
+// the alignment one diagonal per row, so below a diagonal whose last hit
+// leaves t read bases uncovered (t <= kEndRows, or any t for the read's last
+// hit) the band reaches t diagonals down, and likewise up from a diagonal
+// whose first hit starts h bases into the read.  Two implementations give the
+// same results: a thread per pair (k_featurize_t, below) and, for pairs with
+// more voted diagonals than a thread keeps, a warp per pair with a histogram
+// over all diagonals (featurize_pair, k_featurize_slow).
 constexpr int kFeatWarps = kFeatWarpsPerBlock;
 constexpr int kHitCap = 256;
 constexpr int kEndRows = 24;   // horizon of the per-diagonal end triangles
 constexpr int kUnitChunk = 32;
-constexpr int kCtlInts = 72;  // chunk control block of the featuriser (ints)
 constexpr int kHistSlots = kBandMaxRead + kBandMaxHap;  // d + R in [0, R + H)
 // histogram slot: votes << 18 | first read position << 9 | last read position
 // (read positions < 2^9 because reads over kBandMaxRead bases are not banded)
@@ -173,6 +173,42 @@ __device__ __forceinline__ void no_seed(const BandParams& p, long long pi, int l
 // Sampling stride of a read of R bases: kSeedStride, or wider so that at
 // most 32 positions (0, stride, 2 stride, ... and R - 11) are sampled.
 __device__ __forceinline__ int seed_stride(int last_pos) { return max(kSeedStride, (last_pos + 30) / 31); }
+
+// The 16 scalar features of a pair (after the 64 histogram bins), as two
+// 16-byte stores of BF16 pairs: hits, hits outside the window, read length,
+// haplotype length, d*'s position, a constant, the mode's hits, the window's
+// non-empty bins, the uncovered read ends, the first and last hit's diagonal
+// and the mismatches of the read ends along them, the voted extent.  Both
+// featurisers call it, so their outputs agree bit for bit.
+__device__ __forceinline__ void write_scalars(__nv_bfloat16* f, int total, int win, int R, int H, int ds, int peak,
+                                              int nonzero, float inv, int t_pre, int t_suf, int d_first, int d_last,
+                                              int mis_pre, int mis_suf, bool overflow, int dmin, int dmax) {
+  const float v[16] = {(float)total * inv,
+                       (float)(total - win) * inv,
+                       (float)R / 256.f,
+                       (float)H / 1024.f,
+                       __fdiv_rn((float)(ds + R), (float)(R + H)),
+                       1.f,
+                       (float)peak * inv,
+                       (float)nonzero / (float)kHistBins,
+                       (float)t_pre / 32.f,
+                       (float)t_suf / 32.f,
+                       (float)(d_first - ds) / 32.f,
+                       (float)(d_last - ds) / 32.f,
+                       (float)mis_pre / 16.f,
+                       (float)mis_suf / 16.f,
+                       overflow ? -2.f : fmaxf((float)(dmin - ds) / 32.f, -2.f),
+                       overflow ? 2.f : fminf((float)(dmax - ds) / 32.f, 2.f)};
+  uint32_t w[8];
+#pragma unroll
+  for (int x = 0; x < 8; ++x) {
+    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * x], v[2 * x + 1]);
+    w[x] = *reinterpret_cast<const uint32_t*>(&b2);
+  }
+  uint4* dst = reinterpret_cast<uint4*>(f + kHistBins);
+  dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+  dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
 
 __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, const uint32_t* tbl, uint32_t* hist,
                                int* hits, int* nhit, int lane) {
@@ -362,34 +398,9 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
     nonzero = __reduce_add_sync(0xffffffffu, nonzero);
     peak = __reduce_max_sync(0xffffffffu, peak);
     if (overflow) total = max(total, win);
-    if (lane == 0) {
-      // 16 scalars, written as two 16-byte stores
-      const float v[16] = {(float)total * inv,
-                           (float)(total - win) * inv,
-                           (float)R / 256.f,
-                           (float)H / 1024.f,
-                           __fdividef((float)(ds + R), (float)(R + H)),
-                           1.f,
-                           (float)peak * inv,
-                           (float)nonzero / (float)kHistBins,
-                           (float)t_pre / 32.f,
-                           (float)t_suf / 32.f,
-                           (float)(d_first - ds) / 32.f,
-                           (float)(d_last - ds) / 32.f,
-                           (float)mis_pre / 16.f,
-                           (float)mis_suf / 16.f,
-                           overflow ? -2.f : fmaxf((float)(smin - R - ds) / 32.f, -2.f),
-                           overflow ? 2.f : fminf((float)(smax - R - ds) / 32.f, 2.f)};
-      uint32_t w[8];
-#pragma unroll
-      for (int x = 0; x < 8; ++x) {
-        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * x], v[2 * x + 1]);
-        w[x] = *reinterpret_cast<const uint32_t*>(&b2);
-      }
-      uint4* dst = reinterpret_cast<uint4*>(f + kHistBins);
-      dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
-      dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
-    }
+    if (lane == 0)
+      write_scalars(f, total, win, R, H, ds, peak, nonzero, inv, t_pre, t_suf, d_first, d_last, mis_pre, mis_suf,
+                    overflow, smin - R, smax - R);
     if (lane == 0) {
       p.dstar[pi] = ds;
       // voted extent and end triangles (a hit list overflow widens it to everything)
@@ -408,86 +419,241 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kFeatWarps * 32) k_featurize(BandParams p) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// Slow path: the pairs the thread featuriser handed back (more distinct voted
+// diagonals than it keeps), one warp per pair, each warp with a histogram of
+// kHistSlots words in global scratch (zero between pairs) and its slot list in
+// shared memory; the haplotype tables are read from global memory.
+__global__ void __launch_bounds__(kFeatWarps * 32) k_featurize_slow(BandParams p) {
+  __shared__ int s_hits[kFeatWarps][kHitCap + 1];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  // block-shared: the staged haplotype table and the chunk's units sorted by
-  // first haplotype; per warp: histogram and voted-slot list
-  uint32_t* tbl = reinterpret_cast<uint32_t*>(smem);
-  Unit* su = reinterpret_cast<Unit*>(smem + (size_t)(2 * kBandMaxHap + 4) * 4);
-  // [0] chunk, [1] max nh, [2] groups, [3..3+33) group starts, [36..68) group max nh
-  int* sctl = reinterpret_cast<int*>(su + kUnitChunk);
-  // the repeated-11-mer histogram of each warp lives in global scratch (rarely touched), which
-  // leaves the block ~17 KB of shared memory and five blocks per SM
   uint32_t* hist = p.feat_hist + ((size_t)blockIdx.x * kFeatWarps + wib) * kHistSlots;
-  int* hits = reinterpret_cast<int*>(sctl + kCtlInts) + (size_t)wib * (kHitCap + 1);
+  int* hits = s_hits[wib];
   int* nhit = hits + kHitCap;
+  const unsigned long long n = min(p.bctr->feat_slow_count, (unsigned long long)max(p.n_pairs, 1ll));
+  if (n == 0) return;
   for (int x = lane; x < kHistSlots; x += 32) hist[x] = 0u;
-  const long long nchunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
+  __syncwarp();
   for (;;) {
-    __syncthreads();  // the previous chunk is done with su / tbl
-    if (threadIdx.x == 0) sctl[0] = (int)min((long long)atomicAdd(&p.bctr->feat_next, 1ull), nchunks);
+    unsigned long long w = 0;
+    if (lane == 0) w = atomicAdd(&p.bctr->feat_slow_next, 1ull);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= n) break;
+    const long long pi = p.feat_slow[w];
+    const int r = p.pair_read[pi], h = p.pair_hap[pi];
+    featurize_pair(p, pi, r, h, p.hap_table + tbl_base(p.batch.hap_off[h], h), hist, hits, nhit, lane);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Thread featuriser: one thread per pair.  A block takes a chunk of
+// kUnitChunk work units and spreads the chunk's pairs over its threads.  A
+// thread looks the read's sampled 11-mers up in the haplotype's hash table
+// (global memory, eight samples' loads in flight at a time) and keeps up to
+// kCand distinct voted diagonals with their vote count and first and last
+// voting read position -- what the warp featuriser's histogram holds, for all
+// but pairs with many repeats.  A pair that votes for more diagonals goes to
+// the slow list.  Features are assembled in a per-thread row of shared
+// memory, then copied out in 16-byte stores.
+// ---------------------------------------------------------------------------
+constexpr int kCand = 8;
+constexpr int kFeatT = 128;          // threads per block
+constexpr int kFeatTBatch = 4;       // samples whose loads are issued together
+constexpr int kFeatRowWords = kFeat / 2;
+
+__device__ __forceinline__ void no_seed_thread(const BandParams& p, long long pi) {
+  p.dstar[pi] = INT32_MIN;
+  p.kmin[pi] = INT32_MIN;
+  p.kmax[pi] = INT32_MAX;
+  uint4* f = reinterpret_cast<uint4*>(p.feat + pi * kFeat);
+#pragma unroll
+  for (int x = 0; x < kFeat / 8; ++x) f[x] = make_uint4(0, 0, 0, 0);
+}
+
+__device__ __forceinline__ void featurize_thread(const BandParams& p, long long pi, int r, int h, uint32_t* row) {
+  const int64_t ro = p.batch.read_off[r], ho = p.batch.hap_off[h];
+  const int R = (int)(p.batch.read_off[r + 1] - ro), H = (int)(p.batch.hap_off[h + 1] - ho);
+  if (H < kK || H > kBandMaxHap || R < kK || R > kBandMaxRead) {
+    no_seed_thread(p, pi);
+    return;
+  }
+  const uint32_t* tbl = p.hap_table + tbl_base(ho, h);
+  const uint32_t nb = (uint32_t)(H + 1) / 2;
+  const int last_pos = R - kK;
+  const int stride = seed_stride(last_pos);
+  const int q_s = last_pos / stride;
+  const int n_samp = q_s + 1 + (q_s * stride != last_pos);  // <= 32
+  // voted diagonals as slots d + R: slot, votes, first and last voting read position
+  int cs[kCand], cn[kCand], cf[kCand], cl[kCand];
+#pragma unroll
+  for (int c = 0; c < kCand; ++c) { cs[c] = -1; cn[c] = 0; cf[c] = 0; cl[c] = 0; }
+  int nc = 0;
+  bool ovf = false;
+  auto vote = [&](int v, int i) {
+    bool found = false;
+#pragma unroll
+    for (int c = 0; c < kCand; ++c) {
+      if (cs[c] == v) { cn[c] += 1; cl[c] = i; found = true; }
+    }
+    if (!found) {
+      if (nc < kCand) {
+#pragma unroll
+        for (int c = 0; c < kCand; ++c) {
+          if (c == nc) { cs[c] = v; cn[c] = 1; cf[c] = i; cl[c] = i; }
+        }
+        ++nc;
+      } else {
+        ovf = true;
+      }
+    }
+  };
+  for (int s0 = 0; s0 < n_samp; s0 += kFeatTBatch) {
+    uint32_t code[kFeatTBatch], bk[kFeatTBatch];
+    int ip[kFeatTBatch];
+    uint4 q[kFeatTBatch];
+#pragma unroll
+    for (int u = 0; u < kFeatTBatch; ++u) {
+      ip[u] = min((s0 + u) * stride, last_pos);
+      code[u] = s0 + u < n_samp ? __ldg(p.read_kmers + ro + ip[u]) : kNoCode;
+    }
+#pragma unroll
+    for (int u = 0; u < kFeatTBatch; ++u) {
+      bk[u] = code[u] != kNoCode ? tbl_bucket(code[u], nb) : 0u;
+      q[u] = code[u] != kNoCode ? __ldg(reinterpret_cast<const uint4*>(tbl + 4 * bk[u]))
+                                : make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
+    }
+#pragma unroll
+    for (int u = 0; u < kFeatTBatch; ++u) {
+      const uint32_t cd = code[u];
+      if (cd == kNoCode) continue;
+      uint4 qq = q[u];
+      uint32_t b = bk[u];
+      for (uint32_t guard = 0; guard < nb; ++guard) {
+        const uint32_t e4[4] = {qq.x, qq.y, qq.z, qq.w};
+        bool has_free = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (e4[k] == kEmpty) has_free = true;
+          else if ((e4[k] >> 10) == cd) vote((int)(e4[k] & 1023u) - ip[u] + R, ip[u]);
+        }
+        if (has_free) break;
+        b = b + 1 == nb ? 0 : b + 1;
+        qq = __ldg(reinterpret_cast<const uint4*>(tbl + 4 * b));
+      }
+    }
+  }
+  if (ovf) {
+    const unsigned long long at = atomicAdd(&p.bctr->feat_slow_count, 1ull);
+    if (at < (unsigned long long)p.n_pairs) p.feat_slow[at] = pi;
+    return;
+  }
+  if (nc == 0) {
+    no_seed_thread(p, pi);
+    return;
+  }
+  // summary: mode (most votes, smallest slot on ties), first / last sampled hit
+  // (smallest slot on ties), voted extent, end triangles, vote total
+  uint32_t best = 0u, fkey = 0xffffffffu, lkey = 0u;
+  int smin = INT32_MAX, smax = -1, tri_lo = INT32_MAX, tri_hi = INT32_MIN, total = 0;
+#pragma unroll
+  for (int c = 0; c < kCand; ++c) {
+    if (c < nc) {
+      best = max(best, ((uint32_t)cn[c] << 16) | (0xffffu - (uint32_t)cs[c]));
+      fkey = min(fkey, ((uint32_t)cf[c] << 16) | (uint32_t)cs[c]);
+      lkey = max(lkey, ((uint32_t)cl[c] << 16) | (0xffffu - (uint32_t)cs[c]));
+      smin = min(smin, cs[c]);
+      smax = max(smax, cs[c]);
+      const int d = cs[c] - R, tail = R - kK - cl[c], head = cf[c];
+      if (tail <= kEndRows) tri_lo = min(tri_lo, d - tail);
+      if (head <= kEndRows) tri_hi = max(tri_hi, d + head);
+      total += cn[c];
+    }
+  }
+  const int best_slot = (int)(0xffffu - (best & 0xffffu));
+  const int ds = best_slot - R;
+  const int first_i = (int)(fkey >> 16), first_s = (int)(fkey & 0xffffu);
+  const int last_i = (int)(lkey >> 16), last_s = (int)(0xffffu - (lkey & 0xffffu));
+  const int t_pre = first_i, t_suf = R - kK - last_i;
+  const int d_first = first_s - R, d_last = last_s - R;
+  tri_lo = min(tri_lo, d_last - t_suf);
+  tri_hi = max(tri_hi, d_first + t_pre);
+  // mismatches of the first / last 16 read bases along those diagonals
+  const uint8_t* rb = p.batch.read_bases + ro;
+  const uint8_t* hb = p.batch.hap_bases + ho;
+  const int n_end = min(16, R);
+  int mis_pre = 0, mis_suf = 0;
+#pragma unroll
+  for (int l = 0; l < 16; ++l) {
+    if (l < n_end) {
+      const int jp = l + d_first, is = R - 1 - l, js = is + d_last;
+      mis_pre += (jp < 0 || jp >= H || !bases_match(__ldg(rb + l), __ldg(hb + jp))) ? 1 : 0;
+      mis_suf += (js < 0 || js >= H || !bases_match(__ldg(rb + is), __ldg(hb + js))) ? 1 : 0;
+    }
+  }
+  // 64 histogram bins d* - 32 .. d* + 31 (the mode's bin is 32)
+  const float inv = __frcp_rn((float)n_samp);
+#pragma unroll
+  for (int x = 0; x < kHistBins / 2; ++x) row[x] = 0u;
+  int win = 0, nonzero = 0;
+  __nv_bfloat16* rowb = reinterpret_cast<__nv_bfloat16*>(row);
+#pragma unroll
+  for (int c = 0; c < kCand; ++c) {
+    const int bin = cs[c] - (best_slot - kHistBins / 2);
+    if (c < nc && bin >= 0 && bin < kHistBins) {
+      rowb[bin] = __float2bfloat16_rn((float)cn[c] * inv);
+      win += cn[c];
+      nonzero += 1;
+    }
+  }
+  write_scalars(rowb, total, win, R, H, ds, (int)(best >> 16), nonzero, inv, t_pre, t_suf, d_first, d_last,
+                mis_pre, mis_suf, false, smin - R, smax - R);
+  uint4* dst = reinterpret_cast<uint4*>(p.feat + pi * kFeat);
+  const uint4* src = reinterpret_cast<const uint4*>(row);
+#pragma unroll
+  for (int x = 0; x < kFeat / 8; ++x) dst[x] = src[x];
+  p.dstar[pi] = ds;
+  p.kmin[pi] = min(smin - R, tri_lo);
+  p.kmax[pi] = max(smax - R, tri_hi);
+}
+
+__global__ void __launch_bounds__(kFeatT, 5) k_featurize_t(BandParams p) {
+  __shared__ __align__(16) uint32_t s_row[kFeatT][kFeatRowWords];
+  __shared__ Unit s_units[kUnitChunk];
+  __shared__ int s_pre[kUnitChunk + 1];
+  __shared__ long long s_chunk;
+  const long long nchunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    __syncthreads();  // the previous chunk is done with s_units / s_pre
+    if (threadIdx.x == 0) s_chunk = (long long)min((long long)atomicAdd(&p.bctr->feat_next, 1ull), nchunks);
     __syncthreads();
-    const long long c = sctl[0];
+    const long long c = s_chunk;
     if (c >= nchunks) break;
     const long long u0 = c * kUnitChunk;
     const int nu = (int)min((long long)kUnitChunk, p.n_units - u0);
-    if (wib == 0) {
-      // sort the units by first haplotype; groups of equal first haplotype
+    if (threadIdx.x < 32) {
       Unit un{};
       if (lane < nu) un = p.units[u0 + lane];
-      const long long key = lane < nu ? ((long long)un.hap0 << 5) | lane : LLONG_MAX;
-      int rank = 0;
-      for (int o = 0; o < 32; ++o) rank += __shfl_sync(0xffffffffu, key, o) < key;
-      if (lane < nu) su[rank] = un;
-      __syncwarp();
-      const int hap_r = lane < nu ? su[lane].hap0 : -1, nh_r = lane < nu ? su[lane].nh : 0;
-      // lane q (in sorted order) starts a group when its first haplotype differs from lane q - 1's
-      const int prev = __shfl_up_sync(0xffffffffu, hap_r, 1);
-      const bool start = lane < nu && (lane == 0 || prev != hap_r);
-      const unsigned starts = __ballot_sync(0xffffffffu, start);
-      const int g = __popc(starts & ((2u << lane) - 1u)) - 1;  // group of sorted lane q
-      int gmax = lane < nu ? nh_r : 0;  // max nh within the group (segmented reduction)
+      int x = lane < nu ? un.nh : 0;  // inclusive scan of the units' pair counts
+#pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_down_sync(0xffffffffu, gmax, o);
-        const int gv = __shfl_down_sync(0xffffffffu, g, o);
-        if (lane + o < nu && gv == g) gmax = max(gmax, v);
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
       }
-      if (start) { sctl[3 + g] = lane; sctl[36 + g] = gmax; }
-      int mx = lane < nu ? nh_r : 0;
-      for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      if (lane == 0) { sctl[1] = mx; sctl[2] = __popc(starts); sctl[3 + __popc(starts)] = nu; }
+      if (lane < nu) s_units[lane] = un;
+      s_pre[lane + 1] = x;
+      if (lane == 0) s_pre[0] = 0;
     }
     __syncthreads();
-    const int max_nh = sctl[1], ngroups = sctl[2];
-    for (int k = 0; k < max_nh; ++k) {
-      for (int gi = 0; gi < ngroups; ++gi) {
-        // a group: consecutive sorted units with the same first haplotype, so one haplotype h
-        const int q0 = sctl[3 + gi], q1 = sctl[4 + gi];
-        const int h = su[q0].hap0 + k;
-        if (k < sctl[36 + gi]) {
-          const int64_t ho = p.batch.hap_off[h];
-          const int H = (int)(p.batch.hap_off[h + 1] - ho);
-          const bool tab = H >= kK && H <= kBandMaxHap;
-          if (tab) {
-            const uint32_t* src_tbl = p.hap_table + tbl_base(ho, h);
-            for (int x = threadIdx.x; x < 4 * ((H + 1) / 2); x += blockDim.x) tbl[x] = src_tbl[x];
-          }
-          __syncthreads();
-          for (int q = q0 + wib; q < q1; q += kFeatWarps) {
-            const Unit un = su[q];
-            if (k >= un.nh) continue;
-            const long long pi = un.out0 + k;
-            const int R = (int)(p.batch.read_off[un.read + 1] - p.batch.read_off[un.read]);
-            if (!tab || R < kK || R > kBandMaxRead) {
-              no_seed(p, pi, lane);
-              continue;
-            }
-            featurize_pair(p, pi, un.read, h, tbl, hist, hits, nhit, lane);
-          }
-          __syncthreads();  // before the table is restaged
-        }
+    const int npairs = s_pre[nu];
+    for (int q = threadIdx.x; q < npairs; q += kFeatT) {
+      int lo = 0, hi = nu - 1;  // the unit holding pair q: largest u with s_pre[u] <= q
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_pre[mid] <= q) lo = mid; else hi = mid - 1;
       }
+      const Unit un = s_units[lo];
+      const int k = q - s_pre[lo];
+      featurize_thread(p, un.out0 + k, un.read, un.hap0 + k, s_row[threadIdx.x]);
     }
   }
 }
@@ -1048,20 +1214,20 @@ cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, l
   return cudaGetLastError();
 }
 
-constexpr int kFeatSmem = (2 * kBandMaxHap + 4) * 4 + kUnitChunk * (int)sizeof(Unit) + kCtlInts * 4 +
-                          kFeatWarps * (kHitCap + 1) * 4;
-
 cudaError_t prepare_band_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(k_featurize, cudaFuncAttributeMaxDynamicSharedMemorySize, kFeatSmem);
-  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
 }
 
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
   if (p.n_units <= 0) return cudaSuccess;
   const long long chunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
-  const long long blocks = std::min<long long>(chunks, (long long)feat_blocks(sms));
-  k_featurize<<<(int)blocks, kFeatWarps * 32, kFeatSmem, st>>>(p);
+  const long long blocks = std::min<long long>(chunks, (long long)sms * 5);  // five resident blocks per SM
+  k_featurize_t<<<(int)blocks, kFeatT, 0, st>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // the slow list's length is known only on the device: the warp featuriser
+  // reads it and returns at once when it is empty
+  k_featurize_slow<<<feat_blocks(sms), kFeatWarps * 32, 0, st>>>(p);
   return cudaGetLastError();
 }
 

@@ -4,10 +4,12 @@
 //   k_pairs_from_units  expand work units into one (read, hap) per result slot
 //   k_hap_table         per haplotype: 11-mer hash table (code -> positions)
 //   k_read_kmers        per read position: 11-mer code
-//   k_featurize         per pair (units in chunks, haplotype tables staged in
-//                       shared memory): shared 11-mer diagonal histogram ->
-//                       features, seed diagonal d* (the histogram's mode),
-//                       band extent (voted diagonals and read-end triangles)
+//   k_featurize_t       one thread per pair: shared 11-mer diagonal votes ->
+//                       features, seed diagonal d* (the votes' mode), band
+//                       extent (voted diagonals and read-end triangles); a
+//                       pair voting for more diagonals than a thread keeps
+//                       goes to k_featurize_slow (one warp per pair, a
+//                       histogram in global scratch), with the same results
 //   k_mlp_forward       per pair: BF16 MLP 80-128-128-2 (FP32 accumulation) ->
 //                       lower and upper band edge relative to d*
 //   k_band_route        band (by width class and read-length bucket) or full DP
@@ -77,6 +79,8 @@ struct BandCounters {
   unsigned long long fallback_route;                      // pairs routed to the full DP up front
   unsigned long long band_cells;
   unsigned long long feat_next;                           // work-queue head of the featuriser
+  unsigned long long feat_slow_count;                     // pairs left to the warp featuriser (many distinct diagonals)
+  unsigned long long feat_slow_next;                      // its work-queue head
 };
 
 struct BandParams {
@@ -85,11 +89,12 @@ struct BandParams {
   long long n_pairs;
   const int32_t* pair_read;   // [n_pairs]
   const int32_t* pair_hap;    // [n_pairs]
-  const uint32_t* hap_table;  // 11-mer hash tables, 2 slots per haplotype base + 4 per haplotype
+  const uint32_t* hap_table;  // 11-mer hash tables, 16-byte aligned, hap_table_words() words
   const Unit* units;          // work units (featuriser order)
   long long n_units;
   const uint32_t* read_kmers; // 11-mer code per read position
   uint32_t* feat_hist;        // featuriser scratch: one histogram of kBandMaxRead + kBandMaxHap slots per warp
+  int64_t* feat_slow;         // [n_pairs] pairs the thread featuriser hands to the warp featuriser
   int32_t* dstar;             // [n_pairs] seed diagonal (INT32_MIN: no seed)
   int32_t* kmin;              // [n_pairs] lowest / highest diagonal of a shared 11-mer
   int32_t* kmax;
@@ -115,6 +120,9 @@ struct BandParams {
   long long rescue_cap;
 };
 
+// Words of the per-haplotype 11-mer hash tables of a batch.
+inline long long hap_table_words(long long n_hap_bytes, long long n_haps) { return 2 * n_hap_bytes + 8 * n_haps + 4; }
+
 cudaError_t launch_pairs_from_units(const Unit* units, long long n_units, int32_t* pair_read, int32_t* pair_hap,
                                     int sms, cudaStream_t st);
 cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint32_t* codes, int sms, cudaStream_t st);
@@ -126,9 +134,9 @@ cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream
 cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st);
 cudaError_t launch_band_dp(const BandParams& p, int width_class, int sms, cudaStream_t st);
 inline int band_dp_blocks(int sms) { return sms * 4; }
-// featuriser grid and its per-warp scratch histograms (words)
+// warp featuriser (the slow path) grid and its per-warp scratch histograms (words)
 constexpr int kFeatWarpsPerBlock = 4;
-inline int feat_blocks(int sms) { return sms * 10; }
+inline int feat_blocks(int sms) { return sms * 4; }
 inline long long feat_hist_words(int sms) { return (long long)feat_blocks(sms) * kFeatWarpsPerBlock * (kBandMaxRead + kBandMaxHap); }
 // Sets the dynamic shared-memory limits of the band kernels (before any capture).
 cudaError_t prepare_band_kernels();

@@ -165,8 +165,8 @@ bv_status Engine::validate(const bv_region_batch& b) {
       if (l < 0) return fail(BV_ERR_INVALID_ARG, "read offsets decrease");
       if (l > BV_PHMM_MAX_READ_LEN) return fail(BV_ERR_INVALID_ARG, "read longer than BV_PHMM_MAX_READ_LEN");
     }
-    if (b.read_offsets[b.num_reads] > 0 &&
-        (!b.read_bases || !b.read_q || !b.read_i || !b.read_d || !b.read_c))
+    const int n_gap_arrays = (b.read_i != nullptr) + (b.read_d != nullptr) + (b.read_c != nullptr);
+    if (b.read_offsets[b.num_reads] > 0 && (!b.read_bases || !b.read_q || (n_gap_arrays != 0 && n_gap_arrays != 3)))
       return fail(BV_ERR_INVALID_ARG, "read arrays missing");
   }
   if (b.num_haps > 0) {
@@ -315,10 +315,17 @@ bv_status Engine::upload_inputs(const bv_region_batch& b) {
   n_hap_bytes_ = b.num_haps > 0 ? b.hap_offsets[b.num_haps] : 0;
   const size_t rb = (size_t)std::max<int64_t>(n_read_bytes_, 1);
   BV_CUDA(d_read_bases_.reserve(rb + 16), "alloc reads");  // tail padding for the k-mer kernel's word loads
+  // uniform gap penalties: no per-base i, d, c arrays to copy (see bv_region_batch)
+  uniform_gaps_ = !b.read_i && !b.read_d && !b.read_c;
+  gap_ins_ = b.gap_ins;
+  gap_del_ = b.gap_del;
+  gap_gcp_ = b.gap_gcp;
   BV_CUDA(d_q_.reserve(rb), "alloc q");
-  BV_CUDA(d_i_.reserve(rb), "alloc i");
-  BV_CUDA(d_d_.reserve(rb), "alloc d");
-  BV_CUDA(d_c_.reserve(rb), "alloc c");
+  if (!uniform_gaps_) {
+    BV_CUDA(d_i_.reserve(rb), "alloc i");
+    BV_CUDA(d_d_.reserve(rb), "alloc d");
+    BV_CUDA(d_c_.reserve(rb), "alloc c");
+  }
   BV_CUDA(d_quals4_.reserve(rb * 4), "alloc quals");
   BV_CUDA(d_read_off_.reserve(sizeof(int64_t) * (n_reads_ + 1)), "alloc read offsets");
   BV_CUDA(d_hap_bases_.reserve((size_t)std::max<int64_t>(n_hap_bytes_, 1)), "alloc haps");
@@ -329,9 +336,11 @@ bv_status Engine::upload_inputs(const bv_region_batch& b) {
   if (n_read_bytes_ > 0) {
     BV_CUDA(cudaMemcpyAsync(d_read_bases_.get(), b.read_bases, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
     BV_CUDA(cudaMemcpyAsync(d_q_.get(), b.read_q, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
-    BV_CUDA(cudaMemcpyAsync(d_i_.get(), b.read_i, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
-    BV_CUDA(cudaMemcpyAsync(d_d_.get(), b.read_d, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
-    BV_CUDA(cudaMemcpyAsync(d_c_.get(), b.read_c, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+    if (!uniform_gaps_) {
+      BV_CUDA(cudaMemcpyAsync(d_i_.get(), b.read_i, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+      BV_CUDA(cudaMemcpyAsync(d_d_.get(), b.read_d, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+      BV_CUDA(cudaMemcpyAsync(d_c_.get(), b.read_c, n_read_bytes_, cudaMemcpyHostToDevice, stream_), "H2D");
+    }
   }
   if (n_reads_ > 0)
     BV_CUDA(cudaMemcpyAsync(d_read_off_.get(), b.read_offsets, sizeof(int64_t) * (n_reads_ + 1), cudaMemcpyHostToDevice,
@@ -364,8 +373,12 @@ bv_status Engine::upload_plan() {
   if (!f64_items_.empty())
     BV_CUDA(cudaMemcpyAsync(d_rescue_.get(), f64_items_.data(), sizeof(PairRef) * f64_items_.size(),
                             cudaMemcpyHostToDevice, stream_), "H2D");
-  BV_CUDA(launch_pack_quals(d_q_.as<uint8_t>(), d_i_.as<uint8_t>(), d_d_.as<uint8_t>(), d_c_.as<uint8_t>(),
-                            d_quals4_.as<uchar4>(), n_read_bytes_, sms_, stream_), "pack quals");
+  if (uniform_gaps_)
+    BV_CUDA(launch_pack_quals_uniform(d_q_.as<uint8_t>(), gap_ins_, gap_del_, gap_gcp_, d_quals4_.as<uchar4>(),
+                                      n_read_bytes_, sms_, stream_), "pack quals");
+  else
+    BV_CUDA(launch_pack_quals(d_q_.as<uint8_t>(), d_i_.as<uint8_t>(), d_d_.as<uint8_t>(), d_c_.as<uint8_t>(),
+                              d_quals4_.as<uchar4>(), n_read_bytes_, sms_, stream_), "pack quals");
   BV_CUDA(cudaEventRecord(ev_[1], stream_), "event");
   h2d_time_pending_ = true;
   return BV_OK;

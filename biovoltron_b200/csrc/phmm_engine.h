@@ -65,6 +65,61 @@ struct ChunkCut {
 // chunk takes the rest).
 std::vector<ChunkCut> plan_chunks(const bv_region_batch& b, int chunks);
 
+// A chunk of regions [g0, g1) as a batch of its own: offsets rebased to the
+// chunk's first read / haplotype, byte pointers moved to match.
+struct Chunk {
+  int64_t g0 = 0, g1 = 0, out0 = 0, n_out = 0;
+  std::vector<int64_t> region_reads, region_haps, read_off, hap_off;
+  bv_region_batch view{};
+
+  void build(const bv_region_batch& b) {
+    const int64_t r0 = b.region_reads[g0], r1 = b.region_reads[g1];
+    const int64_t h0 = b.region_haps[g0], h1 = b.region_haps[g1];
+    region_reads.resize(g1 - g0 + 1);
+    region_haps.resize(g1 - g0 + 1);
+    for (int64_t g = g0; g <= g1; ++g) {
+      region_reads[g - g0] = b.region_reads[g] - r0;
+      region_haps[g - g0] = b.region_haps[g] - h0;
+    }
+    read_off.resize(r1 - r0 + 1);
+    const int64_t rb0 = r1 > r0 ? b.read_offsets[r0] : 0;
+    for (int64_t r = r0; r <= r1 && r1 > r0; ++r) read_off[r - r0] = b.read_offsets[r] - rb0;
+    if (r1 == r0) read_off[0] = 0;
+    hap_off.resize(h1 - h0 + 1);
+    const int64_t hb0 = h1 > h0 ? b.hap_offsets[h0] : 0;
+    for (int64_t h = h0; h <= h1 && h1 > h0; ++h) hap_off[h - h0] = b.hap_offsets[h] - hb0;
+    if (h1 == h0) hap_off[0] = 0;
+    view = b;
+    view.num_regions = g1 - g0;
+    view.region_reads = region_reads.data();
+    view.region_haps = region_haps.data();
+    view.num_reads = r1 - r0;
+    view.read_offsets = read_off.data();
+    view.num_haps = h1 - h0;
+    view.hap_offsets = hap_off.data();
+    auto shift = [](const uint8_t* p, int64_t o) { return p ? p + o : p; };
+    view.read_bases = shift(b.read_bases, rb0);
+    view.read_q = shift(b.read_q, rb0);
+    view.read_i = shift(b.read_i, rb0);
+    view.read_d = shift(b.read_d, rb0);
+    view.read_c = shift(b.read_c, rb0);
+    view.hap_bases = shift(b.hap_bases, hb0);
+  }
+};
+
+// Adds a call's statistics into a running total (chunks, contexts).
+void add_stats(bv_phmm_stats& t, const bv_phmm_stats& s);
+
+// Regions split over n_parts devices: contiguous blocks of about equal DP
+// cells (block b = regions [block_start[b], block_start[b+1]), its results at
+// block_out0[b]), dealt by greedy LPT on the blocks' cells (block_part[b]).
+struct Partition {
+  std::vector<int64_t> block_start, block_cells, block_out0, block_pairs, part_cells;
+  std::vector<int> block_part;
+};
+Partition plan_partition(const bv_region_batch& b, int n_parts, int n_blocks);
+
+
 class Engine {
  public:
   explicit Engine(const bv_phmm_options& opt);
@@ -151,6 +206,8 @@ class Engine {
   int64_t n_results_ = 0;
   int64_t n_cells_ = 0;
   int64_t n_read_bytes_ = 0;
+  bool uniform_gaps_ = false;  // the staged batch gave no per-base i, d, c arrays
+  uint8_t gap_ins_ = 0, gap_del_ = 0, gap_gcp_ = 0;
   int64_t n_hap_bytes_ = 0;
   int64_t n_reads_ = 0;
   int64_t n_haps_ = 0;
@@ -167,7 +224,7 @@ class Engine {
   bv_band_options band_opt_{};
   bool mlp_ready_ = false;
   DevBuf d_pair_read_, d_pair_hap_, d_hap_table_, d_dstar_, d_feat_, d_mlp_out_, d_mlp_, d_bctr_;
-  DevBuf d_kmin_, d_kmax_, d_read_kmers_, d_feat_hist_;
+  DevBuf d_kmin_, d_kmax_, d_read_kmers_, d_feat_hist_, d_feat_slow_;
   DevBuf d_band_items_, d_full_items_, d_audit_pairs_, d_audit_units_, d_audit_out_, d_audit_err_;
   long long item_cap_ = 0, full_cap_ = 0, audit_cap_ = 0;
   LaunchPlan full_plans_[9];

@@ -50,6 +50,7 @@ BandParams Engine::band_params() const {
   p.n_units = (long long)units_.size();
   p.read_kmers = d_read_kmers_.as<uint32_t>();
   p.feat_hist = d_feat_hist_.as<uint32_t>();
+  p.feat_slow = d_feat_slow_.as<int64_t>();
   p.dstar = d_dstar_.as<int32_t>();
   p.kmin = d_kmin_.as<int32_t>();
   p.kmax = d_kmax_.as<int32_t>();
@@ -81,9 +82,11 @@ bv_status Engine::band_prepare() {
   BV_CUDA(prepare_band_kernels(), "band kernel attributes");
   BV_CUDA(d_pair_read_.reserve(sizeof(int32_t) * n), "alloc pairs");
   BV_CUDA(d_pair_hap_.reserve(sizeof(int32_t) * n), "alloc pairs");
-  BV_CUDA(d_hap_table_.reserve(sizeof(uint32_t) * (2 * std::max<int64_t>(n_hap_bytes_, 1) + 4 * n_haps_)), "alloc hap tables");
+  BV_CUDA(d_hap_table_.reserve(sizeof(uint32_t) * (size_t)hap_table_words(std::max<int64_t>(n_hap_bytes_, 1), n_haps_)),
+          "alloc hap tables");
   BV_CUDA(d_read_kmers_.reserve(sizeof(uint32_t) * std::max<int64_t>(n_read_bytes_, 1)), "alloc kmers");
   BV_CUDA(d_feat_hist_.reserve(sizeof(uint32_t) * (size_t)feat_hist_words(sms_)), "alloc featuriser scratch");
+  BV_CUDA(d_feat_slow_.reserve(sizeof(int64_t) * n), "alloc featuriser list");
   BV_CUDA(d_dstar_.reserve(sizeof(int32_t) * n), "alloc seeds");
   BV_CUDA(d_kmin_.reserve(sizeof(int32_t) * n), "alloc seeds");
   BV_CUDA(d_kmax_.reserve(sizeof(int32_t) * n), "alloc seeds");

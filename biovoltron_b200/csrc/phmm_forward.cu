@@ -94,6 +94,12 @@ __global__ void k_pack_quals(const uint8_t* __restrict__ q, const uint8_t* __res
     out[x] = make_uchar4(q[x], i[x], d[x], c[x]);
 }
 
+__global__ void k_pack_quals_uniform(const uint8_t* __restrict__ q, uint8_t gi, uint8_t gd, uint8_t gc,
+                                     uchar4* __restrict__ out, long long n) {
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n; x += (long long)gridDim.x * blockDim.x)
+    out[x] = make_uchar4(q[x], gi, gd, gc);
+}
+
 __global__ void k_set_u64(unsigned long long* dst, unsigned long long v) { *dst = v; }
 
 cudaError_t launch_set_u64(unsigned long long* dst, unsigned long long v, cudaStream_t st) {
@@ -203,6 +209,15 @@ cudaError_t launch_pack_quals(const uint8_t* q, const uint8_t* i, const uint8_t*
   long long blocks = (n + 255) / 256;
   if (blocks > (long long)sms * 8) blocks = (long long)sms * 8;
   k_pack_quals<<<(int)blocks, 256, 0, st>>>(q, i, d, c, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_quals_uniform(const uint8_t* q, uint8_t gi, uint8_t gd, uint8_t gc, uchar4* out, long long n,
+                                      int sms, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  long long blocks = (n + 255) / 256;
+  if (blocks > (long long)sms * 8) blocks = (long long)sms * 8;
+  k_pack_quals_uniform<<<(int)blocks, 256, 0, st>>>(q, gi, gd, gc, out, n);
   return cudaGetLastError();
 }
 

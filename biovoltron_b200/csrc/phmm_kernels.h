@@ -43,6 +43,9 @@ cudaError_t prepare_variant(int variant, int smem_per_block);
 cudaError_t launch_forward(int variant, const KernelParams& p, int grid, cudaStream_t st);
 cudaError_t launch_pack_quals(const uint8_t* q, const uint8_t* i, const uint8_t* d, const uint8_t* c, uchar4* out,
                               long long n, int sms, cudaStream_t st);
+// The same with the insertion, deletion and continuation qualities constant.
+cudaError_t launch_pack_quals_uniform(const uint8_t* q, uint8_t gi, uint8_t gd, uint8_t gc, uchar4* out, long long n,
+                                      int sms, cudaStream_t st);
 
 // Writes one 64-bit value on the device (graph-capturable).
 cudaError_t launch_set_u64(unsigned long long* dst, unsigned long long v, cudaStream_t st);

@@ -113,6 +113,7 @@ class RegionBatchC(C.Structure):
         ("read_bases", C.c_void_p), ("read_q", C.c_void_p), ("read_i", C.c_void_p), ("read_d", C.c_void_p),
         ("read_c", C.c_void_p),
         ("num_haps", C.c_int64), ("hap_offsets", C.c_void_p), ("hap_bases", C.c_void_p),
+        ("gap_ins", C.c_uint8), ("gap_del", C.c_uint8), ("gap_gcp", C.c_uint8), ("reserved_", C.c_uint8 * 5),
     ]
 
 
@@ -176,6 +177,8 @@ def load() -> C.CDLL:
         "bv_phmm_debug_jacobian_table": (C.c_int, [V, C.c_int]),
         "bv_phmm_debug_chunks": (C.c_int64, [P(RegionBatchC), C.c_int32, V, C.c_int64]),
         "bv_phmm_get_transitions": (C.c_int, [V, P(C.c_double)]),
+        "bv_phmm_plan_partition": (C.c_int64, [P(RegionBatchC), C.c_int32, C.c_int32, V, V, V]),
+        "bv_phmm_compute_regions_multi": (C.c_int, [P(V), C.c_int32, P(RegionBatchC), V, P(Stats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -18,7 +18,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import math
-from typing import List, Optional, Sequence
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -44,18 +44,27 @@ def _ptr(a: np.ndarray) -> int:
 
 
 class _BatchView:
-    """Keeps the numpy arrays of a RegionBatch alive behind a C struct."""
+    """Keeps the numpy arrays of a RegionBatch alive behind a C struct.
 
-    def __init__(self, b: RegionBatch):
+    With ``uniform_gaps`` = (insertion, deletion, continuation) Phred values
+    the per-base i, d and c arrays are not passed (NULL): every read base
+    takes those values and only bases and base qualities are copied."""
+
+    def __init__(self, b: RegionBatch, uniform_gaps: Optional[Tuple[int, int, int]] = None):
         self.b = b
         self.arrs = [np.ascontiguousarray(x) for x in (
             b.region_reads.astype(np.int64), b.region_haps.astype(np.int64), b.read_offsets.astype(np.int64),
             b.read_bases, b.read_q, b.read_i, b.read_d, b.read_c, b.hap_offsets.astype(np.int64), b.hap_bases)]
         rr, rh, ro, rb, rq, ri, rd, rc, ho, hb = self.arrs
+        gi = gd = gc = 0
+        if uniform_gaps is not None:
+            gi, gd, gc = (int(x) for x in uniform_gaps)
+            ri = rd = rc = np.zeros(0, np.uint8)  # NULL pointers
         self.c = N.RegionBatchC(
             num_regions=b.n_regions, region_reads=_ptr(rr), region_haps=_ptr(rh),
             num_reads=b.n_reads, read_offsets=_ptr(ro), read_bases=_ptr(rb), read_q=_ptr(rq), read_i=_ptr(ri),
-            read_d=_ptr(rd), read_c=_ptr(rc), num_haps=b.n_haps, hap_offsets=_ptr(ho), hap_bases=_ptr(hb))
+            read_d=_ptr(rd), read_c=_ptr(rc), num_haps=b.n_haps, hap_offsets=_ptr(ho), hap_bases=_ptr(hb),
+            gap_ins=gi, gap_del=gd, gap_gcp=gc)
 
 
 class PairHMMEngine:
@@ -104,8 +113,12 @@ class PairHMMEngine:
             raise N.NativeError(st, (msg or b"").decode())
 
     # --- batched entry points ---------------------------------------------
-    def compute_regions(self, batch: RegionBatch, out: Optional[np.ndarray] = None, with_stats: bool = False):
-        v = _BatchView(batch)
+    def compute_regions(self, batch: RegionBatch, out: Optional[np.ndarray] = None, with_stats: bool = False,
+                        uniform_gaps: Optional[Tuple[int, int, int]] = None):
+        """Scores every region of the batch (bv_phmm_compute_regions).  With
+        ``uniform_gaps`` = (ins, del, gcp) the batch's per-base gap arrays are
+        replaced by those constants (see _BatchView)."""
+        v = _BatchView(batch, uniform_gaps)
         n = int(self.lib.bv_phmm_region_results(C.byref(v.c)))
         if out is None:
             out = np.empty(max(n, 1), np.float64)
@@ -115,8 +128,8 @@ class PairHMMEngine:
         res = out[:n]
         return (res, st.as_dict()) if with_stats else res
 
-    def stage(self, batch: RegionBatch) -> int:
-        v = _BatchView(batch)
+    def stage(self, batch: RegionBatch, uniform_gaps: Optional[Tuple[int, int, int]] = None) -> int:
+        v = _BatchView(batch, uniform_gaps)
         self._check(self.lib.bv_phmm_stage_regions(self.h, C.byref(v.c)))
         self._staged = v
         self._staged_n = int(self.lib.bv_phmm_region_results(C.byref(v.c)))
@@ -316,6 +329,48 @@ class PairHMMEngine:
         return res[: len(reads) * len(haps)].reshape(len(reads), len(haps))
 
 
+def plan_partition(batch: RegionBatch, n_parts: int, n_blocks: Optional[int] = None):
+    """The split of ``batch`` over ``n_parts`` devices (bv_phmm_plan_partition):
+    contiguous region blocks of about equal DP cells dealt by greedy LPT.
+    Returns (block_start [n_blocks + 1], block_part [n_blocks], part_cells
+    [n_parts]); ``n_blocks`` defaults to one block per region."""
+    lib = N.load()
+    v = _BatchView(batch)
+    nb = max(1, batch.n_regions if n_blocks is None else int(n_blocks))
+    bs = np.zeros(nb + 1, np.int64)
+    bp = np.zeros(nb, np.int32)
+    pc = np.zeros(n_parts, np.int64)
+    got = int(lib.bv_phmm_plan_partition(C.byref(v.c), n_parts, nb, _ptr(bs), _ptr(bp), _ptr(pc)))
+    if got < 0:
+        raise ValueError("invalid batch or part count")
+    return bs[:got + 1], bp[:got], pc
+
+
+def regions_of_part(block_start: np.ndarray, block_part: np.ndarray, part: int) -> np.ndarray:
+    """The regions one part scores, in region order."""
+    return np.concatenate([np.arange(block_start[b], block_start[b + 1]) for b in range(len(block_part))
+                           if block_part[b] == part] or [np.zeros(0, np.int64)]).astype(np.int64)
+
+
+def compute_regions_multi(engines: Sequence["PairHMMEngine"], batch: RegionBatch,
+                          out: Optional[np.ndarray] = None, with_stats: bool = False,
+                          uniform_gaps: Optional[Tuple[int, int, int]] = None):
+    """Scores one batch over several engines (one per GPU) with the LPT split
+    of bv_phmm_compute_regions_multi; results in region order."""
+    lib = N.load()
+    v = _BatchView(batch, uniform_gaps)
+    n = int(lib.bv_phmm_region_results(C.byref(v.c)))
+    if out is None:
+        out = np.empty(max(n, 1), np.float64)
+    hs = (C.c_void_p * len(engines))(*[e.h for e in engines])
+    st = N.Stats()
+    status = lib.bv_phmm_compute_regions_multi(hs, len(engines), C.byref(v.c), _ptr(out), C.byref(st))
+    if status != N.BV_OK:
+        msgs = "; ".join((lib.bv_phmm_last_error(e.h) or b"").decode() for e in engines)
+        raise N.NativeError(status, msgs)
+    return (out[:n], st.as_dict()) if with_stats else out[:n]
+
+
 # --- reference-shaped objects ------------------------------------------------
 class Haplotype:
     """The field of ``biovoltron::Haplotype`` the PairHMM reads (haplotype.hpp:12)."""
@@ -380,6 +435,42 @@ def filter_poorly_modeled_reads(reads: list, ll: List[List[float]]) -> None:
 ORIGINAL_DEFAULT = (0.9998, 0.0001, 0.0001, 0.9, 0.1, 0.9, 0.1)  # pairhmm.hpp:32-33
 
 
+def _windows_batch(windows: Sequence[tuple], scalar: bool):
+    """One region per (haplotypes, reads) window, as bv_phmm_compute_regions
+    takes them, and the uniform gap penalties to pass instead of the per-base
+    arrays when every read's three penalty views hold one byte throughout
+    (SamRecord fills them from constant strings); the scalar model reads no
+    gap bytes at all."""
+    rb, rq, ri, rd, rc, hb = [], [], [], [], [], []
+    nreads, nhaps = [], []
+    for haps, reads in windows:
+        for r in reads:
+            q = np.frombuffer(r.qual, np.uint8)
+            rb.append(np.frombuffer(r.seq, np.uint8))
+            rq.append(q)
+            ri.append(q if scalar else np.frombuffer(r.insertion_gop(), np.uint8))
+            rd.append(q if scalar else np.frombuffer(r.deletion_gop(), np.uint8))
+            rc.append(q if scalar else np.frombuffer(r.overall_gcp(), np.uint8))
+        hb.extend(np.frombuffer(h.seq, np.uint8) for h in haps)
+        nreads.append(len(reads))
+        nhaps.append(len(haps))
+
+    def cat(parts):
+        if not parts:
+            return np.zeros(0, np.uint8), np.zeros(1, np.int64)
+        lens = np.array([len(p) for p in parts], np.int64)
+        return np.concatenate(parts).astype(np.uint8), np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+
+    read_bases, read_off = cat(rb)
+    batch = RegionBatch(read_bases=read_bases, read_q=cat(rq)[0], read_i=cat(ri)[0], read_d=cat(rd)[0],
+                        read_c=cat(rc)[0], read_offsets=read_off, hap_bases=cat(hb)[0], hap_offsets=cat(hb)[1],
+                        region_reads=np.concatenate([[0], np.cumsum(nreads)]).astype(np.int64),
+                        region_haps=np.concatenate([[0], np.cumsum(nhaps)]).astype(np.int64),
+                        name="windows")
+    uniform = (0, 0, 0) if scalar else batch.uniform_gaps()
+    return batch, uniform
+
+
 class GpuScalarPairHMM:
     """Drop-in for the scalar ``biovoltron::PairHMM`` (pairhmm.hpp:14-141) on
     one GPU: constant transitions, the base qualities' emission prior, then
@@ -395,8 +486,8 @@ class GpuScalarPairHMM:
             return []
         self.engine.set_transitions(trans)
         try:
-            tcs = [(r.seq, r.qual, r.qual, r.qual, r.qual, h.seq) for r in reads for h in haplotypes]
-            flat = self.engine.compute_testcases(tcs) if tcs else np.zeros(0)
+            batch, gaps = _windows_batch([(list(haplotypes), reads)], scalar=True)
+            flat = self.engine.compute_regions(batch, uniform_gaps=gaps) if nh else np.zeros(0)
         finally:
             self.engine.set_transitions(None)
         ll = [list(map(float, flat[k * nh:(k + 1) * nh])) for k in range(nr)]
@@ -417,12 +508,9 @@ class GpuPairHMM:
         nr, nh = len(reads), len(haplotypes)
         if nr == 0:
             return []
-        tcs = []
-        for r in reads:
-            ins, dele, gcp = r.insertion_gop(), r.deletion_gop(), r.overall_gcp()
-            for h in haplotypes:
-                tcs.append((r.seq, r.qual, ins, dele, gcp, h.seq))
-        flat = self.engine.compute_testcases(tcs) if tcs else np.zeros(0)
+        # the window is one region: each haplotype crosses to the device once
+        batch, gaps = _windows_batch([(list(haplotypes), reads)], scalar=False)
+        flat = self.engine.compute_regions(batch, uniform_gaps=gaps) if nh else np.zeros(0)
         ll = [list(map(float, flat[k * nh:(k + 1) * nh])) for k in range(nr)]
         if nh == 0:
             return ll
@@ -464,36 +552,11 @@ class RegionBatcher:
         if not self._queue:
             return
         scalar = self.model == "scalar"
-        rb, rq, ri, rd, rc, hb = [], [], [], [], [], []
-        nreads, nhaps = [], []
-        for haps, reads in self._queue:
-            for r in reads:
-                q = np.frombuffer(r.qual, np.uint8)
-                rb.append(np.frombuffer(r.seq, np.uint8))
-                rq.append(q)
-                ri.append(q if scalar else np.frombuffer(r.insertion_gop(), np.uint8))
-                rd.append(q if scalar else np.frombuffer(r.deletion_gop(), np.uint8))
-                rc.append(q if scalar else np.frombuffer(r.overall_gcp(), np.uint8))
-            hb.extend(np.frombuffer(h.seq, np.uint8) for h in haps)
-            nreads.append(len(reads))
-            nhaps.append(len(haps))
-
-        def cat(parts):
-            if not parts:
-                return np.zeros(0, np.uint8), np.zeros(1, np.int64)
-            lens = np.array([len(p) for p in parts], np.int64)
-            return np.concatenate(parts).astype(np.uint8), np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
-
-        read_bases, read_off = cat(rb)
-        batch = RegionBatch(read_bases=read_bases, read_q=cat(rq)[0], read_i=cat(ri)[0], read_d=cat(rd)[0],
-                            read_c=cat(rc)[0], read_offsets=read_off, hap_bases=cat(hb)[0], hap_offsets=cat(hb)[1],
-                            region_reads=np.concatenate([[0], np.cumsum(nreads)]).astype(np.int64),
-                            region_haps=np.concatenate([[0], np.cumsum(nhaps)]).astype(np.int64),
-                            name="queued windows")
+        batch, gaps = _windows_batch(self._queue, scalar)
         if scalar:
             self.engine.set_transitions(self.trans)
         try:
-            flat = self.engine.compute_regions(batch)
+            flat = self.engine.compute_regions(batch, uniform_gaps=gaps)
         finally:
             if scalar:
                 self.engine.set_transitions(None)

@@ -8,13 +8,21 @@ process drives one GPU and scores its own regions.  The only collectives are
 scalar reductions of the per-rank counts and times (sum of pairs, max of
 times) and barriers around the timed region, taken by every rank in the same
 order.
+
+One batch held by every rank is split with ``split_batch``: the same greedy
+LPT partition the library's multi-device call uses (bv_phmm_plan_partition,
+one region per block), so every rank computes the same plan without talking
+to the others; ``gather_results`` puts the ranks' results back in region
+order (one all-gather, after the scoring).
 """
 from __future__ import annotations
 
 import datetime
 import os
 from dataclasses import dataclass
-from typing import Optional, Sequence
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
 
 
 @dataclass
@@ -77,3 +85,31 @@ def aggregate(rep: Replicas, pairs: float, seconds: Sequence[float]) -> dict:
     total = rep.allreduce(pairs, "sum")
     t = rep.allreduce(float(sum(seconds)), "max")
     return {"pairs": total, "seconds": t, "pairs_per_s": total / t if t > 0 else 0.0}
+
+
+def split_batch(rep: Replicas, batch) -> Tuple[object, np.ndarray]:
+    """This rank's share of ``batch`` (regions dealt by greedy LPT on their DP
+    cells, in region order) and the batch-wide result slots of the share's
+    results, in the share's result order."""
+    from .pairhmm import plan_partition, regions_of_part
+    from .workloads import subsample_regions
+    bs, bp, _ = plan_partition(batch, rep.world)
+    regions = regions_of_part(bs, bp, rep.rank)
+    offs = batch.result_offsets()
+    slots = np.concatenate([np.arange(offs[g], offs[g + 1]) for g in regions] or [np.zeros(0, np.int64)])
+    return subsample_regions(batch, regions.tolist()), slots.astype(np.int64)
+
+
+def gather_results(rep: Replicas, local: np.ndarray, slots: np.ndarray, n_total: int) -> np.ndarray:
+    """Every rank's results at their batch-wide slots: the whole batch's
+    result array, on every rank."""
+    out = np.full(n_total, np.nan, np.float64)
+    if rep.backend is None:
+        out[slots] = local
+        return out
+    import torch.distributed as dist
+    parts = [None] * rep.world
+    dist.all_gather_object(parts, (np.asarray(slots, np.int64), np.asarray(local, np.float64)))
+    for sl, val in parts:
+        out[sl] = val
+    return out

@@ -125,6 +125,20 @@ class RegionBatch:
             )
         )
 
+    def uniform_gaps(self) -> Optional[Tuple[int, int, int]]:
+        """(i, d, c) when every read base has the same insertion, deletion and
+        continuation quality (then the batch can be passed without those
+        arrays), else None."""
+        if self.read_i.size == 0:
+            return None
+        vals = []
+        for a in (self.read_i, self.read_d, self.read_c):
+            v = int(a[0])
+            if not np.all(a == v):
+                return None
+            vals.append(v)
+        return tuple(vals)
+
     # ---- accessors ---------------------------------------------------------
     def read(self, k: int) -> Tuple[bytes, bytes, bytes, bytes, bytes]:
         a, b = int(self.read_offsets[k]), int(self.read_offsets[k + 1])

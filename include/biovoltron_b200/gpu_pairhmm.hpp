@@ -5,9 +5,10 @@
 // AvxPairHMM::compute_likelihoods (include/biovoltron/algo/align/
 // inexact_match/pairhmm_avx.hpp:160-171), which HaplotypeCaller calls through
 // PairHMM::compute_likelihoods (haplotypecaller.hpp:90):
-//   1. testcases are built as AvxPairHMM::getData builds them (:38-81): read
-//      bases, qual, insertion_gop(), deletion_gop(), overall_gcp() and each
-//      haplotype's seq, borrowed for the call;
+//   1. the inputs are those AvxPairHMM::getData gathers (:38-81): read bases,
+//      qual, insertion_gop(), deletion_gop(), overall_gcp() and each
+//      haplotype's seq; the window goes to the device as one region (each
+//      haplotype once, constant penalty views as three bytes);
 //   2. log10 likelihoods come from the GPU (FP32, FP64 below 1e-28);
 //   3. PairHMM::normalize_likelihoods (pairhmm.hpp:83-93) caps every value at
 //      the row's best - 4.5;
@@ -93,34 +94,71 @@ class GpuPairHMM {
 
  protected:
   // Scores every read against every haplotype into ll (no normalising or
-  // filtering); `scalar` takes only the base qualities (constant transitions).
+  // filtering); `scalar` takes only the base qualities (constant
+  // transitions).  The window is one region of bv_phmm_compute_regions, so
+  // each haplotype crosses to the device once; when every read's three
+  // penalty views hold one and the same byte (SamRecord fills them from
+  // constant strings) they go as the batch's uniform gap penalties instead of
+  // per-base arrays.
   template <class HapVec, class ReadVec>
   void score(const HapVec& haplotypes, const ReadVec& reads, bool scalar, std::vector<std::vector<double>>& ll) {
     const size_t nr = reads.size(), nh = haplotypes.size();
-    std::vector<bv_testcase> tcs;
-    tcs.reserve(nr * nh);
-    for (const auto& r : reads) {
-      const int len = static_cast<int>(r.seq.size());
-      const char* q = r.qual.data();
-      const char* ins = scalar ? q : r.insertion_gop().data();
-      const char* del = scalar ? q : r.deletion_gop().data();
-      const char* gcp = scalar ? q : r.overall_gcp().data();
-      for (const auto& h : haplotypes) {
-        bv_testcase t{};
-        t.rslen = len;
-        t.haplen = static_cast<int>(h.seq.size());
-        t.q = q;
-        t.i = ins;
-        t.d = del;
-        t.c = gcp;
-        t.hap = h.seq.data();
-        t.rs = r.seq.data();
-        tcs.push_back(t);
+    std::vector<int64_t> region_reads{0, static_cast<int64_t>(nr)}, region_haps{0, static_cast<int64_t>(nh)};
+    std::vector<int64_t> read_off{0}, hap_off{0};
+    std::string rb, rq, ri, rd, rc, hb;
+    int gap[3] = {-1, -1, -1};
+    bool uniform = true;
+    if (!scalar) {
+      for (const auto& r : reads) {
+        const size_t n = r.seq.size();
+        const char* v[3] = {r.insertion_gop().data(), r.deletion_gop().data(), r.overall_gcp().data()};
+        for (int k = 0; k < 3 && uniform; ++k)
+          for (size_t x = 0; x < n && uniform; ++x) {
+            const int b = static_cast<unsigned char>(v[k][x]);
+            if (gap[k] < 0) gap[k] = b;
+            uniform = b == gap[k];
+          }
+        if (!uniform) break;
       }
     }
+    for (const auto& r : reads) {
+      rb.append(r.seq.data(), r.seq.size());
+      rq.append(r.qual.data(), r.qual.size());
+      if (!scalar && !uniform) {
+        ri.append(r.insertion_gop().data(), r.seq.size());
+        rd.append(r.deletion_gop().data(), r.seq.size());
+        rc.append(r.overall_gcp().data(), r.seq.size());
+      }
+      read_off.push_back(static_cast<int64_t>(rb.size()));
+    }
+    for (const auto& h : haplotypes) {
+      hb.append(h.seq.data(), h.seq.size());
+      hap_off.push_back(static_cast<int64_t>(hb.size()));
+    }
+    auto u8 = [](const std::string& x) { return reinterpret_cast<const uint8_t*>(x.data()); };
+    bv_region_batch b{};
+    b.num_regions = 1;
+    b.region_reads = region_reads.data();
+    b.region_haps = region_haps.data();
+    b.num_reads = static_cast<int64_t>(nr);
+    b.read_offsets = read_off.data();
+    b.read_bases = u8(rb);
+    b.read_q = u8(rq);
+    if (scalar || uniform) {
+      // the scalar model's transitions are constant; its gap bytes are unused
+      b.gap_ins = static_cast<uint8_t>(gap[0] < 0 ? 0 : gap[0]);
+      b.gap_del = static_cast<uint8_t>(gap[1] < 0 ? 0 : gap[1]);
+      b.gap_gcp = static_cast<uint8_t>(gap[2] < 0 ? 0 : gap[2]);
+    } else {
+      b.read_i = u8(ri);
+      b.read_d = u8(rd);
+      b.read_c = u8(rc);
+    }
+    b.num_haps = static_cast<int64_t>(nh);
+    b.hap_offsets = hap_off.data();
+    b.hap_bases = u8(hb);
     std::vector<double> flat(nr * nh);
-    check(bv_phmm_compute_testcases(ctx_, tcs.data(), static_cast<int64_t>(tcs.size()), flat.data(), nullptr),
-          "bv_phmm_compute_testcases");
+    check(bv_phmm_compute_regions(ctx_, &b, flat.data(), nullptr), "bv_phmm_compute_regions");
     for (size_t r = 0; r < nr; ++r)
       std::copy(flat.begin() + r * nh, flat.begin() + (r + 1) * nh, ll[r].begin());
   }
@@ -198,15 +236,27 @@ class RegionBatcher {
     if (queue_.empty()) return;
     std::vector<int64_t> region_reads{0}, region_haps{0}, read_off{0}, hap_off{0};
     std::string rb, rq, ri, rd, rc, hb;
+    // penalty views that hold one byte throughout go as uniform gap penalties
+    // (the scalar model does not read them at all)
+    int gap[3] = {-1, -1, -1};
+    bool uniform = true;
+    for (const auto& w : queue_) {
+      for (const auto& r : *w.reads) {
+        if (scalar_ || !uniform) break;
+        const char* v[3] = {r.insertion_gop().data(), r.deletion_gop().data(), r.overall_gcp().data()};
+        for (int k = 0; k < 3 && uniform; ++k)
+          for (size_t x = 0; x < r.seq.size() && uniform; ++x) {
+            const int b = static_cast<unsigned char>(v[k][x]);
+            if (gap[k] < 0) gap[k] = b;
+            uniform = b == gap[k];
+          }
+      }
+    }
     for (const auto& w : queue_) {
       for (const auto& r : *w.reads) {
         rb.append(r.seq.data(), r.seq.size());
         rq.append(r.qual.data(), r.qual.size());
-        if (scalar_) {
-          ri.append(r.qual.data(), r.qual.size());
-          rd.append(r.qual.data(), r.qual.size());
-          rc.append(r.qual.data(), r.qual.size());
-        } else {
+        if (!scalar_ && !uniform) {
           ri.append(r.insertion_gop().data(), r.seq.size());
           rd.append(r.deletion_gop().data(), r.seq.size());
           rc.append(r.overall_gcp().data(), r.seq.size());
@@ -229,9 +279,15 @@ class RegionBatcher {
     b.read_offsets = read_off.data();
     b.read_bases = u8(rb);
     b.read_q = u8(rq);
-    b.read_i = u8(ri);
-    b.read_d = u8(rd);
-    b.read_c = u8(rc);
+    if (scalar_ || uniform) {
+      b.gap_ins = static_cast<uint8_t>(gap[0] < 0 ? 0 : gap[0]);
+      b.gap_del = static_cast<uint8_t>(gap[1] < 0 ? 0 : gap[1]);
+      b.gap_gcp = static_cast<uint8_t>(gap[2] < 0 ? 0 : gap[2]);
+    } else {
+      b.read_i = u8(ri);
+      b.read_d = u8(rd);
+      b.read_c = u8(rc);
+    }
     b.num_haps = static_cast<int64_t>(hap_off.size() - 1);
     b.hap_offsets = hap_off.data();
     b.hap_bases = u8(hb);

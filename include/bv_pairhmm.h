@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define BV_PHMM_ABI_VERSION 2
+#define BV_PHMM_ABI_VERSION 3
 
 typedef enum bv_status {
   BV_OK = 0,
@@ -213,6 +213,18 @@ typedef struct bv_region_batch {
   int64_t num_haps;
   const int64_t* hap_offsets; /* [num_haps + 1] */
   const uint8_t* hap_bases;
+  /* Uniform gap penalties.  When read_i, read_d and read_c are all NULL,
+   * every read base takes these Phred values (insertion open, deletion open,
+   * gap continuation), and only bases and base qualities are copied to the
+   * device: 2 bytes per read base instead of 5.  Biovoltron's SamRecord fills
+   * its insertion/deletion GOP and GCP views from one constant string each
+   * (include/biovoltron/file_io/sam.hpp:19-31, 451-475), so a caller holding
+   * SamRecords passes those constants here.  Ignored when the per-base arrays
+   * are given; giving some of them but not all three is an error. */
+  uint8_t gap_ins;
+  uint8_t gap_del;
+  uint8_t gap_gcp;
+  uint8_t reserved_[5];
 } bv_region_batch;
 
 /* Number of result slots the batch produces (sum over regions of reads*haps). */
@@ -220,6 +232,30 @@ int64_t bv_phmm_region_results(const bv_region_batch* batch);
 
 bv_status bv_phmm_compute_regions(bv_phmm_ctx* ctx, const bv_region_batch* batch, double* out_log10,
                                   bv_phmm_stats* stats);
+
+/* --- one batch over several GPUs (no counterpart in the reference, whose
+ * AvxPairHMM parallelises over reads with OpenMP, pairhmm_avx.hpp:133-135) --
+ * Regions are independent, so the batch is split with no exchange between
+ * devices: its regions are cut into contiguous blocks of about equal DP cells
+ * (sum over a block's regions of read bases x haplotype bases, at most 16
+ * blocks per context) and the blocks are dealt to the contexts by greedy LPT
+ * -- the largest block first, each to the context with the fewest cells so
+ * far (lower index on ties).  Each context scores its blocks with
+ * bv_phmm_compute_regions on views of the caller's arrays, one host thread
+ * per context; results land in region order, as one context writes them.
+ * The contexts must be distinct (one per GPU, or several on one GPU) and are
+ * used with their own options: give them the same band options and weights.
+ * Returns the first failing context's status. */
+bv_status bv_phmm_compute_regions_multi(bv_phmm_ctx* const* ctxs, int32_t num_ctx, const bv_region_batch* batch,
+                                        double* out_log10, bv_phmm_stats* stats);
+/* The partition bv_phmm_compute_regions_multi uses, for num_parts devices and
+ * at most num_blocks blocks (host only, no device): block b holds regions
+ * [block_start[b], block_start[b+1]) (num_blocks+1 entries at most) and goes
+ * to part block_part[b]; part_cells[p] is the cells part p gets.  Returns the
+ * number of blocks, or -1 for an invalid batch or count.  Any output may be
+ * NULL. */
+int64_t bv_phmm_plan_partition(const bv_region_batch* batch, int32_t num_parts, int32_t num_blocks,
+                               int64_t* block_start, int32_t* block_part, int64_t* part_cells);
 
 /* Device-resident form of the same computation, for callers that score one
  * batch repeatedly: stage copies the batch into context-owned device memory;

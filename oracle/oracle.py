@@ -328,3 +328,73 @@ def seed_extent(read: bytes, hap: bytes, k: int = 11):
         if head <= END_ROWS:
             hi = max(hi, d + head)
     return lo, hi
+
+
+def _bf16(x: np.ndarray) -> np.ndarray:
+    """Round FP32 values to BF16 (round to nearest even), returned as FP32."""
+    b = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def _onehot(c: int) -> int:
+    # the banded kernels' match nibble: N matches everything, other unknown bytes read as A
+    return {ord("C"): 2, ord("T"): 4, ord("G"): 8, ord("N"): 15}.get(c, 1)
+
+
+HIST_BINS = 64
+
+
+def seed_features(read: bytes, hap: bytes, k: int = 11) -> np.ndarray:
+    """The 80 MLP inputs of a pair (BF16 values as FP32), zeros without a
+    shared k-mer: 64 bins of the sampled-hit histogram over diagonals
+    d* - 32 .. d* + 31, each divided by the number of sampled read positions,
+    and 16 scalars -- hits, hits outside the window, read length / 256,
+    haplotype length / 1024, (d* + R) / (R + H), 1, the mode's hits, the
+    window's non-empty bins / 64, t_pre / 32, t_suf / 32, the first and last
+    hit's diagonal relative to d* / 32, the mismatches of the first and last
+    16 read bases along those diagonals / 16, and the lowest and highest hit
+    diagonal relative to d* / 32 clipped to [-2, 2].  FP32 arithmetic in the
+    kernel's order, then BF16 rounding."""
+    f = np.zeros(80, np.float32)
+    R, H = len(read), len(hap)
+    if R < k or H < k:
+        return f
+    hits = _seed_hits(read, hap, k)
+    if not hits:
+        return f
+    n_samp = len(_sample_positions(R, k))
+    inv = np.float32(1.0) / np.float32(n_samp)
+    counts = {}
+    for _, d in hits:
+        counts[d + R] = counts.get(d + R, 0) + 1
+    best = max(counts.values())
+    best_slot = min(s for s, c in counts.items() if c == best)
+    ds = best_slot - R
+    i0 = min(i for i, _ in hits)
+    i1 = max(i for i, _ in hits)
+    d_first = min(d for i, d in hits if i == i0)
+    d_last = min(d for i, d in hits if i == i1)
+    t_pre, t_suf = i0, R - k - i1
+    n_end = min(16, R)
+    mis_pre = sum(1 for ip in range(n_end)
+                  if not (0 <= ip + d_first < H) or not (_onehot(read[ip]) & _onehot(hap[ip + d_first])))
+    mis_suf = sum(1 for l in range(n_end)
+                  if not (0 <= R - 1 - l + d_last < H) or not (_onehot(read[R - 1 - l]) & _onehot(hap[R - 1 - l + d_last])))
+    win = nonzero = peak = 0
+    for t in range(HIST_BINS):
+        s = best_slot - HIST_BINS // 2 + t
+        cb = counts.get(s, 0) if 0 <= s < R + H else 0
+        f[t] = np.float32(cb) * inv
+        win += cb
+        nonzero += cb > 0
+        peak = max(peak, cb)
+    total = len(hits)
+    smin, smax = min(counts), max(counts)
+    F = np.float32
+    v = [F(total) * inv, F(total - win) * inv, F(R) / F(256), F(H) / F(1024), F(ds + R) / F(R + H), F(1),
+         F(peak) * inv, F(nonzero) / F(HIST_BINS), F(t_pre) / F(32), F(t_suf) / F(32), F(d_first - ds) / F(32),
+         F(d_last - ds) / F(32), F(mis_pre) / F(16), F(mis_suf) / F(16),
+         max(F(smin - R - ds) / F(32), F(-2)), min(F(smax - R - ds) / F(32), F(2))]
+    f[HIST_BINS:] = np.array(v, np.float32)
+    return _bf16(f)

@@ -43,7 +43,7 @@ def test_default_options_and_abi():
     assert o.struct_size == C.sizeof(N.Options)
     assert o.rescue_threshold == 1e-28
     assert o.precision == N.BV_PRECISION_AUTO and o.mode == N.BV_MODE_FULL
-    assert lib.bv_phmm_abi_version() == 2
+    assert lib.bv_phmm_abi_version() == 3
     assert lib.bv_phmm_status_string(N.BV_ERR_INVALID_ARG) == b"invalid argument"
 
 

@@ -98,3 +98,44 @@ def test_band_staged_replay_is_deterministic():
             st = e.run()
             assert st["band_pairs"] > 0
             assert np.array_equal(e.fetch(n), direct)
+
+
+def _repeat_pairs(seed):
+    """Pairs whose sampled 11-mers vote for many diagonals: haplotypes made of
+    a repeated unit (period 40 and 25), reads cut from them with a few
+    substitutions; the thread featuriser hands these to the warp featuriser."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for period, copies, n in ((40, 10, 150), (25, 16, 120), (40, 6, 90)):
+        unit = W._random_seq(rng, period)
+        hap = np.tile(unit, copies)
+        hap = W._substitute(rng, hap, 0.005)
+        start = int(rng.integers(0, len(hap) - n))
+        read = W._substitute(rng, hap[start:start + n], 0.01)
+        q = rng.integers(10, 41, size=n).astype(np.uint8)
+        out.append((bytes(read), bytes(q), bytes([45]) * n, bytes([45]) * n, bytes([10]) * n, bytes(hap)))
+    return W.from_pairs(out, "repeats")
+
+
+def test_features_match_oracle_restatement():
+    """Every pair's 80 MLP inputs, seed diagonal and voted extent equal the
+    oracle's restatement of the featuriser bit for bit: config-1- and
+    config-4-shaped regions (thread per pair) and repeat-rich pairs (the warp
+    featuriser's list)."""
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    from oracle.oracle import seed_features
+    batches = [W.config1(seed=43, n_regions=3), W.config4(seed=7, n_regions=3), _repeat_pairs(3)]
+    for b in batches:
+        with PairHMMEngine(device=0) as e:
+            ds, _, _, feat, km, kx = e.band_labels(b, tau=1e-4, features=True, extent=True)
+        r, h = b.pair_index()
+        for k in range(b.n_pairs):
+            rd, hp = b.read(int(r[k]))[0], b.hap(int(h[k]))
+            exp_ds = seed_diagonal(rd, hp)
+            assert ds[k] == (np.iinfo(np.int32).min if exp_ds is None else exp_ds), (b.name, k)
+            if exp_ds is not None and len(rd) <= 511:
+                assert (km[k], kx[k]) == seed_extent(rd, hp), (b.name, k)
+            if len(rd) <= 511 and len(hp) <= 1024:
+                f = seed_features(rd, hp)
+                assert np.array_equal(feat[k], f), (b.name, k, np.nonzero(feat[k] != f)[0], feat[k][feat[k] != f],
+                                                    f[feat[k] != f])

@@ -379,3 +379,64 @@ def test_device_genotyper_equals_reference_steps(band):
         al_off += nr[g] * A[g]
         ge_off += A[g] * (A[g] + 1) // 2
     assert out["kernel_ms"] > 0
+
+
+def test_uniform_gap_penalties_equal_per_base_arrays():
+    """A batch passed without its i, d, c arrays (uniform gap penalties, the
+    way SamRecord's constant views are sent) scores exactly as with the
+    per-base arrays: full DP, band mode, and the chunked call over two
+    contexts; giving only some of the three arrays is rejected."""
+    import ctypes as C
+    from biovoltron_b200.native import NativeError
+    from biovoltron_b200.pairhmm import PairHMMEngine, _BatchView
+    b = W.config4(seed=5, n_regions=40)
+    g = b.uniform_gaps()
+    assert g == (45, 45, 10)
+    with PairHMMEngine() as e:
+        want = e.compute_regions(b)
+        assert np.array_equal(e.compute_regions(b, uniform_gaps=g), want)
+        n = e.stage(b, uniform_gaps=g)
+        e.run()
+        assert np.array_equal(e.fetch(n), want)
+        e.set_band_options(fixed_half=8, margin=2)
+        band = e.compute_regions(b)
+        assert np.array_equal(e.compute_regions(b, uniform_gaps=g), band)
+        v = _BatchView(b)
+        v.c.read_d = None
+        out = np.empty(n, np.float64)
+        assert e.lib.bv_phmm_compute_regions(e.h, C.byref(v.c), out.ctypes.data, None) == 1
+    with PairHMMEngine(pipeline_chunks=3, pipeline_min_pairs=1) as e:
+        assert np.array_equal(e.compute_regions(b, uniform_gaps=g), want)
+        e.set_band_options(fixed_half=8, margin=2)
+        assert np.array_equal(e.compute_regions(b, uniform_gaps=g), band)
+    # a batch whose gap bytes differ per base is not uniform
+    c1 = W.config0(0)
+    c1.read_i = c1.read_i.copy()
+    c1.read_i[3] = 40
+    assert c1.uniform_gaps() is None
+
+
+def test_multi_context_split_equals_one_context():
+    """bv_phmm_compute_regions_multi over three contexts (on one GPU here; one
+    per GPU in use) returns the single-context results in region order, in
+    full-DP and band mode, and refuses a context given twice."""
+    from biovoltron_b200.native import NativeError
+    from biovoltron_b200.pairhmm import PairHMMEngine, compute_regions_multi
+    b = W.config1(seed=51, n_regions=30)
+    with PairHMMEngine() as one:
+        want = one.compute_regions(b)
+        one.set_band_options(fixed_half=8, margin=2)
+        want_band = one.compute_regions(b)
+    engines = [PairHMMEngine() for _ in range(3)]
+    try:
+        got, st = compute_regions_multi(engines, b, with_stats=True)
+        assert np.array_equal(got, want)
+        assert st["pairs"] == b.n_pairs and st["cells"] == b.n_cells()
+        for e in engines:
+            e.set_band_options(fixed_half=8, margin=2)
+        assert np.array_equal(compute_regions_multi(engines, b, uniform_gaps=b.uniform_gaps()), want_band)
+        with pytest.raises(NativeError):
+            compute_regions_multi([engines[0], engines[0]], b)
+    finally:
+        for e in engines:
+            e.close()

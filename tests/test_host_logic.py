@@ -30,14 +30,20 @@ def test_filter_keeps_rows_below_threshold_like_the_reference():
 
 
 class _OracleEngine:
-    """Stand-in for PairHMMEngine that scores testcases with the CPU oracle."""
+    """Stand-in for PairHMMEngine that scores a region batch with the CPU
+    oracle; uniform gap penalties fill the per-base arrays as the library
+    does."""
 
     def __init__(self, oracle):
         self.oracle = oracle
+        self.calls = []
 
-    def compute_testcases(self, tcs):
-        b = W.from_pairs(tcs)
-        out, _ = self.oracle.log10_reference_rule(TestcaseArray.for_batch(b))
+    def compute_regions(self, batch, uniform_gaps=None):
+        self.calls.append((batch.n_regions, batch.n_haps, uniform_gaps))
+        if uniform_gaps is not None:
+            n = batch.read_bases.size
+            batch.read_i, batch.read_d, batch.read_c = (np.full(n, v, np.uint8) for v in uniform_gaps)
+        out, _ = self.oracle.log10_reference_rule(TestcaseArray.for_batch(batch))
         return out
 
 
@@ -64,6 +70,8 @@ def test_gpu_pairhmm_wrapper_semantics(oracle):
     filter_poorly_modeled_reads(exp_reads, raw)
     assert ll == raw
     assert [r.seq for r in reads] == [r.seq for r in exp_reads]
+    # one window is one region, each haplotype sent once, SAM's constant penalties as three bytes
+    assert w.engine.calls == [(1, 3, (73, 73, 43))]
 
 
 def test_sam_penalty_views_have_read_length():
@@ -176,9 +184,12 @@ class _OracleRegionEngine:
                          self.oracle.log10_rescaled(_tcs_array((rs, q, i, d, c, hap)))[0]
                          for rs, q, i, d, c, hap in tcs])
 
-    def compute_regions(self, batch):
+    def compute_regions(self, batch, uniform_gaps=None):
         self.calls += 1
         if self.trans is None:
+            if uniform_gaps is not None:  # the library fills every read base with the three values
+                n = batch.read_bases.size
+                batch.read_i, batch.read_d, batch.read_c = (np.full(n, v, np.uint8) for v in uniform_gaps)
             return self.oracle.log10_rescaled(TestcaseArray.for_batch(batch))
         r, h = batch.pair_index()
         ro, ho = batch.read_offsets, batch.hap_offsets
@@ -257,3 +268,50 @@ def test_scalar_drop_in_host_logic():
     filter_poorly_modeled_reads(er, exp)
     assert ll == exp and [id(r) for r in rr] == [id(r) for r in er]
     assert tuple(ORIGINAL_DEFAULT) == (0.9998, 0.0001, 0.0001, 0.9, 0.1, 0.9, 0.1)
+
+
+def _lpt_restatement(cells, n_parts):
+    """Greedy LPT on per-block cells: largest first (lower index on ties), to
+    the part with the fewest cells (lower index on ties)."""
+    order = sorted(range(len(cells)), key=lambda k: (-cells[k], k))
+    load = [0] * n_parts
+    part = [0] * len(cells)
+    for k in order:
+        p = min(range(n_parts), key=lambda q: (load[q], q))
+        part[k] = p
+        load[p] += cells[k]
+    return part, load
+
+
+@pytest.mark.parametrize("parts", [1, 2, 3, 8])
+def test_partition_is_greedy_lpt_over_region_cells(parts):
+    """bv_phmm_plan_partition with one block per region deals the regions by
+    greedy LPT on their DP cells; every region is in exactly one part and the
+    largest part exceeds the mean by less than the largest region."""
+    from biovoltron_b200.pairhmm import plan_partition, regions_of_part
+    b = W.config1(seed=21, n_regions=60)
+    bs, bp, pc = plan_partition(b, parts)
+    assert np.array_equal(bs, np.arange(b.n_regions + 1))
+    rl, hl = b.read_lengths(), b.hap_lengths()
+    cells = [int(rl[b.region_reads[g]:b.region_reads[g + 1]].sum()) * int(hl[b.region_haps[g]:b.region_haps[g + 1]].sum())
+             for g in range(b.n_regions)]
+    part, load = _lpt_restatement(cells, parts)
+    assert bp.tolist() == part and pc.tolist() == load
+    got = np.sort(np.concatenate([regions_of_part(bs, bp, p) for p in range(parts)]))
+    assert np.array_equal(got, np.arange(b.n_regions))
+    assert max(load) - sum(load) / parts < max(cells)
+
+
+def test_partition_blocks_are_contiguous_and_balanced():
+    """With fewer blocks than regions, blocks are contiguous runs of about
+    equal cells, dealt by LPT; bad arguments are refused."""
+    import ctypes as C
+    from biovoltron_b200.native import load
+    from biovoltron_b200.pairhmm import _BatchView, plan_partition
+    b = W.config4(seed=3, n_regions=400)
+    bs, bp, pc = plan_partition(b, 4, 64)
+    assert bs[0] == 0 and bs[-1] == b.n_regions and np.all(np.diff(bs) > 0)
+    assert len(bp) <= 64 and pc.sum() == b.n_cells()
+    assert pc.max() / pc.mean() < 1.1
+    v = _BatchView(b)
+    assert load().bv_phmm_plan_partition(C.byref(v.c), 0, 4, None, None, None) == -1
