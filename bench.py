@@ -25,7 +25,9 @@ full-DP kernels score the same batch in the same run for the comparison.
                page-locked host buffers: validation, planning, host->device
                copies, all kernels and the device->host copy of the results
                (the call splits the batch into region chunks over two
-               contexts so copies overlap kernels).
+               contexts so copies overlap kernels).  The workloads' gap
+               penalties are constant (as SamRecord's are), so they go as the
+               batch's three uniform gap bytes: 2 bytes cross per read base.
 * genotype     the device genotyper on the staged batch's matrix (normalise,
                filter, marginalise, diploid genotype likelihoods), outside
                the timed region.
@@ -41,7 +43,9 @@ full-DP kernels score the same batch in the same run for the comparison.
                the same regions.
 
 --impl reference times that CPU kernel alone, on the same workload.
---workload config0|config1|config2 --form plain|band run the other configs.
+--workload config0|config1|config2|config3 --form plain|band run the other configs
+(config3 = the learned band on config 1's workload, with the plain full DP of
+the same batch beside it and every pair's band-vs-full difference).
 Multi-GPU (torchrun): every rank scores its own batch (different seed) on its
 own GPU, no data-path collective (weak scaling); time is the max over ranks.
 """
@@ -78,7 +82,7 @@ def log(*a):
 
 
 def make_workload(name: str, seed: int, regions: int = 0) -> W.RegionBatch:
-    if name == "config1":
+    if name in ("config1", "config3"):  # config 3 is the learned band on config 1's workload
         return W.config1(seed=seed, n_regions=regions or 4096)
     if name == "config0":
         return W.config0(seed)
@@ -320,13 +324,15 @@ def main():
     ap.add_argument("--margin", type=int, default=2, help="diagonals added on both sides of the predicted band")
     ap.add_argument("--pipeline-chunks", type=int, default=0,
                     help="region chunks of the end-to-end call (0: the library default, one per 4M pairs; 1: one pass)")
+    ap.add_argument("--per-base-gaps", action="store_true",
+                    help="e2e: pass the per-base i, d, c arrays even when they are uniform")
     ap.add_argument("--tune-regions", type=int, default=500,
                     help="regions of the workload the launch-shape autotuner times (0: default shapes)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
         return
-    form = args.form or ("band" if args.workload in ("config4", "config1") else "plain")
+    form = args.form or ("band" if args.workload in ("config4", "config3", "config1") else "plain")
 
     rep = replicas.setup("nccl")
     world, rank, local = rep.world, rep.rank, rep.local
@@ -343,6 +349,8 @@ def main():
     peak = C.c_double(0)
     st = lib.bv_phmm_measure_fp32_peak(local, C.byref(peak))
     fp32_peak = peak.value if st == 0 else None
+    st = lib.bv_phmm_measure_fp64_peak(local, C.byref(peak))
+    fp64_peak = peak.value if st == 0 else None
 
     plain = band = None
     train_rep = None
@@ -390,20 +398,27 @@ def main():
     # ---- end to end through the public API (host buffers) ---------------------
     e2e_eng = eb if eb is not None else PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp,
                                                       pipeline_chunks=args.pipeline_chunks)
-    arrays = [batch.read_bases, batch.read_q, batch.read_i, batch.read_d, batch.read_c, batch.hap_bases]
+    # the caller's view of a SamRecord batch: when every read base has the same
+    # gap-open and gap-continuation qualities they go as three bytes
+    gaps = None if args.per_base_gaps else batch.uniform_gaps()
+    arrays = [batch.read_bases, batch.read_q, batch.hap_bases]
+    if gaps is None:
+        arrays += [batch.read_i, batch.read_d, batch.read_c]
     for a in arrays:
         e2e_eng.host_register(a)
     out = np.empty(max(n, 1), np.float64)
     e2e_eng.host_register(out)
     for _ in range(max(1, min(args.warmup, 2))):
-        e2e_eng.compute_regions(batch, out=out)
+        e2e_eng.compute_regions(batch, out=out, uniform_gaps=gaps)
     rep.barrier()
     e2e_t = []
     e2e_st = None
     for _ in range(args.steps):
         t1 = time.perf_counter()
-        _, e2e_st = e2e_eng.compute_regions(batch, out=out, with_stats=True)
+        _, e2e_st = e2e_eng.compute_regions(batch, out=out, with_stats=True, uniform_gaps=gaps)
         e2e_t.append(time.perf_counter() - t1)
+    h2d_bytes = int(sum(a.nbytes for a in arrays) + batch.read_offsets.nbytes + batch.hap_offsets.nbytes +
+                    batch.region_reads.nbytes + batch.region_haps.nbytes)
     clk = clocks.stop()
     rep.barrier()
     for a in arrays + [out]:
@@ -469,14 +484,16 @@ def main():
         if band is not None:
             ms_band = mean(band, "ms_band")
             band_cells = int(last["band_cells"])
+            result_cells = int(last["band_result_cells"])
             ach = FLOPS_PER_CELL * band_cells / (ms_band / 1e3) / 1e12 if ms_band > 0 else 0.0
+            ach_result = FLOPS_PER_CELL * result_cells / (ms_band / 1e3) / 1e12 if ms_band > 0 else 0.0
             line["band"] = {
                 "kernel_ms": {"seed_features_mlp_route": mean(band, "ms_seed"), "banded_dp": ms_band,
                               "fallback_full_dp": mean(band, "ms_full"), "fp64_rescue": mean(band, "ms_fp64")},
                 "band_pairs": int(last["band_pairs"]), "routed_full": int(last["band_routed_full"]),
                 "edge_fallback": int(last["band_fallback"]), "promoted": int(last["band_promoted"]),
                 "fallback_rate": (int(last["band_routed_full"]) + int(last["band_fallback"])) / max(n, 1),
-                "band_cells": band_cells,
+                "band_cells": band_cells, "band_result_cells": result_cells,
                 # computed cells per second of the banded kernels (band + ring + inner band)
                 "gcups_computed_banded_dp": band_cells / (ms_band / 1e3) / 1e9 if ms_band > 0 else None,
                 "rescued": int(last["rescued"]),
@@ -485,17 +502,32 @@ def main():
             line["roofline"] = {"bound": "fp32", "kernel": "k_band_ring_f32<W> (banded forward, band and ring, W = 8/16/24/32)",
                                 "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
                                 "frac": (ach / fp32_peak) if fp32_peak else None,
+                                "cells_counted": "both sweeps: the result band (band + ring) and the inner band "
+                                                 "the ring test recomputes",
+                                "achieved_result_band": ach_result,
+                                "frac_result_band": (ach_result / fp32_peak) if fp32_peak else None,
                                 "flops_per_cell": FLOPS_PER_CELL,
                                 "traffic": DRAM_BYTES_PER_BAND_PAIR * int(last["band_pairs"])
                                 if args.workload == "config4" else None,
                                 "traffic_source": TRAFFIC_SOURCE if args.workload == "config4" else None}
         else:
             line["roofline"] = line.get("roofline_plain")
-        line["peak_source"] = "measured: FP32 FMA probe kernel in this run (bv_phmm_measure_fp32_peak)"
+        line["peak_source"] = ("measured: FP32 and FP64 FMA probe kernels in this run (bv_phmm_measure_fp32_peak, "
+                               "bv_phmm_measure_fp64_peak); MEASURED_PEAKS.json holds HBM and bf16 tensor peaks only")
+        fp64_ms = mean(main_run, "ms_fp64")
+        fp64_cells = int(last["rescued_cells"])
+        if fp64_cells > 0 and fp64_ms > 0:
+            a64 = FLOPS_PER_CELL * fp64_cells / (fp64_ms / 1e3) / 1e12
+            line["roofline_fp64"] = {"bound": "fp64", "kernel": "k_forward<double, 4, multi-strip> (FP64 rescue)",
+                                     "achieved": a64, "peak": fp64_peak, "unit": "TFLOP/s",
+                                     "frac": (a64 / fp64_peak) if fp64_peak else None,
+                                     "cells": fp64_cells, "ms": fp64_ms, "flops_per_cell": FLOPS_PER_CELL}
         line["accuracy"] = acc
         if geno is not None:
             line["genotype"] = geno
-        line["e2e"] = {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(batch.nbytes()),
+        line["e2e"] = {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d_bytes,
+                       "inputs": ("bases, base qualities and offsets; uniform gap penalties "
+                                  f"(ins, del, gcp) = {gaps}") if gaps else "per-base q, i, d, c arrays",
                        "d2h_bytes_per_step": int(8 * n), "results_identical_to_device_run": same}
         if e2e_st is not None:
             # last step: copies (first H2D to packed qualities, events; they overlap the host's

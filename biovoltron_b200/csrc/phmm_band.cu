@@ -1127,7 +1127,7 @@ __global__ void __launch_bounds__(128, W <= 8 ? 4 : 2) k_band_ring_f32(BandParam
   const BandItem* items = p.items + (size_t)cls * p.item_cap;
   const unsigned long long nthreads = (unsigned long long)gridDim.x * blockDim.x;
   const unsigned long long tid = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
-  unsigned long long cells = 0;
+  unsigned long long cells = 0, rcells = 0;
   for (unsigned long long ii = tid; ii < total; ii += nthreads) {
     const BandItem it = items[ii];
     const int64_t ro = p.batch.read_off[it.read], ho = p.batch.hap_off[it.hap];
@@ -1145,14 +1145,21 @@ __global__ void __launch_bounds__(128, W <= 8 ? 4 : 2) k_band_ring_f32(BandParam
       lout = band_forward_pass<W + 2 * kRing>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
     }
     cells += (unsigned long long)R * (2 * W + 2 * kRing);
+    rcells += (unsigned long long)R * (W + 2 * kRing);
     bool fall_back = !(lout > 0.f);
     const bool rescue = !fall_back && (!(lout >= (float)kMinAccepted) || isinf(lout));
     // the ring's share of the outer likelihood (NaN or a negative share fall back too)
     if (!fall_back && !rescue) fall_back = !(lout - lin <= p.edge_threshold * lout && lin >= 0.f);
     band_outcome(p, cls, it, R, lout, fall_back, rescue);
   }
-  for (int o = 16; o > 0; o >>= 1) cells += __shfl_xor_sync(0xffffffffu, cells, o);
-  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(&p.bctr->band_cells, cells);
+  for (int o = 16; o > 0; o >>= 1) {
+    cells += __shfl_xor_sync(0xffffffffu, cells, o);
+    rcells += __shfl_xor_sync(0xffffffffu, rcells, o);
+  }
+  if ((threadIdx.x & 31) == 0 && cells) {
+    atomicAdd(&p.bctr->band_cells, cells);
+    atomicAdd(&p.bctr->band_result_cells, rcells);
+  }
 }
 
 __global__ void k_audit_units(BandParams p, Unit* units) {

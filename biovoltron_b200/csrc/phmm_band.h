@@ -77,7 +77,8 @@ struct BandCounters {
   unsigned long long audit_var[16];                       // audit units per full-DP variant
   unsigned long long fallback_edge;                       // pairs sent back by the edge check
   unsigned long long fallback_route;                      // pairs routed to the full DP up front
-  unsigned long long band_cells;
+  unsigned long long band_cells;                          // cells of both sweeps (result band and inner band)
+  unsigned long long band_result_cells;                   // cells of the result band (band plus ring)
   unsigned long long feat_next;                           // work-queue head of the featuriser
   unsigned long long feat_slow_count;                     // pairs left to the warp featuriser (many distinct diagonals)
   unsigned long long feat_slow_next;                      // its work-queue head

@@ -90,6 +90,7 @@ struct Counters {
   unsigned long long rescue_next;
   unsigned long long underflow_count;  // FP64 results that stayed non-positive
   unsigned long long status;           // nonzero: a kernel met an inconsistent input
+  unsigned long long rescued_cells;    // DP cells the FP64 pass computed
 };
 
 }  // namespace bvphmm

@@ -598,6 +598,35 @@ __device__ __forceinline__ void write_result(const KernelParams& p, int read, in
   }
 }
 
+// Whether an FP32 multi-strip pair's result is certain to fall below
+// kMinAccepted, from its last strip's bottom row in the boundary buffer
+// (column c at buffer row c + 31; values M, X/pMX, Y/pMY).  The mass a row
+// passes to the next one is at most its own (every state's transitions into
+// the next row sum to <= 1 and emissions are <= 1); only the in-row deletion
+// chain adds, at most a factor 1 + pMY/(1 - pYY) per row.  The bottom row's
+// M + X/pMX + Y/pMY bounds its M + X + Y from above; times the chain factor
+// over all rows, and twice that against the rounding of the FP32 sums, it
+// bounds the result.  Kept out of line: it runs once per strip.
+static __device__ __noinline__ bool fp32_result_below_threshold(const Tables* tb, const float* bnd, int H,
+                                                         const uchar4* quals, int R, int lane) {
+  float mass = 0.f;
+  for (int c = 1 + lane; c <= H; c += kWarp) {
+    const float4 v = *reinterpret_cast<const float4*>(bnd + (size_t)(c + 31) * 4);
+    mass += v.x + v.y + v.z;
+  }
+  for (int o = 16; o > 0; o >>= 1) mass += __shfl_xor_sync(0xffffffffu, mass, o);
+  if (!(isfinite(mass) && mass < (float)kMinAccepted)) return false;
+  float growth = 0.f;  // log2 of the deletion-chain factor
+  for (int r = lane; r < R; r += kWarp) {
+    float pmy, pyy;
+    if (tb->const_mode) { pmy = tb->cf[2]; pyy = tb->cf[6]; }
+    else { pmy = tb->ph2pr_f[quals[r].z & kQualMask]; pyy = tb->ph2pr_f[quals[r].w & kQualMask]; }
+    growth += pyy < 1.f ? __log2f(1.f + pmy / (1.f - pyy)) * 1.0001f + 1e-6f : 1e30f;
+  }
+  for (int o = 16; o > 0; o >>= 1) growth += __shfl_xor_sync(0xffffffffu, growth, o);
+  return growth < 100.f && 2.f * mass * exp2f(growth) < (float)kMinAccepted;
+}
+
 template <typename T, int RT, bool MULTI, bool PAIR = false>
 __device__ void process_item(const KernelParams& p, const Item& it, unsigned char* wsm, int lane, T* bnd) {
   using S = WarpSmem<T, RT>;
@@ -681,11 +710,16 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
     __syncwarp();
     T lastM, lastY, sumM, sumX, bmax;
     long long kexp = 0;  // stored values are true values * 2^-kexp
+    bool handed_over = false;  // FP32: the pair went to the FP64 list before its last strip
     if constexpr (MULTI) {
       // boundary row of "strip -1": all zero
       for (int x = lane; x < nsteps + 96; x += kWarp) {
         bnd[(size_t)x * 4 + 0] = T(0); bnd[(size_t)x * 4 + 1] = T(0); bnd[(size_t)x * 4 + 2] = T(0);
       }
+      // FP32 early hand-off: once a strip's bottom row proves that the FP32
+      // result will fall below kMinAccepted (fp32_result_below_threshold), the
+      // reference's rule sends the pair to FP64; it goes there now instead of
+      // after its remaining strips.
       T in_scale = T(1);
       for (int st = 0; st < nstrips; ++st) {
         __syncwarp();
@@ -698,6 +732,13 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
           run_strip<T, RT, true, 32>(rw, el, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
                                      lastY, sumM, sumX, bmax);
         __syncwarp();
+        if constexpr (sizeof(T) == 4) {
+          if (st + 1 < nstrips && p.rescue &&
+              fp32_result_below_threshold(p.tables, reinterpret_cast<const float*>(bnd), H, quals, R, lane)) {
+            handed_over = true;
+            break;
+          }
+        }
         in_scale = T(1);
         if (p.rescale && st + 1 < nstrips) {
           const T m = __shfl_sync(0xffffffffu, bmax, kWarp - 1);
@@ -720,9 +761,11 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
                                    lastY, sumM, sumX, bmax);
     }
     if (lane == kWarp - 1) {
-      // FP32: the summing row's Y + M; FP64: the accumulated last-row sums.
-      const T res = SumRow<T>::value ? lastY + lastM : sumM + sumX;
+      // FP32: the summing row's Y + M; FP64: the accumulated last-row sums;
+      // a pair handed over early counts as below the rescue threshold.
+      const T res = handed_over ? T(0) : SumRow<T>::value ? lastY + lastM : sumM + sumX;
       write_result<T>(p, it.read, h, it.out0 + k, res, kexp);
+      if (is_f64 && p.cells_ctr) atomicAdd(p.cells_ctr, (unsigned long long)R * (unsigned long long)H);
     }
   }
 }

@@ -478,7 +478,9 @@ bv_status Engine::enqueue_kernels(bool capturing) {
     p.bnd_cols = lp.bnd_cols;
     p.rescale = 1;
     p.rescale_target = kRescaleTarget;
+    p.cells_ctr = &d_counters_.as<Counters>()->rescued_cells;
     BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP64 forward launch");
+    p.cells_ctr = nullptr;
   }
   BV_CUDA(rec(ev_[4]), "event");
   if (band_enabled() && band_opt_.audit_period > 0) {
@@ -555,6 +557,7 @@ bv_status Engine::finish(bv_phmm_stats* stats) {
     stats->pairs = n_results_;
     stats->cells = n_cells_;
     stats->rescued = (int64_t)c.rescue_count;
+    stats->rescued_cells = (int64_t)c.rescued_cells;
     stats->underflow = (int64_t)c.underflow_count;
     stats->kernel_launches = band_enabled()
                                  ? 6 + (band_opt_.use_mlp ? 1 : 0) + kBandWidths + 9 +

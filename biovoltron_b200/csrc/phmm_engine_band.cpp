@@ -192,6 +192,7 @@ bv_status Engine::band_stats(bv_phmm_stats* st) {
   st->band_fallback = (int64_t)bc.fallback_edge;
   st->band_routed_full = (int64_t)bc.fallback_route;
   st->band_cells = (int64_t)bc.band_cells;
+  st->band_result_cells = (int64_t)bc.band_result_cells;
   st->band_promoted = 0;
   for (int c = 0; c < kBandWidths; ++c) st->band_promoted += (int64_t)bc.promoted[c];
   const long long na = std::min<long long>((long long)bc.audit_count, audit_cap_);

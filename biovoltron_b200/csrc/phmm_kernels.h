@@ -30,6 +30,7 @@ struct KernelParams {
   long long bnd_cols;     // rows of 4 values per warp buffer
   int rescale;            // renormalise between strips (FP64 variants)
   int rescale_target;     // binary exponent the boundary maximum is scaled to
+  unsigned long long* cells_ctr;  // if set, FP64 launches add read x haplotype length per pair here
 };
 
 // Variant table: (precision, rows per lane, multi-strip, two haplotypes per

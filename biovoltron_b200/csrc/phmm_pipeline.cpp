@@ -37,6 +37,8 @@ void add_stats(bv_phmm_stats& t, const bv_phmm_stats& s) {
   t.pairs += s.pairs;
   t.cells += s.cells;
   t.rescued += s.rescued;
+  t.rescued_cells += s.rescued_cells;
+  t.band_result_cells += s.band_result_cells;
   t.underflow += s.underflow;
   t.band_pairs += s.band_pairs;
   t.band_fallback += s.band_fallback;

@@ -47,7 +47,7 @@ class Stats(C.Structure):
         ("ms_d2h", C.c_double), ("ms_total", C.c_double),
         ("band_routed_full", C.c_int64), ("audit_pairs", C.c_int64), ("audit_max_err", C.c_double),
         ("audit_p99_err", C.c_double), ("band_promoted", C.c_int64), ("ms_seed", C.c_double),
-        ("ms_full", C.c_double),
+        ("ms_full", C.c_double), ("rescued_cells", C.c_int64), ("band_result_cells", C.c_int64),
     ]
 
     def as_dict(self):
@@ -159,6 +159,7 @@ def load() -> C.CDLL:
         "bv_phmm_default_band_options": (None, [P(BandOptions)]),
         "bv_phmm_set_band_options": (C.c_int, [V, P(BandOptions)]),
         "bv_phmm_measure_fp32_peak": (C.c_int, [C.c_int, P(C.c_double)]),
+        "bv_phmm_measure_fp64_peak": (C.c_int, [C.c_int, P(C.c_double)]),
         "bv_phmm_default_band_train_options": (None, [P(BandTrainOptions)]),
         "bv_phmm_band_train": (C.c_int, [V, P(RegionBatchC), P(BandTrainOptions), P(BandTrainReport)]),
         "bv_phmm_band_labels": (C.c_int, [V, P(RegionBatchC), C.c_float, V, V, V, V, V, V]),

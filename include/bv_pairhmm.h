@@ -100,6 +100,9 @@ typedef struct bv_phmm_stats {
   int64_t band_promoted;    /* banded pairs retried on the next wider band after the edge check */
   double ms_seed;           /* band mode: k-mer tables, featuriser, band MLP and routing kernels */
   double ms_full;           /* full-DP FP32 kernels (band mode: the fallback pairs) */
+  int64_t rescued_cells;    /* DP cells the FP64 pass computed (read x haplotype length of its pairs) */
+  int64_t band_result_cells; /* band mode: cells of the bands whose likelihood is the result (band plus
+                                ring); band_cells adds the inner band the ring test recomputes */
 } bv_phmm_stats;
 
 typedef struct bv_phmm_ctx bv_phmm_ctx;
@@ -475,6 +478,8 @@ int bv_phmm_debug_jacobian_table(double* out, int n);
  * 2 flops per FMA), the roofline denominator of the forward kernels, which
  * run on the CUDA-core FP32 pipe.  Returns a bv_status. */
 int bv_phmm_measure_fp32_peak(int device, double* tflops);
+/* The same for FP64 FMAs: the roofline denominator of the FP64 rescue kernel. */
+int bv_phmm_measure_fp64_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }
