@@ -144,6 +144,24 @@ class ClockSampler:
                 "power_w_max": pmax}
 
 
+def pinned_h2d_gbps(device: int, nbytes: int = 1 << 30) -> float:
+    """One page-locked host->device copy of ``nbytes``, timed with CUDA events
+    (best of three): the link rate the end-to-end copies can reach."""
+    import torch
+    src = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    dst = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{device}")
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        best = max(best, nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del src, dst
+    return best
+
+
 def cpu_reference_rate(batch: W.RegionBatch, target_s: float, seed: int = 0):
     """Times Biovoltron's AVX kernel (or, if it was not built, the C oracle) on
     all host threads over a seeded sample of regions sized for ~target_s."""
@@ -361,6 +379,7 @@ def main():
                                                 replace=False)
         with PairHMMEngine(device=local) as et:
             tuning = et.autotune(W.subsample_regions(batch, sorted(picks.tolist())), repeats=3)
+    h2d_link = pinned_h2d_gbps(local)
     clocks = ClockSampler(local)  # sampled over every timed section below
     clocks.start()
     # ---- plain full DP, device-resident --------------------------------------
@@ -526,6 +545,7 @@ def main():
         if geno is not None:
             line["genotype"] = geno
         line["e2e"] = {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d_bytes,
+                       "pinned_h2d_gbps_one_copy": h2d_link,
                        "inputs": ("bases, base qualities and offsets; uniform gap penalties "
                                   f"(ins, del, gcp) = {gaps}") if gaps else "per-base q, i, d, c arrays",
                        "d2h_bytes_per_step": int(8 * n), "results_identical_to_device_run": same}

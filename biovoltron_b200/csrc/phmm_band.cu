@@ -1103,6 +1103,133 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
   return make_float2(tot, toti);
 }
 
+// The same two sweeps with the inner band's cells packed beside the outer
+// band's: the inner band (diagonals OFF .. OFF + WI - 1 of the outer band) is
+// the same matrix cells under another DP, with the same emission and row
+// constants, so each such cell updates both DPs with packed FP32x2
+// operations (fma.rn.f32x2 of sm_100) -- each half the scalar operation
+// sequence, so the results are bit-identical to band_forward_body.  Outer
+// cells without an inner twin (the rings) stay scalar.
+template <int WB, int WI>
+__device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const Tables* tb,
+                                                      const uchar4* __restrict__ quals,
+                                                      const uint8_t* __restrict__ rbase, const uint8_t* __restrict__ hap,
+                                                      int R, int H, int d) {
+  constexpr int NW = WB / 8;
+  constexpr int OFF = (WB - WI) / 2;   // outer cells 0 .. OFF-1: lower ring; OFF+WI .. WB-1: upper ring
+  constexpr int NHI = WB - OFF - WI;
+  static_assert(WI > 0 && OFF > 0 && NHI > 0, "paired sweep needs rings on both sides");
+  float Ml[OFF], Xl[OFF], Yl[OFF];     // lower ring (outer only)
+  float2 P_M[WI], P_X[WI], P_Y[WI];    // .x outer cell OFF + k, .y inner cell k
+  float Mh[NHI], Xh[NHI], Yh[NHI];     // upper ring (outer only)
+  const float init_y = tb->init_f / (float)H;
+  auto y0 = [&](int k) { const int c = d + k; return (c >= 0 && c <= H) ? init_y : 0.f; };
+#pragma unroll
+  for (int k = 0; k < OFF; ++k) { Ml[k] = 0.f; Xl[k] = 0.f; Yl[k] = y0(k); }
+#pragma unroll
+  for (int k = 0; k < WI; ++k) {
+    P_M[k] = make_float2(0.f, 0.f);
+    P_X[k] = make_float2(0.f, 0.f);
+    const float y = y0(OFF + k);
+    P_Y[k] = make_float2(y, y);
+  }
+#pragma unroll
+  for (int k = 0; k < NHI; ++k) { Mh[k] = 0.f; Xh[k] = 0.f; Yh[k] = y0(OFF + WI + k); }
+  uint32_t win[NW];  // row 1: columns d + 1 + k
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int c = d + 1 + w * 8 + t;
+      v |= ((c >= 1 && c <= H) ? onehot(hap[c - 1]) : 0u) << (4 * t);
+    }
+    win[w] = v;
+  }
+  float pmx_last = 1.f;
+  FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);
+  uchar4 qn = quals[min(1, R - 1)];
+  uint8_t bn = rbase[min(1, R - 1)];
+  for (int r = 1; r <= R; ++r) {
+    const FwdRow nxt = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
+    {
+      const int rn = min(r + 1, R - 1);
+      qn = quals[rn];
+      bn = rbase[rn];
+    }
+    const int cn = r + 1 + d + WB - 1;
+    const uint8_t hb = (cn >= 1 && cn <= H) ? hap[cn - 1] : (uint8_t)0;
+    const float2 cx2 = make_float2(cur.cx, cur.cx), cy2 = make_float2(cur.cy, cur.cy);
+    const float2 kap2 = make_float2(cur.kap, cur.kap), g2 = make_float2(cur.g, cur.g);
+    auto emis = [&](int k) {
+      const bool match = (win[k >> 3] & cur.rb & (0xFu << (4 * (k & 7)))) != 0u;
+      return match ? cur.em : cur.ex;
+    };
+    float lm = 0.f, ly = 0.f;
+    // lower ring
+#pragma unroll
+    for (int k = 0; k < OFF; ++k) {
+      const float e = emis(k);
+      const float upm = k + 1 < OFF ? Ml[k + 1] : P_M[0].x;
+      const float upx = k + 1 < OFF ? Xl[k + 1] : P_X[0].x;
+      const float mn = e * __fmaf_rn(cur.cy, Yl[k], __fmaf_rn(cur.cx, Xl[k], Ml[k]));
+      const float xn = __fmaf_rn(cur.kap, upx, upm);
+      const float yn = __fmaf_rn(cur.g, ly, lm);
+      Ml[k] = mn; Xl[k] = xn; Yl[k] = yn;
+      lm = mn; ly = yn;
+    }
+    // paired cells: the inner band's row starts with no left neighbour
+    float2 lm2 = make_float2(lm, 0.f), ly2 = make_float2(ly, 0.f);
+#pragma unroll
+    for (int k = 0; k < WI; ++k) {
+      const float e = emis(OFF + k);
+      const float2 upm = k + 1 < WI ? P_M[k + 1] : make_float2(Mh[0], 0.f);
+      const float2 upx = k + 1 < WI ? P_X[k + 1] : make_float2(Xh[0], 0.f);
+      const float2 t = __ffma2_rn(cy2, P_Y[k], __ffma2_rn(cx2, P_X[k], P_M[k]));
+      const float2 mn = make_float2(e * t.x, e * t.y);
+      const float2 xn = __ffma2_rn(kap2, upx, upm);
+      const float2 yn = __ffma2_rn(g2, ly2, lm2);
+      P_M[k] = mn; P_X[k] = xn; P_Y[k] = yn;
+      lm2 = mn; ly2 = yn;
+    }
+    lm = lm2.x;
+    ly = ly2.x;
+    // upper ring
+#pragma unroll
+    for (int k = 0; k < NHI; ++k) {
+      const float e = emis(OFF + WI + k);
+      const float upm = k + 1 < NHI ? Mh[k + 1] : 0.f;
+      const float upx = k + 1 < NHI ? Xh[k + 1] : 0.f;
+      const float mn = e * __fmaf_rn(cur.cy, Yh[k], __fmaf_rn(cur.cx, Xh[k], Mh[k]));
+      const float xn = __fmaf_rn(cur.kap, upx, upm);
+      const float yn = __fmaf_rn(cur.g, ly, lm);
+      Mh[k] = mn; Xh[k] = xn; Yh[k] = yn;
+      lm = mn; ly = yn;
+    }
+    const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
+#pragma unroll
+    for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
+    win[NW - 1] = (win[NW - 1] >> 4) | (nib << 28);
+    pmx_last = cur.pmx;
+    cur = nxt;
+  }
+  // last row sums, in the scalar body's order (outer cells 0 .. WB-1, then inner 0 .. WI-1)
+  float tot = 0.f, toti = 0.f;
+#pragma unroll
+  for (int k = 0; k < WB; ++k) {
+    const int c = R + d + k;
+    const float m = k < OFF ? Ml[k] : k < OFF + WI ? P_M[k - OFF].x : Mh[k - OFF - WI];
+    const float x = k < OFF ? Xl[k] : k < OFF + WI ? P_X[k - OFF].x : Xh[k - OFF - WI];
+    tot += (c >= 1 && c <= H) ? m + pmx_last * x : 0.f;
+  }
+#pragma unroll
+  for (int k = 0; k < WI; ++k) {
+    const int c = R + d + OFF + k;
+    toti += (c >= 1 && c <= H) ? P_M[k].y + pmx_last * P_X[k].y : 0.f;
+  }
+  return make_float2(tot, toti);
+}
+
 // One band alone, not inlined: the two passes of the wider classes then hold
 // one band's state at a time.
 template <int WB>
@@ -1111,9 +1238,9 @@ __device__ __noinline__ float band_forward_pass(const BandSmem& sm, const Tables
   return band_forward_body<WB, 0>(sm, tb, quals, rbase, hap, R, H, d).x;
 }
 
-// W = 8 keeps four blocks per SM (128 registers); the wider classes two.
+// W = 8 keeps three blocks per SM (up to 168 registers); the wider classes two.
 template <int W>
-__global__ void __launch_bounds__(128, W <= 8 ? 4 : 2) k_band_ring_f32(BandParams p, int cls) {
+__global__ void __launch_bounds__(128, W <= 8 ? 3 : 2) k_band_ring_f32(BandParams p, int cls) {
   constexpr bool kDual = W <= 16;  // both bands in one sweep
   // ring width on each side: pairs routed to wider bands have indel-rich alignments whose
   // alternatives lie farther out, so W >= 16 test eight diagonals
@@ -1137,7 +1264,7 @@ __global__ void __launch_bounds__(128, W <= 8 ? 4 : 2) k_band_ring_f32(BandParam
     const uint8_t* hap = p.batch.hap_bases + ho;
     float lin, lout;
     if constexpr (kDual) {
-      const float2 t = band_forward_body<W + 2 * kRing, W>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
+      const float2 t = band_forward_paired<W + 2 * kRing, W>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
       lout = t.x;
       lin = t.y;
     } else {
@@ -1260,7 +1387,7 @@ cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st) {
 }
 
 cudaError_t launch_band_dp(const BandParams& p, int cls, int sms, cudaStream_t st) {
-  const int blocks = band_dp_blocks(sms);
+  const int blocks = band_dp_blocks(sms, cls);
   if (cls == 0) {
     k_band_ring_f32<8><<<blocks, 128, 0, st>>>(p, 0);
   } else if (cls == 1) {

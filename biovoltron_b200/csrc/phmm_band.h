@@ -134,7 +134,8 @@ cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st);
 cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st);
 cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st);
 cudaError_t launch_band_dp(const BandParams& p, int width_class, int sms, cudaStream_t st);
-inline int band_dp_blocks(int sms) { return sms * 4; }
+// banded kernels: 128-thread blocks, as many as fit at once (3 per SM for W = 8, 2 for the wider classes)
+inline int band_dp_blocks(int sms, int width_class) { return sms * (width_class == 0 ? 3 : 2); }
 // warp featuriser (the slow path) grid and its per-warp scratch histograms (words)
 constexpr int kFeatWarpsPerBlock = 4;
 inline int feat_blocks(int sms) { return sms * 4; }

@@ -4,7 +4,6 @@
 // phmm_forward.cu, which instantiates the kernels.
 #pragma once
 #include <cuda_runtime.h>
-#include <cuda_pipeline.h>
 #include <cstdint>
 #include <cmath>
 #include <type_traits>
@@ -143,8 +142,48 @@ struct WarpSmem {
   static constexpr int kRingInCols = 64;
   static constexpr int kRingOutCols = 32;
   static constexpr int kColBytes = 4 * (int)sizeof(T);     // M, Xh, Yh, unused
-  static constexpr int kRingBytes = (kRingInCols + kRingOutCols) * kColBytes;
+  // the two input-ring halves' transaction barriers follow the rings
+  static constexpr int kRingBytes = (kRingInCols + kRingOutCols) * kColBytes + 16;
 };
+
+// Bulk (TMA) copies of the strip-boundary rows.  One lane moves a 32-row
+// chunk of the boundary buffer (global memory written by this warp's previous
+// strip) into a ring half in shared memory with cp.async.bulk, completing on
+// that half's mbarrier; the reader waits on the barrier's phase.  Sources and
+// destinations are 16-byte aligned and sizes multiples of 16 (rows of 16 or 32
+// bytes, 32 rows); the source is this GPU's own memory and no multicast is
+// used.  Every wait is bounded: after kBulkWaitLimit polls it sets status bit
+// 8 (the host reports BV_ERR_INTERNAL) and goes on.
+constexpr unsigned kBulkWaitLimit = 1u << 22;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mb)), "r"(count) : "memory");
+}
+// Makes barrier initialisation and this thread's earlier generic writes to
+// global memory visible to the async proxy (the bulk copies).
+__device__ __forceinline__ void fence_for_bulk() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n\tfence.proxy.async.global;\n\tfence.proxy.async.shared::cta;" ::
+                   : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* mb) {
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%2], %3;\n\t"
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %3, [%2];"
+      ::"r"(smem_addr(dst)), "l"(src), "r"(smem_addr(mb)), "r"(bytes) : "memory");
+}
+// Waits until the barrier's current phase (parity `phase`) completes.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mb, unsigned phase) {
+  for (unsigned it = 0; it < kBulkWaitLimit; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done) : "r"(smem_addr(mb)), "r"(phase) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 // FP32 adds a summing row below the read's last row: with e = 1, pMM = 1,
 // the X coefficient = pMX(R) (undoing the X/pMX scaling) and pYY = 1, its M is
@@ -340,7 +379,8 @@ template <typename T, int RT, bool MULTI, int CH, bool FOLD = false>
 __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
                                           const unsigned char* __restrict__ hc_lane, int nsteps, int lane,
                                           T* __restrict__ bnd, unsigned char* ring, T in_scale, T& lastM,
-                                          T& lastY, T& sumM, T& sumX, T& bmax) {
+                                          T& lastY, T& sumM, T& sumX, T& bmax,
+                                          unsigned long long* status = nullptr) {
   using S = WarpSmem<T, RT>;
   constexpr bool kScale = sizeof(T) == 8;  // only the FP64 path renormalises
   constexpr bool kSums = !SumRow<T>::value;
@@ -356,20 +396,30 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
   T dM = upM, dX = upX, dY = upY;
   T* ring_in = reinterpret_cast<T*>(ring);
   T* ring_out = reinterpret_cast<T*>(ring + S::kRingInCols * S::kColBytes);
+  uint64_t* mb = reinterpret_cast<uint64_t*>(ring + (S::kRingInCols + S::kRingOutCols) * S::kColBytes);
+  constexpr unsigned kChunkBytes = 32u * S::kColBytes;
+  unsigned phase = 0;     // lane 0: bit h = parity of ring half h's next completion
+  bool bulk_ok = true;    // lane 0: every bulk wait completed
   if constexpr (MULTI) {
     static_assert(CH == 32, "multi-strip runs 32-step chunks");
     // Lane 0 needs, at step s, buffer row s + 32 (column s + 1); those rows
     // are streamed into a 64-row ring: chunk k (steps 32k..32k+31) uses ring
-    // half k&1, prefetched during chunk k-1.  Step 0's diagonal is row 31.
-    const T* src = bnd + (size_t)(32 + lane) * 4;
-    __pipeline_memcpy_async(ring_in + lane * 4, src, 16);
-    if constexpr (sizeof(T) == 8) __pipeline_memcpy_async(ring_in + lane * 4 + 2, src + 2, 16);
-    __pipeline_commit();
+    // half k&1, prefetched by a bulk copy during chunk k-1.  Step 0's
+    // diagonal is row 31.  The boundary rows were written by every lane
+    // (previous strip, or the zeroing): each lane fences them towards the
+    // async proxy before lane 0 issues the copies.
+    fence_for_bulk();
+    __syncwarp();
     if (lane == 0) {
+      mbar_init(mb, 1);
+      mbar_init(mb + 1, 1);
+      fence_for_bulk();
+      bulk_g2s(ring_in, bnd + (size_t)32 * 4, kChunkBytes, mb);
       dM = bnd[31 * 4 + 0]; dX = bnd[31 * 4 + 1]; dY = bnd[31 * 4 + 2];
       if constexpr (kScale) { dM *= in_scale; dX *= in_scale; dY *= in_scale; }
+      bulk_ok &= mbar_wait(mb, 0);
+      phase ^= 1u;
     }
-    __pipeline_wait_prior(0);
     __syncwarp();
   } else if constexpr (!SumRow<T>::value) {
     if (lane == 0) { upM = T(0); dM = T(0); }
@@ -377,12 +427,8 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
 
   for (int s0 = 0; s0 < nsteps; s0 += CH) {
     if constexpr (MULTI) {
-      const int nk = s0 / 32 + 1;
-      const T* src = bnd + (size_t)(32 * nk + 32 + lane) * 4;
-      T* dst = ring_in + ((nk & 1) * 32 + lane) * 4;
-      __pipeline_memcpy_async(dst, src, 16);
-      if constexpr (sizeof(T) == 8) __pipeline_memcpy_async(dst + 2, src + 2, 16);
-      __pipeline_commit();
+      const int nk = s0 / 32 + 1;  // prefetch of the next chunk's rows into half nk & 1
+      if (lane == 0) bulk_g2s(ring_in + (nk & 1) * 32 * 4, bnd + (size_t)(32 * nk + 32) * 4, kChunkBytes, mb + (nk & 1));
     }
 #pragma unroll
     for (int u = 0; u < CH; ++u) {
@@ -452,9 +498,16 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
         reinterpret_cast<double2*>(dstb)[1] = reinterpret_cast<const double2*>(srco)[1];
       }
       __threadfence_block();
-      __pipeline_wait_prior(0);
+      if (lane == 0) {
+        const int h = (s0 / 32 + 1) & 1;  // the prefetched half
+        bulk_ok &= mbar_wait(mb + h, (phase >> h) & 1u);
+        phase ^= 1u << h;
+      }
       __syncwarp();
     }
+  }
+  if constexpr (MULTI) {
+    if (lane == 0 && !bulk_ok && status) atomicOr(status, 8ull);
   }
   lastM = M[RT - 1];
   lastY = Y[RT - 1];
@@ -727,10 +780,10 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
         __syncwarp();
         if (fold)
           run_strip<T, RT, true, 32, true>(rw, el, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
-                                           lastY, sumM, sumX, bmax);
+                                           lastY, sumM, sumX, bmax, &p.ctr->status);
         else
           run_strip<T, RT, true, 32>(rw, el, hc + kHapLead - lane, nsteps, lane, bnd, ring, in_scale, lastM,
-                                     lastY, sumM, sumX, bmax);
+                                     lastY, sumM, sumX, bmax, &p.ctr->status);
         __syncwarp();
         if constexpr (sizeof(T) == 4) {
           if (st + 1 < nstrips && p.rescue &&
