@@ -1349,7 +1349,7 @@ cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, l
 }
 
 cudaError_t prepare_band_kernels() {
-  return cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpSmem));
+  return raise_dynamic_smem(reinterpret_cast<const void*>(&k_mlp_forward), (int)sizeof(MlpSmem));
 }
 
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {

@@ -48,6 +48,10 @@
 //   FP64 kernel renormalises the strip boundary row by an exact power of two
 //   so reads of many kilobases stay finite.
 #include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <utility>
 #include <cstdint>
 #include <cmath>
 
@@ -56,6 +60,26 @@
 #include "phmm_kernels.h"
 
 namespace bvphmm {
+
+// A kernel's dynamic shared-memory limit is one value per function and
+// device, shared by every context of the process.  Contexts that plan
+// different haplotype lengths (several on one GPU, from different host
+// threads) would otherwise lower it under each other's launches, so the
+// limit only ever rises: a process-wide record of each (device, kernel)'s
+// current limit, under a lock.
+cudaError_t raise_dynamic_smem(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> limit;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  int& cur = limit[{dev, func}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
 
 template <typename T, int RT, bool MULTI, bool PAIR>
 __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
@@ -125,15 +149,14 @@ static cudaError_t launch_one(const KernelParams& p, int grid, cudaStream_t st) 
 
 template <typename T, int RT, bool MULTI, bool PAIR>
 static cudaError_t prepare_one(int smem_per_block) {
-  return cudaFuncSetAttribute(&k_forward<T, RT, MULTI, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              smem_per_block);
+  return raise_dynamic_smem(reinterpret_cast<const void*>(&k_forward<T, RT, MULTI, PAIR>), smem_per_block);
 }
 
 template <typename T, int RT, bool MULTI, bool PAIR>
 static int occupancy_one(int smem_per_block, int threads) {
   int nb = 0;
   auto k = &k_forward<T, RT, MULTI, PAIR>;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_per_block);
+  if (raise_dynamic_smem(reinterpret_cast<const void*>(k), smem_per_block) != cudaSuccess) return 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem_per_block) != cudaSuccess) return 0;
   return nb;
 }

@@ -39,6 +39,9 @@ int variant_index(bool f64, int rows_per_lane, bool multi, bool paired = false);
 bool variant_paired(int variant);
 int warp_smem_bytes(int variant, int hap_bytes);
 int blocks_per_sm(int variant, int smem_per_block, int threads = kThreadsPerBlock);
+// Raises (never lowers) a kernel's dynamic shared-memory limit on the current
+// device to at least `bytes`; safe to call from several host threads.
+cudaError_t raise_dynamic_smem(const void* func, int bytes);
 // Sets the variant's dynamic shared-memory limit; call before launching or capturing it.
 cudaError_t prepare_variant(int variant, int smem_per_block);
 cudaError_t launch_forward(int variant, const KernelParams& p, int grid, cudaStream_t st);

@@ -23,6 +23,7 @@
 
 #include "phmm_band.h"
 #include "phmm_common.h"
+#include "phmm_kernels.h"
 
 namespace bvphmm {
 namespace {
@@ -246,7 +247,7 @@ cudaError_t launch_posterior_spread(const DeviceBatch& b, const Tables* tb, cons
                                     long long fbuf_stride, int32_t* lo, int32_t* hi, int blocks, cudaStream_t st) {
   if (n_pairs <= 0) return cudaSuccess;
   const int smem = label_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(k_posterior_spread, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_posterior_spread), smem);
   if (e != cudaSuccess) return e;
   k_posterior_spread<<<blocks, kLabelWarps * 32, smem, st>>>(b, tb, pair_read, pair_hap, n_pairs, tau, fbuf,
                                                              fbuf_stride, lo, hi);
