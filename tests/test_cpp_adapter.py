@@ -12,6 +12,13 @@ LIBDIR = os.path.join(ROOT, "biovoltron_b200", "_native")
 EXE = os.path.join(ROOT, "tests", "cpp", "_build", "adapter_check")
 
 
+def _run(args, txt):
+    """Runs the adapter check program; its stderr is shown when it fails."""
+    p = subprocess.run([EXE] + args, input=txt, capture_output=True, text=True)
+    assert p.returncode == 0, f"adapter_check {args} exited {p.returncode}: {p.stderr[-2000:]}"
+    return p.stdout.splitlines()
+
+
 def _build():
     os.makedirs(os.path.dirname(EXE), exist_ok=True)
     cmd = ["g++", "-std=c++20", "-O2", "-Wall", "-I" + os.path.join(ROOT, "include"), SRC, "-o", EXE,
@@ -37,7 +44,7 @@ def test_adapter_matches_python_mirror(engine):
              (base[200:260], b"5" * 60), (bytes(W._random_seq(rng, 90)), b"+" * 90),
              (base[0:200], b";" * 200)]
     txt = "".join(f"H {h.decode()}\n" for h in haps) + "".join(f"R {s.decode()} {q.decode()}\n" for s, q in reads)
-    out = subprocess.run([EXE], input=txt, capture_output=True, text=True, check=True).stdout.splitlines()
+    out = _run([], txt)
     kept = [int(x) for x in out[0].split()[1:]]
     mat = [[float(x) for x in l.split()] for l in out[1:]]
     py_reads = [SamRecord(s, q) for s, q in reads]
@@ -58,7 +65,7 @@ def test_scalar_adapter_matches_python_mirror():
     reads = [(base[50:200], bytes(rng.integers(43, 74, size=150).astype(np.uint8))),
              (bytes(W._random_seq(rng, 70)), b"+" * 70), (base[100:180], b"5" * 80)]
     txt = "".join(f"H {h.decode()}\n" for h in haps) + "".join(f"R {s.decode()} {q.decode()}\n" for s, q in reads)
-    out = subprocess.run([EXE, "scalar"], input=txt, capture_output=True, text=True, check=True).stdout.splitlines()
+    out = _run(["scalar"], txt)
     kept = [int(x) for x in out[0].split()[1:]]
     mat = [[float(x) for x in l.split()] for l in out[1:]]
     py_reads = [SamRecord(s, q) for s, q in reads]
@@ -78,8 +85,8 @@ def test_region_batcher_adapter_matches_one_call():
     reads = [(base[30:180], bytes(rng.integers(43, 74, size=150).astype(np.uint8))),
              (bytes(W._random_seq(rng, 70)), b"+" * 70), (base[150:250], b"5" * 100)]
     txt = "".join(f"H {h.decode()}\n" for h in haps) + "".join(f"R {s.decode()} {q.decode()}\n" for s, q in reads)
-    one = subprocess.run([EXE], input=txt, capture_output=True, text=True, check=True).stdout.splitlines()
-    two = subprocess.run([EXE, "batch"], input=txt, capture_output=True, text=True, check=True).stdout.splitlines()
+    one = _run([], txt)
+    two = _run(["batch"], txt)
     n = len(one)
     assert len(two) == 2 * n
     assert two[:n] == one and two[n:] == one
