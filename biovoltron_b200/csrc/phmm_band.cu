@@ -1000,6 +1000,137 @@ __device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb
 }
 
 // ---------------------------------------------------------------------------
+// Read-end insertion wedges.  A read end that does not fit the haplotype near
+// the band (bases a haplotype-specific indel separates from the rest of the
+// read, or sequencing junk) is explained by insertion runs: at the read's
+// start a path may begin above the band and run down into it (X steps keep
+// the column and lower the diagonal), at its end leave the band's bottom
+// edge and run down to the last row -- with a few matches in between.  Such
+// paths lie in two triangles next to the result band: above it in the first
+// kp rows (row r: diagonals hi + 1 .. hi + kp + 1 - r, i.e. every column up to
+// hi + kp + 1) and below it in the last kp rows (row R - kp + m: diagonals
+// lo - m .. lo - 1, i.e. every column from lo + R - kp on), kp = min(kWedge,
+// (R - 1) / 2).  The result band's DP covers those cells too, with the same
+// recurrence, so the banded value is the exact likelihood of every path in
+// the band plus the wedges.  The wedge cells live in shared memory (cell j of
+// a thread at wd[j * kBandThreads], threads interleaved so float4 accesses are
+// conflict-free; kWedge + 1 cells, the last always zero); only the active
+// cells of a row are touched.
+// ---------------------------------------------------------------------------
+constexpr int kWedge = 16;
+constexpr int kBandThreads = 128;
+static_assert(kWedge * 4 <= 64, "wedge nibbles fit one 64-bit word");
+
+struct EndWedges {
+  float4* wd;                 // this thread's cell 0
+  int kp;                     // wedge depth of this pair
+  unsigned long long above;   // one-hot haplotype nibbles of the above wedge's cells (cell j: bits 4j..4j+3)
+  unsigned long long below;   // the same for the below wedge
+  int cells;                  // wedge cells computed
+
+  // Row 0: every cell zero but the above wedge's start states (Y = INITIAL / H
+  // on its columns); the above wedge's row-1 columns d + WB + 1 + j.
+  __device__ __forceinline__ void init(float4* base, int R, int H, int d, int WB, float init_y,
+                                       const uint8_t* __restrict__ hap) {
+    wd = base;
+    kp = max(0, min(kWedge, (R - 1) / 2));
+    cells = 0;
+    above = 0ull;
+    below = 0ull;
+    wd[kWedge * kBandThreads] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < kWedge; ++j) {
+      const int c = d + WB + j;
+      wd[j * kBandThreads] = make_float4(0.f, 0.f, (j < kp && c >= 0 && c <= H) ? init_y : 0.f, 0.f);
+      const int c1 = c + 1;
+      if (j < kp && c1 >= 1 && c1 <= H) above |= (unsigned long long)onehot(hap[c1 - 1]) << (4 * j);
+    }
+  }
+
+  // Below wedge at row r, before the band's cells: farthest cell first (the
+  // deletion chain runs towards the band); returns the chain's M and Y for the
+  // band's lowest cell.  m0 / x0: that cell's values in row r - 1.
+  __device__ __forceinline__ void below_row(int r, int R, const FwdRow& cur, float m0, float x0, float& lm,
+                                            float& ly) {
+    lm = 0.f;
+    ly = 0.f;
+    if (r <= R - kp) return;
+    const int m = r - (R - kp);  // active cells 0 .. m-1
+    const uint32_t rnib = cur.rb & 0xFu;
+    for (int j = m - 1; j >= 0; --j) {
+      const float4 prev = wd[j * kBandThreads];
+      float upm = m0, upx = x0;
+      if (j >= 1) {
+        const float4 u = wd[(j - 1) * kBandThreads];
+        upm = u.x;
+        upx = u.y;
+      }
+      const float e = ((uint32_t)(below >> (4 * j)) & rnib) ? cur.em : cur.ex;
+      const float mn = e * __fmaf_rn(cur.cy, prev.z, __fmaf_rn(cur.cx, prev.y, prev.x));
+      const float xn = __fmaf_rn(cur.kap, upx, upm);
+      const float yn = __fmaf_rn(cur.g, ly, lm);
+      wd[j * kBandThreads] = make_float4(mn, xn, yn, 0.f);
+      lm = mn;
+      ly = yn;
+    }
+    cells += m;
+  }
+
+  // The above wedge's cell 0 in row r - 1 (the band's top cell takes its X
+  // from there), zero once the wedge has ended.
+  __device__ __forceinline__ float4 above_prev0(int r) const {
+    return r <= kp + 1 ? wd[0] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+
+  // Above wedge at row r, after the band's cells, chained from the band's top
+  // cell (lm, ly); the cell that leaves the triangle this row is cleared.
+  __device__ __forceinline__ void above_row(int r, const FwdRow& cur, float lm, float ly) {
+    if (r > kp + 1) return;
+    const int na = kp - r + 1;  // active cells 0 .. na-1
+    const uint32_t rnib = cur.rb & 0xFu;
+    for (int j = 0; j < na; ++j) {
+      const float4 prev = wd[j * kBandThreads];
+      const float4 up = wd[(j + 1) * kBandThreads];  // j + 1 <= kp <= kWedge: an active, cleared or spare cell
+      const float e = ((uint32_t)(above >> (4 * j)) & rnib) ? cur.em : cur.ex;
+      const float mn = e * __fmaf_rn(cur.cy, prev.z, __fmaf_rn(cur.cx, prev.y, prev.x));
+      const float xn = __fmaf_rn(cur.kap, up.y, up.x);
+      const float yn = __fmaf_rn(cur.g, ly, lm);
+      wd[j * kBandThreads] = make_float4(mn, xn, yn, 0.f);
+      lm = mn;
+      ly = yn;
+    }
+    wd[na * kBandThreads] = make_float4(0.f, 0.f, 0.f, 0.f);
+    cells += na;
+  }
+
+  // End of row r: the above wedge's columns move one cell down, a new one
+  // enters at the far end; the column leaving the band's window (`dropped`,
+  // column r + d) becomes the below wedge's nearest one.
+  __device__ __forceinline__ void shift(int r, int R, int H, int d, int WB, const uint8_t* __restrict__ hap,
+                                        uint32_t dropped) {
+    if (r <= kp) {
+      above >>= 4;
+      const int c = r + 1 + d + WB + kWedge - 1;
+      if (c >= 1 && c <= H) above |= (unsigned long long)onehot(hap[c - 1]) << (4 * (kWedge - 1));
+    }
+    if (r >= R - kp) below = (below << 4) | dropped;
+  }
+
+  // The below wedge's share of the result (last row, columns R + d - 1 - j).
+  __device__ __forceinline__ float last_row(int R, int H, int d, float pmx_last) const {
+    float t = 0.f;
+    for (int j = 0; j < kp; ++j) {
+      const int c = R + d - 1 - j;
+      if (c >= 1 && c <= H) {
+        const float4 v = wd[j * kBandThreads];
+        t += v.x + pmx_last * v.y;
+      }
+    }
+    return t;
+  }
+};
+
+// ---------------------------------------------------------------------------
 // Ring test.  A pair banded on [d_lo, d_lo + W) is also scored on the band
 // widened by a ring of four diagonals on each side (eight for W >= 16); the
 // wider band's likelihood is the result, and the pair is promoted to the next
@@ -1010,10 +1141,11 @@ __device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb
 // model cannot represent.  W = 8, 16 run both bands in one row sweep (shared
 // row constants and emissions); W = 24, 32 run them one after the other.
 // ---------------------------------------------------------------------------
-template <int WB, int WI>
+template <int WB, int WI, bool WEDGE = false>
 __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Tables* tb, const uchar4* __restrict__ quals,
                                                const uint8_t* __restrict__ rbase, const uint8_t* __restrict__ hap,
-                                               int R, int H, int d) {
+                                               int R, int H, int d, float4* wedge_cells = nullptr,
+                                               int* wedge_count = nullptr) {
   constexpr int NW = WB / 8;
   constexpr int OFF = (WB - WI) / 2;  // inner band = outer diagonals OFF .. OFF + WI - 1
   constexpr int WIN = WI > 0 ? WI : 1;
@@ -1042,6 +1174,8 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
     }
     win[w] = v;
   }
+  EndWedges wg;
+  if constexpr (WEDGE) wg.init(wedge_cells, R, H, d, WB, init_y, hap);
   float pmx_last = 1.f;
   FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
   uchar4 qn = quals[min(1, R - 1)];
@@ -1056,13 +1190,18 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
     const int cn = r + 1 + d + WB - 1;  // next row's window: shift, append column cn
     const uint8_t hb = (cn >= 1 && cn <= H) ? hap[cn - 1] : (uint8_t)0;
     float lm = 0.f, ly = 0.f, lmi = 0.f, lyi = 0.f;
+    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (WEDGE) {
+      wg.below_row(r, R, cur, M[0], X[0], lm, ly);
+      a0 = wg.above_prev0(r);
+    }
 #pragma unroll
     for (int k = 0; k < WB; ++k) {
       const bool match = (win[k >> 3] & cur.rb & (0xFu << (4 * (k & 7)))) != 0u;
       const float e = match ? cur.em : cur.ex;
       {
-        const float upm = (k + 1 < WB) ? M[k + 1] : 0.f;
-        const float upx = (k + 1 < WB) ? X[k + 1] : 0.f;
+        const float upm = (k + 1 < WB) ? M[k + 1] : a0.x;
+        const float upx = (k + 1 < WB) ? X[k + 1] : a0.y;
         const float mn = e * __fmaf_rn(cur.cy, Y[k], __fmaf_rn(cur.cx, X[k], M[k]));
         const float xn = __fmaf_rn(cur.kap, upx, upm);
         const float yn = __fmaf_rn(cur.g, ly, lm);
@@ -1082,6 +1221,10 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
         }
       }
     }
+    if constexpr (WEDGE) {
+      wg.above_row(r, cur, lm, ly);
+      wg.shift(r, R, H, d, WB, hap, win[0] & 0xFu);
+    }
     const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
 #pragma unroll
     for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
@@ -1094,6 +1237,10 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
   for (int k = 0; k < WB; ++k) {
     const int c = R + d + k;
     tot += (c >= 1 && c <= H) ? M[k] + pmx_last * X[k] : 0.f;
+  }
+  if constexpr (WEDGE) {
+    tot += wg.last_row(R, H, d, pmx_last);
+    *wedge_count = wg.cells;
   }
 #pragma unroll
   for (int k = 0; k < WIN; ++k) {
@@ -1114,7 +1261,7 @@ template <int WB, int WI>
 __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const Tables* tb,
                                                       const uchar4* __restrict__ quals,
                                                       const uint8_t* __restrict__ rbase, const uint8_t* __restrict__ hap,
-                                                      int R, int H, int d) {
+                                                      int R, int H, int d, float4* wedge_cells, int* wedge_count) {
   constexpr int NW = WB / 8;
   constexpr int OFF = (WB - WI) / 2;   // outer cells 0 .. OFF-1: lower ring; OFF+WI .. WB-1: upper ring
   constexpr int NHI = WB - OFF - WI;
@@ -1146,6 +1293,8 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
     }
     win[w] = v;
   }
+  EndWedges wg;  // the read ends' insertion wedges on the outer (result) band
+  wg.init(wedge_cells, R, H, d, WB, init_y, hap);
   float pmx_last = 1.f;
   FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);
   uchar4 qn = quals[min(1, R - 1)];
@@ -1165,7 +1314,9 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
       const bool match = (win[k >> 3] & cur.rb & (0xFu << (4 * (k & 7)))) != 0u;
       return match ? cur.em : cur.ex;
     };
-    float lm = 0.f, ly = 0.f;
+    float lm, ly;
+    wg.below_row(r, R, cur, Ml[0], Xl[0], lm, ly);
+    const float4 a0 = wg.above_prev0(r);
     // lower ring
 #pragma unroll
     for (int k = 0; k < OFF; ++k) {
@@ -1198,14 +1349,16 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
 #pragma unroll
     for (int k = 0; k < NHI; ++k) {
       const float e = emis(OFF + WI + k);
-      const float upm = k + 1 < NHI ? Mh[k + 1] : 0.f;
-      const float upx = k + 1 < NHI ? Xh[k + 1] : 0.f;
+      const float upm = k + 1 < NHI ? Mh[k + 1] : a0.x;
+      const float upx = k + 1 < NHI ? Xh[k + 1] : a0.y;
       const float mn = e * __fmaf_rn(cur.cy, Yh[k], __fmaf_rn(cur.cx, Xh[k], Mh[k]));
       const float xn = __fmaf_rn(cur.kap, upx, upm);
       const float yn = __fmaf_rn(cur.g, ly, lm);
       Mh[k] = mn; Xh[k] = xn; Yh[k] = yn;
       lm = mn; ly = yn;
     }
+    wg.above_row(r, cur, lm, ly);
+    wg.shift(r, R, H, d, WB, hap, win[0] & 0xFu);
     const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
 #pragma unroll
     for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
@@ -1222,6 +1375,8 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
     const float x = k < OFF ? Xl[k] : k < OFF + WI ? P_X[k - OFF].x : Xh[k - OFF - WI];
     tot += (c >= 1 && c <= H) ? m + pmx_last * x : 0.f;
   }
+  tot += wg.last_row(R, H, d, pmx_last);
+  *wedge_count = wg.cells;
 #pragma unroll
   for (int k = 0; k < WI; ++k) {
     const int c = R + d + OFF + k;
@@ -1232,21 +1387,24 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
 
 // One band alone, not inlined: the two passes of the wider classes then hold
 // one band's state at a time.
-template <int WB>
+template <int WB, bool WEDGE>
 __device__ __noinline__ float band_forward_pass(const BandSmem& sm, const Tables* tb, const uchar4* quals,
-                                                const uint8_t* rbase, const uint8_t* hap, int R, int H, int d) {
-  return band_forward_body<WB, 0>(sm, tb, quals, rbase, hap, R, H, d).x;
+                                                const uint8_t* rbase, const uint8_t* hap, int R, int H, int d,
+                                                float4* wedge_cells, int* wedge_count) {
+  return band_forward_body<WB, 0, WEDGE>(sm, tb, quals, rbase, hap, R, H, d, wedge_cells, wedge_count).x;
 }
 
 // W = 8 keeps three blocks per SM (up to 168 registers); the wider classes two.
 template <int W>
-__global__ void __launch_bounds__(128, W <= 8 ? 3 : 2) k_band_ring_f32(BandParams p, int cls) {
+__global__ void __launch_bounds__(kBandThreads, W <= 8 ? 3 : 2) k_band_ring_f32(BandParams p, int cls) {
   constexpr bool kDual = W <= 16;  // both bands in one sweep
   // ring width on each side: pairs routed to wider bands have indel-rich alignments whose
   // alternatives lie farther out, so W >= 16 test eight diagonals
   constexpr int kRing = W >= 16 ? 8 : 4;
   const Tables* tb = p.tables;
   __shared__ BandSmem sm;
+  extern __shared__ float4 wedge_smem[];  // (kWedge + 1) x kBandThreads cells
+  float4* wcells = wedge_smem + threadIdx.x;
   stage_band_tables(sm, tb);
   // routed items (bucketed by read length), then items promoted from the next narrower class
   const unsigned long long total =
@@ -1263,16 +1421,18 @@ __global__ void __launch_bounds__(128, W <= 8 ? 3 : 2) k_band_ring_f32(BandParam
     const uint8_t* rbase = p.batch.read_bases + ro;
     const uint8_t* hap = p.batch.hap_bases + ho;
     float lin, lout;
+    int wcount = 0;
     if constexpr (kDual) {
-      const float2 t = band_forward_paired<W + 2 * kRing, W>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
+      const float2 t = band_forward_paired<W + 2 * kRing, W>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing,
+                                                              wcells, &wcount);
       lout = t.x;
       lin = t.y;
     } else {
-      lin = band_forward_pass<W>(sm, tb, quals, rbase, hap, R, H, it.d_lo);
-      lout = band_forward_pass<W + 2 * kRing>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
+      lin = band_forward_pass<W, false>(sm, tb, quals, rbase, hap, R, H, it.d_lo, nullptr, nullptr);
+      lout = band_forward_pass<W + 2 * kRing, true>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing, wcells, &wcount);
     }
-    cells += (unsigned long long)R * (2 * W + 2 * kRing);
-    rcells += (unsigned long long)R * (W + 2 * kRing);
+    cells += (unsigned long long)R * (2 * W + 2 * kRing) + (unsigned long long)wcount;
+    rcells += (unsigned long long)R * (W + 2 * kRing) + (unsigned long long)wcount;
     bool fall_back = !(lout > 0.f);
     const bool rescue = !fall_back && (!(lout >= (float)kMinAccepted) || isinf(lout));
     // the ring's share of the outer likelihood (NaN or a negative share fall back too)
@@ -1348,8 +1508,15 @@ cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, l
   return cudaGetLastError();
 }
 
+constexpr int kWedgeSmem = (kWedge + 1) * kBandThreads * (int)sizeof(float4);
+
 cudaError_t prepare_band_kernels() {
-  return raise_dynamic_smem(reinterpret_cast<const void*>(&k_mlp_forward), (int)sizeof(MlpSmem));
+  cudaError_t e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_mlp_forward), (int)sizeof(MlpSmem));
+  if (e == cudaSuccess) e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_band_ring_f32<8>), kWedgeSmem);
+  if (e == cudaSuccess) e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_band_ring_f32<16>), kWedgeSmem);
+  if (e == cudaSuccess) e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_band_ring_f32<24>), kWedgeSmem);
+  if (e == cudaSuccess) e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_band_ring_f32<32>), kWedgeSmem);
+  return e;
 }
 
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
@@ -1389,13 +1556,13 @@ cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st) {
 cudaError_t launch_band_dp(const BandParams& p, int cls, int sms, cudaStream_t st) {
   const int blocks = band_dp_blocks(sms, cls);
   if (cls == 0) {
-    k_band_ring_f32<8><<<blocks, 128, 0, st>>>(p, 0);
+    k_band_ring_f32<8><<<blocks, kBandThreads, kWedgeSmem, st>>>(p, 0);
   } else if (cls == 1) {
-    k_band_ring_f32<16><<<blocks, 128, 0, st>>>(p, 1);
+    k_band_ring_f32<16><<<blocks, kBandThreads, kWedgeSmem, st>>>(p, 1);
   } else if (cls == 2) {
-    k_band_ring_f32<24><<<blocks, 128, 0, st>>>(p, 2);
+    k_band_ring_f32<24><<<blocks, kBandThreads, kWedgeSmem, st>>>(p, 2);
   } else {
-    k_band_ring_f32<32><<<blocks, 128, 0, st>>>(p, 3);
+    k_band_ring_f32<32><<<blocks, kBandThreads, kWedgeSmem, st>>>(p, 3);
   }
   return cudaGetLastError();
 }
