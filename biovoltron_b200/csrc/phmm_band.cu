@@ -979,7 +979,7 @@ __device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, con
   c.g = qpg.p;
   const float gp = qpg.q;
   const int mi = mm_index(qi, qd);
-  const float mm = mmt[mi], inv = __ldg(minv + mi);
+  const float mm = __ldg(mmt + mi), inv = __ldg(minv + mi);
   c.cx = gp * ap * inv;
   c.cy = gp * bp * inv;
   c.kap = c.g * ap * qpi.inv;
@@ -988,14 +988,14 @@ __device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, con
   c.rb = onehot(base) * 0x11111111u;
   return c;
 }
-// Stages the probability tables the band kernels read per row into shared memory.
+// Stages the Phred table the band kernels read four times per row into shared
+// memory; the match-to-match entries (one per row, few distinct indices) are
+// read through the read-only cache, which leaves shared memory to the wedges.
 struct BandSmem {
   QProb qp[128];
-  float mm[kMMEntries];
 };
 __device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb) {
   for (int x = threadIdx.x; x < 128; x += blockDim.x) sm.qp[x] = tb->qp[x];
-  for (int x = threadIdx.x; x < kMMEntries; x += blockDim.x) sm.mm[x] = tb->mm_f[x];
   __syncthreads();
 }
 
@@ -1017,15 +1017,16 @@ __device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb
 // conflict-free; kWedge + 1 cells, the last always zero); only the active
 // cells of a row are touched.
 // ---------------------------------------------------------------------------
-constexpr int kWedge = 16;
+constexpr int kWedge = 24;
 constexpr int kBandThreads = 128;
-static_assert(kWedge * 4 <= 64, "wedge nibbles fit one 64-bit word");
+static_assert(kWedge * 4 <= 128, "wedge nibbles fit one 128-bit word");
+using WedgeBits = unsigned __int128;
 
 struct EndWedges {
   float4* wd;                 // this thread's cell 0
   int kp;                     // wedge depth of this pair
-  unsigned long long above;   // one-hot haplotype nibbles of the above wedge's cells (cell j: bits 4j..4j+3)
-  unsigned long long below;   // the same for the below wedge
+  WedgeBits above;           // one-hot haplotype nibbles of the above wedge's cells (cell j: bits 4j..4j+3)
+  WedgeBits below;           // the same for the below wedge
   int cells;                  // wedge cells computed
 
   // Row 0: every cell zero but the above wedge's start states (Y = INITIAL / H
@@ -1035,15 +1036,15 @@ struct EndWedges {
     wd = base;
     kp = max(0, min(kWedge, (R - 1) / 2));
     cells = 0;
-    above = 0ull;
-    below = 0ull;
+    above = 0;
+    below = 0;
     wd[kWedge * kBandThreads] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int j = 0; j < kWedge; ++j) {
       const int c = d + WB + j;
       wd[j * kBandThreads] = make_float4(0.f, 0.f, (j < kp && c >= 0 && c <= H) ? init_y : 0.f, 0.f);
       const int c1 = c + 1;
-      if (j < kp && c1 >= 1 && c1 <= H) above |= (unsigned long long)onehot(hap[c1 - 1]) << (4 * j);
+      if (j < kp && c1 >= 1 && c1 <= H) above |= (WedgeBits)onehot(hap[c1 - 1]) << (4 * j);
     }
   }
 
@@ -1111,9 +1112,9 @@ struct EndWedges {
     if (r <= kp) {
       above >>= 4;
       const int c = r + 1 + d + WB + kWedge - 1;
-      if (c >= 1 && c <= H) above |= (unsigned long long)onehot(hap[c - 1]) << (4 * (kWedge - 1));
+      if (c >= 1 && c <= H) above |= (WedgeBits)onehot(hap[c - 1]) << (4 * (kWedge - 1));
     }
-    if (r >= R - kp) below = (below << 4) | dropped;
+    if (r >= R - kp) below = (below << 4) | (WedgeBits)dropped;
   }
 
   // The below wedge's share of the result (last row, columns R + d - 1 - j).
@@ -1177,11 +1178,11 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
   EndWedges wg;
   if constexpr (WEDGE) wg.init(wedge_cells, R, H, d, WB, init_y, hap);
   float pmx_last = 1.f;
-  FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
+  FwdRow cur = fwd_row(sm.qp, tb->mm_f, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
+    const FwdRow nxt = fwd_row(sm.qp, tb->mm_f, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
     {
       const int rn = min(r + 1, R - 1);  // row r + 2
       qn = quals[rn];
@@ -1296,11 +1297,11 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
   EndWedges wg;  // the read ends' insertion wedges on the outer (result) band
   wg.init(wedge_cells, R, H, d, WB, init_y, hap);
   float pmx_last = 1.f;
-  FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);
+  FwdRow cur = fwd_row(sm.qp, tb->mm_f, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
+    const FwdRow nxt = fwd_row(sm.qp, tb->mm_f, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
     {
       const int rn = min(r + 1, R - 1);
       qn = quals[rn];

@@ -161,6 +161,11 @@ __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)
 __device__ __forceinline__ void mbar_init(uint64_t* mb, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mb)), "r"(count) : "memory");
 }
+// A live barrier may not be initialised again: each strip invalidates its
+// barriers once their last phase has completed.
+__device__ __forceinline__ void mbar_inval(uint64_t* mb) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(mb)) : "memory");
+}
 // Makes barrier initialisation and this thread's earlier generic writes to
 // global memory visible to the async proxy (the bulk copies).
 __device__ __forceinline__ void fence_for_bulk() {
@@ -507,7 +512,18 @@ __device__ __forceinline__ void run_strip(const Rows<T, RT>& rw, const ELane el,
     }
   }
   if constexpr (MULTI) {
-    if (lane == 0 && !bulk_ok && status) atomicOr(status, 8ull);
+    // Every copy has been waited for (the last chunk waits for the half it
+    // prefetched), unless a wait gave up; then the copy may still land, and
+    // the barriers stay as they are (the status already fails the call).
+    if (lane == 0) {
+      if (bulk_ok) {
+        mbar_inval(mb);
+        mbar_inval(mb + 1);
+      } else if (status) {
+        atomicOr(status, 8ull);
+      }
+    }
+    __syncwarp();
   }
   lastM = M[RT - 1];
   lastY = Y[RT - 1];

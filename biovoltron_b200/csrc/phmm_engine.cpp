@@ -87,6 +87,23 @@ bv_status Engine::fail(bv_status s, const std::string& msg) {
   return s;
 }
 
+bv_status Engine::status_fail(unsigned long long status) {
+  // Kernel status bits: 1 FP64 list overflow, 2 invalid pair, 4 band list
+  // overflow, 8 a boundary-row bulk copy did not complete in time.
+  static const char* const kNames[] = {"FP64 list overflow", "invalid pair", "band list overflow",
+                                       "boundary copy wait gave up"};
+  std::string msg = "kernel reported an inconsistent state (";
+  bool first = true;
+  for (int b = 0; b < 4; ++b) {
+    if (!(status >> b & 1ull)) continue;
+    msg += first ? "" : ", ";
+    msg += kNames[b];
+    first = false;
+  }
+  if (status >> 4) msg += std::string(first ? "" : ", ") + "status " + std::to_string(status);
+  return fail(BV_ERR_INTERNAL, msg + ")");
+}
+
 bv_status Engine::cuda_fail(cudaError_t e, const char* what) {
   err_ = std::string(what) + ": " + cudaGetErrorString(e);
   if (e == cudaErrorMemoryAllocation) return BV_ERR_OOM;
@@ -544,7 +561,7 @@ bv_status Engine::finish(bv_phmm_stats* stats) {
     h2d_time_pending_ = false;
   }
   const Counters c = *h_counters_;
-  if (c.status != 0) return fail(BV_ERR_INTERNAL, "kernel reported an inconsistent state");
+  if (c.status != 0) return status_fail(c.status);
   if (stats) *stats = bv_phmm_stats{};
   if (stats && band_enabled()) {
     bv_status bs = band_stats(stats);

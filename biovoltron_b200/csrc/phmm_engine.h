@@ -154,6 +154,8 @@ class Engine {
 
   const char* last_error() const { return err_.c_str(); }
   bv_status fail(bv_status s, const std::string& msg);
+  // BV_ERR_INTERNAL naming the kernel status bits that were set.
+  bv_status status_fail(unsigned long long status);
   bv_status cuda_fail(cudaError_t e, const char* what);
   int64_t staged_results() const { return n_results_; }
   cudaStream_t stream() const { return stream_; }

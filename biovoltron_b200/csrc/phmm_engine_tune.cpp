@@ -100,7 +100,7 @@ bv_status Engine::autotune(const bv_region_batch& sample, int repeats, bv_phmm_t
         break;
       }
       if (cc.status != 0) {
-        s = fail(BV_ERR_INTERNAL, "kernel reported an inconsistent state");
+        s = status_fail(cc.status);
         break;
       }
       if (k == 0) continue;

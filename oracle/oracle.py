@@ -122,7 +122,7 @@ class Oracle:
         W = np.broadcast_to(np.asarray(W, np.int64), (tcs.n,))
         return np.array([self._band(C.pointer(tcs.arr[k]), int(d_lo[k]), int(W[k])) for k in range(tcs.n)])
 
-    def band_wedge_log10(self, tcs: TestcaseArray, d_lo, W, kmax: int = 16) -> np.ndarray:
+    def band_wedge_log10(self, tcs: TestcaseArray, d_lo, W, kmax: int = 24) -> np.ndarray:
         """The band plus the read ends' insertion wedges of depth min(kmax, (R - 1) / 2)."""
         d_lo = np.broadcast_to(np.asarray(d_lo, np.int64), (tcs.n,))
         W = np.broadcast_to(np.asarray(W, np.int64), (tcs.n,))

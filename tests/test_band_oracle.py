@@ -69,12 +69,12 @@ def test_band_with_end_wedges_brackets_band_and_full(oracle):
     ds = np.array([0 if seed_diagonal(b.read(int(r[k]))[0], b.hap(int(h[k]))) is None
                    else seed_diagonal(b.read(int(r[k]))[0], b.hap(int(h[k]))) for k in sel])
     band = oracle.band_log10(tcs, ds - 6, 12)
-    wedge = oracle.band_wedge_log10(tcs, ds - 6, 12, kmax=16)
+    wedge = oracle.band_wedge_log10(tcs, ds - 6, 12, kmax=24)
     none = oracle.band_wedge_log10(tcs, ds - 6, 12, kmax=0)
     fin = np.isfinite(band)
     assert np.all(wedge[fin] >= band[fin] - 1e-12) and np.all(wedge <= full + 1e-9)
     assert np.allclose(none[fin], band[fin], rtol=0, atol=1e-12)
     R = b.read_lengths()[r[sel]]
     H = b.hap_lengths()[h[sel]]
-    whole = oracle.band_wedge_log10(tcs, -R, R + H + 1, kmax=16)
+    whole = oracle.band_wedge_log10(tcs, -R, R + H + 1, kmax=24)
     assert np.allclose(whole, full, rtol=0, atol=1e-9)

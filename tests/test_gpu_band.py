@@ -52,9 +52,9 @@ def test_fixed_band_matches_oracle_band(oracle):
     sel = np.array(sel)
     sub = TestcaseArray(b, r[sel], h[sel])
     # the result is the band widened by the ring (4 diagonals on each side, 8 from W = 16) plus the
-    # read ends' insertion wedges (16 rows deep)
+    # read ends' insertion wedges (24 rows deep)
     ring = np.where(np.array(wcls) >= 16, 8, 4)
-    exp = oracle.band_wedge_log10(sub, np.array(d_lo) - ring, np.array(wcls) + 2 * ring, kmax=16)
+    exp = oracle.band_wedge_log10(sub, np.array(d_lo) - ring, np.array(wcls) + 2 * ring, kmax=24)
     fin = np.isfinite(exp) & (exp > -60)
     assert np.max(np.abs(got[sel][fin] - exp[fin])) <= TOL_FP32
 
