@@ -310,7 +310,27 @@ def accuracy(batch, got_band, got_plain, n_sample: int, seed: int):
         out["band_vs_full_dp_all_pairs"] = {"max": float(d.max(initial=0)),
                                             "p99": float(np.quantile(d, 0.99)) if d.size else 0.0,
                                             "over_1e-3": int(np.sum(d > 1e-3)), "pairs": int(both.sum())}
+        nb, nf = normalized(batch, got_band), normalized(batch, got_plain)
+        both = np.isfinite(nb) & np.isfinite(nf)
+        d = np.abs(nb[both] - nf[both])
+        out["band_vs_full_dp_normalized"] = {
+            "what": "the call's result: each read's row capped at its best - 4.5 (PairHMM::normalize_likelihoods)",
+            "max": float(d.max(initial=0)), "over_1e-3": int(np.sum(d > 1e-3)), "pairs": int(both.sum())}
     return out
+
+
+def normalized(batch, lk):
+    """Each read's likelihoods raised to at least the read's best - 4.5, as
+    PairHMM::normalize_likelihoods (pairhmm.hpp:83-93) does to the call's result.
+    Results are region by region, read-major: a read's haplotypes are contiguous."""
+    nr = np.diff(batch.region_reads)
+    nh = np.diff(batch.region_haps)
+    per_read = np.repeat(nh, nr)
+    keep = per_read > 0
+    starts = np.concatenate([[0], np.cumsum(per_read)[:-1]])[keep]
+    best = np.maximum.reduceat(lk, starts) if starts.size else np.zeros(0)
+    cap = np.repeat(best - 4.5, per_read[keep])
+    return np.maximum(lk, cap)
 
 
 def main():

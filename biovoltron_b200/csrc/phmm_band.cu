@@ -979,7 +979,7 @@ __device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, con
   c.g = qpg.p;
   const float gp = qpg.q;
   const int mi = mm_index(qi, qd);
-  const float mm = __ldg(mmt + mi), inv = __ldg(minv + mi);
+  const float mm = mmt[mi], inv = __ldg(minv + mi);
   c.cx = gp * ap * inv;
   c.cy = gp * bp * inv;
   c.kap = c.g * ap * qpi.inv;
@@ -988,148 +988,16 @@ __device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, con
   c.rb = onehot(base) * 0x11111111u;
   return c;
 }
-// Stages the Phred table the band kernels read four times per row into shared
-// memory; the match-to-match entries (one per row, few distinct indices) are
-// read through the read-only cache, which leaves shared memory to the wedges.
+// Stages the probability tables the band kernels read per row into shared memory.
 struct BandSmem {
   QProb qp[128];
+  float mm[kMMEntries];
 };
 __device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb) {
   for (int x = threadIdx.x; x < 128; x += blockDim.x) sm.qp[x] = tb->qp[x];
+  for (int x = threadIdx.x; x < kMMEntries; x += blockDim.x) sm.mm[x] = tb->mm_f[x];
   __syncthreads();
 }
-
-// ---------------------------------------------------------------------------
-// Read-end insertion wedges.  A read end that does not fit the haplotype near
-// the band (bases a haplotype-specific indel separates from the rest of the
-// read, or sequencing junk) is explained by insertion runs: at the read's
-// start a path may begin above the band and run down into it (X steps keep
-// the column and lower the diagonal), at its end leave the band's bottom
-// edge and run down to the last row -- with a few matches in between.  Such
-// paths lie in two triangles next to the result band: above it in the first
-// kp rows (row r: diagonals hi + 1 .. hi + kp + 1 - r, i.e. every column up to
-// hi + kp + 1) and below it in the last kp rows (row R - kp + m: diagonals
-// lo - m .. lo - 1, i.e. every column from lo + R - kp on), kp = min(kWedge,
-// (R - 1) / 2).  The result band's DP covers those cells too, with the same
-// recurrence, so the banded value is the exact likelihood of every path in
-// the band plus the wedges.  The wedge cells live in shared memory (cell j of
-// a thread at wd[j * kBandThreads], threads interleaved so float4 accesses are
-// conflict-free; kWedge + 1 cells, the last always zero); only the active
-// cells of a row are touched.
-// ---------------------------------------------------------------------------
-constexpr int kWedge = 24;
-constexpr int kBandThreads = 128;
-static_assert(kWedge * 4 <= 128, "wedge nibbles fit one 128-bit word");
-using WedgeBits = unsigned __int128;
-
-struct EndWedges {
-  float4* wd;                 // this thread's cell 0
-  int kp;                     // wedge depth of this pair
-  WedgeBits above;           // one-hot haplotype nibbles of the above wedge's cells (cell j: bits 4j..4j+3)
-  WedgeBits below;           // the same for the below wedge
-  int cells;                  // wedge cells computed
-
-  // Row 0: every cell zero but the above wedge's start states (Y = INITIAL / H
-  // on its columns); the above wedge's row-1 columns d + WB + 1 + j.
-  __device__ __forceinline__ void init(float4* base, int R, int H, int d, int WB, float init_y,
-                                       const uint8_t* __restrict__ hap) {
-    wd = base;
-    kp = max(0, min(kWedge, (R - 1) / 2));
-    cells = 0;
-    above = 0;
-    below = 0;
-    wd[kWedge * kBandThreads] = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-    for (int j = 0; j < kWedge; ++j) {
-      const int c = d + WB + j;
-      wd[j * kBandThreads] = make_float4(0.f, 0.f, (j < kp && c >= 0 && c <= H) ? init_y : 0.f, 0.f);
-      const int c1 = c + 1;
-      if (j < kp && c1 >= 1 && c1 <= H) above |= (WedgeBits)onehot(hap[c1 - 1]) << (4 * j);
-    }
-  }
-
-  // Below wedge at row r, before the band's cells: farthest cell first (the
-  // deletion chain runs towards the band); returns the chain's M and Y for the
-  // band's lowest cell.  m0 / x0: that cell's values in row r - 1.
-  __device__ __forceinline__ void below_row(int r, int R, const FwdRow& cur, float m0, float x0, float& lm,
-                                            float& ly) {
-    lm = 0.f;
-    ly = 0.f;
-    if (r <= R - kp) return;
-    const int m = r - (R - kp);  // active cells 0 .. m-1
-    const uint32_t rnib = cur.rb & 0xFu;
-    for (int j = m - 1; j >= 0; --j) {
-      const float4 prev = wd[j * kBandThreads];
-      float upm = m0, upx = x0;
-      if (j >= 1) {
-        const float4 u = wd[(j - 1) * kBandThreads];
-        upm = u.x;
-        upx = u.y;
-      }
-      const float e = ((uint32_t)(below >> (4 * j)) & rnib) ? cur.em : cur.ex;
-      const float mn = e * __fmaf_rn(cur.cy, prev.z, __fmaf_rn(cur.cx, prev.y, prev.x));
-      const float xn = __fmaf_rn(cur.kap, upx, upm);
-      const float yn = __fmaf_rn(cur.g, ly, lm);
-      wd[j * kBandThreads] = make_float4(mn, xn, yn, 0.f);
-      lm = mn;
-      ly = yn;
-    }
-    cells += m;
-  }
-
-  // The above wedge's cell 0 in row r - 1 (the band's top cell takes its X
-  // from there), zero once the wedge has ended.
-  __device__ __forceinline__ float4 above_prev0(int r) const {
-    return r <= kp + 1 ? wd[0] : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-
-  // Above wedge at row r, after the band's cells, chained from the band's top
-  // cell (lm, ly); the cell that leaves the triangle this row is cleared.
-  __device__ __forceinline__ void above_row(int r, const FwdRow& cur, float lm, float ly) {
-    if (r > kp + 1) return;
-    const int na = kp - r + 1;  // active cells 0 .. na-1
-    const uint32_t rnib = cur.rb & 0xFu;
-    for (int j = 0; j < na; ++j) {
-      const float4 prev = wd[j * kBandThreads];
-      const float4 up = wd[(j + 1) * kBandThreads];  // j + 1 <= kp <= kWedge: an active, cleared or spare cell
-      const float e = ((uint32_t)(above >> (4 * j)) & rnib) ? cur.em : cur.ex;
-      const float mn = e * __fmaf_rn(cur.cy, prev.z, __fmaf_rn(cur.cx, prev.y, prev.x));
-      const float xn = __fmaf_rn(cur.kap, up.y, up.x);
-      const float yn = __fmaf_rn(cur.g, ly, lm);
-      wd[j * kBandThreads] = make_float4(mn, xn, yn, 0.f);
-      lm = mn;
-      ly = yn;
-    }
-    wd[na * kBandThreads] = make_float4(0.f, 0.f, 0.f, 0.f);
-    cells += na;
-  }
-
-  // End of row r: the above wedge's columns move one cell down, a new one
-  // enters at the far end; the column leaving the band's window (`dropped`,
-  // column r + d) becomes the below wedge's nearest one.
-  __device__ __forceinline__ void shift(int r, int R, int H, int d, int WB, const uint8_t* __restrict__ hap,
-                                        uint32_t dropped) {
-    if (r <= kp) {
-      above >>= 4;
-      const int c = r + 1 + d + WB + kWedge - 1;
-      if (c >= 1 && c <= H) above |= (WedgeBits)onehot(hap[c - 1]) << (4 * (kWedge - 1));
-    }
-    if (r >= R - kp) below = (below << 4) | (WedgeBits)dropped;
-  }
-
-  // The below wedge's share of the result (last row, columns R + d - 1 - j).
-  __device__ __forceinline__ float last_row(int R, int H, int d, float pmx_last) const {
-    float t = 0.f;
-    for (int j = 0; j < kp; ++j) {
-      const int c = R + d - 1 - j;
-      if (c >= 1 && c <= H) {
-        const float4 v = wd[j * kBandThreads];
-        t += v.x + pmx_last * v.y;
-      }
-    }
-    return t;
-  }
-};
 
 // ---------------------------------------------------------------------------
 // Ring test.  A pair banded on [d_lo, d_lo + W) is also scored on the band
@@ -1142,11 +1010,10 @@ struct EndWedges {
 // model cannot represent.  W = 8, 16 run both bands in one row sweep (shared
 // row constants and emissions); W = 24, 32 run them one after the other.
 // ---------------------------------------------------------------------------
-template <int WB, int WI, bool WEDGE = false>
+template <int WB, int WI>
 __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Tables* tb, const uchar4* __restrict__ quals,
                                                const uint8_t* __restrict__ rbase, const uint8_t* __restrict__ hap,
-                                               int R, int H, int d, float4* wedge_cells = nullptr,
-                                               int* wedge_count = nullptr) {
+                                               int R, int H, int d) {
   constexpr int NW = WB / 8;
   constexpr int OFF = (WB - WI) / 2;  // inner band = outer diagonals OFF .. OFF + WI - 1
   constexpr int WIN = WI > 0 ? WI : 1;
@@ -1175,14 +1042,12 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
     }
     win[w] = v;
   }
-  EndWedges wg;
-  if constexpr (WEDGE) wg.init(wedge_cells, R, H, d, WB, init_y, hap);
   float pmx_last = 1.f;
-  FwdRow cur = fwd_row(sm.qp, tb->mm_f, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
+  FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm.qp, tb->mm_f, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
+    const FwdRow nxt = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
     {
       const int rn = min(r + 1, R - 1);  // row r + 2
       qn = quals[rn];
@@ -1191,18 +1056,13 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
     const int cn = r + 1 + d + WB - 1;  // next row's window: shift, append column cn
     const uint8_t hb = (cn >= 1 && cn <= H) ? hap[cn - 1] : (uint8_t)0;
     float lm = 0.f, ly = 0.f, lmi = 0.f, lyi = 0.f;
-    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if constexpr (WEDGE) {
-      wg.below_row(r, R, cur, M[0], X[0], lm, ly);
-      a0 = wg.above_prev0(r);
-    }
 #pragma unroll
     for (int k = 0; k < WB; ++k) {
       const bool match = (win[k >> 3] & cur.rb & (0xFu << (4 * (k & 7)))) != 0u;
       const float e = match ? cur.em : cur.ex;
       {
-        const float upm = (k + 1 < WB) ? M[k + 1] : a0.x;
-        const float upx = (k + 1 < WB) ? X[k + 1] : a0.y;
+        const float upm = (k + 1 < WB) ? M[k + 1] : 0.f;
+        const float upx = (k + 1 < WB) ? X[k + 1] : 0.f;
         const float mn = e * __fmaf_rn(cur.cy, Y[k], __fmaf_rn(cur.cx, X[k], M[k]));
         const float xn = __fmaf_rn(cur.kap, upx, upm);
         const float yn = __fmaf_rn(cur.g, ly, lm);
@@ -1222,10 +1082,6 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
         }
       }
     }
-    if constexpr (WEDGE) {
-      wg.above_row(r, cur, lm, ly);
-      wg.shift(r, R, H, d, WB, hap, win[0] & 0xFu);
-    }
     const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
 #pragma unroll
     for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
@@ -1238,10 +1094,6 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
   for (int k = 0; k < WB; ++k) {
     const int c = R + d + k;
     tot += (c >= 1 && c <= H) ? M[k] + pmx_last * X[k] : 0.f;
-  }
-  if constexpr (WEDGE) {
-    tot += wg.last_row(R, H, d, pmx_last);
-    *wedge_count = wg.cells;
   }
 #pragma unroll
   for (int k = 0; k < WIN; ++k) {
@@ -1262,7 +1114,7 @@ template <int WB, int WI>
 __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const Tables* tb,
                                                       const uchar4* __restrict__ quals,
                                                       const uint8_t* __restrict__ rbase, const uint8_t* __restrict__ hap,
-                                                      int R, int H, int d, float4* wedge_cells, int* wedge_count) {
+                                                      int R, int H, int d) {
   constexpr int NW = WB / 8;
   constexpr int OFF = (WB - WI) / 2;   // outer cells 0 .. OFF-1: lower ring; OFF+WI .. WB-1: upper ring
   constexpr int NHI = WB - OFF - WI;
@@ -1294,14 +1146,12 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
     }
     win[w] = v;
   }
-  EndWedges wg;  // the read ends' insertion wedges on the outer (result) band
-  wg.init(wedge_cells, R, H, d, WB, init_y, hap);
   float pmx_last = 1.f;
-  FwdRow cur = fwd_row(sm.qp, tb->mm_f, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);
+  FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm.qp, tb->mm_f, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
+    const FwdRow nxt = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
     {
       const int rn = min(r + 1, R - 1);
       qn = quals[rn];
@@ -1315,9 +1165,7 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
       const bool match = (win[k >> 3] & cur.rb & (0xFu << (4 * (k & 7)))) != 0u;
       return match ? cur.em : cur.ex;
     };
-    float lm, ly;
-    wg.below_row(r, R, cur, Ml[0], Xl[0], lm, ly);
-    const float4 a0 = wg.above_prev0(r);
+    float lm = 0.f, ly = 0.f;
     // lower ring
 #pragma unroll
     for (int k = 0; k < OFF; ++k) {
@@ -1350,16 +1198,14 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
 #pragma unroll
     for (int k = 0; k < NHI; ++k) {
       const float e = emis(OFF + WI + k);
-      const float upm = k + 1 < NHI ? Mh[k + 1] : a0.x;
-      const float upx = k + 1 < NHI ? Xh[k + 1] : a0.y;
+      const float upm = k + 1 < NHI ? Mh[k + 1] : 0.f;
+      const float upx = k + 1 < NHI ? Xh[k + 1] : 0.f;
       const float mn = e * __fmaf_rn(cur.cy, Yh[k], __fmaf_rn(cur.cx, Xh[k], Mh[k]));
       const float xn = __fmaf_rn(cur.kap, upx, upm);
       const float yn = __fmaf_rn(cur.g, ly, lm);
       Mh[k] = mn; Xh[k] = xn; Yh[k] = yn;
       lm = mn; ly = yn;
     }
-    wg.above_row(r, cur, lm, ly);
-    wg.shift(r, R, H, d, WB, hap, win[0] & 0xFu);
     const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
 #pragma unroll
     for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
@@ -1376,8 +1222,6 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
     const float x = k < OFF ? Xl[k] : k < OFF + WI ? P_X[k - OFF].x : Xh[k - OFF - WI];
     tot += (c >= 1 && c <= H) ? m + pmx_last * x : 0.f;
   }
-  tot += wg.last_row(R, H, d, pmx_last);
-  *wedge_count = wg.cells;
 #pragma unroll
   for (int k = 0; k < WI; ++k) {
     const int c = R + d + OFF + k;
@@ -1388,24 +1232,21 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
 
 // One band alone, not inlined: the two passes of the wider classes then hold
 // one band's state at a time.
-template <int WB, bool WEDGE>
+template <int WB>
 __device__ __noinline__ float band_forward_pass(const BandSmem& sm, const Tables* tb, const uchar4* quals,
-                                                const uint8_t* rbase, const uint8_t* hap, int R, int H, int d,
-                                                float4* wedge_cells, int* wedge_count) {
-  return band_forward_body<WB, 0, WEDGE>(sm, tb, quals, rbase, hap, R, H, d, wedge_cells, wedge_count).x;
+                                                const uint8_t* rbase, const uint8_t* hap, int R, int H, int d) {
+  return band_forward_body<WB, 0>(sm, tb, quals, rbase, hap, R, H, d).x;
 }
 
 // W = 8 keeps three blocks per SM (up to 168 registers); the wider classes two.
 template <int W>
-__global__ void __launch_bounds__(kBandThreads, W <= 8 ? 3 : 2) k_band_ring_f32(BandParams p, int cls) {
+__global__ void __launch_bounds__(128, W <= 8 ? 3 : 2) k_band_ring_f32(BandParams p, int cls) {
   constexpr bool kDual = W <= 16;  // both bands in one sweep
   // ring width on each side: pairs routed to wider bands have indel-rich alignments whose
   // alternatives lie farther out, so W >= 16 test eight diagonals
   constexpr int kRing = W >= 16 ? 8 : 4;
   const Tables* tb = p.tables;
   __shared__ BandSmem sm;
-  extern __shared__ float4 wedge_smem[];  // (kWedge + 1) x kBandThreads cells
-  float4* wcells = wedge_smem + threadIdx.x;
   stage_band_tables(sm, tb);
   // routed items (bucketed by read length), then items promoted from the next narrower class
   const unsigned long long total =
@@ -1422,18 +1263,16 @@ __global__ void __launch_bounds__(kBandThreads, W <= 8 ? 3 : 2) k_band_ring_f32(
     const uint8_t* rbase = p.batch.read_bases + ro;
     const uint8_t* hap = p.batch.hap_bases + ho;
     float lin, lout;
-    int wcount = 0;
     if constexpr (kDual) {
-      const float2 t = band_forward_paired<W + 2 * kRing, W>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing,
-                                                              wcells, &wcount);
+      const float2 t = band_forward_paired<W + 2 * kRing, W>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
       lout = t.x;
       lin = t.y;
     } else {
-      lin = band_forward_pass<W, false>(sm, tb, quals, rbase, hap, R, H, it.d_lo, nullptr, nullptr);
-      lout = band_forward_pass<W + 2 * kRing, true>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing, wcells, &wcount);
+      lin = band_forward_pass<W>(sm, tb, quals, rbase, hap, R, H, it.d_lo);
+      lout = band_forward_pass<W + 2 * kRing>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
     }
-    cells += (unsigned long long)R * (2 * W + 2 * kRing) + (unsigned long long)wcount;
-    rcells += (unsigned long long)R * (W + 2 * kRing) + (unsigned long long)wcount;
+    cells += (unsigned long long)R * (2 * W + 2 * kRing);
+    rcells += (unsigned long long)R * (W + 2 * kRing);
     bool fall_back = !(lout > 0.f);
     const bool rescue = !fall_back && (!(lout >= (float)kMinAccepted) || isinf(lout));
     // the ring's share of the outer likelihood (NaN or a negative share fall back too)
@@ -1509,15 +1348,8 @@ cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, l
   return cudaGetLastError();
 }
 
-constexpr int kWedgeSmem = (kWedge + 1) * kBandThreads * (int)sizeof(float4);
-
 cudaError_t prepare_band_kernels() {
-  cudaError_t e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_mlp_forward), (int)sizeof(MlpSmem));
-  if (e == cudaSuccess) e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_band_ring_f32<8>), kWedgeSmem);
-  if (e == cudaSuccess) e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_band_ring_f32<16>), kWedgeSmem);
-  if (e == cudaSuccess) e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_band_ring_f32<24>), kWedgeSmem);
-  if (e == cudaSuccess) e = raise_dynamic_smem(reinterpret_cast<const void*>(&k_band_ring_f32<32>), kWedgeSmem);
-  return e;
+  return raise_dynamic_smem(reinterpret_cast<const void*>(&k_mlp_forward), (int)sizeof(MlpSmem));
 }
 
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
@@ -1557,13 +1389,13 @@ cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st) {
 cudaError_t launch_band_dp(const BandParams& p, int cls, int sms, cudaStream_t st) {
   const int blocks = band_dp_blocks(sms, cls);
   if (cls == 0) {
-    k_band_ring_f32<8><<<blocks, kBandThreads, kWedgeSmem, st>>>(p, 0);
+    k_band_ring_f32<8><<<blocks, 128, 0, st>>>(p, 0);
   } else if (cls == 1) {
-    k_band_ring_f32<16><<<blocks, kBandThreads, kWedgeSmem, st>>>(p, 1);
+    k_band_ring_f32<16><<<blocks, 128, 0, st>>>(p, 1);
   } else if (cls == 2) {
-    k_band_ring_f32<24><<<blocks, kBandThreads, kWedgeSmem, st>>>(p, 2);
+    k_band_ring_f32<24><<<blocks, 128, 0, st>>>(p, 2);
   } else {
-    k_band_ring_f32<32><<<blocks, kBandThreads, kWedgeSmem, st>>>(p, 3);
+    k_band_ring_f32<32><<<blocks, 128, 0, st>>>(p, 3);
   }
   return cudaGetLastError();
 }

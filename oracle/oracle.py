@@ -107,7 +107,6 @@ class Oracle:
             _bind(L, nm, C.POINTER(t), [])
         _bind(L, "orc_table_mm_size", C.c_int, [])
         self._band = _bind(L, "orc_band_log10", C.c_double, [P, C.c_int, C.c_int])
-        self._band_wedge = _bind(L, "orc_band_wedge_log10", C.c_double, [P, C.c_int, C.c_int, C.c_int])
         self._post = _bind(L, "orc_posterior_diag", C.c_int, [P, C.c_void_p])
         self._leak = _bind(L, "orc_band_leak_bound", C.c_double, [])
         self.set_rho = _bind(L, "orc_band_set_rho", None, [C.c_double])
@@ -121,12 +120,6 @@ class Oracle:
         d_lo = np.broadcast_to(np.asarray(d_lo, np.int64), (tcs.n,))
         W = np.broadcast_to(np.asarray(W, np.int64), (tcs.n,))
         return np.array([self._band(C.pointer(tcs.arr[k]), int(d_lo[k]), int(W[k])) for k in range(tcs.n)])
-
-    def band_wedge_log10(self, tcs: TestcaseArray, d_lo, W, kmax: int = 24) -> np.ndarray:
-        """The band plus the read ends' insertion wedges of depth min(kmax, (R - 1) / 2)."""
-        d_lo = np.broadcast_to(np.asarray(d_lo, np.int64), (tcs.n,))
-        W = np.broadcast_to(np.asarray(W, np.int64), (tcs.n,))
-        return np.array([self._band_wedge(C.pointer(tcs.arr[k]), int(d_lo[k]), int(W[k]), kmax) for k in range(tcs.n)])
 
     def band_detail(self, tcs: TestcaseArray, d_lo, W):
         """Banded log10 plus the kernel's edge statistics (row_ratio, end_frac)."""

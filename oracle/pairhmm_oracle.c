@@ -438,74 +438,6 @@ double orc_band_log10(const orc_testcase *tc, int d_lo, int W) {
 }
 
 /*
- * The banded DP of orc_band_log10 on the band [d_lo, d_lo + W) together with
- * the read ends' insertion wedges the banded kernels add to their result
- * band: above the band in rows 1 .. kp (row r: diagonals up to
- * d_lo + W - 1 + kp + 1 - r) and below it in rows R - kp + 1 .. R (row
- * R - kp + m: diagonals down to d_lo - m), kp = min(kmax, (R - 1) / 2); the
- * start states Y(0, c) = 1/H cover the band's and the upper wedge's row-1
- * diagonals.  The region's cells follow the recurrence of orc_band_log10
- * (every other cell is zero); FP64 with each row rescaled by a power of two.
- */
-static int orc_in_wedged(int r, int dg, int R, int lo, int hi, int kp) {
-    if (dg >= lo && dg <= hi) return 1;
-    if (r <= kp && dg > hi && dg <= hi + kp + 1 - r) return 1;
-    if (r > R - kp && dg < lo && dg >= lo - (r - (R - kp))) return 1;
-    return 0;
-}
-
-double orc_band_wedge_log10(const orc_testcase *tc, int d_lo, int W, int kmax) {
-    orc_init();
-    const int R = tc->rslen, H = tc->haplen;
-    if (R == 0 || H == 0 || W <= 0) return -INFINITY;
-    int kp = (R - 1) / 2;
-    if (kp > kmax) kp = kmax;
-    if (kp < 0) kp = 0;
-    const int lo = d_lo, hi = d_lo + W - 1;
-    double *buf = (double *)calloc((size_t)6 * (H + 2), sizeof(double));
-    double *Mp = buf, *Xp = buf + (H + 2), *Yp = buf + 2 * (H + 2);
-    double *Mc = buf + 3 * (H + 2), *Xc = buf + 4 * (H + 2), *Yc = buf + 5 * (H + 2);
-    for (int c = 0; c <= H; c++) {
-        /* row 0: the start state of diagonal c feeds row 1's M on diagonal c */
-        Yp[c] = ((c >= lo && c <= hi) || (kp >= 1 && c > hi && c <= hi + kp)) ? 1.0 / (double)H : 0.0;
-    }
-    long long e2sum = 0;
-    for (int r = 1; r <= R; r++) {
-        const int qi = tc->i[r - 1] & 127, qd = tc->d[r - 1] & 127;
-        const int qc = tc->c[r - 1] & 127, qq = tc->q[r - 1] & 127;
-        const double pMM = set_mm_prob_d(qi, qd), gp = 1.0 - ph2pr_d[qc];
-        const double pMX = ph2pr_d[qi], pMY = ph2pr_d[qd], g = ph2pr_d[qc];
-        const double eps = ph2pr_d[qq], one_m = 1.0 - eps, mis = eps / 3.0;
-        const uint8_t rc = base_code[(uint8_t)tc->rs[r - 1]];
-        double mx = 0;
-        Mc[0] = Xc[0] = Yc[0] = 0;
-        for (int c = 1; c <= H; c++) {
-            if (!orc_in_wedged(r, c - r, R, lo, hi, kp)) { Mc[c] = Xc[c] = Yc[c] = 0; continue; }
-            const double e = is_match(rc, base_code[(uint8_t)tc->hap[c - 1]]) ? one_m : mis;
-            Mc[c] = e * (pMM * Mp[c - 1] + gp * Xp[c - 1] + gp * Yp[c - 1]);
-            Xc[c] = pMX * Mp[c] + g * Xp[c];
-            Yc[c] = pMY * Mc[c - 1] + g * Yc[c - 1];
-            double m = Mc[c] > Xc[c] ? Mc[c] : Xc[c];
-            m = m > Yc[c] ? m : Yc[c];
-            mx = mx > m ? mx : m;
-        }
-        if (mx > 0) {
-            int e2; frexp(mx, &e2);
-            const double sc = ldexp(1.0, -e2);
-            for (int c = 0; c <= H; c++) { Mc[c] *= sc; Xc[c] *= sc; Yc[c] *= sc; }
-            e2sum += e2;
-        }
-        double *t;
-        t = Mp; Mp = Mc; Mc = t; t = Xp; Xp = Xc; Xc = t; t = Yp; Yp = Yc; Yc = t;
-    }
-    double s = 0;
-    for (int c = 1; c <= H; c++) s += Mp[c] + Xp[c];
-    free(buf);
-    if (!(s > 0)) return -INFINITY;
-    return log10(s) + (double)e2sum * log10(2.0);
-}
-
-/*
  * Posterior spread over diagonals from the full forward-backward DP.
  * For each row r >= 1 the posterior of the cells, p_r(c) ~ sum over states
  * of F_s(r,c) B_s(r,c), is normalised to sum 1 over the row; pstar[d - dmin]

@@ -5,7 +5,7 @@ posterior concentrates on the diagonal the read was sampled from."""
 import numpy as np
 
 from biovoltron_b200 import workloads as W
-from oracle.oracle import TestcaseArray, seed_diagonal
+from oracle.oracle import TestcaseArray
 
 
 def _pairs(seed, n=6):
@@ -54,27 +54,3 @@ def test_posterior_peaks_on_the_sampled_diagonal(oracle):
         assert p.max() > 0.9
         far = np.abs(np.arange(len(p)) + dmin - offs[k]) > 20
         assert p[far].max() < 1e-6
-
-
-def test_band_with_end_wedges_brackets_band_and_full(oracle):
-    """The band plus the read ends' insertion wedges holds every banded path
-    and more: its likelihood lies between the band's and the full DP's, equals
-    the band's with no wedge, and equals the full DP once the band covers the
-    whole matrix."""
-    b = W.config1(seed=12, n_regions=2)
-    r, h = b.pair_index()
-    sel = np.arange(0, b.n_pairs, 11)
-    tcs = TestcaseArray(b, r[sel], h[sel])
-    full = oracle.log10_rescaled(tcs)
-    ds = np.array([0 if seed_diagonal(b.read(int(r[k]))[0], b.hap(int(h[k]))) is None
-                   else seed_diagonal(b.read(int(r[k]))[0], b.hap(int(h[k]))) for k in sel])
-    band = oracle.band_log10(tcs, ds - 6, 12)
-    wedge = oracle.band_wedge_log10(tcs, ds - 6, 12, kmax=24)
-    none = oracle.band_wedge_log10(tcs, ds - 6, 12, kmax=0)
-    fin = np.isfinite(band)
-    assert np.all(wedge[fin] >= band[fin] - 1e-12) and np.all(wedge <= full + 1e-9)
-    assert np.allclose(none[fin], band[fin], rtol=0, atol=1e-12)
-    R = b.read_lengths()[r[sel]]
-    H = b.hap_lengths()[h[sel]]
-    whole = oracle.band_wedge_log10(tcs, -R, R + H + 1, kmax=24)
-    assert np.allclose(whole, full, rtol=0, atol=1e-9)

