@@ -35,7 +35,6 @@ __device__ __forceinline__ int kmer_code(uint8_t b) {
 __device__ __forceinline__ uint32_t onehot(uint8_t b) {
   return b == 'C' ? 2u : b == 'T' ? 4u : b == 'G' ? 8u : b == 'N' ? 15u : 1u;
 }
-__device__ __forceinline__ bool bases_match(uint8_t a, uint8_t b) { return (onehot(a) & onehot(b)) != 0u; }
 
 __global__ void k_pairs_from_units(const Unit* __restrict__ units, long long n_units, int32_t* pair_read,
                                    int32_t* pair_hap) {
@@ -151,14 +150,14 @@ __global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n
 // the alignment one diagonal per row, so below a diagonal whose last hit
 // leaves t read bases uncovered (t <= kEndRows, or any t for the read's last
 // hit) the band reaches t diagonals down, and likewise up from a diagonal
-// whose first hit starts h bases into the read.  Two implementations give the
-// same results: a thread per pair (k_featurize_t, below) and, for pairs with
-// more voted diagonals than a thread keeps, a warp per pair with a histogram
-// over all diagonals (featurize_pair, k_featurize_slow).
+// whose first hit starts h bases into the read.  Two kernels give the same
+// results: a warp per work unit with at most one vote per lane and pair
+// (k_featurize_u, below) and, for pairs with repeated 11-mers, a warp per pair
+// with a histogram over all diagonals (featurize_pair, k_featurize_slow); both
+// share feature_summary.
 constexpr int kFeatWarps = kFeatWarpsPerBlock;
 constexpr int kHitCap = 256;
 constexpr int kEndRows = 24;   // horizon of the per-diagonal end triangles
-constexpr int kUnitChunk = 32;
 constexpr int kHistSlots = kBandMaxRead + kBandMaxHap;  // d + R in [0, R + H)
 // histogram slot: votes << 18 | first read position << 9 | last read position
 // (read positions < 2^9 because reads over kBandMaxRead bases are not banded)
@@ -210,11 +209,57 @@ __device__ __forceinline__ void write_scalars(__nv_bfloat16* f, int total, int w
   dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
 }
 
+// A seeded pair's scalar block and band bounds, as the summary leaves them to
+// one lane (the unit featuriser collects a unit's pairs in lanes 0.. and
+// writes them together).
+struct PairScalars {
+  long long pi;
+  int total, win, R, H, ds, peak, nonzero, n_samp, t_pre, t_suf, d_first, d_last, mis_pre, mis_suf, dmin, dmax, kmin,
+      kmax;
+  bool overflow;
+};
+__device__ __forceinline__ void emit_scalars(const BandParams& p, const PairScalars& c) {
+  write_scalars(p.feat + c.pi * kFeat, c.total, c.win, c.R, c.H, c.ds, c.peak, c.nonzero, __frcp_rn((float)c.n_samp),
+                c.t_pre, c.t_suf, c.d_first, c.d_last, c.mis_pre, c.mis_suf, c.overflow, c.dmin, c.dmax);
+  p.dstar[c.pi] = c.ds;
+  p.kmin[c.pi] = c.kmin;
+  p.kmax[c.pi] = c.kmax;
+}
+
+// The votes of one sampled 11-mer (lane): its table's bucket `bk`, already
+// loaded into q, and the buckets after it while they are full; nv counts the
+// entries holding the code, v0 is the first one's slot d + R.
+__device__ __forceinline__ void probe_votes(const uint32_t* tbl, uint32_t nb, uint32_t code, int i, int R, uint4 q,
+                                            uint32_t bk, int& v0, int& nv) {
+  v0 = -1;
+  nv = 0;
+  if (code == kNoCode) return;
+  for (uint32_t guard = 0; guard < nb; ++guard) {
+    const uint32_t e4[4] = {q.x, q.y, q.z, q.w};
+    bool has_free = false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (e4[k] == kEmpty) { has_free = true; continue; }
+      if ((e4[k] >> 10) == code) {
+        if (nv == 0) v0 = (int)(e4[k] & 1023u) - i + R;
+        ++nv;
+      }
+    }
+    if (has_free) break;
+    bk = bk + 1 == nb ? 0 : bk + 1;
+    q = __ldg(reinterpret_cast<const uint4*>(tbl + 4 * bk));
+  }
+}
+
+__device__ __forceinline__ void feature_summary(const BandParams& p, long long pi, int R, int H, int64_t ro, int64_t ho,
+                                                const uint32_t* tbl, uint32_t nb, uint32_t code, int i, int stride,
+                                                int last_pos, int n_samp, int v0, int nv, uint32_t* hist, int* hits,
+                                                int* nhit, const uint8_t* oh, int lane, PairScalars* out = nullptr, int out_lane = 0);
+
 __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, const uint32_t* tbl, uint32_t* hist,
-                               int* hits, int* nhit, int lane) {
+                               int* hits, int* nhit, const uint8_t* oh, int lane) {
   const int64_t ro = p.batch.read_off[r], ho = p.batch.hap_off[h];
   const int R = (int)(p.batch.read_off[r + 1] - ro), H = (int)(p.batch.hap_off[h + 1] - ho);
-  __nv_bfloat16* f = p.feat + pi * kFeat;
   const uint32_t nb = (uint32_t)(H + 1) / 2;
   const int last_pos = R - kK;
   const int stride = seed_stride(last_pos);
@@ -224,25 +269,21 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
   // the haplotype is a vote for slot d + R (d = j - i)
   const int i = min(lane * stride, last_pos);
   const uint32_t code = lane < n_samp ? p.read_kmers[ro + i] : kNoCode;
-  int v0 = -1, nv = 0;
-  if (code != kNoCode) {
-    uint32_t bk = tbl_bucket(code, nb);
-    for (uint32_t guard = 0; guard < nb; ++guard) {
-      const uint4 q = *reinterpret_cast<const uint4*>(tbl + 4 * bk);
-      const uint32_t e4[4] = {q.x, q.y, q.z, q.w};
-      bool has_free = false;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        if (e4[k] == kEmpty) { has_free = true; continue; }
-        if ((e4[k] >> 10) == code) {
-          if (nv == 0) v0 = (int)(e4[k] & 1023u) - i + R;
-          ++nv;
-        }
-      }
-      if (has_free) break;
-      bk = bk + 1 == nb ? 0 : bk + 1;
-    }
-  }
+  int v0, nv;
+  const uint32_t bk = code != kNoCode ? tbl_bucket(code, nb) : 0u;
+  const uint4 q = code != kNoCode ? __ldg(reinterpret_cast<const uint4*>(tbl + 4 * bk)) : make_uint4(0, 0, 0, 0);
+  probe_votes(tbl, nb, code, i, R, q, bk, v0, nv);
+  feature_summary(p, pi, R, H, ro, ho, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, hist, hits, nhit, oh, lane);
+}
+
+// Everything after the probes, for both featurisers: the fast path (at most
+// one vote per lane) groups lanes by slot; repeated 11-mers (hist != null
+// only) build a per-warp histogram over all slots.
+__device__ __forceinline__ void feature_summary(const BandParams& p, long long pi, int R, int H, int64_t ro, int64_t ho,
+                                                const uint32_t* tbl, uint32_t nb, uint32_t code, int i, int stride,
+                                                int last_pos, int n_samp, int v0, int nv, uint32_t* hist, int* hits,
+                                                int* nhit, const uint8_t* oh, int lane, PairScalars* out, int out_lane) {
+  __nv_bfloat16* f = p.feat + pi * kFeat;
   // summary of the votes: mode (most votes, smallest slot on ties), voted
   // extent, first and last sampled hit (smallest slot on ties), per-diagonal
   // end triangles, vote total, and the 64 histogram bins around the mode
@@ -377,8 +418,8 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
     if (lane < n_end) {
       const int ip = lane, jp = ip + d_first;
       const int is = R - 1 - lane, js = is + d_last;
-      mp = jp < 0 || jp >= H || !bases_match(rb[ip], hb[jp]);
-      ms = js < 0 || js >= H || !bases_match(rb[is], hb[js]);
+      mp = jp < 0 || jp >= H || (oh[rb[ip]] & oh[hb[jp]]) == 0;
+      ms = js < 0 || js >= H || (oh[rb[is]] & oh[hb[js]]) == 0;
     }
     const int mis_pre = __popc(__ballot_sync(0xffffffffu, mp));
     const int mis_suf = __popc(__ballot_sync(0xffffffffu, ms));
@@ -398,14 +439,14 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
     nonzero = __reduce_add_sync(0xffffffffu, nonzero);
     peak = __reduce_max_sync(0xffffffffu, peak);
     if (overflow) total = max(total, win);
-    if (lane == 0)
-      write_scalars(f, total, win, R, H, ds, peak, nonzero, inv, t_pre, t_suf, d_first, d_last, mis_pre, mis_suf,
-                    overflow, smin - R, smax - R);
-    if (lane == 0) {
-      p.dstar[pi] = ds;
-      // voted extent and end triangles (a hit list overflow widens it to everything)
-      p.kmin[pi] = overflow ? INT32_MIN : min(smin - R, tri_lo);
-      p.kmax[pi] = overflow ? INT32_MAX : max(smax - R, tri_hi);
+    // voted extent and end triangles (a hit list overflow widens it to everything)
+    const PairScalars c{pi, total, win, R, H, ds, peak, nonzero, n_samp, t_pre, t_suf, d_first, d_last, mis_pre,
+                        mis_suf, smin - R, smax - R, overflow ? INT32_MIN : min(smin - R, tri_lo),
+                        overflow ? INT32_MAX : max(smax - R, tri_hi), overflow};
+    if (out) {
+      if (lane == out_lane) *out = c;
+    } else if (lane == 0) {
+      emit_scalars(p, c);
     }
   }
   __syncwarp();
@@ -419,12 +460,15 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
   __syncwarp();
 }
 
-// Slow path: the pairs the thread featuriser handed back (more distinct voted
+// Slow path: the pairs the unit featuriser handed back (repeated 11-mers,
 // diagonals than it keeps), one warp per pair, each warp with a histogram of
 // kHistSlots words in global scratch (zero between pairs) and its slot list in
 // shared memory; the haplotype tables are read from global memory.
 __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize_slow(BandParams p) {
   __shared__ int s_hits[kFeatWarps][kHitCap + 1];
+  __shared__ uint8_t s_oh[256];
+  for (int x = threadIdx.x; x < 256; x += blockDim.x) s_oh[x] = (uint8_t)onehot((uint8_t)x);
+  __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   uint32_t* hist = p.feat_hist + ((size_t)blockIdx.x * kFeatWarps + wib) * kHistSlots;
   int* hits = s_hits[wib];
@@ -440,221 +484,96 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize_slow(BandParams p
     if (w >= n) break;
     const long long pi = p.feat_slow[w];
     const int r = p.pair_read[pi], h = p.pair_hap[pi];
-    featurize_pair(p, pi, r, h, p.hap_table + tbl_base(p.batch.hap_off[h], h), hist, hits, nhit, lane);
+    featurize_pair(p, pi, r, h, p.hap_table + tbl_base(p.batch.hap_off[h], h), hist, hits, nhit, s_oh, lane);
   }
 }
 
 // ---------------------------------------------------------------------------
-// Thread featuriser: one thread per pair.  A block takes a chunk of
-// kUnitChunk work units and spreads the chunk's pairs over its threads.  A
-// thread looks the read's sampled 11-mers up in the haplotype's hash table
-// (global memory, eight samples' loads in flight at a time) and keeps up to
-// kCand distinct voted diagonals with their vote count and first and last
-// voting read position -- what the warp featuriser's histogram holds, for all
-// but pairs with many repeats.  A pair that votes for more diagonals goes to
-// the slow list.  Features are assembled in a per-thread row of shared
-// memory, then copied out in 16-byte stores.
+// Unit featuriser: one warp per work unit (a read and up to haps_per_unit of
+// its region's haplotypes).  The warp loads the read's sampled 11-mer codes
+// once (lane t: sample t), then, kFeatUBatch haplotypes at a time, issues
+// every lane's first bucket load for each haplotype before it summarises them
+// one by one with the warp featuriser's fast path (match_any groups, one
+// REDUX per summary key).  A pair for which some lane sees the same 11-mer
+// more than once goes to the slow list (k_featurize_slow).  Grid-strided over
+// the units: consecutive warps take consecutive units, so a region's tables
+// are read by warps running at the same time and stay in L2.
 // ---------------------------------------------------------------------------
-constexpr int kCand = 8;
-constexpr int kFeatT = 128;          // threads per block
-constexpr int kFeatTBatch = 4;       // samples whose loads are issued together
-constexpr int kFeatRowWords = kFeat / 2;
+constexpr int kFeatUWarps = 8;   // warps per block
+constexpr int kFeatUBatch = 2;   // haplotypes whose bucket loads are in flight together
+constexpr int kFeatUBlocksPerSm = 3;
 
-__device__ __forceinline__ void no_seed_thread(const BandParams& p, long long pi) {
-  p.dstar[pi] = INT32_MIN;
-  p.kmin[pi] = INT32_MIN;
-  p.kmax[pi] = INT32_MAX;
-  uint4* f = reinterpret_cast<uint4*>(p.feat + pi * kFeat);
+__global__ void __launch_bounds__(kFeatUWarps * 32, kFeatUBlocksPerSm) k_featurize_u(BandParams p) {
+  __shared__ int s_bins[kFeatUWarps][kHistBins];
+  __shared__ uint8_t s_oh[256];
+  for (int x = threadIdx.x; x < 256; x += blockDim.x) s_oh[x] = (uint8_t)onehot((uint8_t)x);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int* bins = s_bins[wib];
+  const long long nwarps = (long long)gridDim.x * kFeatUWarps;
+  for (long long u = blockIdx.x * (long long)kFeatUWarps + wib; u < p.n_units; u += nwarps) {
+    const Unit un = p.units[u];
+    const int64_t ro = p.batch.read_off[un.read];
+    const int R = (int)(p.batch.read_off[un.read + 1] - ro);
+    const bool read_ok = R >= kK && R <= kBandMaxRead;
+    const int last_pos = R - kK;
+    const int stride = read_ok ? seed_stride(last_pos) : 1;
+    const int q_s = read_ok ? last_pos / stride : 0;
+    const int n_samp = read_ok ? q_s + 1 + (q_s * stride != last_pos) : 0;  // <= 32
+    const int i = read_ok ? min(lane * stride, last_pos) : 0;
+    const uint32_t code = lane < n_samp ? __ldg(p.read_kmers + ro + i) : kNoCode;
+    // lane k holds the scalar block of the unit's pair k (k < 32) until the
+    // unit's pairs are written together
+    PairScalars mine;
+    mine.pi = -1;
+    for (int k0 = 0; k0 < un.nh; k0 += kFeatUBatch) {
+      uint4 q[kFeatUBatch];
+      uint32_t bk[kFeatUBatch];
+      int64_t hos[kFeatUBatch];
+      int Hs[kFeatUBatch];
 #pragma unroll
-  for (int x = 0; x < kFeat / 8; ++x) f[x] = make_uint4(0, 0, 0, 0);
-}
-
-__device__ __forceinline__ void featurize_thread(const BandParams& p, long long pi, int r, int h, uint32_t* row) {
-  const int64_t ro = p.batch.read_off[r], ho = p.batch.hap_off[h];
-  const int R = (int)(p.batch.read_off[r + 1] - ro), H = (int)(p.batch.hap_off[h + 1] - ho);
-  if (H < kK || H > kBandMaxHap || R < kK || R > kBandMaxRead) {
-    no_seed_thread(p, pi);
-    return;
-  }
-  const uint32_t* tbl = p.hap_table + tbl_base(ho, h);
-  const uint32_t nb = (uint32_t)(H + 1) / 2;
-  const int last_pos = R - kK;
-  const int stride = seed_stride(last_pos);
-  const int q_s = last_pos / stride;
-  const int n_samp = q_s + 1 + (q_s * stride != last_pos);  // <= 32
-  // voted diagonals as slots d + R: slot, votes, first and last voting read position
-  int cs[kCand], cn[kCand], cf[kCand], cl[kCand];
+      for (int t = 0; t < kFeatUBatch; ++t) {
+        const int k = k0 + t;
+        const int h = un.hap0 + min(k, un.nh - 1);
+        hos[t] = p.batch.hap_off[h];
+        Hs[t] = (int)(p.batch.hap_off[h + 1] - hos[t]);
+        const bool ok = k < un.nh && read_ok && Hs[t] >= kK && Hs[t] <= kBandMaxHap && code != kNoCode;
+        bk[t] = ok ? tbl_bucket(code, (uint32_t)(Hs[t] + 1) / 2) : 0u;
+        q[t] = ok ? __ldg(reinterpret_cast<const uint4*>(p.hap_table + tbl_base(hos[t], h) + 4 * bk[t]))
+                  : make_uint4(0, 0, 0, 0);
+      }
 #pragma unroll
-  for (int c = 0; c < kCand; ++c) { cs[c] = -1; cn[c] = 0; cf[c] = 0; cl[c] = 0; }
-  int nc = 0;
-  bool ovf = false;
-  auto vote = [&](int v, int i) {
-    bool found = false;
-#pragma unroll
-    for (int c = 0; c < kCand; ++c) {
-      if (cs[c] == v) { cn[c] += 1; cl[c] = i; found = true; }
-    }
-    if (!found) {
-      if (nc < kCand) {
-#pragma unroll
-        for (int c = 0; c < kCand; ++c) {
-          if (c == nc) { cs[c] = v; cn[c] = 1; cf[c] = i; cl[c] = i; }
+      for (int t = 0; t < kFeatUBatch; ++t) {
+        const int k = k0 + t;
+        if (k >= un.nh) break;
+        const int h = un.hap0 + k;
+        const long long pi = un.out0 + k;
+        const int64_t ho = hos[t];
+        const int H = Hs[t];
+        if (!read_ok || H < kK || H > kBandMaxHap) {
+          no_seed(p, pi, lane);
+          continue;
         }
-        ++nc;
-      } else {
-        ovf = true;
-      }
-    }
-  };
-  for (int s0 = 0; s0 < n_samp; s0 += kFeatTBatch) {
-    uint32_t code[kFeatTBatch], bk[kFeatTBatch];
-    int ip[kFeatTBatch];
-    uint4 q[kFeatTBatch];
-#pragma unroll
-    for (int u = 0; u < kFeatTBatch; ++u) {
-      ip[u] = min((s0 + u) * stride, last_pos);
-      code[u] = s0 + u < n_samp ? __ldg(p.read_kmers + ro + ip[u]) : kNoCode;
-    }
-#pragma unroll
-    for (int u = 0; u < kFeatTBatch; ++u) {
-      bk[u] = code[u] != kNoCode ? tbl_bucket(code[u], nb) : 0u;
-      q[u] = code[u] != kNoCode ? __ldg(reinterpret_cast<const uint4*>(tbl + 4 * bk[u]))
-                                : make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
-    }
-#pragma unroll
-    for (int u = 0; u < kFeatTBatch; ++u) {
-      const uint32_t cd = code[u];
-      if (cd == kNoCode) continue;
-      uint4 qq = q[u];
-      uint32_t b = bk[u];
-      for (uint32_t guard = 0; guard < nb; ++guard) {
-        const uint32_t e4[4] = {qq.x, qq.y, qq.z, qq.w};
-        bool has_free = false;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          if (e4[k] == kEmpty) has_free = true;
-          else if ((e4[k] >> 10) == cd) vote((int)(e4[k] & 1023u) - ip[u] + R, ip[u]);
+        const uint32_t* tbl = p.hap_table + tbl_base(ho, h);
+        const uint32_t nb = (uint32_t)(H + 1) / 2;
+        int v0, nv;
+        probe_votes(tbl, nb, code, i, R, q[t], bk[t], v0, nv);
+        if (__any_sync(0xffffffffu, nv > 1)) {
+          if (lane == 0) {
+            const unsigned long long at = atomicAdd(&p.bctr->feat_slow_count, 1ull);
+            if (at < (unsigned long long)p.n_pairs) p.feat_slow[at] = pi;
+          }
+          continue;
         }
-        if (has_free) break;
-        b = b + 1 == nb ? 0 : b + 1;
-        qq = __ldg(reinterpret_cast<const uint4*>(tbl + 4 * b));
+        feature_summary(p, pi, R, H, ro, ho, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, nullptr, bins,
+                        nullptr, s_oh, lane, &mine, k & 31);
+        if ((k & 31) == 31) {
+          if (mine.pi >= 0) emit_scalars(p, mine);
+          mine.pi = -1;
+        }
       }
     }
-  }
-  if (ovf) {
-    const unsigned long long at = atomicAdd(&p.bctr->feat_slow_count, 1ull);
-    if (at < (unsigned long long)p.n_pairs) p.feat_slow[at] = pi;
-    return;
-  }
-  if (nc == 0) {
-    no_seed_thread(p, pi);
-    return;
-  }
-  // summary: mode (most votes, smallest slot on ties), first / last sampled hit
-  // (smallest slot on ties), voted extent, end triangles, vote total
-  uint32_t best = 0u, fkey = 0xffffffffu, lkey = 0u;
-  int smin = INT32_MAX, smax = -1, tri_lo = INT32_MAX, tri_hi = INT32_MIN, total = 0;
-#pragma unroll
-  for (int c = 0; c < kCand; ++c) {
-    if (c < nc) {
-      best = max(best, ((uint32_t)cn[c] << 16) | (0xffffu - (uint32_t)cs[c]));
-      fkey = min(fkey, ((uint32_t)cf[c] << 16) | (uint32_t)cs[c]);
-      lkey = max(lkey, ((uint32_t)cl[c] << 16) | (0xffffu - (uint32_t)cs[c]));
-      smin = min(smin, cs[c]);
-      smax = max(smax, cs[c]);
-      const int d = cs[c] - R, tail = R - kK - cl[c], head = cf[c];
-      if (tail <= kEndRows) tri_lo = min(tri_lo, d - tail);
-      if (head <= kEndRows) tri_hi = max(tri_hi, d + head);
-      total += cn[c];
-    }
-  }
-  const int best_slot = (int)(0xffffu - (best & 0xffffu));
-  const int ds = best_slot - R;
-  const int first_i = (int)(fkey >> 16), first_s = (int)(fkey & 0xffffu);
-  const int last_i = (int)(lkey >> 16), last_s = (int)(0xffffu - (lkey & 0xffffu));
-  const int t_pre = first_i, t_suf = R - kK - last_i;
-  const int d_first = first_s - R, d_last = last_s - R;
-  tri_lo = min(tri_lo, d_last - t_suf);
-  tri_hi = max(tri_hi, d_first + t_pre);
-  // mismatches of the first / last 16 read bases along those diagonals
-  const uint8_t* rb = p.batch.read_bases + ro;
-  const uint8_t* hb = p.batch.hap_bases + ho;
-  const int n_end = min(16, R);
-  int mis_pre = 0, mis_suf = 0;
-#pragma unroll
-  for (int l = 0; l < 16; ++l) {
-    if (l < n_end) {
-      const int jp = l + d_first, is = R - 1 - l, js = is + d_last;
-      mis_pre += (jp < 0 || jp >= H || !bases_match(__ldg(rb + l), __ldg(hb + jp))) ? 1 : 0;
-      mis_suf += (js < 0 || js >= H || !bases_match(__ldg(rb + is), __ldg(hb + js))) ? 1 : 0;
-    }
-  }
-  // 64 histogram bins d* - 32 .. d* + 31 (the mode's bin is 32)
-  const float inv = __frcp_rn((float)n_samp);
-#pragma unroll
-  for (int x = 0; x < kHistBins / 2; ++x) row[x] = 0u;
-  int win = 0, nonzero = 0;
-  __nv_bfloat16* rowb = reinterpret_cast<__nv_bfloat16*>(row);
-#pragma unroll
-  for (int c = 0; c < kCand; ++c) {
-    const int bin = cs[c] - (best_slot - kHistBins / 2);
-    if (c < nc && bin >= 0 && bin < kHistBins) {
-      rowb[bin] = __float2bfloat16_rn((float)cn[c] * inv);
-      win += cn[c];
-      nonzero += 1;
-    }
-  }
-  write_scalars(rowb, total, win, R, H, ds, (int)(best >> 16), nonzero, inv, t_pre, t_suf, d_first, d_last,
-                mis_pre, mis_suf, false, smin - R, smax - R);
-  uint4* dst = reinterpret_cast<uint4*>(p.feat + pi * kFeat);
-  const uint4* src = reinterpret_cast<const uint4*>(row);
-#pragma unroll
-  for (int x = 0; x < kFeat / 8; ++x) dst[x] = src[x];
-  p.dstar[pi] = ds;
-  p.kmin[pi] = min(smin - R, tri_lo);
-  p.kmax[pi] = max(smax - R, tri_hi);
-}
-
-__global__ void __launch_bounds__(kFeatT, 5) k_featurize_t(BandParams p) {
-  __shared__ __align__(16) uint32_t s_row[kFeatT][kFeatRowWords];
-  __shared__ Unit s_units[kUnitChunk];
-  __shared__ int s_pre[kUnitChunk + 1];
-  __shared__ long long s_chunk;
-  const long long nchunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
-  const int lane = threadIdx.x & 31;
-  for (;;) {
-    __syncthreads();  // the previous chunk is done with s_units / s_pre
-    if (threadIdx.x == 0) s_chunk = (long long)min((long long)atomicAdd(&p.bctr->feat_next, 1ull), nchunks);
-    __syncthreads();
-    const long long c = s_chunk;
-    if (c >= nchunks) break;
-    const long long u0 = c * kUnitChunk;
-    const int nu = (int)min((long long)kUnitChunk, p.n_units - u0);
-    if (threadIdx.x < 32) {
-      Unit un{};
-      if (lane < nu) un = p.units[u0 + lane];
-      int x = lane < nu ? un.nh : 0;  // inclusive scan of the units' pair counts
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-      }
-      if (lane < nu) s_units[lane] = un;
-      s_pre[lane + 1] = x;
-      if (lane == 0) s_pre[0] = 0;
-    }
-    __syncthreads();
-    const int npairs = s_pre[nu];
-    for (int q = threadIdx.x; q < npairs; q += kFeatT) {
-      int lo = 0, hi = nu - 1;  // the unit holding pair q: largest u with s_pre[u] <= q
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s_pre[mid] <= q) lo = mid; else hi = mid - 1;
-      }
-      const Unit un = s_units[lo];
-      const int k = q - s_pre[lo];
-      featurize_thread(p, un.out0 + k, un.read, un.hap0 + k, s_row[threadIdx.x]);
-    }
+    if (mine.pi >= 0) emit_scalars(p, mine);
   }
 }
 
@@ -965,12 +884,26 @@ __device__ __forceinline__ int mm_index(int qi, int qd) {
 // table entry is NaN, which makes the banded sums NaN, and such pairs end in
 // the full DP (which keeps the plain form for them) like any pair whose
 // banded sum is not positive.
+// Stages the probability tables the band kernels read per row into shared memory.
+struct BandSmem {
+  QProb qp[128];
+  uint8_t oh[256];  // one-hot nibble of every byte (onehot)
+  float mm[kMMEntries];
+};
+__device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb) {
+  for (int x = threadIdx.x; x < 128; x += blockDim.x) sm.qp[x] = tb->qp[x];
+  for (int x = threadIdx.x; x < 256; x += blockDim.x) sm.oh[x] = (uint8_t)onehot((uint8_t)x);
+  for (int x = threadIdx.x; x < kMMEntries; x += blockDim.x) sm.mm[x] = tb->mm_f[x];
+  __syncthreads();
+}
 struct FwdRow {
   float cx, cy, kap, g, pmx, pmy, em, ex;
   uint32_t rb;  // the read base's one-hot nibble, replicated 8 times
 };
-__device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, const float* __restrict__ minv,
-                                          uchar4 qv, uint8_t base, float ap, float bp) {
+__device__ __forceinline__ FwdRow fwd_row(const BandSmem& sm, const float* __restrict__ minv, uchar4 qv, uint8_t base,
+                                          float ap, float bp) {
+  const QProb* qp = sm.qp;
+  const float* mmt = sm.mm;
   FwdRow c;
   const int qi = qv.y & kQualMask, qd = qv.z & kQualMask;
   const QProb qpi = qp[qi], qpg = qp[qv.w & kQualMask], qpb = qp[qv.x & kQualMask];
@@ -985,18 +918,8 @@ __device__ __forceinline__ FwdRow fwd_row(const QProb* qp, const float* mmt, con
   c.kap = c.g * ap * qpi.inv;
   c.em = qpb.q * mm;
   c.ex = qpb.third * mm;
-  c.rb = onehot(base) * 0x11111111u;
+  c.rb = (uint32_t)sm.oh[base] * 0x11111111u;
   return c;
-}
-// Stages the probability tables the band kernels read per row into shared memory.
-struct BandSmem {
-  QProb qp[128];
-  float mm[kMMEntries];
-};
-__device__ __forceinline__ void stage_band_tables(BandSmem& sm, const Tables* tb) {
-  for (int x = threadIdx.x; x < 128; x += blockDim.x) sm.qp[x] = tb->qp[x];
-  for (int x = threadIdx.x; x < kMMEntries; x += blockDim.x) sm.mm[x] = tb->mm_f[x];
-  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -1038,16 +961,16 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
       const int c = d + 1 + w * 8 + t;
-      v |= ((c >= 1 && c <= H) ? onehot(hap[c - 1]) : 0u) << (4 * t);
+      v |= ((c >= 1 && c <= H) ? (uint32_t)sm.oh[hap[c - 1]] : 0u) << (4 * t);
     }
     win[w] = v;
   }
   float pmx_last = 1.f;
-  FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
+  FwdRow cur = fwd_row(sm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);  // row 1; row 0 has pMX = pMY = 1
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
+    const FwdRow nxt = fwd_row(sm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
     {
       const int rn = min(r + 1, R - 1);  // row r + 2
       qn = quals[rn];
@@ -1082,7 +1005,7 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
         }
       }
     }
-    const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
+    const uint32_t nib = (cn >= 1 && cn <= H) ? (uint32_t)sm.oh[hb] : 0u;
 #pragma unroll
     for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
     win[NW - 1] = (win[NW - 1] >> 4) | (nib << 28);
@@ -1142,16 +1065,16 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
       const int c = d + 1 + w * 8 + t;
-      v |= ((c >= 1 && c <= H) ? onehot(hap[c - 1]) : 0u) << (4 * t);
+      v |= ((c >= 1 && c <= H) ? (uint32_t)sm.oh[hap[c - 1]] : 0u) << (4 * t);
     }
     win[w] = v;
   }
   float pmx_last = 1.f;
-  FwdRow cur = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);
+  FwdRow cur = fwd_row(sm, tb->mm_inv_f, quals[0], rbase[0], 1.f, 1.f);
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm.qp, sm.mm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
+    const FwdRow nxt = fwd_row(sm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
     {
       const int rn = min(r + 1, R - 1);
       qn = quals[rn];
@@ -1206,7 +1129,7 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
       Mh[k] = mn; Xh[k] = xn; Yh[k] = yn;
       lm = mn; ly = yn;
     }
-    const uint32_t nib = (cn >= 1 && cn <= H) ? onehot(hb) : 0u;
+    const uint32_t nib = (cn >= 1 && cn <= H) ? (uint32_t)sm.oh[hb] : 0u;
 #pragma unroll
     for (int w = 0; w < NW - 1; ++w) win[w] = __funnelshift_r(win[w], win[w + 1], 4);
     win[NW - 1] = (win[NW - 1] >> 4) | (nib << 28);
@@ -1354,9 +1277,9 @@ cudaError_t prepare_band_kernels() {
 
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
   if (p.n_units <= 0) return cudaSuccess;
-  const long long chunks = (p.n_units + kUnitChunk - 1) / kUnitChunk;
-  const long long blocks = std::min<long long>(chunks, (long long)sms * 5);  // five resident blocks per SM
-  k_featurize_t<<<(int)blocks, kFeatT, 0, st>>>(p);
+  const long long need = (p.n_units + kFeatUWarps - 1) / kFeatUWarps;
+  const long long blocks = std::min<long long>(need, (long long)sms * kFeatUBlocksPerSm);
+  k_featurize_u<<<(int)blocks, kFeatUWarps * 32, 0, st>>>(p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   // the slow list's length is known only on the device: the warp featuriser

@@ -79,7 +79,6 @@ struct BandCounters {
   unsigned long long fallback_route;                      // pairs routed to the full DP up front
   unsigned long long band_cells;                          // cells of both sweeps (result band and inner band)
   unsigned long long band_result_cells;                   // cells of the result band (band plus ring)
-  unsigned long long feat_next;                           // work-queue head of the featuriser
   unsigned long long feat_slow_count;                     // pairs left to the warp featuriser (many distinct diagonals)
   unsigned long long feat_slow_next;                      // its work-queue head
 };
@@ -95,7 +94,7 @@ struct BandParams {
   long long n_units;
   const uint32_t* read_kmers; // 11-mer code per read position
   uint32_t* feat_hist;        // featuriser scratch: one histogram of kBandMaxRead + kBandMaxHap slots per warp
-  int64_t* feat_slow;         // [n_pairs] pairs the thread featuriser hands to the warp featuriser
+  int64_t* feat_slow;         // [n_pairs] pairs the unit featuriser hands to the slow featuriser
   int32_t* dstar;             // [n_pairs] seed diagonal (INT32_MIN: no seed)
   int32_t* kmin;              // [n_pairs] lowest / highest diagonal of a shared 11-mer
   int32_t* kmax;

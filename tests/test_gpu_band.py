@@ -103,7 +103,7 @@ def test_band_staged_replay_is_deterministic():
 def _repeat_pairs(seed):
     """Pairs whose sampled 11-mers vote for many diagonals: haplotypes made of
     a repeated unit (period 40 and 25), reads cut from them with a few
-    substitutions; the thread featuriser hands these to the warp featuriser."""
+    substitutions; the unit featuriser hands these to the slow featuriser."""
     rng = np.random.default_rng(seed)
     out = []
     for period, copies, n in ((40, 10, 150), (25, 16, 120), (40, 6, 90)):
