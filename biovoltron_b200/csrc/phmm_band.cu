@@ -578,145 +578,6 @@ __global__ void __launch_bounds__(kFeatUWarps * 32, kFeatUBlocksPerSm) k_featuri
 }
 
 // ---------------------------------------------------------------------------
-// MLP forward on tensor cores: mma.sync m16n8k16, BF16 operands, FP32
-// accumulation.  One warp scores 16 pairs per pass; the weights live in shared
-// memory transposed ([out][in]) so B fragments load with ldmatrix directly.
-// ---------------------------------------------------------------------------
-constexpr int kMlpWarps = 8;
-constexpr int kLdF = kFeat + 8;   // padded row strides (bf16 elements) against bank conflicts
-constexpr int kLdH = kHid + 8;
-
-struct MlpSmem {
-  __nv_bfloat16 w1t[kHid * kLdF];
-  __nv_bfloat16 w2t[kHid * kLdH];
-  __nv_bfloat16 w3t[8 * kLdH];
-  float b1[kHid], b2[kHid], b3[8];
-  __nv_bfloat16 act[kMlpWarps][16 * kLdH];  // per-warp 16-row activation tile
-};
-
-__device__ __forceinline__ void ldmatrix_x4(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3, const void* p) {
-  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
-}
-__device__ __forceinline__ void ldmatrix_x2(uint32_t& r0, uint32_t& r1, const void* p) {
-  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
-  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0, %1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(a));
-}
-__device__ __forceinline__ void mma_bf16(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-      "{%0, %1, %2, %3};"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-// acc[nt][4] += A[16 x K] (smem, row stride lda) * Bt[N x K]^T (smem, row stride ldb)
-template <int K, int NT>
-__device__ __forceinline__ void warp_gemm(float (*acc)[4], const __nv_bfloat16* A, int lda, const __nv_bfloat16* Bt,
-                                          int ldb, int lane) {
-#pragma unroll
-  for (int k0 = 0; k0 < K; k0 += 16) {
-    uint32_t a0, a1, a2, a3;
-    {
-      const int m = lane >> 3, rr = (lane & 7) + 8 * (m & 1), cc = k0 + 8 * (m >> 1);
-      ldmatrix_x4(a0, a1, a2, a3, A + rr * lda + cc);
-    }
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-      uint32_t b0, b1;
-      const int l = lane & 15;
-      ldmatrix_x2(b0, b1, Bt + (nt * 8 + (l & 7)) * ldb + k0 + 8 * (l >> 3));
-      mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
-    }
-  }
-}
-
-// bias + ReLU, write the 16 x (8*NT) tile back as bf16 (row stride kLdH)
-template <int NT>
-__device__ __forceinline__ void store_hidden(float (*acc)[4], const float* bias, __nv_bfloat16* out, int lane) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int nt = 0; nt < NT; ++nt) {
-    const int col = nt * 8 + 2 * t;
-    const float v0 = fmaxf(acc[nt][0] + bias[col], 0.f), v1 = fmaxf(acc[nt][1] + bias[col + 1], 0.f);
-    const float v2 = fmaxf(acc[nt][2] + bias[col], 0.f), v3 = fmaxf(acc[nt][3] + bias[col + 1], 0.f);
-    *reinterpret_cast<__nv_bfloat162*>(out + g * kLdH + col) = __floats2bfloat162_rn(v0, v1);
-    *reinterpret_cast<__nv_bfloat162*>(out + (g + 8) * kLdH + col) = __floats2bfloat162_rn(v2, v3);
-  }
-}
-
-__global__ void __launch_bounds__(kMlpWarps * 32) k_mlp_forward(BandParams p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  MlpSmem& s = *reinterpret_cast<MlpSmem*>(smem_raw);
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const MlpParams* W = p.mlp;
-  for (int x = threadIdx.x; x < kHid * kFeat; x += blockDim.x) s.w1t[(x / kFeat) * kLdF + x % kFeat] = W->w1[x];
-  for (int x = threadIdx.x; x < kHid * kHid; x += blockDim.x) s.w2t[(x / kHid) * kLdH + x % kHid] = W->w2[x];
-  for (int x = threadIdx.x; x < 8 * kHid; x += blockDim.x)
-    s.w3t[(x / kHid) * kLdH + x % kHid] = (x / kHid) < kOut ? W->w3[x] : __float2bfloat16(0.f);
-  for (int x = threadIdx.x; x < kHid; x += blockDim.x) { s.b1[x] = W->b1[x]; s.b2[x] = W->b2[x]; }
-  if (threadIdx.x < 8) s.b3[threadIdx.x] = threadIdx.x < kOut ? W->b3[threadIdx.x] : 0.f;
-  __syncthreads();
-  __nv_bfloat16* act = s.act[wib];
-  const long long ntiles = (p.n_pairs + 15) / 16;
-  const long long tstride = (long long)gridDim.x * kMlpWarps;
-  // input tiles (16 pairs x kFeat, zero rows past the end) are loaded one tile ahead into registers
-  constexpr int kVec = 16 * kFeat / 8 / 32;  // 16-byte vectors per lane
-  static_assert(kVec * 32 * 8 == 16 * kFeat, "tile split");
-  uint4 pre[kVec];
-  auto load_tile = [&](long long tile) {
-#pragma unroll
-    for (int u = 0; u < kVec; ++u) {
-      const int x = lane + 32 * u, rr = x / (kFeat / 8), cc = (x % (kFeat / 8)) * 8;
-      const long long row = tile * 16 + rr;
-      pre[u] = (tile < ntiles && row < p.n_pairs) ? *reinterpret_cast<const uint4*>(p.feat + row * kFeat + cc)
-                                                  : make_uint4(0, 0, 0, 0);
-    }
-  };
-  long long tile = blockIdx.x * (long long)kMlpWarps + wib;
-  load_tile(tile);
-  for (; tile < ntiles; tile += tstride) {
-    const long long row0 = tile * 16;
-#pragma unroll
-    for (int u = 0; u < kVec; ++u) {
-      const int x = lane + 32 * u, rr = x / (kFeat / 8), cc = (x % (kFeat / 8)) * 8;
-      *reinterpret_cast<uint4*>(act + rr * kLdH + cc) = pre[u];
-    }
-    __syncwarp();
-    load_tile(tile + tstride);
-    float acc[16][4];
-#pragma unroll
-    for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-    warp_gemm<kFeat, 16>(acc, act, kLdH, s.w1t, kLdF, lane);
-    __syncwarp();
-    store_hidden<16>(acc, s.b1, act, lane);
-    __syncwarp();
-#pragma unroll
-    for (int nt = 0; nt < 16; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-    warp_gemm<kHid, 16>(acc, act, kLdH, s.w2t, kLdH, lane);
-    __syncwarp();
-    store_hidden<16>(acc, s.b2, act, lane);
-    __syncwarp();
-    float o[1][4] = {{0.f, 0.f, 0.f, 0.f}};
-    warp_gemm<kHid, 1>(o, act, kLdH, s.w3t, kLdH, lane);
-    const int g = lane >> 2, t = lane & 3;
-    if (t == 0) {
-      if (row0 + g < p.n_pairs) {
-        p.mlp_out[(row0 + g) * kOut + 0] = o[0][0] + s.b3[0];
-        p.mlp_out[(row0 + g) * kOut + 1] = o[0][1] + s.b3[1];
-      }
-      if (row0 + g + 8 < p.n_pairs) {
-        p.mlp_out[(row0 + g + 8) * kOut + 0] = o[0][2] + s.b3[0];
-        p.mlp_out[(row0 + g + 8) * kOut + 1] = o[0][3] + s.b3[1];
-      }
-    }
-    __syncwarp();
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Routing.  Pass 0 counts band items per (width class, read-length bucket)
 // and writes full-DP fallback units; pass 1 places band items at their
 // bucket's offset so that each warp of the banded kernel gets reads of nearly
@@ -1271,9 +1132,7 @@ cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, l
   return cudaGetLastError();
 }
 
-cudaError_t prepare_band_kernels() {
-  return raise_dynamic_smem(reinterpret_cast<const void*>(&k_mlp_forward), (int)sizeof(MlpSmem));
-}
+cudaError_t prepare_band_kernels() { return prepare_mlp_tc(); }
 
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
   if (p.n_units <= 0) return cudaSuccess;
@@ -1289,12 +1148,7 @@ cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st) {
 }
 
 cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st) {
-  if (p.n_pairs <= 0) return cudaSuccess;
-  const int smem = (int)sizeof(MlpSmem);
-  const long long tiles = (p.n_pairs + 15) / 16;
-  const long long blocks = std::min<long long>((tiles + kMlpWarps - 1) / kMlpWarps, (long long)sms * 2);
-  k_mlp_forward<<<(int)blocks, kMlpWarps * 32, smem, st>>>(p);
-  return cudaGetLastError();
+  return launch_mlp_forward_tc(p, sms, st);
 }
 
 cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st) {

@@ -141,6 +141,9 @@ inline int feat_blocks(int sms) { return sms * 4; }
 inline long long feat_hist_words(int sms) { return (long long)feat_blocks(sms) * kFeatWarpsPerBlock * (kBandMaxRead + kBandMaxHap); }
 // Sets the dynamic shared-memory limits of the band kernels (before any capture).
 cudaError_t prepare_band_kernels();
+// The MLP inference kernel on tcgen05 tensor cores (phmm_mlp_tc.cu).
+cudaError_t prepare_mlp_tc();
+cudaError_t launch_mlp_forward_tc(const BandParams& p, int sms, cudaStream_t st);
 // audit: full-DP units for the sampled pairs (out = audit slot), listed per full-DP
 // variant ([9][audit_cap]), then the differences
 cudaError_t launch_audit_units(const BandParams& p, Unit* units, cudaStream_t st);

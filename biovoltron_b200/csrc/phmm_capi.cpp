@@ -374,6 +374,11 @@ bv_status bv_phmm_band_mlp_eval(bv_phmm_ctx* ctx, const float* w, const float* x
   return guard(ctx, [&] { return ctx->engine.band_mlp_eval(w, x, targets, n, alpha, out, loss, grad); });
 }
 
+bv_status bv_phmm_band_mlp_infer(bv_phmm_ctx* ctx, const float* x, int64_t n, float* out) {
+  if (!ctx || !x || !out || n <= 0) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.band_mlp_infer(x, n, out); });
+}
+
 bv_status bv_phmm_autotune(bv_phmm_ctx* ctx, const bv_region_batch* sample, int32_t repeats, bv_phmm_tune_entry* out,
                            int32_t* num_out) {
   if (!ctx || !sample || !out || !num_out) return BV_ERR_INVALID_ARG;

@@ -172,6 +172,9 @@ class Engine {
   bv_status band_load(const char* path);
   bv_status band_mlp_eval(const float* w, const float* x, const float* t, int64_t n, float alpha, float* out,
                           float* loss, float* grad);
+  // The inference kernel on [n][80] features (rounded to BF16) with the
+  // installed weights: outputs [n][2].
+  bv_status band_mlp_infer(const float* x, int64_t n, float* out);
   bv_status autotune(const bv_region_batch& sample, int repeats, bv_phmm_tune_entry* out, int32_t* n_out);
   bv_status set_tuning(const bv_phmm_tune_entry* entries, int32_t n);
   bv_status get_tuning(bv_phmm_tune_entry* out, int32_t* n_out);

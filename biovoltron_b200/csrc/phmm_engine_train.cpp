@@ -221,6 +221,40 @@ bv_status Engine::band_mlp_eval(const float* w, const float* x, const float* t, 
   return BV_OK;
 }
 
+bv_status Engine::band_mlp_infer(const float* x, int64_t n, float* out) {
+  BV_CUDA(cudaSetDevice(opt_.device), "cudaSetDevice");
+  if (!mlp_ready_) return fail(BV_ERR_INVALID_ARG, "no band MLP weights (train or load)");
+  if (n < 0 || n > (1 << 24)) return fail(BV_ERR_INVALID_ARG, "row count out of range");
+  if (n == 0) return BV_OK;
+  // features to BF16, round to nearest even (the featuriser's rounding)
+  std::vector<uint16_t> xb((size_t)n * kFeat);
+  for (size_t i = 0; i < xb.size(); ++i) {
+    uint32_t u;
+    std::memcpy(&u, &x[i], 4);
+    xb[i] = (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+  }
+  DevBuf df, dout, dctr;
+  BV_CUDA(df.reserve(xb.size() * 2), "alloc features");
+  BV_CUDA(dout.reserve(sizeof(float) * kOut * (size_t)n), "alloc outputs");
+  BV_CUDA(dctr.reserve(sizeof(Counters)), "alloc counters");
+  BV_CUDA(cudaMemsetAsync(dctr.get(), 0, sizeof(Counters), stream_), "memset");
+  BV_CUDA(cudaMemcpyAsync(df.get(), xb.data(), xb.size() * 2, cudaMemcpyHostToDevice, stream_), "H2D");
+  BandParams p{};
+  p.n_pairs = n;
+  p.feat = df.as<__nv_bfloat16>();
+  p.mlp_out = dout.as<float>();
+  p.mlp = d_mlp_.as<MlpParams>();
+  p.ctr = dctr.as<Counters>();
+  BV_CUDA(prepare_band_kernels(), "band kernel attributes");
+  BV_CUDA(launch_mlp_forward(p, sms_, stream_), "mlp forward");
+  Counters c{};
+  BV_CUDA(cudaMemcpyAsync(out, dout.get(), sizeof(float) * kOut * (size_t)n, cudaMemcpyDeviceToHost, stream_), "D2H");
+  BV_CUDA(cudaMemcpyAsync(&c, dctr.get(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_), "D2H");
+  BV_CUDA(cudaStreamSynchronize(stream_), "infer sync");
+  if (c.status != 0) return status_fail(c.status);
+  return BV_OK;
+}
+
 bv_status Engine::band_train(const bv_region_batch& bt, const bv_band_train_options& o, bv_band_train_report* rep) {
   if (o.struct_size != (int32_t)sizeof(bv_band_train_options)) return fail(BV_ERR_INVALID_ARG, "train options size");
   if (o.epochs < 1 || o.batch < 16 || o.batch > (1 << 20) || !(o.lr > 0) || !(o.alpha >= 1) || !(o.tau > 0) ||

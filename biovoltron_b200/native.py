@@ -170,6 +170,7 @@ def load() -> C.CDLL:
         "bv_phmm_band_save": (C.c_int, [V, C.c_char_p]),
         "bv_phmm_band_load": (C.c_int, [V, C.c_char_p]),
         "bv_phmm_band_mlp_eval": (C.c_int, [V, V, V, V, C.c_int64, C.c_float, V, V, V]),
+        "bv_phmm_band_mlp_infer": (C.c_int, [V, V, C.c_int64, V]),
         "bv_phmm_autotune": (C.c_int, [V, P(RegionBatchC), C.c_int32, P(TuneEntry), P(C.c_int32)]),
         "bv_phmm_set_tuning": (C.c_int, [V, P(TuneEntry), C.c_int32]),
         "bv_phmm_get_tuning": (C.c_int, [V, P(TuneEntry), P(C.c_int32)]),

@@ -246,6 +246,15 @@ class PairHMMEngine:
     def band_load(self, path: str):
         self._check(self.lib.bv_phmm_band_load(self.h, os.fsencode(path)))
 
+    def band_mlp_infer(self, x: np.ndarray) -> np.ndarray:
+        """The band MLP inference kernel on features x [n, 80] with the installed
+        weights (bv_phmm_band_mlp_infer): outputs [n, 2]."""
+        x = np.ascontiguousarray(x, np.float32)
+        n = x.shape[0]
+        out = np.empty((max(n, 1), 2), np.float32)
+        self._check(self.lib.bv_phmm_band_mlp_infer(self.h, _ptr(x), n, _ptr(out)))
+        return out[:n]
+
     def band_mlp_eval(self, w: np.ndarray, x: np.ndarray, targets: np.ndarray, alpha: float, grad: bool = True):
         """Training objective on the GPU: (outputs [n, 2], loss, gradient or None)."""
         w = np.ascontiguousarray(w, np.float32)

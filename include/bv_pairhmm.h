@@ -340,6 +340,10 @@ bv_status bv_phmm_band_load(bv_phmm_ctx* ctx, const char* path);
  * [n][80], targets [n][2].  For gradient checks. */
 bv_status bv_phmm_band_mlp_eval(bv_phmm_ctx* ctx, const float* w, const float* x, const float* targets, int64_t n,
                                 float alpha, float* out, float* loss, float* grad);
+/* The band pipeline's MLP inference kernel (tcgen05 tensor cores) on x
+ * ([n][80], rounded to BF16 as the featuriser stores them) with the installed
+ * weights: out [n][2].  For checks against the objective's forward pass. */
+bv_status bv_phmm_band_mlp_infer(bv_phmm_ctx* ctx, const float* x, int64_t n, float* out);
 
 /* --- scoring without any allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc when they need scores: e.g. a

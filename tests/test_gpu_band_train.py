@@ -71,6 +71,29 @@ def test_objective_matches_cpu_restatement():
     assert np.linalg.norm(g - eg) <= 2e-3 * np.linalg.norm(eg)
 
 
+def test_mlp_inference_kernel_matches_cpu_forward():
+    """The band pipeline's MLP inference (tcgen05 tensor cores, 128-pair
+    tiles, rows past the end of a partial tile ignored) against the CPU
+    restatement's forward pass with the same BF16 rounding of weights,
+    features and hidden activations."""
+    rng = np.random.default_rng(9)
+    w = M.init_weights(21, out_scale=1.0).astype(np.float32)
+    for n in (1, 127, 128, 1000):
+        x = M.bf16_round(rng.uniform(0, 1, (n, M.FEAT))).astype(np.float32)
+        with _engine() as e:
+            e.set_band_weights(w)
+            got = e.band_mlp_infer(x)
+        exp, _, _ = M.objective(w.astype(np.float64), x, np.zeros((n, 2)), 1.0, rounding=True)
+        scale = max(1.0, float(np.max(np.abs(exp))))
+        err = np.abs(got - exp)
+        # FP32 accumulation order differs from the FP64 restatement; where a
+        # hidden value sits on a BF16 rounding boundary the two round it to
+        # neighbouring BF16 values (one part in 256), which moves an output by
+        # at most a few 1e-3
+        assert np.quantile(err, 0.99) <= 1e-5 * scale, (n, np.quantile(err, 0.99))
+        assert err.max() <= 2e-2 * scale, (n, err.max(), scale)
+
+
 def test_training_reduces_loss_and_covers_labels(trained):
     _, rep = trained
     assert rep["labelled"] >= 0.9 * rep["pairs"]
