@@ -91,6 +91,8 @@ struct Counters {
   unsigned long long underflow_count;  // FP64 results that stayed non-positive
   unsigned long long status;           // nonzero: a kernel met an inconsistent input
   unsigned long long rescued_cells;    // DP cells the FP64 pass computed
+  unsigned long long rescue_long_count;  // FP64 list entries of long reads (at the list's far end)
+  unsigned long long rescue_long_next;
 };
 
 }  // namespace bvphmm

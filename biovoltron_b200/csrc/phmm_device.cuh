@@ -357,6 +357,15 @@ __device__ __forceinline__ void stage_hap(const uint8_t* __restrict__ hap, int H
   }
 }
 
+// The same for all threads of a block (the long-read kernel's shared codes).
+__device__ __forceinline__ void stage_hap_block(const uint8_t* __restrict__ hap, int H, unsigned char* hc,
+                                                int n_total) {
+  for (int x = threadIdx.x; x < n_total; x += blockDim.x) {
+    const int c = x - kHapLead + 1;
+    hc[x] = (c >= 1 && c <= H) ? (unsigned char)base_code(hap[c - 1]) : (unsigned char)kPadCode;
+  }
+}
+
 // Stages two haplotypes for a paired warp: entry x holds the emission-table
 // offsets of both haplotypes' codes at column kHapLead + c - 1 (first in the
 // low 16 bits), so one 32-bit shared load per step serves both.
@@ -644,11 +653,15 @@ __device__ __forceinline__ void write_result(const KernelParams& p, int read, in
     if (!p.rescue && (!(res >= (T)kMinAccepted) || isinf((double)res))) {
       p.out[o] = __longlong_as_double(0x7ff8000000000000ll);
     } else if (!(res >= (T)kMinAccepted) || isinf((double)res)) {
-      const unsigned long long slot = atomicAdd(&p.ctr->rescue_count, 1ull);
+      // reads of at least long_rows bases go to the long list, filled from the
+      // list's far end for the several-warps-per-pair FP64 kernel
+      const bool lng = p.long_rows > 0 && p.batch.read_off[read + 1] - p.batch.read_off[read] >= p.long_rows;
+      const unsigned long long slot = atomicAdd(lng ? &p.ctr->rescue_long_count : &p.ctr->rescue_count, 1ull);
       if (slot < (unsigned long long)p.rescue_cap) {
-        p.rescue[slot].read = read;
-        p.rescue[slot].hap = hap;
-        p.rescue[slot].out = o;
+        const long long at = lng ? p.rescue_cap - 1 - (long long)slot : (long long)slot;
+        p.rescue[at].read = read;
+        p.rescue[at].hap = hap;
+        p.rescue[at].out = o;
       } else {
         atomicOr(&p.ctr->status, 1ull);
       }

@@ -89,18 +89,19 @@ bv_status Engine::fail(bv_status s, const std::string& msg) {
 
 bv_status Engine::status_fail(unsigned long long status) {
   // Kernel status bits: 1 FP64 list overflow, 2 invalid pair, 4 band list
-  // overflow, 8 a boundary-row bulk copy did not complete in time.
+  // overflow, 8 a boundary-row copy or strip hand-over wait gave up, 16 a
+  // tensor-core completion wait gave up.
   static const char* const kNames[] = {"FP64 list overflow", "invalid pair", "band list overflow",
-                                       "boundary copy wait gave up"};
+                                       "boundary wait gave up", "tensor-core wait gave up"};
   std::string msg = "kernel reported an inconsistent state (";
   bool first = true;
-  for (int b = 0; b < 4; ++b) {
+  for (int b = 0; b < 5; ++b) {
     if (!(status >> b & 1ull)) continue;
     msg += first ? "" : ", ";
     msg += kNames[b];
     first = false;
   }
-  if (status >> 4) msg += std::string(first ? "" : ", ") + "status " + std::to_string(status);
+  if (status >> 5) msg += std::string(first ? "" : ", ") + "status " + std::to_string(status);
   return fail(BV_ERR_INTERNAL, msg + ")");
 }
 
@@ -201,7 +202,9 @@ bv_status Engine::validate(const bv_region_batch& b) {
 bv_status Engine::plan(const bv_region_batch& b) {
   units_.clear();
   f64_items_.clear();
+  f64_long_items_.clear();
   plans_.clear();
+  int64_t max_read = 0;
   n_results_ = 0;
   n_cells_ = 0;
   max_hap_ = 0;
@@ -255,9 +258,11 @@ bv_status Engine::plan(const bv_region_batch& b) {
     for (int64_t r = r0; r < r0 + nr; ++r) {
       const int64_t rl = b.read_offsets[r + 1] - b.read_offsets[r];
       n_cells_ += rl * hap_bases;
+      max_read = std::max(max_read, rl);
       if (all_f64) {
+        auto& list = rl >= kLongRows ? f64_long_items_ : f64_items_;
         for (int64_t k = 0; k < nh; ++k)
-          f64_items_.push_back(PairRef{(int32_t)r, (int32_t)(h0 + k), res + (r - r0) * nh + k});
+          list.push_back(PairRef{(int32_t)r, (int32_t)(h0 + k), res + (r - r0) * nh + k});
         continue;
       }
       const int v = variant_of(rl);
@@ -320,6 +325,29 @@ bv_status Engine::plan(const bv_region_batch& b) {
   rp.grid = sms_ * bps;
   rp.bnd_cols = bnd_cols_for(std::max(max_hap_, 1));
   rescue_plan_ = rp;
+  // FP64 long reads: one block per pair, longest pairs first (the long list is
+  // read from its far end, so the host list is in ascending order of cells)
+  long_plan_ = LaunchPlan{};
+  if (max_read >= kLongRows) {
+    long_smem_ = long_smem_bytes(rp.hap_bytes);
+    if (long_smem_ <= 227 * 1024) {
+      BV_CUDA(prepare_long(long_smem_), "kernel attribute");
+      long_plan_.grid = sms_ * std::max(1, long_blocks_per_sm(long_smem_));
+      long_plan_.hap_bytes = rp.hap_bytes;
+      long_plan_.bnd_cols = rp.bnd_cols;
+      long_plan_.f64 = true;
+      long_plan_.multi = true;
+    }
+  }
+  if (long_plan_.grid == 0) {  // no long kernel: the long reads stay on the one-warp FP64 kernel
+    f64_items_.insert(f64_items_.end(), f64_long_items_.begin(), f64_long_items_.end());
+    f64_long_items_.clear();
+  }
+  auto cells = [&](const PairRef& x) {
+    return (b.read_offsets[x.read + 1] - b.read_offsets[x.read]) * (b.hap_offsets[x.hap + 1] - b.hap_offsets[x.hap]);
+  };
+  std::sort(f64_long_items_.begin(), f64_long_items_.end(),
+            [&](const PairRef& x, const PairRef& y) { return cells(x) < cells(y); });
   return BV_OK;
 }
 
@@ -382,7 +410,8 @@ bv_status Engine::upload_plan() {
   for (const auto& lp : plans_)
     if (lp.multi) need32 = std::max<size_t>(need32, (size_t)lp.grid * lp.warps_per_block * (size_t)lp.bnd_cols * 4 * sizeof(float));
   if (need32) BV_CUDA(d_bnd32_.reserve(need32), "alloc boundary buffers");
-  const size_t need64 = (size_t)rescue_plan_.grid * (kThreadsPerBlock / kWarp) * (size_t)rescue_plan_.bnd_cols * 4 * sizeof(double);
+  const size_t need64 = std::max((size_t)rescue_plan_.grid * (kThreadsPerBlock / kWarp) * (size_t)rescue_plan_.bnd_cols,
+                                 (size_t)long_plan_.grid * (size_t)long_plan_.bnd_cols) * 4 * sizeof(double);
   BV_CUDA(d_bnd64_.reserve(need64), "alloc FP64 boundary buffers");
   if (!units_.empty())
     BV_CUDA(cudaMemcpyAsync(d_units_.get(), units_.data(), sizeof(Unit) * units_.size(), cudaMemcpyHostToDevice,
@@ -390,6 +419,10 @@ bv_status Engine::upload_plan() {
   if (!f64_items_.empty())
     BV_CUDA(cudaMemcpyAsync(d_rescue_.get(), f64_items_.data(), sizeof(PairRef) * f64_items_.size(),
                             cudaMemcpyHostToDevice, stream_), "H2D");
+  if (!f64_long_items_.empty())  // at the list's far end
+    BV_CUDA(cudaMemcpyAsync(d_rescue_.as<PairRef>() + (std::max<int64_t>(n_results_, 1) - (int64_t)f64_long_items_.size()),
+                            f64_long_items_.data(), sizeof(PairRef) * f64_long_items_.size(), cudaMemcpyHostToDevice,
+                            stream_), "H2D");
   if (uniform_gaps_)
     BV_CUDA(launch_pack_quals_uniform(d_q_.as<uint8_t>(), gap_ins_, gap_del_, gap_gcp_, d_quals4_.as<uchar4>(),
                                       n_read_bytes_, sms_, stream_), "pack quals");
@@ -435,6 +468,10 @@ bv_status Engine::enqueue_kernels(bool capturing) {
     BV_CUDA(launch_set_u64(&d_counters_.as<Counters>()->rescue_count, (unsigned long long)f64_items_.size(), stream_),
             "set FP64 count");
   }
+  if (!f64_long_items_.empty()) {
+    BV_CUDA(launch_set_u64(&d_counters_.as<Counters>()->rescue_long_count, (unsigned long long)f64_long_items_.size(),
+                           stream_), "set FP64 count");
+  }
   KernelParams p{};
   p.batch.read_bases = d_read_bases_.as<uint8_t>();
   p.batch.read_quals = d_quals4_.as<uchar4>();
@@ -447,6 +484,7 @@ bv_status Engine::enqueue_kernels(bool capturing) {
   p.out = d_out_.as<double>();
   p.rescue = d_rescue_.as<PairRef>();
   p.rescue_cap = std::max<int64_t>(n_results_, 1);
+  p.long_rows = long_plan_.grid > 0 ? kLongRows : 0;
   p.warps_per_block = kThreadsPerBlock / kWarp;  // band-path fallback and audit launches
   BV_CUDA(rec(ev_[2]), "event");
   if (band_enabled()) {
@@ -496,6 +534,12 @@ bv_status Engine::enqueue_kernels(bool capturing) {
     p.rescale = 1;
     p.rescale_target = kRescaleTarget;
     p.cells_ctr = &d_counters_.as<Counters>()->rescued_cells;
+    if (long_plan_.grid > 0) {  // long reads first: a block per pair, longest first
+      KernelParams q = p;
+      q.hap_bytes = long_plan_.hap_bytes;
+      q.bnd_cols = long_plan_.bnd_cols;
+      BV_CUDA(launch_forward_long(q, long_plan_.grid, long_smem_, stream_), "FP64 long-read launch");
+    }
     BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP64 forward launch");
     p.cells_ctr = nullptr;
   }
@@ -573,7 +617,7 @@ bv_status Engine::finish(bv_phmm_stats* stats) {
     cudaEventElapsedTime(&ms64, ev_[3], ev_[4]);
     stats->pairs = n_results_;
     stats->cells = n_cells_;
-    stats->rescued = (int64_t)c.rescue_count;
+    stats->rescued = (int64_t)(c.rescue_count + c.rescue_long_count);
     stats->rescued_cells = (int64_t)c.rescued_cells;
     stats->underflow = (int64_t)c.underflow_count;
     stats->kernel_launches = band_enabled()

@@ -206,8 +206,11 @@ class Engine {
   // staged batch
   std::vector<Unit> units_;
   std::vector<PairRef> f64_items_;  // pairs sent straight to FP64 (precision F64)
+  std::vector<PairRef> f64_long_items_;  // the long reads among them, ascending cells (the list's far end first)
   std::vector<LaunchPlan> plans_;
   LaunchPlan rescue_plan_;
+  LaunchPlan long_plan_;  // FP64 long reads, a block of kLongWarps warps per pair (grid 0: none)
+  int long_smem_ = 0;
   int64_t n_results_ = 0;
   int64_t n_cells_ = 0;
   int64_t n_read_bytes_ = 0;

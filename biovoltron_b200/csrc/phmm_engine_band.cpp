@@ -250,6 +250,11 @@ bv_status Engine::band_routes(int64_t n, int32_t* d_lo, int32_t* width, int32_t*
   const unsigned long long nr = std::min<unsigned long long>(cc.rescue_count, (unsigned long long)std::max<int64_t>(n_results_, 1));
   std::vector<PairRef> rl(nr);
   if (nr) BV_CUDA(cudaMemcpy(rl.data(), d_rescue_.get(), sizeof(PairRef) * nr, cudaMemcpyDeviceToHost), "rescue list");
+  const unsigned long long nl =
+      std::min<unsigned long long>(cc.rescue_long_count, (unsigned long long)std::max<int64_t>(n_results_, 1) - nr);
+  rl.resize(nr + nl);
+  if (nl) BV_CUDA(cudaMemcpy(rl.data() + nr, d_rescue_.as<PairRef>() + (std::max<int64_t>(n_results_, 1) - (int64_t)nl),
+                             sizeof(PairRef) * nl, cudaMemcpyDeviceToHost), "rescue list");
   for (const auto& x : rl)
     if (x.out >= 0 && x.out < n && route[x.out] == 0) route[x.out] = 3;
   return BV_OK;

@@ -31,7 +31,17 @@ struct KernelParams {
   int rescale;            // renormalise between strips (FP64 variants)
   int rescale_target;     // binary exponent the boundary maximum is scaled to
   unsigned long long* cells_ctr;  // if set, FP64 launches add read x haplotype length per pair here
+  int long_rows;          // > 0: FP32 results of reads this long or longer go to the FP64 list's long part
 };
+
+// Long reads in FP64: a block of kLongWarps warps per pair (phmm_long.cu);
+// reads from kLongRows bases on (four strips of 128 rows) take it.
+constexpr int kLongWarps = 4;
+constexpr int kLongRows = kLongWarps * 128;
+int long_smem_bytes(int hap_bytes);
+cudaError_t prepare_long(int smem);
+int long_blocks_per_sm(int smem);
+cudaError_t launch_forward_long(const KernelParams& p, int grid, int smem, cudaStream_t st);
 
 // Variant table: (precision, rows per lane, multi-strip, two haplotypes per
 // warp).  Paired variants exist for FP32 single strip only.

@@ -76,6 +76,47 @@ def test_config2_long_reads_vs_rescaled_oracle(engine, oracle):
     assert st["rescued"] == b.n_pairs  # all far below 1e-28 (log10 ~ -hundreds)
 
 
+def test_config2_full_length_long_reads(oracle):
+    """Full-length config-2 pairs (reads up to 10 kb against haplotypes up to
+    12 kb): every pair falls below 1e-28 in FP32 and is rescued; reads of 512
+    bases or more run on the several-warps-per-pair FP64 kernel, whose groups
+    of strips are renormalised between groups.  Against the rescaled FP64
+    oracle, in the default precision and with every pair in FP64."""
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    b = W.config2(seed=23, n_pairs=6)
+    assert b.read_lengths().max() > 6000
+    truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
+    for precision in ("auto", "f64"):
+        with PairHMMEngine(device=0, precision=precision) as e:
+            got, st = e.compute_regions(b, with_stats=True)
+        assert np.all(np.isfinite(got))
+        assert np.max(np.abs(got - truth)) <= 1e-9, (precision, got - truth)
+        assert st["rescued"] == b.n_pairs
+
+
+def test_long_read_lengths_around_the_group_boundaries(oracle):
+    """Reads whose strip counts fall on either side of a group of four strips
+    (and of the long-read threshold of 512 bases), mixed with short reads in
+    one batch, all in FP64: the long and the one-warp FP64 kernels share the
+    FP64 list."""
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    rng = np.random.default_rng(31)
+    regions = []
+    for rl in (100, 383, 511, 512, 513, 639, 640, 767, 1023, 1024, 1025, 1600):
+        hap = W._random_seq(rng, rl + 300)
+        start = int(rng.integers(0, 250))
+        read = W._mutate_read(rng, hap, start, rl, 0.02, 0.01, 1, 2)
+        q, i, d, c = W._quals(rng, len(read), 10, 40)
+        regions.append(([(read, q, i, d, c)], [hap, W._random_seq(rng, rl + 200)]))
+    b = W._build(regions, "long-read lengths around the strip groups")
+    truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
+    with PairHMMEngine(device=0, precision="f64") as e:
+        got = e.compute_regions(b)
+    fin = np.isfinite(truth)
+    assert np.array_equal(np.isfinite(got), fin)
+    assert np.max(np.abs(got[fin] - truth[fin])) <= 1e-9
+
+
 def test_staged_graph_replay_is_deterministic(engine):
     b = W.config1(seed=3, n_regions=16)
     direct = engine.compute_regions(b)
