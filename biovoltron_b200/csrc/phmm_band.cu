@@ -64,39 +64,60 @@ __device__ __forceinline__ uint32_t tbl_bucket(uint32_t code, uint32_t nb) {
   return (uint32_t)(((uint64_t)(code * 0x9E3779B1u) * nb) >> 32);
 }
 
-__global__ void __launch_bounds__(256) k_hap_table(const uint8_t* __restrict__ hap_bases,
-                                                   const int64_t* __restrict__ hap_off, long long n_haps,
-                                                   uint32_t* __restrict__ table) {
-  __shared__ uint32_t st[2 * kBandMaxHap + 4];
-  __shared__ uint8_t sb[kBandMaxHap];
-  for (long long h = blockIdx.x; h < n_haps; h += gridDim.x) {
+// A warp per haplotype: lane l takes a run of consecutive positions and rolls
+// the 11-mer code along it (one new base per position; an 11-bit shift
+// register marks windows holding a non-ACGT byte), inserting with atomicCAS
+// into the warp's table in shared memory; the table then goes out coalesced.
+// Insertion order does not matter to the lookups: a key sits in its bucket
+// or in a later one that was full when it was inserted, and buckets only
+// fill up, so a probe that stops at the first bucket with a free slot sees it.
+constexpr int kHapTblWarps = 4;
+constexpr int kHapTblWords = 2 * kBandMaxHap + 4;
+
+__global__ void __launch_bounds__(kHapTblWarps * 32) k_hap_table(const uint8_t* __restrict__ hap_bases,
+                                                                 const int64_t* __restrict__ hap_off, long long n_haps,
+                                                                 uint32_t* __restrict__ table) {
+  __shared__ uint32_t s_tbl[kHapTblWarps][kHapTblWords];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  uint32_t* st = s_tbl[wib];
+  const long long nwarps = (long long)gridDim.x * kHapTblWarps;
+  for (long long h = blockIdx.x * (long long)kHapTblWarps + wib; h < n_haps; h += nwarps) {
     const int64_t off = hap_off[h];
     const int H = (int)(hap_off[h + 1] - off);
     if (H > kBandMaxHap || H < kK) continue;
     const uint32_t nb = (uint32_t)(H + 1) / 2;
-    __syncthreads();
-    for (int x = threadIdx.x; x < H; x += blockDim.x) sb[x] = hap_bases[off + x];
-    for (uint32_t x = threadIdx.x; x < 4 * nb; x += blockDim.x) st[x] = kEmpty;
-    __syncthreads();
-    for (int x = threadIdx.x; x + kK <= H; x += blockDim.x) {
-      uint32_t code = 0;
-      bool ok = true;
-      for (int t = 0; t < kK; ++t) {
-        const int c = kmer_code(sb[x + t]);
-        ok &= c >= 0;
+    for (uint32_t x = lane; x < 4 * nb; x += 32) st[x] = kEmpty;
+    __syncwarp();
+    const uint8_t* hb = hap_bases + off;
+    const int npos = H - kK + 1;
+    const int seg = (npos + 31) / 32;
+    const int x0 = lane * seg, x1 = min(npos, x0 + seg);
+    if (x0 < x1) {
+      uint32_t code = 0, bad = 0;
+      for (int t = 0; t < kK - 1; ++t) {
+        const int c = kmer_code(hb[x0 + t]);
         code = (code << 2) | (uint32_t)(c & 3);
+        bad = (bad << 1) | (c < 0 ? 1u : 0u);
       }
-      if (!ok) continue;
-      const uint32_t e = (code << 10) | (uint32_t)x;
-      uint32_t bk = tbl_bucket(code, nb);
-      for (bool done = false; !done; bk = bk + 1 == nb ? 0 : bk + 1)
-        for (int t = 0; t < 4 && !done; ++t) done = atomicCAS(&st[4 * bk + t], kEmpty, e) == kEmpty;
+      for (int x = x0; x < x1; ++x) {
+        const int c = kmer_code(hb[x + kK - 1]);
+        code = ((code << 2) | (uint32_t)(c & 3)) & ((1u << (2 * kK)) - 1u);
+        bad = ((bad << 1) | (c < 0 ? 1u : 0u)) & ((1u << kK) - 1u);
+        if (bad) continue;
+        const uint32_t e = (code << 10) | (uint32_t)x;
+        uint32_t bk = tbl_bucket(code, nb);
+        bool done = false;
+        for (uint32_t tries = 0; tries < nb && !done; ++tries, bk = bk + 1 == nb ? 0 : bk + 1)
+          for (int t = 0; t < 4 && !done; ++t) done = atomicCAS(&st[4 * bk + t], kEmpty, e) == kEmpty;
+      }
     }
-    __syncthreads();
+    __syncwarp();
     uint32_t* dst = table + tbl_base(off, h);
-    for (uint32_t x = threadIdx.x; x < 4 * nb; x += blockDim.x) dst[x] = st[x];
+    for (uint32_t x = lane; x < 4 * nb; x += 32) dst[x] = st[x];
+    __syncwarp();
   }
 }
+
 
 // Per read: the 2-bit code of the 11-mer starting at each position (or
 // kNoCode when it holds a byte other than A/C/G/T), computed once per read
@@ -104,28 +125,34 @@ __global__ void __launch_bounds__(256) k_hap_table(const uint8_t* __restrict__ h
 constexpr uint32_t kNoCode = 0xffffffffu;
 
 __global__ void k_read_kmers(const uint8_t* __restrict__ read_bases, long long n_bytes, uint32_t* __restrict__ codes) {
-  // Four positions per thread from four aligned 32-bit loads (bytes x0 .. x0+15;
-  // the buffer carries 16 bytes of tail padding): each base is converted once.
+  // Four positions per thread from four aligned 32-bit loads (bytes x0 ..
+  // x0+15; the buffer carries 16 bytes of tail padding), four bytes at a time:
+  // the 2-bit code of A C T G is (byte >> 1) & 3 (ConvertChar's order), byte
+  // compares give the valid mask.  lo holds base k's code at bits 2k, 2k+1.
   const long long n4 = (n_bytes + 3) / 4;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n4; t += (long long)gridDim.x * blockDim.x) {
     const long long x0 = 4 * t;
-    uint32_t code16 = 0, bad = 0;  // bases x0 .. x0+15: 2-bit codes (first base highest), invalid-base mask
+    uint32_t lo = 0, valid = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const uint32_t w = x0 + 4 * j < n_bytes ? *reinterpret_cast<const uint32_t*>(read_bases + x0 + 4 * j) : 0u;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const long long x = x0 + 4 * j + b;
-        const int c = x < n_bytes ? kmer_code((uint8_t)(w >> (8 * b))) : -1;
-        code16 = (code16 << 2) | (uint32_t)(c & 3);
-        bad |= (c < 0 ? 1u : 0u) << (4 * j + b);
-      }
+      const long long rem = n_bytes - (x0 + 4 * j);
+      const uint32_t w = rem > 0 ? *reinterpret_cast<const uint32_t*>(read_bases + x0 + 4 * j) : 0u;
+      const uint32_t c4 = (w >> 1) & 0x03030303u;
+      uint32_t v4 = __vcmpeq4(w, 0x41414141u) | __vcmpeq4(w, 0x43434343u) | __vcmpeq4(w, 0x47474747u) |
+                    __vcmpeq4(w, 0x54545454u);
+      if (rem < 4) v4 &= rem <= 0 ? 0u : (0xFFFFFFFFu >> (8 * (4 - rem)));  // bytes past the end
+      const uint32_t y = c4 | (c4 >> 6);
+      lo |= ((y | (y >> 12)) & 0xFFu) << (8 * j);
+      valid |= (((v4 & 0x01010101u) * 0x01020408u) >> 24) << (4 * j);
     }
     uint32_t out[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const bool ok = x0 + q + kK <= n_bytes && ((bad >> q) & 0x7ffu) == 0u;
-      out[q] = ok ? (code16 >> (2 * (16 - kK - q))) & ((1u << (2 * kK)) - 1u) : kNoCode;
+      const bool ok = x0 + q + kK <= n_bytes && ((valid >> q) & 0x7ffu) == 0x7ffu;
+      // bases q .. q+10, first base highest: reverse the 2-bit groups
+      uint32_t r = __brev((lo >> (2 * q)) & ((1u << (2 * kK)) - 1u)) >> (32 - 2 * kK);
+      r = ((r >> 1) & 0x155555u) | ((r & 0x155555u) << 1);
+      out[q] = ok ? r : kNoCode;
     }
     // positions too close to a read's end are masked by the caller
     if (x0 + 4 <= n_bytes) {
@@ -1127,8 +1154,8 @@ cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint
 cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint32_t* table,
                              int sms, cudaStream_t st) {
   if (n_haps <= 0) return cudaSuccess;
-  const long long blocks = std::min<long long>(n_haps, (long long)sms * 8);
-  k_hap_table<<<(int)blocks, 256, 0, st>>>(hap_bases, hap_off, n_haps, table);
+  const long long blocks = std::min<long long>((n_haps + kHapTblWarps - 1) / kHapTblWarps, (long long)sms * 6);
+  k_hap_table<<<(int)blocks, kHapTblWarps * 32, 0, st>>>(hap_bases, hap_off, n_haps, table);
   return cudaGetLastError();
 }
 

@@ -91,7 +91,12 @@ __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
   T* bnd = MULTI ? reinterpret_cast<T*>(p.bnd) + (size_t)warp_global * p.bnd_cols * 4 : nullptr;
   const unsigned long long n = p.from_rescue ? p.ctr->rescue_count
                                : p.n_units_dev ? *p.n_units_dev : (unsigned long long)p.n_units;
-  const unsigned long long n_eff = p.from_rescue && n > (unsigned long long)p.rescue_cap ? p.rescue_cap : n;
+  const unsigned long long n_short = p.from_rescue && n > (unsigned long long)p.rescue_cap ? p.rescue_cap : n;
+  // FP64 pass: after the short list, the long list's entries the long-read
+  // kernel handed back (read index complemented)
+  const unsigned long long n_long =
+      p.from_rescue && p.long_rows > 0 ? min(p.ctr->rescue_long_count, (unsigned long long)p.rescue_cap) : 0ull;
+  const unsigned long long n_eff = n_short + n_long;
   unsigned long long* next = p.from_rescue ? &p.ctr->rescue_next : &p.ctr->unit_next[p.slot];
   for (;;) {
     unsigned long long w = 0;
@@ -99,14 +104,25 @@ __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
     w = __shfl_sync(0xffffffffu, w, 0);
     if (w >= n_eff) break;
     Item it;
+    long long handed_back = -1;  // list slot of an entry the long-read kernel handed back
     if (p.from_rescue) {
-      const PairRef pr = p.rescue[w];
+      PairRef pr;
+      if (w < n_short) {
+        pr = p.rescue[w];
+      } else {
+        handed_back = p.rescue_cap - 1 - (long long)(w - n_short);
+        pr = p.rescue[handed_back];
+        if (pr.read >= 0) continue;  // scored by the long-read kernel
+        pr.read = ~pr.read;
+      }
       it.read = pr.read; it.hap0 = pr.hap; it.nh = 1; it.out0 = pr.out;
     } else {
       const Unit u = p.units[p.unit_base + w];
       it.read = u.read; it.hap0 = u.hap0; it.nh = u.nh; it.out0 = u.out0;
     }
     process_item<T, RT, MULTI, PAIR>(p, it, wsm, lane, bnd);
+    // the mark is cleared: a replayed batch finds the list as it was staged
+    if (handed_back >= 0 && lane == 0) p.rescue[handed_back].read = it.read;
   }
 }
 

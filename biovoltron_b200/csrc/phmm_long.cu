@@ -20,6 +20,10 @@
 // shrink over its 128 K rows before the next renormalisation (the one-warp
 // kernel renormalises every 128 rows).
 //
+// A pair whose group-end row maximum falls below 2^kLongMinExp, or whose
+// result is not a positive finite number, is handed back to the one-warp FP64
+// kernel (its list entry marked), which runs after this one.
+//
 // The haplotype codes are staged once per pair for all warps.  Every wait is
 // bounded (status bit 8 when one gives up); after the first wait of a block
 // that gives up the others are skipped, so a broken hand-over ends after one
@@ -37,6 +41,10 @@ namespace bvphmm {
 namespace {
 
 constexpr int kLongRT = 4;     // rows per lane (FP64)
+// a group whose last row's maximum is below 2^kLongMinExp (relative to the
+// 2^1000 its first row started from, more than 1,600 binary orders) hands the
+// pair back: the one-warp kernel renormalises every 128 rows instead of 512
+constexpr int kLongMinExp = -600;
 constexpr int kLongSlots = 4;  // chunk slots per channel
 using LS = WarpSmem<double, kLongRT>;
 constexpr int kColB = LS::kColBytes;  // bytes per boundary column (M, X, Y, unused)
@@ -65,6 +73,7 @@ struct LongShared {  // at LongLayout::kScalars
   long long kexp;    // current group's exponent: stored values are true values * 2^-kexp
   long long item;
   int fail;
+  int redo;          // the pair goes back to the one-warp FP64 kernel
 };
 
 struct LongIO {
@@ -79,7 +88,7 @@ struct LongIO {
   double* ring_in;
   uint64_t* ring_mb;
   double* ring_out;
-  double in_scale;
+  double in_scale, in_scale2;  // the group-start renormalisation, as two exact power-of-two factors
 };
 constexpr int kInZero = 0, kInChan = 1, kInGlobal = 2;
 constexpr int kOutNone = 0, kOutChan = 1, kOutGlobal = 2;
@@ -140,9 +149,9 @@ __device__ __forceinline__ void run_strip_long(const Rows<double, RT>& rw, const
       mbar_init(io.ring_mb + 1, 1);
       fence_for_bulk();
       bulk_g2s(io.ring_in, io.bnd + (size_t)32 * 4, kChunkB, io.ring_mb);
-      dM = io.bnd[31 * 4 + 0] * io.in_scale;
-      dX = io.bnd[31 * 4 + 1] * io.in_scale;
-      dY = io.bnd[31 * 4 + 2] * io.in_scale;
+      dM = io.bnd[31 * 4 + 0] * io.in_scale * io.in_scale2;
+      dX = io.bnd[31 * 4 + 1] * io.in_scale * io.in_scale2;
+      dY = io.bnd[31 * 4 + 2] * io.in_scale * io.in_scale2;
       if (!*fail && !mbar_wait(io.ring_mb, 0)) { ok = false; *fail = 1; }
       rphase ^= 1u;
     }
@@ -171,7 +180,9 @@ __device__ __forceinline__ void run_strip_long(const Rows<double, RT>& rw, const
           else { upM = T(0); upX = T(0); upY = T(0); }
         } else if (io.in_mode == kInGlobal) {
           const T* rin = io.ring_in + ((k & 1) * 32 + u) * 4;
-          upM = rin[0] * io.in_scale; upX = rin[1] * io.in_scale; upY = rin[2] * io.in_scale;
+          upM = rin[0] * io.in_scale * io.in_scale2;
+          upX = rin[1] * io.in_scale * io.in_scale2;
+          upY = rin[2] * io.in_scale * io.in_scale2;
         } else {
           upM = T(0); upX = T(0); upY = T(0);
         }
@@ -302,7 +313,10 @@ __global__ void __launch_bounds__(K * kWarp) k_forward_long(KernelParams p) {
       r[0] = 0.0; r[1] = 0.0; r[2] = 0.0;
     }
     fence_for_bulk();  // those rows are read by bulk copies
-    if (threadIdx.x == 0) sh.kexp = 0;
+    if (threadIdx.x == 0) {
+      sh.kexp = 0;
+      sh.redo = 0;
+    }
     __syncthreads();
     for (int s = w; s < nstrips; s += K) {
       Rows<double, kLongRT> rw;
@@ -312,8 +326,10 @@ __global__ void __launch_bounds__(K * kWarp) k_forward_long(KernelParams p) {
       io.in_mode = s == 0 ? kInZero : (s % K == 0 ? kInGlobal : kInChan);
       io.out_mode = s == nstrips - 1 ? kOutNone : (s % K == K - 1 ? kOutGlobal : kOutChan);
       io.in_scale = 1.0;
+      io.in_scale2 = 1.0;
       if (io.in_mode == kInGlobal) {
         // renormalise: the previous group's last row, maximum scaled to 2^target
+        // (a factor up to 2^2074 does not fit one double: two factors, each exact)
         double m = 0.0;
         if (lane == 0) {
           ok &= wait_flip(grp_done, gph, 0, fail);
@@ -324,8 +340,14 @@ __global__ void __launch_bounds__(K * kWarp) k_forward_long(KernelParams p) {
           int e2;
           frexp(m, &e2);
           const int shift = e2 - p.rescale_target;
-          io.in_scale = ldexp(1.0, -shift);
+          const int a = min(-shift, 1023), b2 = min(-shift - a, 1023);
+          io.in_scale = ldexp(1.0, a);
+          io.in_scale2 = ldexp(1.0, b2);
           if (lane == 0) sh.kexp += shift;
+          // the group fell far below the one-warp kernel's per-strip range: that kernel redoes the pair
+          if (lane == 0 && e2 < kLongMinExp) sh.redo = 1;
+        } else if (lane == 0) {
+          sh.redo = 1;
         }
         __syncwarp();
       }
@@ -339,11 +361,18 @@ __global__ void __launch_bounds__(K * kWarp) k_forward_long(KernelParams p) {
         if (lane == 0) mbar_arrive(grp_done);
       }
       if (s == nstrips - 1 && lane == kWarp - 1) {
-        write_result<double>(p, pr.read, pr.hap, pr.out, sumM + sumX, sh.kexp);
-        if (p.cells_ctr) atomicAdd(p.cells_ctr, (unsigned long long)R * (unsigned long long)H);
+        const double res = sumM + sumX;
+        if (sh.redo || !(res > 0.0 && isfinite(res))) {
+          sh.redo = 1;
+        } else {
+          write_result<double>(p, pr.read, pr.hap, pr.out, res, sh.kexp);
+          if (p.cells_ctr) atomicAdd(p.cells_ctr, (unsigned long long)R * (unsigned long long)H);
+        }
       }
     }
     __syncthreads();
+    // handed back: the entry is marked (read index complemented) for the one-warp FP64 kernel
+    if (threadIdx.x == 0 && sh.redo) p.rescue[p.rescue_cap - 1 - wi].read = ~pr.read;
   }
   if (!ok) atomicOr(&p.ctr->status, 8ull);
 }

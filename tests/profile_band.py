@@ -21,12 +21,14 @@ from biovoltron_b200.pairhmm import PairHMMEngine  # noqa: E402
 def _batch(workload: str, regions: int, seed: int):
     if workload == "config4":
         return W.config4(seed=seed, n_regions=regions)
+    if workload == "config2":  # long pairs: `regions` pairs
+        return W.config2(seed=seed, n_pairs=regions)
     return W.config1(seed=seed, n_regions=regions)
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="config1", choices=["config1", "config4"])
+    ap.add_argument("--workload", default="config1", choices=["config1", "config2", "config4"])
     ap.add_argument("--regions", type=int, default=512)
     ap.add_argument("--half", type=int, default=6)
     ap.add_argument("--margin", type=int, default=2)
@@ -36,6 +38,7 @@ def main():
     ap.add_argument("--train-regions", type=int, default=0)
     ap.add_argument("--epochs", type=int, default=8)
     ap.add_argument("--full", action="store_true", help="also time the full DP on the same batch")
+    ap.add_argument("--plain-only", action="store_true", help="only the full DP (FP32 with FP64 rescue)")
     a = ap.parse_args()
     if a.weights and a.train_regions > 0:
         with PairHMMEngine() as e:
@@ -44,6 +47,12 @@ def main():
         print(json.dumps({"train": rep}))
     b = _batch(a.workload, a.regions, 1)
     print(json.dumps({"pairs": b.n_pairs, "cells": b.n_cells()}))
+    if a.plain_only:
+        with PairHMMEngine() as e:
+            e.stage(b)
+            for _ in range(a.runs):
+                print(json.dumps({"full": e.run()}))
+        return
     with PairHMMEngine() as e:
         use_mlp = bool(a.weights) and os.path.exists(a.weights)
         if use_mlp:

@@ -112,6 +112,13 @@ def test_long_read_lengths_around_the_group_boundaries(oracle):
     truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
     with PairHMMEngine(device=0, precision="f64") as e:
         got = e.compute_regions(b)
+        # staged runs (the second replays a graph) give the same results: the
+        # pairs the long-read kernel hands back (the unrelated haplotypes fall
+        # too far within a group of strips) are scored again each time
+        n = e.stage(b)
+        for _ in range(2):
+            e.run()
+            assert np.array_equal(e.fetch(n), got)
     fin = np.isfinite(truth)
     assert np.array_equal(np.isfinite(got), fin)
     assert np.max(np.abs(got[fin] - truth[fin])) <= 1e-9
