@@ -71,7 +71,7 @@ FLOPS_PER_CELL = 12  # computeMXY: 8 mul + 4 add (avx-pairhmm-template.h:183-198
 # DRAM bytes (read + write) per pair from one ncu capture of a config-4-shaped
 # batch of 2,000 regions: the full-size step is too large to capture, and both
 # kernels' traffic grows with the pairs.
-DRAM_BYTES_PER_PAIR_PLAIN = 103.3  # k_forward<float, 5, 0, 1>: 113 MB per launch, 1.094e6 pairs
+DRAM_BYTES_PER_PAIR_PLAIN = 101.6  # k_forward<float, 5, 0, 1>: 111.2 MB per launch, 1.094e6 pairs
 DRAM_BYTES_PER_BAND_PAIR = 179.4   # k_band_ring_f32<8..32>: 194.8 MB per step, 1.086e6 banded pairs
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum on 2,000 config-4 regions, "
                   "scaled by the step's pairs")

@@ -89,15 +89,18 @@ __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
   const int warp_global = blockIdx.x * p.warps_per_block + wib;
   unsigned char* wsm = smem + (size_t)wib * p.warp_smem_bytes;
   T* bnd = MULTI ? reinterpret_cast<T*>(p.bnd) + (size_t)warp_global * p.bnd_cols * 4 : nullptr;
-  const unsigned long long n = p.from_rescue ? p.ctr->rescue_count
+  // only the FP64 variants drain the FP64 list
+  constexpr bool kList = sizeof(T) == 8;
+  const bool from_list = kList && p.from_rescue;
+  const unsigned long long n = from_list ? p.ctr->rescue_count
                                : p.n_units_dev ? *p.n_units_dev : (unsigned long long)p.n_units;
-  const unsigned long long n_short = p.from_rescue && n > (unsigned long long)p.rescue_cap ? p.rescue_cap : n;
+  const unsigned long long n_short = from_list && n > (unsigned long long)p.rescue_cap ? p.rescue_cap : n;
   // FP64 pass: after the short list, the long list's entries the long-read
   // kernel handed back (read index complemented)
   const unsigned long long n_long =
-      p.from_rescue && p.long_rows > 0 ? min(p.ctr->rescue_long_count, (unsigned long long)p.rescue_cap) : 0ull;
+      from_list && p.long_rows > 0 ? min(p.ctr->rescue_long_count, (unsigned long long)p.rescue_cap) : 0ull;
   const unsigned long long n_eff = n_short + n_long;
-  unsigned long long* next = p.from_rescue ? &p.ctr->rescue_next : &p.ctr->unit_next[p.slot];
+  unsigned long long* next = from_list ? &p.ctr->rescue_next : &p.ctr->unit_next[p.slot];
   for (;;) {
     unsigned long long w = 0;
     if (lane == 0) w = atomicAdd(next, 1ull);
@@ -105,7 +108,7 @@ __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
     if (w >= n_eff) break;
     Item it;
     long long handed_back = -1;  // list slot of an entry the long-read kernel handed back
-    if (p.from_rescue) {
+    if (kList && from_list) {
       PairRef pr;
       if (w < n_short) {
         pr = p.rescue[w];
@@ -122,7 +125,7 @@ __global__ void __launch_bounds__(kThreadsPerBlock) k_forward(KernelParams p) {
     }
     process_item<T, RT, MULTI, PAIR>(p, it, wsm, lane, bnd);
     // the mark is cleared: a replayed batch finds the list as it was staged
-    if (handed_back >= 0 && lane == 0) p.rescue[handed_back].read = it.read;
+    if (kList && handed_back >= 0 && lane == 0) p.rescue[handed_back].read = it.read;
   }
 }
 
