@@ -52,9 +52,12 @@ class _BatchView:
 
     def __init__(self, b: RegionBatch, uniform_gaps: Optional[Tuple[int, int, int]] = None):
         self.b = b
-        self.arrs = [np.ascontiguousarray(x) for x in (
-            b.region_reads.astype(np.int64), b.region_haps.astype(np.int64), b.read_offsets.astype(np.int64),
-            b.read_bases, b.read_q, b.read_i, b.read_d, b.read_c, b.hap_offsets.astype(np.int64), b.hap_bases)]
+        # no copies of arrays that already have the C layout (a copy would cost
+        # host time on every call and lose a page-locked registration)
+        i64 = lambda x: np.ascontiguousarray(x, dtype=np.int64)
+        self.arrs = [i64(b.region_reads), i64(b.region_haps), i64(b.read_offsets)] + [
+            np.ascontiguousarray(x) for x in (b.read_bases, b.read_q, b.read_i, b.read_d, b.read_c)] + [
+            i64(b.hap_offsets), np.ascontiguousarray(b.hap_bases)]
         rr, rh, ro, rb, rq, ri, rd, rc, ho, hb = self.arrs
         gi = gd = gc = 0
         if uniform_gaps is not None:
