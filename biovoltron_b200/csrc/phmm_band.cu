@@ -281,7 +281,8 @@ __device__ __forceinline__ void probe_votes(const uint32_t* tbl, uint32_t nb, ui
 __device__ __forceinline__ void feature_summary(const BandParams& p, long long pi, int R, int H, int64_t ro, int64_t ho,
                                                 const uint32_t* tbl, uint32_t nb, uint32_t code, int i, int stride,
                                                 int last_pos, int n_samp, int v0, int nv, uint32_t* hist, int* hits,
-                                                int* nhit, const uint8_t* oh, int lane, PairScalars* out = nullptr, int out_lane = 0);
+                                                int* nhit, const uint8_t* oh, uint32_t rpre, uint32_t rsuf, int lane,
+                                                PairScalars* out = nullptr, int out_lane = 0);
 
 __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, const uint32_t* tbl, uint32_t* hist,
                                int* hits, int* nhit, const uint8_t* oh, int lane) {
@@ -300,7 +301,11 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
   const uint32_t bk = code != kNoCode ? tbl_bucket(code, nb) : 0u;
   const uint4 q = code != kNoCode ? __ldg(reinterpret_cast<const uint4*>(tbl + 4 * bk)) : make_uint4(0, 0, 0, 0);
   probe_votes(tbl, nb, code, i, R, q, bk, v0, nv);
-  feature_summary(p, pi, R, H, ro, ho, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, hist, hits, nhit, oh, lane);
+  const bool rend = lane < min(16, R);
+  const uint32_t rpre = rend ? oh[p.batch.read_bases[ro + lane]] : 0u;
+  const uint32_t rsuf = rend ? oh[p.batch.read_bases[ro + R - 1 - lane]] : 0u;
+  feature_summary(p, pi, R, H, ro, ho, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, hist, hits, nhit, oh, rpre,
+                  rsuf, lane);
 }
 
 // Everything after the probes, for both featurisers: the fast path (at most
@@ -309,7 +314,8 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
 __device__ __forceinline__ void feature_summary(const BandParams& p, long long pi, int R, int H, int64_t ro, int64_t ho,
                                                 const uint32_t* tbl, uint32_t nb, uint32_t code, int i, int stride,
                                                 int last_pos, int n_samp, int v0, int nv, uint32_t* hist, int* hits,
-                                                int* nhit, const uint8_t* oh, int lane, PairScalars* out, int out_lane) {
+                                                int* nhit, const uint8_t* oh, uint32_t rpre, uint32_t rsuf, int lane,
+                                                PairScalars* out, int out_lane) {
   __nv_bfloat16* f = p.feat + pi * kFeat;
   // summary of the votes: mode (most votes, smallest slot on ties), voted
   // extent, first and last sampled hit (smallest slot on ties), per-diagonal
@@ -438,15 +444,15 @@ __device__ __forceinline__ void feature_summary(const BandParams& p, long long p
     tri_lo = min(tri_lo, d_last - t_suf);
     tri_hi = max(tri_hi, d_first + t_pre);
     // mismatches of the first / last 16 read bases along those diagonals
+    // (the read's nibbles rpre / rsuf: bases lane and R-1-lane, loaded by the caller)
     const int n_end = min(16, R);
-    const uint8_t* rb = p.batch.read_bases + ro;
     const uint8_t* hb = p.batch.hap_bases + ho;
     bool mp = false, ms = false;
     if (lane < n_end) {
-      const int ip = lane, jp = ip + d_first;
-      const int is = R - 1 - lane, js = is + d_last;
-      mp = jp < 0 || jp >= H || (oh[rb[ip]] & oh[hb[jp]]) == 0;
-      ms = js < 0 || js >= H || (oh[rb[is]] & oh[hb[js]]) == 0;
+      const int jp = lane + d_first;
+      const int js = R - 1 - lane + d_last;
+      mp = jp < 0 || jp >= H || (rpre & oh[hb[jp]]) == 0;
+      ms = js < 0 || js >= H || (rsuf & oh[hb[js]]) == 0;
     }
     const int mis_pre = __popc(__ballot_sync(0xffffffffu, mp));
     const int mis_suf = __popc(__ballot_sync(0xffffffffu, ms));
@@ -549,6 +555,13 @@ __global__ void __launch_bounds__(kFeatUWarps * 32, kFeatUBlocksPerSm) k_featuri
     const int n_samp = read_ok ? q_s + 1 + (q_s * stride != last_pos) : 0;  // <= 32
     const int i = read_ok ? min(lane * stride, last_pos) : 0;
     const uint32_t code = lane < n_samp ? __ldg(p.read_kmers + ro + i) : kNoCode;
+    // once per unit: lane k's haplotype offset hap_off[hap0 + k] (k <= 31),
+    // and the one-hot nibbles of the read's first and last 16 bases (lane l:
+    // bases l and R-1-l) for the end-mismatch counts
+    const int64_t unit_off = lane <= min(un.nh, 31) ? p.batch.hap_off[un.hap0 + lane] : 0;
+    const bool rend = read_ok && lane < min(16, R);
+    const uint32_t rpre = rend ? s_oh[p.batch.read_bases[ro + lane]] : 0u;
+    const uint32_t rsuf = rend ? s_oh[p.batch.read_bases[ro + R - 1 - lane]] : 0u;
     // lane k holds the scalar block of the unit's pair k (k < 32) until the
     // unit's pairs are written together
     PairScalars mine;
@@ -561,9 +574,11 @@ __global__ void __launch_bounds__(kFeatUWarps * 32, kFeatUBlocksPerSm) k_featuri
 #pragma unroll
       for (int t = 0; t < kFeatUBatch; ++t) {
         const int k = k0 + t;
-        const int h = un.hap0 + min(k, un.nh - 1);
-        hos[t] = p.batch.hap_off[h];
-        Hs[t] = (int)(p.batch.hap_off[h + 1] - hos[t]);
+        const int kk = min(k, un.nh - 1);
+        const int h = un.hap0 + kk;
+        const int64_t o0 = __shfl_sync(0xffffffffu, unit_off, kk & 31), o1 = __shfl_sync(0xffffffffu, unit_off, (kk + 1) & 31);
+        hos[t] = kk + 1 <= 31 ? o0 : p.batch.hap_off[h];
+        Hs[t] = (int)((kk + 1 <= 31 ? o1 : p.batch.hap_off[h + 1]) - hos[t]);
         const bool ok = k < un.nh && read_ok && Hs[t] >= kK && Hs[t] <= kBandMaxHap && code != kNoCode;
         bk[t] = ok ? tbl_bucket(code, (uint32_t)(Hs[t] + 1) / 2) : 0u;
         q[t] = ok ? __ldg(reinterpret_cast<const uint4*>(p.hap_table + tbl_base(hos[t], h) + 4 * bk[t]))
@@ -593,7 +608,7 @@ __global__ void __launch_bounds__(kFeatUWarps * 32, kFeatUBlocksPerSm) k_featuri
           continue;
         }
         feature_summary(p, pi, R, H, ro, ho, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, nullptr, bins,
-                        nullptr, s_oh, lane, &mine, k & 31);
+                        nullptr, s_oh, rpre, rsuf, lane, &mine, k & 31);
         if ((k & 31) == 31) {
           if (mine.pi >= 0) emit_scalars(p, mine);
           mine.pi = -1;

@@ -171,7 +171,7 @@ __device__ __forceinline__ void run_strip_long(const Rows<double, RT>& rw, const
     const T* cur = io.chin + (k % kLongSlots) * 32 * 4;
     const T* nxt = io.chin + ((k + 1) % kLongSlots) * 32 * 4;
     T* out_slot = io.chout + (k % kLongSlots) * 32 * 4;
-#pragma unroll
+#pragma unroll 8  // a fully unrolled chunk (32 steps, five I/O modes) overflows the instruction cache
     for (int u = 0; u < 32; ++u) {
       if (lane == 0) {
         if (io.in_mode == kInChan) {
