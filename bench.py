@@ -506,7 +506,10 @@ def main():
         if plain is not None:
             pl = plain["steps"][-1]
             ms_plain = float(np.mean(device_ms(plain)))
-            ach = FLOPS_PER_CELL * batch.n_cells() / (mean(plain, "ms_full") / 1e3) / 1e12
+            # cells the FP32 kernels computed: a pair whose strip proves the FP32 result below the
+            # rescue threshold goes to the FP64 pass without its remaining strips
+            fp32_cells = batch.n_cells() - int(pl.get("fp32_skipped_cells", 0))
+            ach = FLOPS_PER_CELL * fp32_cells / (mean(plain, "ms_full") / 1e3) / 1e12
             line["plain"] = {"value": plain_pps, "unit": "pairs/s", "ms_per_step": ms_plain,
                              "gcups": batch.n_cells() / (ms_plain / 1e3) / 1e9,
                              "rescued_per_step": pl["rescued"], "kernel_ms": {
@@ -514,7 +517,8 @@ def main():
             line["roofline_plain"] = {"bound": "fp32", "kernel": "k_forward<float> (full DP, all variants)",
                                       "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
                                       "frac": (ach / fp32_peak) if fp32_peak else None,
-                                      "flops_per_cell": FLOPS_PER_CELL,
+                                      "flops_per_cell": FLOPS_PER_CELL, "cells": fp32_cells,
+                                      "cells_left_to_fp64": batch.n_cells() - fp32_cells,
                                       "traffic": DRAM_BYTES_PER_PAIR_PLAIN * n if args.workload == "config4" else None,
                                       "traffic_source": TRAFFIC_SOURCE if args.workload == "config4" else None}
             if band is not None:

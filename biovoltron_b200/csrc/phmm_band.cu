@@ -119,6 +119,70 @@ __global__ void __launch_bounds__(kHapTblWarps * 32) k_hap_table(const uint8_t* 
 }
 
 
+// The haplotype bases' one-hot nibbles (onehot): base x of the batch's
+// haplotype buffer at bits 4 (x & 7) .. 4 (x & 7) + 3 of word x >> 3, with
+// kNibPad zero words after the last.  The featuriser counts a pair's read-end
+// mismatches from 16 of them at a time (end_mismatches).
+__global__ void k_hap_nibbles(const uint8_t* __restrict__ hap_bases, long long n_bytes, uint32_t* __restrict__ nib) {
+  const long long nw = (n_bytes + 7) / 8 + kNibPad;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < nw; w += (long long)gridDim.x * blockDim.x) {
+    uint32_t v = 0;
+    const long long x0 = 8 * w;
+    if (x0 + 8 <= n_bytes) {
+      const uint2 b = *reinterpret_cast<const uint2*>(hap_bases + x0);  // 8-byte aligned: x0 is a multiple of 8
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        v |= onehot((uint8_t)(b.x >> (8 * t))) << (4 * t);
+        v |= onehot((uint8_t)(b.y >> (8 * t))) << (4 * (t + 4));
+      }
+    } else {
+      for (int t = 0; t < 8 && x0 + t < n_bytes; ++t) v |= onehot(hap_bases[x0 + t]) << (4 * t);
+    }
+    nib[w] = v;
+  }
+}
+
+// Mismatches of n <= 16 read bases against haplotype bases j0 .. j0 + n - 1
+// (the haplotype starts at base index ho of the nibble image and has H
+// bases); rn holds the read bases' one-hot nibbles (nibble l: the base facing
+// haplotype base j0 + l).  A base matches when the nibbles share a bit (N
+// matches everything); a position outside the haplotype is a mismatch.  One
+// lane, three word loads.
+__device__ __forceinline__ int end_mismatches(const uint32_t* __restrict__ nib, int64_t ho, int H, int j0, uint64_t rn,
+                                              int n) {
+  const int lo = max(0, -j0), hi = min(n, H - j0);  // read positions l in [lo, hi) face the haplotype
+  if (hi <= lo) return n;
+  const long long x = ho + j0 + lo;                 // >= ho >= 0
+  const long long w = x >> 3;
+  const int sh = (int)(x & 7) * 4;
+  const uint64_t a = (uint64_t)__ldg(nib + w) | ((uint64_t)__ldg(nib + w + 1) << 32);
+  const uint64_t c = __ldg(nib + w + 2);
+  const uint64_t win = sh ? (a >> sh) | (c << (64 - sh)) : a;  // nibble t: haplotype base j0 + lo + t
+  uint64_t t = win & (rn >> (4 * lo));
+  t |= t >> 2;
+  t |= t >> 1;
+  const int len = hi - lo;
+  const uint64_t keep = (len >= 16 ? ~0ull : ((1ull << (4 * len)) - 1ull)) & 0x1111111111111111ull;
+  return n - __popcll(t & keep);
+}
+
+// One-hot nibbles of a read's first and last n = min(16, R) bases (nibble l:
+// base l, and base R - n + l), assembled by the warp (lane l < n loads base l
+// and base R - n + l).
+__device__ __forceinline__ void read_end_nibbles(const uint8_t* __restrict__ rb, int R, bool ok, const uint8_t* oh,
+                                                 int lane, uint64_t& pre, uint64_t& suf) {
+  const int n = min(16, R);
+  const bool on = ok && lane < n;
+  const uint32_t np = on ? (uint32_t)oh[rb[lane]] << (4 * (lane & 7)) : 0u;
+  const uint32_t ns = on ? (uint32_t)oh[rb[R - n + lane]] << (4 * (lane & 7)) : 0u;
+  const uint32_t p_lo = __reduce_or_sync(0xffffffffu, lane < 8 ? np : 0u);
+  const uint32_t p_hi = __reduce_or_sync(0xffffffffu, lane < 8 ? 0u : np);
+  const uint32_t s_lo = __reduce_or_sync(0xffffffffu, lane < 8 ? ns : 0u);
+  const uint32_t s_hi = __reduce_or_sync(0xffffffffu, lane < 8 ? 0u : ns);
+  pre = (uint64_t)p_lo | ((uint64_t)p_hi << 32);
+  suf = (uint64_t)s_lo | ((uint64_t)s_hi << 32);
+}
+
 // Per read: the 2-bit code of the 11-mer starting at each position (or
 // kNoCode when it holds a byte other than A/C/G/T), computed once per read
 // rather than once per pair.
@@ -238,19 +302,28 @@ __device__ __forceinline__ void write_scalars(__nv_bfloat16* f, int total, int w
 
 // A seeded pair's scalar block and band bounds, as the summary leaves them to
 // one lane (the unit featuriser collects a unit's pairs in lanes 0.. and
-// writes them together).
-struct PairScalars {
-  long long pi;
-  int total, win, R, H, ds, peak, nonzero, n_samp, t_pre, t_suf, d_first, d_last, mis_pre, mis_suf, dmin, dmax, kmin,
-      kmax;
-  bool overflow;
+// writes them together).  The lane that writes them also counts the read
+// ends' mismatches (from the read's end nibbles pre / suf, read_end_nibbles).
+// The read (R bases, n_samp sampled positions) is the same for all pairs a
+// warp emits together, and the unit featuriser's lane k holds its unit's
+// k-th pair (pair index and haplotype follow from k), so none of these is
+// part of the block; H = 0 marks an empty one.
+struct alignas(16) PairScalars {
+  int total, win, H, ds, peak, nonzero, t_pre, t_suf, d_first, d_last, dmin, dmax, kmin, kmax;
+  int overflow;
 };
-__device__ __forceinline__ void emit_scalars(const BandParams& p, const PairScalars& c) {
-  write_scalars(p.feat + c.pi * kFeat, c.total, c.win, c.R, c.H, c.ds, c.peak, c.nonzero, __frcp_rn((float)c.n_samp),
-                c.t_pre, c.t_suf, c.d_first, c.d_last, c.mis_pre, c.mis_suf, c.overflow, c.dmin, c.dmax);
-  p.dstar[c.pi] = c.ds;
-  p.kmin[c.pi] = c.kmin;
-  p.kmax[c.pi] = c.kmax;
+__device__ __forceinline__ void emit_scalars(const BandParams& p, const PairScalars& c, long long pi, int h, int R,
+                                             int n_samp, uint64_t pre, uint64_t suf) {
+  // mismatches of the first / last n read bases along the first / last hit's diagonal
+  const int n = min(16, R);
+  const int64_t ho = p.batch.hap_off[h];
+  const int mis_pre = end_mismatches(p.hap_nib, ho, c.H, c.d_first, pre, n);
+  const int mis_suf = end_mismatches(p.hap_nib, ho, c.H, R - n + c.d_last, suf, n);
+  write_scalars(p.feat + pi * kFeat, c.total, c.win, R, c.H, c.ds, c.peak, c.nonzero, __frcp_rn((float)n_samp),
+                c.t_pre, c.t_suf, c.d_first, c.d_last, mis_pre, mis_suf, c.overflow, c.dmin, c.dmax);
+  p.dstar[pi] = c.ds;
+  p.kmin[pi] = c.kmin;
+  p.kmax[pi] = c.kmax;
 }
 
 // The votes of one sampled 11-mer (lane): its table's bucket `bk`, already
@@ -278,10 +351,10 @@ __device__ __forceinline__ void probe_votes(const uint32_t* tbl, uint32_t nb, ui
   }
 }
 
-__device__ __forceinline__ void feature_summary(const BandParams& p, long long pi, int R, int H, int64_t ro, int64_t ho,
+__device__ __forceinline__ bool feature_summary(const BandParams& p, long long pi, int R, int H, int h,
                                                 const uint32_t* tbl, uint32_t nb, uint32_t code, int i, int stride,
                                                 int last_pos, int n_samp, int v0, int nv, uint32_t* hist, int* hits,
-                                                int* nhit, const uint8_t* oh, uint32_t rpre, uint32_t rsuf, int lane,
+                                                int* nhit, uint64_t pre, uint64_t suf, int lane,
                                                 PairScalars* out = nullptr, int out_lane = 0);
 
 __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, const uint32_t* tbl, uint32_t* hist,
@@ -301,21 +374,19 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
   const uint32_t bk = code != kNoCode ? tbl_bucket(code, nb) : 0u;
   const uint4 q = code != kNoCode ? __ldg(reinterpret_cast<const uint4*>(tbl + 4 * bk)) : make_uint4(0, 0, 0, 0);
   probe_votes(tbl, nb, code, i, R, q, bk, v0, nv);
-  const bool rend = lane < min(16, R);
-  const uint32_t rpre = rend ? oh[p.batch.read_bases[ro + lane]] : 0u;
-  const uint32_t rsuf = rend ? oh[p.batch.read_bases[ro + R - 1 - lane]] : 0u;
-  feature_summary(p, pi, R, H, ro, ho, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, hist, hits, nhit, oh, rpre,
-                  rsuf, lane);
+  uint64_t pre, suf;
+  read_end_nibbles(p.batch.read_bases + ro, R, true, oh, lane, pre, suf);
+  feature_summary(p, pi, R, H, h, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, hist, hits, nhit, pre, suf, lane);
 }
 
 // Everything after the probes, for both featurisers: the fast path (at most
 // one vote per lane) groups lanes by slot; repeated 11-mers (hist != null
 // only) build a per-warp histogram over all slots.
-__device__ __forceinline__ void feature_summary(const BandParams& p, long long pi, int R, int H, int64_t ro, int64_t ho,
+__device__ __forceinline__ bool feature_summary(const BandParams& p, long long pi, int R, int H, int h,
                                                 const uint32_t* tbl, uint32_t nb, uint32_t code, int i, int stride,
                                                 int last_pos, int n_samp, int v0, int nv, uint32_t* hist, int* hits,
-                                                int* nhit, const uint8_t* oh, uint32_t rpre, uint32_t rsuf, int lane,
-                                                PairScalars* out, int out_lane) {
+                                                int* nhit, uint64_t pre, uint64_t suf, int lane, PairScalars* out,
+                                                int out_lane) {
   __nv_bfloat16* f = p.feat + pi * kFeat;
   // summary of the votes: mode (most votes, smallest slot on ties), voted
   // extent, first and last sampled hit (smallest slot on ties), per-diagonal
@@ -323,6 +394,7 @@ __device__ __forceinline__ void feature_summary(const BandParams& p, long long p
   uint32_t best = 0u, fkey = 0xffffffffu, lkey = 0u;
   int smin = INT32_MAX, smax = -1, tri_lo = INT32_MAX, tri_hi = INT32_MIN, total = 0;
   bool overflow = false;
+  int fwin = 0, fnonzero = 0;  // fast path: votes and distinct slots inside the window
   int* wbin = hits;  // 64 bins (fast path)
   const bool fast = !__any_sync(0xffffffffu, nv > 1);
   if (fast) {
@@ -345,14 +417,21 @@ __device__ __forceinline__ void feature_summary(const BandParams& p, long long p
       if (head <= kEndRows) tri_hi = d + head;
     }
     total = __popc(vmask);
-    // warp reductions (one REDUX each)
+    // the first and last sampled hit are the lowest and highest voting lane
+    // (sampled positions grow with the lane); the rest are warp reductions
+    fkey = __shfl_sync(0xffffffffu, fkey, vmask ? __ffs(vmask) - 1 : 0);
+    lkey = __shfl_sync(0xffffffffu, lkey, vmask ? 31 - __clz(vmask) : 0);
     best = __reduce_max_sync(0xffffffffu, best);
-    fkey = __reduce_min_sync(0xffffffffu, fkey);
-    lkey = __reduce_max_sync(0xffffffffu, lkey);
     smin = __reduce_min_sync(0xffffffffu, smin);
     smax = __reduce_max_sync(0xffffffffu, smax);
     tri_lo = __reduce_min_sync(0xffffffffu, tri_lo);
     tri_hi = __reduce_max_sync(0xffffffffu, tri_hi);
+    {
+      const int bs = (int)(0xffffu - (best & 0xffffu));
+      const bool inwin = valid && (unsigned)(v0 - (bs - kHistBins / 2)) < (unsigned)kHistBins;
+      fwin = __popc(__ballot_sync(0xffffffffu, inwin));
+      fnonzero = __popc(__ballot_sync(0xffffffffu, inwin && lead));
+    }
     wbin[lane] = 0;
     wbin[lane + 32] = 0;
     __syncwarp();
@@ -443,19 +522,6 @@ __device__ __forceinline__ void feature_summary(const BandParams& p, long long p
     const int d_first = first_s - R, d_last = last_s - R;
     tri_lo = min(tri_lo, d_last - t_suf);
     tri_hi = max(tri_hi, d_first + t_pre);
-    // mismatches of the first / last 16 read bases along those diagonals
-    // (the read's nibbles rpre / rsuf: bases lane and R-1-lane, loaded by the caller)
-    const int n_end = min(16, R);
-    const uint8_t* hb = p.batch.hap_bases + ho;
-    bool mp = false, ms = false;
-    if (lane < n_end) {
-      const int jp = lane + d_first;
-      const int js = R - 1 - lane + d_last;
-      mp = jp < 0 || jp >= H || (rpre & oh[hb[jp]]) == 0;
-      ms = js < 0 || js >= H || (rsuf & oh[hb[js]]) == 0;
-    }
-    const int mis_pre = __popc(__ballot_sync(0xffffffffu, mp));
-    const int mis_suf = __popc(__ballot_sync(0xffffffffu, ms));
     // 64 histogram bins d* - 32 .. d* + 31, two adjacent bins per lane
     int win = 0, nonzero = 0, peak = 0;
     const float inv = __frcp_rn((float)n_samp);
@@ -468,18 +534,24 @@ __device__ __forceinline__ void feature_summary(const BandParams& p, long long p
       peak = max(peak, cb[t]);
     }
     *reinterpret_cast<__nv_bfloat162*>(f + 2 * lane) = __floats2bfloat162_rn((float)cb[0] * inv, (float)cb[1] * inv);
-    win = __reduce_add_sync(0xffffffffu, win);
-    nonzero = __reduce_add_sync(0xffffffffu, nonzero);
-    peak = __reduce_max_sync(0xffffffffu, peak);
+    if (fast) {
+      win = fwin;
+      nonzero = fnonzero;
+      peak = (int)(best >> 16);  // the mode lies inside the window and has the most votes
+    } else {
+      win = __reduce_add_sync(0xffffffffu, win);
+      nonzero = __reduce_add_sync(0xffffffffu, nonzero);
+      peak = __reduce_max_sync(0xffffffffu, peak);
+    }
     if (overflow) total = max(total, win);
     // voted extent and end triangles (a hit list overflow widens it to everything)
-    const PairScalars c{pi, total, win, R, H, ds, peak, nonzero, n_samp, t_pre, t_suf, d_first, d_last, mis_pre,
-                        mis_suf, smin - R, smax - R, overflow ? INT32_MIN : min(smin - R, tri_lo),
+    const PairScalars c{total, win, H, ds, peak, nonzero, t_pre, t_suf, d_first, d_last,
+                        smin - R, smax - R, overflow ? INT32_MIN : min(smin - R, tri_lo),
                         overflow ? INT32_MAX : max(smax - R, tri_hi), overflow};
     if (out) {
-      if (lane == out_lane) *out = c;
+      if (lane == 0) out[out_lane] = c;  // the block is warp-uniform
     } else if (lane == 0) {
-      emit_scalars(p, c);
+      emit_scalars(p, c, pi, h, R, n_samp, pre, suf);
     }
   }
   __syncwarp();
@@ -491,6 +563,7 @@ __device__ __forceinline__ void feature_summary(const BandParams& p, long long p
     }
   }
   __syncwarp();
+  return best != 0u;
 }
 
 // Slow path: the pairs the unit featuriser handed back (repeated 11-mers,
@@ -527,17 +600,24 @@ __global__ void __launch_bounds__(kFeatWarps * 32) k_featurize_slow(BandParams p
 // once (lane t: sample t), then, kFeatUBatch haplotypes at a time, issues
 // every lane's first bucket load for each haplotype before it summarises them
 // one by one with the warp featuriser's fast path (match_any groups, one
-// REDUX per summary key).  A pair for which some lane sees the same 11-mer
-// more than once goes to the slow list (k_featurize_slow).  Grid-strided over
-// the units: consecutive warps take consecutive units, so a region's tables
-// are read by warps running at the same time and stay in L2.
+// REDUX per summary key; the first and last hit by lane).  A pair's scalar
+// block waits in shared memory; 32 pairs (or the unit's last) are written
+// together, lane k writing pair k and counting its read-end mismatches from
+// the haplotype nibble image (end_mismatches) -- one lane per pair instead of
+// a warp-wide load and ballot.  A pair for which some lane sees the same
+// 11-mer more than once goes to the slow list (k_featurize_slow).
+// Grid-strided over the units: consecutive warps take consecutive units, so a
+// region's tables are read by warps running at the same time and stay in L2.
+// Four blocks per SM (64 registers, a few spilled) beat three (80, none):
+// the kernel is issue-bound and more warps hide the bucket loads.
 // ---------------------------------------------------------------------------
 constexpr int kFeatUWarps = 8;   // warps per block
 constexpr int kFeatUBatch = 2;   // haplotypes whose bucket loads are in flight together
-constexpr int kFeatUBlocksPerSm = 3;
+constexpr int kFeatUBlocksPerSm = 4;
 
 __global__ void __launch_bounds__(kFeatUWarps * 32, kFeatUBlocksPerSm) k_featurize_u(BandParams p) {
   __shared__ int s_bins[kFeatUWarps][kHistBins];
+  __shared__ PairScalars s_ps[kFeatUWarps][32];  // the scalar blocks of a warp's current 32 pairs
   __shared__ uint8_t s_oh[256];
   for (int x = threadIdx.x; x < 256; x += blockDim.x) s_oh[x] = (uint8_t)onehot((uint8_t)x);
   __syncthreads();
@@ -556,16 +636,15 @@ __global__ void __launch_bounds__(kFeatUWarps * 32, kFeatUBlocksPerSm) k_featuri
     const int i = read_ok ? min(lane * stride, last_pos) : 0;
     const uint32_t code = lane < n_samp ? __ldg(p.read_kmers + ro + i) : kNoCode;
     // once per unit: lane k's haplotype offset hap_off[hap0 + k] (k <= 31),
-    // and the one-hot nibbles of the read's first and last 16 bases (lane l:
-    // bases l and R-1-l) for the end-mismatch counts
+    // and the one-hot nibbles of the read's first and last 16 bases for the
+    // end-mismatch counts
     const int64_t unit_off = lane <= min(un.nh, 31) ? p.batch.hap_off[un.hap0 + lane] : 0;
-    const bool rend = read_ok && lane < min(16, R);
-    const uint32_t rpre = rend ? s_oh[p.batch.read_bases[ro + lane]] : 0u;
-    const uint32_t rsuf = rend ? s_oh[p.batch.read_bases[ro + R - 1 - lane]] : 0u;
-    // lane k holds the scalar block of the unit's pair k (k < 32) until the
-    // unit's pairs are written together
-    PairScalars mine;
-    mine.pi = -1;
+    uint64_t pre, suf;
+    read_end_nibbles(p.batch.read_bases + ro, R, read_ok, s_oh, lane, pre, suf);
+    // the scalar block of the unit's pair k waits in slot k & 31 until 32
+    // pairs (or the unit's last) are written together, lane k writing pair k
+    PairScalars* ps = s_ps[wib];
+    unsigned filled = 0u;  // slots holding a seeded pair
     for (int k0 = 0; k0 < un.nh; k0 += kFeatUBatch) {
       uint4 q[kFeatUBatch];
       uint32_t bk[kFeatUBatch];
@@ -607,15 +686,24 @@ __global__ void __launch_bounds__(kFeatUWarps * 32, kFeatUBlocksPerSm) k_featuri
           }
           continue;
         }
-        feature_summary(p, pi, R, H, ro, ho, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, nullptr, bins,
-                        nullptr, s_oh, rpre, rsuf, lane, &mine, k & 31);
+        if (feature_summary(p, pi, R, H, h, tbl, nb, code, i, stride, last_pos, n_samp, v0, nv, nullptr, bins, nullptr,
+                            pre, suf, lane, ps, k & 31))
+          filled |= 1u << (k & 31);
+
         if ((k & 31) == 31) {
-          if (mine.pi >= 0) emit_scalars(p, mine);
-          mine.pi = -1;
+          __syncwarp();
+          if (filled >> lane & 1u) emit_scalars(p, ps[lane], un.out0 + (k - 31) + lane, un.hap0 + (k - 31) + lane, R, n_samp, pre, suf);
+          filled = 0u;
+          __syncwarp();
         }
       }
     }
-    if (mine.pi >= 0) emit_scalars(p, mine);
+    __syncwarp();
+    if (filled >> lane & 1u) {
+      const int base = (un.nh - 1) & ~31;  // the last round's first pair
+      emit_scalars(p, ps[lane], un.out0 + base + lane, un.hap0 + base + lane, R, n_samp, pre, suf);
+    }
+    __syncwarp();
   }
 }
 
@@ -1166,11 +1254,16 @@ cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint
   return cudaGetLastError();
 }
 
-cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint32_t* table,
-                             int sms, cudaStream_t st) {
+cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, long long n_hap_bytes,
+                             uint32_t* table, uint32_t* nib, int sms, cudaStream_t st) {
   if (n_haps <= 0) return cudaSuccess;
   const long long blocks = std::min<long long>((n_haps + kHapTblWarps - 1) / kHapTblWarps, (long long)sms * 6);
   k_hap_table<<<(int)blocks, kHapTblWarps * 32, 0, st>>>(hap_bases, hap_off, n_haps, table);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long nw = hap_nibble_words(n_hap_bytes);
+  const long long nblk = std::min<long long>((nw + 255) / 256, (long long)sms * 8);
+  k_hap_nibbles<<<(int)nblk, 256, 0, st>>>(hap_bases, n_hap_bytes, nib);
   return cudaGetLastError();
 }
 

@@ -90,6 +90,7 @@ struct BandParams {
   const int32_t* pair_read;   // [n_pairs]
   const int32_t* pair_hap;    // [n_pairs]
   const uint32_t* hap_table;  // 11-mer hash tables, 16-byte aligned, hap_table_words() words
+  const uint32_t* hap_nib;    // one-hot nibbles of the haplotype bases, hap_nibble_words() words
   const Unit* units;          // work units (featuriser order)
   long long n_units;
   const uint32_t* read_kmers; // 11-mer code per read position
@@ -122,12 +123,16 @@ struct BandParams {
 
 // Words of the per-haplotype 11-mer hash tables of a batch.
 inline long long hap_table_words(long long n_hap_bytes, long long n_haps) { return 2 * n_hap_bytes + 8 * n_haps + 4; }
+// Words of the haplotype bases' nibble image (8 bases a word, then kNibPad zero words).
+constexpr int kNibPad = 4;
+inline long long hap_nibble_words(long long n_hap_bytes) { return (n_hap_bytes + 7) / 8 + kNibPad; }
 
 cudaError_t launch_pairs_from_units(const Unit* units, long long n_units, int32_t* pair_read, int32_t* pair_hap,
                                     int sms, cudaStream_t st);
 cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint32_t* codes, int sms, cudaStream_t st);
-cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, uint32_t* table,
-                             int sms, cudaStream_t st);
+// The 11-mer tables and the nibble image of the batch's haplotypes (n_hap_bytes bases).
+cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, long long n_hap_bytes,
+                             uint32_t* table, uint32_t* nib, int sms, cudaStream_t st);
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st);
 cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st);
 cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st);

@@ -93,6 +93,7 @@ struct Counters {
   unsigned long long rescued_cells;    // DP cells the FP64 pass computed
   unsigned long long rescue_long_count;  // FP64 list entries of long reads (at the list's far end)
   unsigned long long rescue_long_next;
+  unsigned long long fp32_skipped_cells;  // cells of strips the FP32 pass skipped by handing a pair over early
 };
 
 }  // namespace bvphmm

@@ -818,6 +818,10 @@ __device__ void process_item(const KernelParams& p, const Item& it, unsigned cha
           if (st + 1 < nstrips && p.rescue &&
               fp32_result_below_threshold(p.tables, reinterpret_cast<const float*>(bnd), H, quals, R, lane)) {
             handed_over = true;
+            // read rows 1 .. R sit at padded rows pad + 1 .. pad + R; strips 0 .. st covered those below (st + 1) strip_rows
+            const int done = min(R, (st + 1) * strip_rows - pad - 1);
+            if (lane == kWarp - 1 && done < R)
+              atomicAdd(&p.ctr->fp32_skipped_cells, (unsigned long long)(R - done) * (unsigned long long)H);
             break;
           }
         }

@@ -46,6 +46,7 @@ BandParams Engine::band_params() const {
   p.pair_read = d_pair_read_.as<int32_t>();
   p.pair_hap = d_pair_hap_.as<int32_t>();
   p.hap_table = d_hap_table_.as<uint32_t>();
+  p.hap_nib = d_hap_nib_.as<uint32_t>();
   p.units = d_units_.as<Unit>();
   p.n_units = (long long)units_.size();
   p.read_kmers = d_read_kmers_.as<uint32_t>();
@@ -84,6 +85,8 @@ bv_status Engine::band_prepare() {
   BV_CUDA(d_pair_hap_.reserve(sizeof(int32_t) * n), "alloc pairs");
   BV_CUDA(d_hap_table_.reserve(sizeof(uint32_t) * (size_t)hap_table_words(std::max<int64_t>(n_hap_bytes_, 1), n_haps_)),
           "alloc hap tables");
+  BV_CUDA(d_hap_nib_.reserve(sizeof(uint32_t) * (size_t)hap_nibble_words(std::max<int64_t>(n_hap_bytes_, 1))),
+          "alloc haplotype nibbles");
   BV_CUDA(d_read_kmers_.reserve(sizeof(uint32_t) * std::max<int64_t>(n_read_bytes_, 1)), "alloc kmers");
   BV_CUDA(d_feat_hist_.reserve(sizeof(uint32_t) * (size_t)feat_hist_words(sms_)), "alloc featuriser scratch");
   BV_CUDA(d_feat_slow_.reserve(sizeof(int64_t) * n), "alloc featuriser list");
@@ -133,7 +136,9 @@ bv_status Engine::enqueue_band(bool capturing, KernelParams& kp) {
   };
   BandParams p = band_params();
   BV_CUDA(cudaMemsetAsync(d_bctr_.get(), 0, sizeof(BandCounters), stream_), "memset band counters");
-  BV_CUDA(launch_hap_table(p.batch.hap_bases, p.batch.hap_off, n_haps_, d_hap_table_.as<uint32_t>(), sms_, stream_), "hap tables");
+  BV_CUDA(launch_hap_table(p.batch.hap_bases, p.batch.hap_off, n_haps_, n_hap_bytes_, d_hap_table_.as<uint32_t>(),
+                           d_hap_nib_.as<uint32_t>(), sms_, stream_),
+          "hap tables");
   BV_CUDA(launch_read_kmers(p.batch.read_bases, n_read_bytes_, d_read_kmers_.as<uint32_t>(), sms_, stream_), "kmers");
   BV_CUDA(launch_featurize(p, sms_, stream_), "featurize");
   if (p.use_mlp) BV_CUDA(launch_mlp_forward(p, sms_, stream_), "mlp");

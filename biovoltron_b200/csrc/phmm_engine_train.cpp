@@ -87,7 +87,9 @@ bv_status Engine::stage_for_labels(const bv_region_batch& b) {
   if (s != BV_OK) return s;
   BandParams p = band_params();
   BV_CUDA(cudaMemsetAsync(d_bctr_.get(), 0, sizeof(BandCounters), stream_), "memset band counters");
-  BV_CUDA(launch_hap_table(p.batch.hap_bases, p.batch.hap_off, n_haps_, d_hap_table_.as<uint32_t>(), sms_, stream_), "hap tables");
+  BV_CUDA(launch_hap_table(p.batch.hap_bases, p.batch.hap_off, n_haps_, n_hap_bytes_, d_hap_table_.as<uint32_t>(),
+                           d_hap_nib_.as<uint32_t>(), sms_, stream_),
+          "hap tables");
   BV_CUDA(launch_read_kmers(p.batch.read_bases, n_read_bytes_, d_read_kmers_.as<uint32_t>(), sms_, stream_), "kmers");
   BV_CUDA(launch_featurize(p, sms_, stream_), "featurize");
   return BV_OK;

@@ -48,6 +48,7 @@ class Stats(C.Structure):
         ("band_routed_full", C.c_int64), ("audit_pairs", C.c_int64), ("audit_max_err", C.c_double),
         ("audit_p99_err", C.c_double), ("band_promoted", C.c_int64), ("ms_seed", C.c_double),
         ("ms_full", C.c_double), ("rescued_cells", C.c_int64), ("band_result_cells", C.c_int64),
+        ("fp32_skipped_cells", C.c_int64),
     ]
 
     def as_dict(self):

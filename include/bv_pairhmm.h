@@ -103,6 +103,8 @@ typedef struct bv_phmm_stats {
   int64_t rescued_cells;    /* DP cells the FP64 pass computed (read x haplotype length of its pairs) */
   int64_t band_result_cells; /* band mode: cells of the bands whose likelihood is the result (band plus
                                 ring); band_cells adds the inner band the ring test recomputes */
+  int64_t fp32_skipped_cells; /* cells of the pairs' remaining strips that the FP32 full DP left to the FP64
+                                 pass when a strip proved the FP32 result below the rescue threshold */
 } bv_phmm_stats;
 
 typedef struct bv_phmm_ctx bv_phmm_ctx;
