@@ -913,6 +913,32 @@ __device__ __forceinline__ FwdRow fwd_row(const BandSmem& sm, const float* __res
   return c;
 }
 
+// Rows 2 .. R of a read whose insertion, deletion and gap-continuation
+// qualities are the same on every base (the batch's, checked by k_gap_check):
+// the transition constants of those rows are those of fwd_row with the
+// previous row's pMX / pMY equal to this row's, computed once (u); only the
+// emissions follow the base and its quality -- the same operations on the
+// same values as fwd_row, so the same bits.
+struct UniRows {
+  FwdRow u;  // transition constants of rows >= 2
+  float mm;  // the rows' match-to-match probability
+};
+__device__ __forceinline__ UniRows uni_rows(const BandSmem& sm, const float* __restrict__ minv, uchar4 q0) {
+  const int qi = q0.y & kQualMask, qd = q0.z & kQualMask;
+  UniRows r;
+  r.u = fwd_row(sm, minv, q0, (uint8_t)'A', sm.qp[qi].p, sm.qp[qd].p);
+  r.mm = sm.mm[mm_index(qi, qd)];
+  return r;
+}
+__device__ __forceinline__ FwdRow uni_row(const BandSmem& sm, const UniRows& ur, uchar4 qv, uint8_t base) {
+  FwdRow c = ur.u;
+  const QProb qpb = sm.qp[qv.x & kQualMask];
+  c.em = qpb.q * ur.mm;
+  c.ex = qpb.third * ur.mm;
+  c.rb = (uint32_t)sm.oh[base] * 0x11111111u;
+  return c;
+}
+
 // ---------------------------------------------------------------------------
 // Ring test.  A pair banded on [d_lo, d_lo + W) is also scored on the band
 // widened by a ring of four diagonals on each side (eight for W >= 16); the
@@ -924,10 +950,10 @@ __device__ __forceinline__ FwdRow fwd_row(const BandSmem& sm, const float* __res
 // model cannot represent.  W = 8, 16 run both bands in one row sweep (shared
 // row constants and emissions); W = 24, 32 run them one after the other.
 // ---------------------------------------------------------------------------
-template <int WB, int WI>
+template <int WB, int WI, bool UNI>
 __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Tables* tb, const uchar4* __restrict__ quals,
                                                const uint8_t* __restrict__ rbase, const uint8_t* __restrict__ hap,
-                                               int R, int H, int d) {
+                                               int R, int H, int d, const UniRows& ur) {
   constexpr int NW = WB / 8;
   constexpr int OFF = (WB - WI) / 2;  // inner band = outer diagonals OFF .. OFF + WI - 1
   constexpr int WIN = WI > 0 ? WI : 1;
@@ -961,7 +987,8 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);  // row r + 1 (unused after row R)
+    // row r + 1 (unused after row R)
+    const FwdRow nxt = UNI ? uni_row(sm, ur, qn, bn) : fwd_row(sm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
     {
       const int rn = min(r + 1, R - 1);  // row r + 2
       qn = quals[rn];
@@ -1024,11 +1051,11 @@ __device__ __forceinline__ float2 band_forward_body(const BandSmem& sm, const Ta
 // operations (fma.rn.f32x2 of sm_100) -- each half the scalar operation
 // sequence, so the results are bit-identical to band_forward_body.  Outer
 // cells without an inner twin (the rings) stay scalar.
-template <int WB, int WI>
+template <int WB, int WI, bool UNI>
 __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const Tables* tb,
                                                       const uchar4* __restrict__ quals,
                                                       const uint8_t* __restrict__ rbase, const uint8_t* __restrict__ hap,
-                                                      int R, int H, int d) {
+                                                      int R, int H, int d, const UniRows& ur) {
   constexpr int NW = WB / 8;
   constexpr int OFF = (WB - WI) / 2;   // outer cells 0 .. OFF-1: lower ring; OFF+WI .. WB-1: upper ring
   constexpr int NHI = WB - OFF - WI;
@@ -1065,7 +1092,7 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
   uchar4 qn = quals[min(1, R - 1)];
   uint8_t bn = rbase[min(1, R - 1)];
   for (int r = 1; r <= R; ++r) {
-    const FwdRow nxt = fwd_row(sm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
+    const FwdRow nxt = UNI ? uni_row(sm, ur, qn, bn) : fwd_row(sm, tb->mm_inv_f, qn, bn, cur.pmx, cur.pmy);
     {
       const int rn = min(r + 1, R - 1);
       qn = quals[rn];
@@ -1146,10 +1173,11 @@ __device__ __forceinline__ float2 band_forward_paired(const BandSmem& sm, const 
 
 // One band alone, not inlined: the two passes of the wider classes then hold
 // one band's state at a time.
-template <int WB>
+template <int WB, bool UNI>
 __device__ __noinline__ float band_forward_pass(const BandSmem& sm, const Tables* tb, const uchar4* quals,
-                                                const uint8_t* rbase, const uint8_t* hap, int R, int H, int d) {
-  return band_forward_body<WB, 0>(sm, tb, quals, rbase, hap, R, H, d).x;
+                                                const uint8_t* rbase, const uint8_t* hap, int R, int H, int d,
+                                                const UniRows& ur) {
+  return band_forward_body<WB, 0, UNI>(sm, tb, quals, rbase, hap, R, H, d, ur).x;
 }
 
 // W = 8 keeps three blocks per SM (up to 168 registers); the wider classes two.
@@ -1162,6 +1190,9 @@ __global__ void __launch_bounds__(128, W <= 8 ? 3 : 2) k_band_ring_f32(BandParam
   const Tables* tb = p.tables;
   __shared__ BandSmem sm;
   stage_band_tables(sm, tb);
+  // uniform gap qualities over the batch (k_gap_check ran): one set of row constants
+  const bool uni = p.bctr->gap_checked != 0u && p.bctr->gap_mixed == 0u;
+  const UniRows ur = uni_rows(sm, tb->mm_inv_f, p.batch.read_quals[0]);
   // routed items (bucketed by read length), then items promoted from the next narrower class
   const unsigned long long total =
       p.bctr->band_total[cls] + min(p.bctr->promoted[cls], (unsigned long long)p.item_cap - p.bctr->band_total[cls]);
@@ -1178,12 +1209,16 @@ __global__ void __launch_bounds__(128, W <= 8 ? 3 : 2) k_band_ring_f32(BandParam
     const uint8_t* hap = p.batch.hap_bases + ho;
     float lin, lout;
     if constexpr (kDual) {
-      const float2 t = band_forward_paired<W + 2 * kRing, W>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
+      const float2 t = uni ? band_forward_paired<W + 2 * kRing, W, true>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing, ur)
+                           : band_forward_paired<W + 2 * kRing, W, false>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing, ur);
       lout = t.x;
       lin = t.y;
+    } else if (uni) {
+      lin = band_forward_pass<W, true>(sm, tb, quals, rbase, hap, R, H, it.d_lo, ur);
+      lout = band_forward_pass<W + 2 * kRing, true>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing, ur);
     } else {
-      lin = band_forward_pass<W>(sm, tb, quals, rbase, hap, R, H, it.d_lo);
-      lout = band_forward_pass<W + 2 * kRing>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing);
+      lin = band_forward_pass<W, false>(sm, tb, quals, rbase, hap, R, H, it.d_lo, ur);
+      lout = band_forward_pass<W + 2 * kRing, false>(sm, tb, quals, rbase, hap, R, H, it.d_lo - kRing, ur);
     }
     cells += (unsigned long long)R * (2 * W + 2 * kRing);
     rcells += (unsigned long long)R * (W + 2 * kRing);
@@ -1201,6 +1236,27 @@ __global__ void __launch_bounds__(128, W <= 8 ? 3 : 2) k_band_ring_f32(BandParam
     atomicAdd(&p.bctr->band_cells, cells);
     atomicAdd(&p.bctr->band_result_cells, rcells);
   }
+}
+
+// Marks the batch whose read bases all carry the first base's insertion,
+// deletion and gap-continuation qualities (Biovoltron's SamRecord fills those
+// from constant strings): the banded kernels then take every row's transition
+// constants from one set (uni_rows).  Four bases per 16-byte load; byte 0 of
+// each packed base is its base quality, which may differ.
+__global__ void k_gap_check(const uchar4* __restrict__ quals, long long n, BandCounters* c) {
+  const uint32_t ref = *reinterpret_cast<const uint32_t*>(quals) & 0x7f7f7f00u;
+  const long long n4 = n / 4;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nt = (long long)gridDim.x * blockDim.x;
+  bool mixed = false;
+  for (long long x = tid; x < n4; x += nt) {
+    const uint4 v = reinterpret_cast<const uint4*>(quals)[x];  // quals is 16-byte aligned (start of its allocation)
+    mixed |= ((v.x & 0x7f7f7f00u) != ref) | ((v.y & 0x7f7f7f00u) != ref) | ((v.z & 0x7f7f7f00u) != ref) |
+             ((v.w & 0x7f7f7f00u) != ref);
+  }
+  for (long long x = 4 * n4 + tid; x < n; x += nt)
+    mixed |= (*reinterpret_cast<const uint32_t*>(quals + x) & 0x7f7f7f00u) != ref;
+  if (__any_sync(0xffffffffu, mixed) && (threadIdx.x & 31) == 0) c->gap_mixed = 1u;
+  if (tid == 0) c->gap_checked = 1u;
 }
 
 __global__ void k_audit_units(BandParams p, Unit* units) {
@@ -1228,6 +1284,13 @@ __global__ void k_audit_compare(BandParams p, double* err) {
 }
 
 }  // namespace
+
+cudaError_t launch_gap_check(const uchar4* quals, long long n_bases, BandCounters* c, int sms, cudaStream_t st) {
+  if (n_bases <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((n_bases / 4 + 255) / 256 + 1, (long long)sms * 8);
+  k_gap_check<<<(int)blocks, 256, 0, st>>>(quals, n_bases, c);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_audit_units(const BandParams& p, Unit* units, cudaStream_t st) {
   k_audit_units<<<64, 256, 0, st>>>(p, units);

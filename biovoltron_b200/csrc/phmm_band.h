@@ -81,6 +81,8 @@ struct BandCounters {
   unsigned long long band_result_cells;                   // cells of the result band (band plus ring)
   unsigned long long feat_slow_count;                     // pairs left to the warp featuriser (many distinct diagonals)
   unsigned long long feat_slow_next;                      // its work-queue head
+  unsigned int gap_checked;                               // k_gap_check ran on this batch
+  unsigned int gap_mixed;                                 // some base's gap qualities differ from the first base's
 };
 
 struct BandParams {
@@ -134,6 +136,9 @@ cudaError_t launch_read_kmers(const uint8_t* read_bases, long long n_bytes, uint
 cudaError_t launch_hap_table(const uint8_t* hap_bases, const int64_t* hap_off, long long n_haps, long long n_hap_bytes,
                              uint32_t* table, uint32_t* nib, int sms, cudaStream_t st);
 cudaError_t launch_featurize(const BandParams& p, int sms, cudaStream_t st);
+// Whether every read base has the first base's insertion, deletion and gap-continuation
+// qualities (BandCounters::gap_checked / gap_mixed; the counters must be zero before).
+cudaError_t launch_gap_check(const uchar4* quals, long long n_bases, BandCounters* c, int sms, cudaStream_t st);
 cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st);
 cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st);
 cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st);

@@ -140,6 +140,7 @@ bv_status Engine::enqueue_band(bool capturing, KernelParams& kp) {
                            d_hap_nib_.as<uint32_t>(), sms_, stream_),
           "hap tables");
   BV_CUDA(launch_read_kmers(p.batch.read_bases, n_read_bytes_, d_read_kmers_.as<uint32_t>(), sms_, stream_), "kmers");
+  BV_CUDA(launch_gap_check(p.batch.read_quals, n_read_bytes_, p.bctr, sms_, stream_), "gap check");
   BV_CUDA(launch_featurize(p, sms_, stream_), "featurize");
   if (p.use_mlp) BV_CUDA(launch_mlp_forward(p, sms_, stream_), "mlp");
   BV_CUDA(launch_band_route(p, 0, sms_, stream_), "route");

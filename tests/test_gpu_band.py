@@ -100,6 +100,29 @@ def test_band_staged_replay_is_deterministic():
             assert np.array_equal(e.fetch(n), direct)
 
 
+def test_uniform_gap_rows_equal_the_general_rows():
+    """A batch whose read bases all carry the same insertion, deletion and
+    gap-continuation qualities lets the banded kernels take every row's
+    transition constants from one set.  Changing one base's insertion quality
+    (of the batch's last read) turns that off; every pair of the other reads
+    must then come out bit for bit the same."""
+    import dataclasses
+    b = W.config1(seed=35, n_regions=8)
+    assert b.uniform_gaps() is not None
+    ri = b.read_i.copy()
+    ri[-1] = 40
+    b2 = dataclasses.replace(b, read_i=ri)
+    assert b2.uniform_gaps() is None
+    with _band_engine(fixed_half=8, margin=2) as e:
+        uni, st1 = e.compute_regions(b, with_stats=True)
+        gen, st2 = e.compute_regions(b2, with_stats=True)
+    r, _ = b.pair_index()
+    other = r != b.n_reads - 1
+    assert st1["band_pairs"] > 0.8 * b.n_pairs and st2["band_pairs"] == st1["band_pairs"]
+    assert np.array_equal(uni[other], gen[other])
+    assert not np.array_equal(uni[~other], gen[~other])
+
+
 def _repeat_pairs(seed):
     """Pairs whose sampled 11-mers vote for many diagonals: haplotypes made of
     a repeated unit (period 40 and 25), reads cut from them with a few
