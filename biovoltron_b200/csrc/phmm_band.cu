@@ -1190,8 +1190,9 @@ __global__ void __launch_bounds__(128, W <= 8 ? 3 : 2) k_band_ring_f32(BandParam
   const Tables* tb = p.tables;
   __shared__ BandSmem sm;
   stage_band_tables(sm, tb);
-  // uniform gap qualities over the batch (k_gap_check ran): one set of row constants
-  const bool uni = p.bctr->gap_checked != 0u && p.bctr->gap_mixed == 0u;
+  // uniform gap qualities over the batch (k_gap_check ran): one set of row constants.  Not for
+  // W = 16: compiled with both row paths it holds 227 registers instead of 219 and ran slower
+  const bool uni = W != 16 && p.bctr->gap_checked != 0u && p.bctr->gap_mixed == 0u;
   const UniRows ur = uni_rows(sm, tb->mm_inv_f, p.batch.read_quals[0]);
   // routed items (bucketed by read length), then items promoted from the next narrower class
   const unsigned long long total =
