@@ -74,6 +74,7 @@ Engine::~Engine() {
   if (stream_) {
     cudaStreamSynchronize(stream_);
     if (h_counters_) cudaFreeHost(h_counters_);
+    if (h_chunk_off_) cudaFreeHost(h_chunk_off_);
     for (auto& e : ev_)
       if (e) cudaEventDestroy(e);
     for (auto& e : tune_ev_)
@@ -160,7 +161,23 @@ bv_status Engine::init() {
   return BV_OK;
 }
 
-bv_status Engine::validate(const bv_region_batch& b) {
+bv_status Engine::reserve_chunk_offsets(int64_t n) {
+  if (n <= chunk_off_cap_) return BV_OK;
+  if (h_chunk_off_) {
+    BV_CUDA(cudaStreamSynchronize(stream_), "chunk offsets sync");
+    cudaFreeHost(h_chunk_off_);
+    h_chunk_off_ = nullptr;
+    chunk_off_cap_ = 0;
+  }
+  BV_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_chunk_off_), sizeof(int64_t) * (size_t)n), "pinned chunk offsets");
+  chunk_off_cap_ = n;
+  return BV_OK;
+}
+
+bv_status Engine::validate(const bv_region_batch& b) { return validate_ranges(b, false); }
+bv_status Engine::validate_outline(const bv_region_batch& b) { return validate_ranges(b, true); }
+
+bv_status Engine::validate_ranges(const bv_region_batch& b, bool outline) {
   if (b.num_regions < 0 || b.num_reads < 0 || b.num_haps < 0) return fail(BV_ERR_INVALID_ARG, "negative count");
   if (b.num_regions > 0 && (!b.region_reads || !b.region_haps))
     return fail(BV_ERR_INVALID_ARG, "region offsets missing");
@@ -178,7 +195,12 @@ bv_status Engine::validate(const bv_region_batch& b) {
   }
   if (b.num_reads > 0) {
     if (b.read_offsets[0] < 0) return fail(BV_ERR_INVALID_ARG, "read offset negative");
+    // outline: only the reads outside [region_reads[0], region_reads[num_regions])
+    const int64_t skip0 = outline && b.num_regions > 0 ? b.region_reads[0] : b.num_reads;
+    const int64_t skip1 = outline && b.num_regions > 0 ? b.region_reads[b.num_regions] : b.num_reads;
     for (int64_t r = 0; r < b.num_reads; ++r) {
+      if (r == skip0 && skip1 > skip0) r = skip1;
+      if (r >= b.num_reads) break;
       const int64_t l = b.read_offsets[r + 1] - b.read_offsets[r];
       if (l < 0) return fail(BV_ERR_INVALID_ARG, "read offsets decrease");
       if (l > BV_PHMM_MAX_READ_LEN) return fail(BV_ERR_INVALID_ARG, "read longer than BV_PHMM_MAX_READ_LEN");
@@ -189,7 +211,11 @@ bv_status Engine::validate(const bv_region_batch& b) {
   }
   if (b.num_haps > 0) {
     if (b.hap_offsets[0] < 0) return fail(BV_ERR_INVALID_ARG, "hap offset negative");
+    const int64_t skip0 = outline && b.num_regions > 0 ? b.region_haps[0] : b.num_haps;
+    const int64_t skip1 = outline && b.num_regions > 0 ? b.region_haps[b.num_regions] : b.num_haps;
     for (int64_t h = 0; h < b.num_haps; ++h) {
+      if (h == skip0 && skip1 > skip0) h = skip1;
+      if (h >= b.num_haps) break;
       const int64_t l = b.hap_offsets[h + 1] - b.hap_offsets[h];
       if (l < 0) return fail(BV_ERR_INVALID_ARG, "hap offsets decrease");
       if (l > BV_PHMM_MAX_HAP_LEN) return fail(BV_ERR_INVALID_ARG, "haplotype longer than BV_PHMM_MAX_HAP_LEN");

@@ -66,13 +66,19 @@ struct ChunkCut {
 std::vector<ChunkCut> plan_chunks(const bv_region_batch& b, int chunks);
 
 // A chunk of regions [g0, g1) as a batch of its own: offsets rebased to the
-// chunk's first read / haplotype, byte pointers moved to match.
+// chunk's first read / haplotype, byte pointers moved to match.  The rebased
+// read and haplotype offsets go to `off` (page-locked memory of the context
+// that stages the chunk, at least n_off() entries) so that their copies to the
+// device do not hold up the host.
 struct Chunk {
   int64_t g0 = 0, g1 = 0, out0 = 0, n_out = 0;
-  std::vector<int64_t> region_reads, region_haps, read_off, hap_off;
+  std::vector<int64_t> region_reads, region_haps;
   bv_region_batch view{};
 
-  void build(const bv_region_batch& b) {
+  int64_t n_off(const bv_region_batch& b) const {
+    return (b.region_reads[g1] - b.region_reads[g0] + 1) + (b.region_haps[g1] - b.region_haps[g0] + 1);
+  }
+  void build(const bv_region_batch& b, int64_t* off) {
     const int64_t r0 = b.region_reads[g0], r1 = b.region_reads[g1];
     const int64_t h0 = b.region_haps[g0], h1 = b.region_haps[g1];
     region_reads.resize(g1 - g0 + 1);
@@ -81,11 +87,11 @@ struct Chunk {
       region_reads[g - g0] = b.region_reads[g] - r0;
       region_haps[g - g0] = b.region_haps[g] - h0;
     }
-    read_off.resize(r1 - r0 + 1);
+    int64_t* read_off = off;
+    int64_t* hap_off = off + (r1 - r0 + 1);
     const int64_t rb0 = r1 > r0 ? b.read_offsets[r0] : 0;
     for (int64_t r = r0; r <= r1 && r1 > r0; ++r) read_off[r - r0] = b.read_offsets[r] - rb0;
     if (r1 == r0) read_off[0] = 0;
-    hap_off.resize(h1 - h0 + 1);
     const int64_t hb0 = h1 > h0 ? b.hap_offsets[h0] : 0;
     for (int64_t h = h0; h <= h1 && h1 > h0; ++h) hap_off[h - h0] = b.hap_offsets[h] - hb0;
     if (h1 == h0) hap_off[0] = 0;
@@ -94,9 +100,9 @@ struct Chunk {
     view.region_reads = region_reads.data();
     view.region_haps = region_haps.data();
     view.num_reads = r1 - r0;
-    view.read_offsets = read_off.data();
+    view.read_offsets = read_off;
     view.num_haps = h1 - h0;
-    view.hap_offsets = hap_off.data();
+    view.hap_offsets = hap_off;
     auto shift = [](const uint8_t* p, int64_t o) { return p ? p + o : p; };
     view.read_bases = shift(b.read_bases, rb0);
     view.read_q = shift(b.read_q, rb0);
@@ -181,6 +187,13 @@ class Engine {
 
  private:
   bv_status validate(const bv_region_batch& b);
+  // validate() but for the reads and haplotypes inside the regions' ranges,
+  // which the chunked call's chunks validate as they are staged
+  bv_status validate_outline(const bv_region_batch& b);
+  bv_status validate_ranges(const bv_region_batch& b, bool outline);
+  // page-locked room for n rebased offsets of a chunk this context stages
+  bv_status reserve_chunk_offsets(int64_t n);
+  int64_t* chunk_offsets() const { return h_chunk_off_; }
   bv_status plan(const bv_region_batch& b);
   bv_status upload_inputs(const bv_region_batch& b);
   bv_status upload_plan();
@@ -224,6 +237,8 @@ class Engine {
   float ms_h2d_ = 0;
   bool h2d_time_pending_ = false;  // ms_h2d_ is read after the next synchronisation
   Counters* h_counters_ = nullptr;  // page-locked copy of the device counters
+  int64_t* h_chunk_off_ = nullptr;  // page-locked rebased offsets of the chunk this context stages
+  int64_t chunk_off_cap_ = 0;
   std::chrono::steady_clock::time_point run_t0_{};
   uint64_t config_version_ = 0;     // bumped by every change a second context must mirror
   uint64_t mirrored_version_ = ~0ull;  // the source's config_version_ this context last mirrored

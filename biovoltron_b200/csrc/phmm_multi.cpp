@@ -123,7 +123,8 @@ extern "C" bv_status bv_phmm_compute_regions_multi(bv_phmm_ctx* const* ctxs, int
       c.g0 = pt.block_start[x];
       c.g1 = pt.block_start[y];
       c.out0 = pt.block_out0[x];
-      c.build(*batch);
+      std::vector<int64_t> off((size_t)c.n_off(*batch));  // the view is copied from within the call below
+      c.build(*batch, off.data());
       bv_phmm_stats s{};
       status[k] = bv_phmm_compute_regions(ctxs[k], &c.view, out_log10 ? out_log10 + c.out0 : nullptr, &s);
       add_stats(acc, s);

@@ -80,7 +80,9 @@ std::vector<ChunkCut> plan_chunks(const bv_region_batch& b, int chunks) {
 bv_status Engine::compute_chunked(Engine& other, const bv_region_batch& b, double* out, bv_phmm_stats* stats,
                                   int chunks) {
   const auto t0 = std::chrono::steady_clock::now();
-  bv_status s = validate(b);
+  // The chunks' reads and haplotypes are validated as each chunk is staged
+  // (an invalid one ends the call with the chunks before it already written).
+  bv_status s = validate_outline(b);
   if (s != BV_OK) return s;
   // results per region and the chunk cuts (about equal numbers of pairs)
   int64_t total = 0;
@@ -97,6 +99,14 @@ bv_status Engine::compute_chunked(Engine& other, const bv_region_batch& b, doubl
     ck.push_back(std::move(c));
   }
   Engine* eng[2] = {this, &other};
+  {
+    int64_t most = 1;
+    for (const Chunk& c : ck) most = std::max(most, c.n_off(b));
+    for (Engine* e : eng) {
+      s = e->reserve_chunk_offsets(most);
+      if (s != BV_OK) return fail(s, e->last_error());
+    }
+  }
   std::vector<bv_phmm_stats> cs(ck.size());
   auto drain = [&](size_t k) -> bv_status {  // results and stats of chunk k
     Engine& e = *eng[k % 2];
@@ -113,7 +123,9 @@ bv_status Engine::compute_chunked(Engine& other, const bv_region_batch& b, doubl
   };
   for (size_t k = 0; k < ck.size(); ++k) {
     Engine& e = *eng[k % 2];
-    ck[k].build(b);  // here rather than up front: the host rebases chunk k while chunk k-1 runs
+    // here rather than up front: the host rebases chunk k while chunk k-1 runs; chunk k-2, the
+    // last user of this context's offset buffer, has been drained
+    ck[k].build(b, e.chunk_offsets());
     s = e.stage(ck[k].view, false);
     if (s == BV_OK) s = e.launch();
     if (s != BV_OK) return abort(fail(s, e.last_error()));

@@ -235,6 +235,11 @@ typedef struct bv_region_batch {
 /* Number of result slots the batch produces (sum over regions of reads*haps). */
 int64_t bv_phmm_region_results(const bv_region_batch* batch);
 
+/* Scores every pair of the batch into out_log10 (bv_phmm_region_results slots,
+ * region by region, read-major).  An invalid batch returns BV_ERR_INVALID_ARG;
+ * a batch scored in chunks (bv_phmm_options.pipeline_chunks) has each chunk's
+ * reads and haplotypes validated as the chunk is staged, so out_log10 may then
+ * hold the results of the chunks before the invalid one. */
 bv_status bv_phmm_compute_regions(bv_phmm_ctx* ctx, const bv_region_batch* batch, double* out_log10,
                                   bv_phmm_stats* stats);
 

@@ -284,6 +284,25 @@ def test_chunked_compute_matches_single_pass(chunks):
     assert bst["band_pairs"] > 0
 
 
+def test_chunked_compute_rejects_an_invalid_chunk():
+    """The chunked call validates each chunk's reads as it stages the chunk: a
+    read whose offsets decrease in the last chunk fails the call with
+    BV_ERR_INVALID_ARG, and the context stays usable."""
+    import dataclasses
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    b = W.config1(seed=43, n_regions=12)
+    ro = b.read_offsets.copy()
+    r = int(b.region_reads[-2]) + 1  # a read of the last region
+    ro[r] = ro[r + 1] + 1
+    bad = dataclasses.replace(b, read_offsets=ro)
+    with PairHMMEngine(pipeline_chunks=3, pipeline_min_pairs=1) as e:
+        with pytest.raises(RuntimeError, match="decrease"):
+            e.compute_regions(bad)
+        # the context stays usable
+        with PairHMMEngine() as one:
+            assert np.array_equal(e.compute_regions(b), one.compute_regions(b))
+
+
 def test_chunked_compute_rejects_bad_options():
     from biovoltron_b200.pairhmm import PairHMMEngine
     with pytest.raises(RuntimeError):
