@@ -55,6 +55,8 @@ struct TrainArena {
     b.dH = take((size_t)cap * kHid);
     b.dH2 = take((size_t)cap * kHid);
     b.loss = take((size_t)std::max(loss_slots, 1));
+    b.part = take((size_t)((cap + 127) / 128) * kHid * kHid);
+    b.tc_fail = reinterpret_cast<unsigned int*>(take(1));
     b.cap = cap;
     bytes = off;
   }
@@ -215,11 +217,15 @@ bv_status Engine::band_mlp_eval(const float* w, const float* x, const float* t, 
   BV_CUDA(cudaMemcpyAsync(b.w, w, sizeof(float) * kMlpParamCount, cudaMemcpyHostToDevice, stream_), "H2D");
   BV_CUDA(cudaMemcpyAsync(b.X, x, sizeof(float) * kFeat * n, cudaMemcpyHostToDevice, stream_), "H2D");
   BV_CUDA(cudaMemcpyAsync(b.T, t, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, stream_), "H2D");
+  BV_CUDA(cudaMemsetAsync(b.tc_fail, 0, sizeof(unsigned int), stream_), "memset");
   BV_CUDA(mlp_forward_backward(b, (int)n, alpha, grad != nullptr, stream_), "mlp eval");
   BV_CUDA(cudaMemcpyAsync(out, b.O, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, stream_), "D2H");
   BV_CUDA(cudaMemcpyAsync(loss, b.loss, sizeof(float), cudaMemcpyDeviceToHost, stream_), "D2H");
   if (grad) BV_CUDA(cudaMemcpyAsync(grad, b.g, sizeof(float) * kMlpParamCount, cudaMemcpyDeviceToHost, stream_), "D2H");
+  unsigned int tc_fail = 0;
+  BV_CUDA(cudaMemcpyAsync(&tc_fail, b.tc_fail, sizeof(tc_fail), cudaMemcpyDeviceToHost, stream_), "D2H");
   BV_CUDA(cudaStreamSynchronize(stream_), "eval sync");
+  if (tc_fail) return status_fail(16);
   return BV_OK;
 }
 
@@ -333,6 +339,7 @@ bv_status Engine::band_train(const bv_region_batch& bt, const bv_band_train_opti
   BV_CUDA(cudaMemcpyAsync(b.w, w.data(), sizeof(float) * kMlpParamCount, cudaMemcpyHostToDevice, stream_), "H2D");
   BV_CUDA(cudaMemsetAsync(b.m, 0, sizeof(float) * kMlpParamCount, stream_), "memset");
   BV_CUDA(cudaMemsetAsync(b.v, 0, sizeof(float) * kMlpParamCount, stream_), "memset");
+  BV_CUDA(cudaMemsetAsync(b.tc_fail, 0, sizeof(unsigned int), stream_), "memset");
   float* loss_hist = b.loss;
   BV_CUDA(cudaEventRecord(ev_[0], stream_), "event");
   int step = 0;
@@ -360,6 +367,11 @@ bv_status Engine::band_train(const bv_region_batch& bt, const bv_band_train_opti
   BV_CUDA(cudaEventElapsedTime(&ms_train, ev_[0], ev_[1]), "event time");
   rep->ms_train = ms_train;
   rep->steps = total_steps;
+  {
+    unsigned int tc_fail = 0;
+    BV_CUDA(cudaMemcpy(&tc_fail, b.tc_fail, sizeof(tc_fail), cudaMemcpyDeviceToHost), "D2H");
+    if (tc_fail) return status_fail(16);
+  }
   std::vector<float> lh(total_steps);
   BV_CUDA(cudaMemcpy(lh.data(), loss_hist, sizeof(float) * total_steps, cudaMemcpyDeviceToHost), "D2H");
   rep->first_loss = (float)(std::accumulate(lh.begin(), lh.begin() + steps_per_epoch, 0.0) / steps_per_epoch);

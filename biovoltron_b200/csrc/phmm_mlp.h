@@ -27,6 +27,8 @@ struct MlpTrainBuffers {
   float* Z1; float* H1; float* Z2; float* H2; float* O;
   float* dO; float* dH; float* dH2;
   float* loss;   // scalar
+  float* part;             // split-K partial products of the weight gradients, ceil(cap / 128) x 128 x 128
+  unsigned int* tc_fail;   // set when a tensor-core GEMM's completion wait gave up
   int cap;
 };
 

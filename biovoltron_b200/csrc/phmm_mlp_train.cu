@@ -3,7 +3,14 @@
 // Master weights are FP32; every step rounds them to BF16 (the precision the
 // tensor-core inference kernel uses) and runs forward and backward in FP32 on
 // those rounded values, so the gradient is that of the deployed network
-// (straight-through rounding).  The loss is an asymmetric squared error on
+// (straight-through rounding).  The GEMMs with 80 or 128 rows on every side
+// run on the tensor cores (tcgen05.mma kind::f16: BF16 operands, FP32
+// accumulation in tensor memory) -- the two hidden layers' forward products
+// (inputs, weights and hidden activations are BF16 values already), the
+// hidden layers' weight gradients and the back-propagated hidden gradient
+// (the FP32 gradient operands rounded to BF16, as mixed-precision training
+// does); the products with the 2-wide output layer stay FP32 SIMT.  The loss
+// is an asymmetric squared error on
 // the band's lower and upper edge (diagonals relative to the seed diagonal):
 //   L = mean( w_lo (o_lo - t_lo)^2 + w_hi (o_hi - t_hi)^2 ),
 //   w_lo = alpha if o_lo > t_lo (band too narrow below) else 1,
@@ -17,6 +24,7 @@
 
 #include "phmm_band.h"
 #include "phmm_mlp.h"
+#include "phmm_tc.cuh"
 
 namespace bvphmm {
 namespace {
@@ -138,16 +146,179 @@ __global__ void k_export_params(const float* __restrict__ w, MlpParams* __restri
 
 inline dim3 grid2(int M, int N) { return dim3((N + TS - 1) / TS, (M + TS - 1) / TS); }
 
+// ---- tensor-core GEMM ---------------------------------------------------------
+// C = A . B^T over K with FP32 operands read through strides and rounded to
+// BF16 while they are staged: A(r, k) = A[r sar + k sak] for r < m_valid and
+// k < k_valid (else 0), B(n, k) = B[n sbn + k sbk] for k < k_valid; C FP32
+// row-major (ldc = N), rows past m_valid not written.  N a multiple of 16, at
+// most 128.  Block (x, y) takes rows 128 x .. 128 x + 127 and the K range
+// y kspan .. (y + 1) kspan (kspan a multiple of 16) and writes its product to
+// C + y c_split (split K: the partial products are summed in a fixed order by
+// k_sum_splits).  Four warps: K in chunks of up to 64 staged into shared
+// memory in the canonical K-major layout without swizzling, one thread issues
+// the chunk's MMAs (K = 16 each) into the FP32 accumulator in tensor memory
+// and commits them to an mbarrier, every thread waits (bounded: a wait that
+// gives up sets *fail and the block skips its epilogue), and the warps drain
+// the accumulator with tcgen05.ld (warp w: rows 32 w .. 32 w + 31).
+constexpr int kTcKc = 64;
+struct GemmTcSmem {
+  __nv_bfloat16 a[128 * kTcKc];
+  __nv_bfloat16 b[128 * kTcKc];
+  uint64_t mbar;
+  uint32_t tmem_base;
+  int fail;
+};
+struct GemmTcArgs {
+  const float* A;
+  long long sar, sak;
+  const float* B;
+  long long sbn, sbk;
+  float* C;
+  long long c_split;
+  int m_valid, N, k_valid, kspan;
+};
+
+// eight consecutive k of one row, rounded to BF16 (nearest even), zero where invalid
+__device__ __forceinline__ uint4 stage8(const float* base, long long sk, bool row_ok, int k, int k_valid) {
+  uint32_t w[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int k0 = k + 2 * t, k1 = k0 + 1;
+    const float v0 = row_ok && k0 < k_valid ? base[(long long)k0 * sk] : 0.f;
+    const float v1 = row_ok && k1 < k_valid ? base[(long long)k1 * sk] : 0.f;
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+    w[t] = *reinterpret_cast<const uint32_t*>(&h);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+__global__ void __launch_bounds__(128, 1) k_gemm_tc(GemmTcArgs g, unsigned int* fail) {
+  using namespace tc;
+  __shared__ __align__(1024) GemmTcSmem s;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int row0 = blockIdx.x * 128;
+  const int kb = blockIdx.y * g.kspan, ke = min(kb + g.kspan, g.k_valid);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
+                 "r"(128)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mbar)) : "memory");
+    s.fail = 0;
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = s.tmem_base;
+  const uint32_t idesc = instr_desc(128, g.N);
+  unsigned char* sa = reinterpret_cast<unsigned char*>(s.a);
+  unsigned char* sb = reinterpret_cast<unsigned char*>(s.b);
+  unsigned phase = 0;
+  bool any = false;  // the accumulator holds a product
+  for (int k0 = kb; k0 < kb + g.kspan; k0 += kTcKc) {
+    const int kc = min(kTcKc, kb + g.kspan - k0);  // a multiple of 16
+    const int pieces = kc / 8;                     // 16-byte row pieces per row
+    for (int x = tid; x < 128 * pieces; x += 128) {
+      const int r = x / pieces, c = 8 * (x % pieces);
+      const int gr = row0 + r;
+      *reinterpret_cast<uint4*>(sa + core_offset(r, c, kc)) =
+          stage8(g.A + (long long)gr * g.sar, g.sak, gr < g.m_valid, k0 + c, ke);
+    }
+    for (int x = tid; x < g.N * pieces; x += 128) {
+      const int r = x / pieces, c = 8 * (x % pieces);
+      *reinterpret_cast<uint4*>(sb + core_offset(r, c, kc)) = stage8(g.B + (long long)r * g.sbn, g.sbk, true, k0 + c, ke);
+    }
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      fence_after_sync();
+      const uint32_t sbo = sbo_for(kc);
+      for (int k = 0; k < kc / 16; ++k)
+        mma_f16(tmem, mat_desc(sa + k * 2 * kLbo, kLbo, sbo), mat_desc(sb + k * 2 * kLbo, kLbo, sbo), idesc,
+                any || k > 0);
+      mma_commit(&s.mbar);
+    }
+    any = true;
+    if (!mbar_wait_parity(&s.mbar, phase)) {
+      s.fail = 1;
+      mbar_wait_parity(&s.mbar, phase);  // again bounded: the MMAs still reading this chunk
+    }
+    phase ^= 1u;
+    fence_after_sync();
+    __syncthreads();  // the chunk's shared memory is free for the next one
+    if (*reinterpret_cast<volatile int*>(&s.fail)) break;
+  }
+  if (!*reinterpret_cast<volatile int*>(&s.fail)) {
+    const int r = row0 + tid;
+    float* C = g.C + blockIdx.y * g.c_split;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int c0 = 0; c0 < g.N; c0 += 32) {
+      float v[32];
+      if (any) {
+        tmem_ld32(trow + (uint32_t)c0, v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = 0.f;
+      }
+      if (r < g.m_valid) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (c0 + j < g.N) C[(size_t)r * g.N + c0 + j] = v[j];
+      }
+    }
+  } else if (tid == 0) {
+    atomicOr(fail, 1u);
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s.tmem_base), "r"(128) : "memory");
+  }
+}
+
+// out[x] = sum over s of part[s * n + x], s = 0, 1, .. in order
+__global__ void k_sum_splits(const float* __restrict__ part, int splits, int n, float* __restrict__ out) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+    float acc = 0.f;
+    for (int sp = 0; sp < splits; ++sp) acc += part[(size_t)sp * n + x];
+    out[x] = acc;
+  }
+}
+
+// C[m x N] = A . B^T on the tensor cores (one K range)
+inline void gemm_tc(GemmTcArgs g, unsigned int* fail, cudaStream_t st) {
+  if (g.m_valid <= 0 || g.k_valid <= 0) return;
+  g.c_split = 0;
+  g.kspan = (g.k_valid + 15) / 16 * 16;
+  k_gemm_tc<<<dim3((g.m_valid + 127) / 128, 1), 128, 0, st>>>(g, fail);
+}
+// C[128 x N] = A . B^T with K = the batch split into ranges of 128 (partials in `part`, summed in order)
+inline void gemm_tc_splitk(GemmTcArgs g, float* part, unsigned int* fail, cudaStream_t st) {
+  if (g.m_valid <= 0 || g.k_valid <= 0) return;
+  float* C = g.C;
+  const int splits = (g.k_valid + 127) / 128;
+  g.C = part;
+  g.c_split = (long long)g.m_valid * g.N;
+  g.kspan = 128;
+  k_gemm_tc<<<dim3((g.m_valid + 127) / 128, splits), 128, 0, st>>>(g, fail);
+  k_sum_splits<<<64, 256, 0, st>>>(part, splits, g.m_valid * g.N, C);
+}
+
 }  // namespace
 
 cudaError_t mlp_forward_backward(const MlpTrainBuffers& b, int n, float alpha, bool backward, cudaStream_t st) {
   const dim3 blk(TS, TS);
   const int o1 = 0, ob1 = kHid * kFeat, o2 = ob1 + kHid, ob2 = o2 + kHid * kHid, o3 = ob2 + kHid, ob3 = o3 + kOut * kHid;
   k_round_bf16<<<64, 256, 0, st>>>(b.w, b.wq, kMlpParamCount);
-  // forward
-  k_gemm<<<grid2(n, kHid), blk, 0, st>>>(b.X, b.wq + o1, b.Z1, n, kHid, kFeat, 0, 1, 0);
+  // forward: the hidden layers on the tensor cores (X and the rounded weights are BF16 values)
+  gemm_tc({b.X, kFeat, 1, b.wq + o1, kFeat, 1, b.Z1, 0, n, kHid, kFeat, 0}, b.tc_fail, st);
   k_bias_relu<<<256, 256, 0, st>>>(b.Z1, b.wq + ob1, b.H1, n, kHid, 1);
-  k_gemm<<<grid2(n, kHid), blk, 0, st>>>(b.H1, b.wq + o2, b.Z2, n, kHid, kHid, 0, 1, 0);
+  gemm_tc({b.H1, kHid, 1, b.wq + o2, kHid, 1, b.Z2, 0, n, kHid, kHid, 0}, b.tc_fail, st);
   k_bias_relu<<<256, 256, 0, st>>>(b.Z2, b.wq + ob2, b.H2, n, kHid, 1);
   k_gemm<<<grid2(n, kOut), blk, 0, st>>>(b.H2, b.wq + o3, b.O, n, kOut, kHid, 0, 1, 0);
   k_bias_relu<<<256, 256, 0, st>>>(b.O, b.wq + ob3, nullptr, n, kOut, 0);
@@ -159,11 +330,14 @@ cudaError_t mlp_forward_backward(const MlpTrainBuffers& b, int n, float alpha, b
   k_colsum<<<1, 32, 0, st>>>(b.dO, b.g + ob3, n, kOut);
   k_gemm<<<grid2(n, kHid), blk, 0, st>>>(b.dO, b.wq + o3, b.dH, n, kHid, kOut, 0, 0, 0);
   k_relu_bwd<<<256, 256, 0, st>>>(b.dH, b.Z2, (long long)n * kHid);
-  k_gemm<<<grid2(kHid, kHid), blk, 0, st>>>(b.dH, b.H1, b.g + o2, kHid, kHid, n, 1, 0, 0);
+  // dW2 = dZ2^T H1 (K = the batch, split in ranges of 128)
+  gemm_tc_splitk({b.dH, 1, kHid, b.H1, 1, kHid, b.g + o2, 0, kHid, kHid, n, 0}, b.part, b.tc_fail, st);
   k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(b.dH, b.g + ob2, n, kHid);
-  k_gemm<<<grid2(n, kHid), blk, 0, st>>>(b.dH, b.wq + o2, b.dH2, n, kHid, kHid, 0, 0, 0);
+  // dH1 = dZ2 W2 (B(i, o) = W2[o][i])
+  gemm_tc({b.dH, kHid, 1, b.wq + o2, 1, kHid, b.dH2, 0, n, kHid, kHid, 0}, b.tc_fail, st);
   k_relu_bwd<<<256, 256, 0, st>>>(b.dH2, b.Z1, (long long)n * kHid);
-  k_gemm<<<grid2(kHid, kFeat), blk, 0, st>>>(b.dH2, b.X, b.g + o1, kHid, kFeat, n, 1, 0, 0);
+  // dW1 = dZ1^T X
+  gemm_tc_splitk({b.dH2, 1, kHid, b.X, 1, kFeat, b.g + o1, 0, kHid, kFeat, n, 0}, b.part, b.tc_fail, st);
   k_colsum<<<(kHid + 127) / 128, 128, 0, st>>>(b.dH2, b.g + ob1, n, kHid);
   return cudaGetLastError();
 }

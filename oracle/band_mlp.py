@@ -1,9 +1,13 @@
 """CPU restatement of the band MLP's training objective (test infrastructure).
 
 Used only by the tests to check the GPU training kernels: forward, loss and
-analytical gradient in FP64, with the same BF16 rounding of the weight
-matrices and hidden activations as the GPU (biases stay FP32) (straight-through gradient), or without any
-rounding for the finite-difference check that pins the analytical gradient.
+analytical gradient in FP64, with the same BF16 rounding as the GPU -- of the
+weight matrices, the inputs and hidden activations (biases stay FP32), and of
+the hidden-layer gradients where they enter the tensor-core products (the
+weight gradients of both hidden layers and the back-propagated gradient of
+the first; the bias gradients sum the unrounded values) -- with the gradient
+passed straight through every rounding, or without any rounding for the
+finite-difference check that pins the analytical gradient.
 
 Network: 80 -> 128 (ReLU) -> 128 (ReLU) -> 2; parameters flattened as
 W1[128][80], b1[128], W2[128][128], b2[128], W3[2][128], b3[2].
@@ -45,7 +49,7 @@ def objective(w: np.ndarray, x: np.ndarray, t: np.ndarray, alpha: float, roundin
     if rounding:
         W1, W2, W3 = bf16_round(W1), bf16_round(W2), bf16_round(W3)
     rnd = bf16_round if rounding else (lambda a: a)
-    x = np.asarray(x, np.float64)
+    x = rnd(np.asarray(x, np.float64))
     t = np.asarray(t, np.float64)
     n = x.shape[0]
     z1 = x @ W1.T + b1
@@ -61,9 +65,9 @@ def objective(w: np.ndarray, x: np.ndarray, t: np.ndarray, alpha: float, roundin
     do = 2.0 * wgt * e / n
     gW3, gb3 = do.T @ h2, do.sum(0)
     dh2 = (do @ W3) * (z2 > 0)
-    gW2, gb2 = dh2.T @ h1, dh2.sum(0)
-    dh1 = (dh2 @ W2) * (z1 > 0)
-    gW1, gb1 = dh1.T @ x, dh1.sum(0)
+    gW2, gb2 = rnd(dh2).T @ h1, dh2.sum(0)
+    dh1 = (rnd(dh2) @ W2) * (z1 > 0)
+    gW1, gb1 = rnd(dh1).T @ x, dh1.sum(0)
     g = np.concatenate([a.ravel() for a in (gW1, gb1, gW2, gb2, gW3, gb3)])
     return o, loss, g
 
