@@ -381,7 +381,10 @@ __device__ void featurize_pair(const BandParams& p, long long pi, int r, int h, 
 
 // Everything after the probes, for both featurisers: the fast path (at most
 // one vote per lane) groups lanes by slot; repeated 11-mers (hist != null
-// only) build a per-warp histogram over all slots.
+// only) build a per-warp histogram over all slots.  Writes the 64 histogram
+// features; the pair's scalar block goes to out[out_lane] (shared memory, the
+// unit featuriser writes it later) or, without `out`, straight to the pair
+// (lane 0).  Returns whether the pair had a seed (false: no_seed wrote it).
 __device__ __forceinline__ bool feature_summary(const BandParams& p, long long pi, int R, int H, int h,
                                                 const uint32_t* tbl, uint32_t nb, uint32_t code, int i, int stride,
                                                 int last_pos, int n_samp, int v0, int nv, uint32_t* hist, int* hits,
