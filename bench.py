@@ -393,20 +393,31 @@ def main():
     plain = band = None
     train_rep = None
     tuning = None
+    long_tuning = None
     if args.tune_regions > 0 and args.haps_per_warp == 0:
-        # launch shapes per rows-per-lane bin, timed on a seeded sample of the workload's regions
+        # launch shapes per rows-per-lane bin, and the long-read kernel's warps per pair when the
+        # workload has reads of 256 bases or more, timed on a seeded sample of the workload's regions
         picks = np.random.default_rng(5).choice(batch.n_regions, size=min(args.tune_regions, batch.n_regions),
                                                 replace=False)
+        sample = W.subsample_regions(batch, sorted(picks.tolist()))
         with PairHMMEngine(device=local) as et:
-            tuning = et.autotune(W.subsample_regions(batch, sorted(picks.tolist())), repeats=3)
+            tuning = et.autotune(sample, repeats=3)
+            if sample.read_lengths().max() >= 256:
+                long_tuning = et.autotune_long(sample, repeats=3)
+
+    def configure(e):
+        if tuning:
+            e.set_tuning(tuning)
+        if long_tuning:
+            e.set_long_warps(long_tuning["warps_per_pair"])
+
     h2d_link = pinned_h2d_gbps(local)
     clocks = ClockSampler(local)  # sampled over every timed section below
     clocks.start()
     # ---- plain full DP, device-resident --------------------------------------
     if form == "plain" or not args.no_plain:
         with PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp) as ep:
-            if tuning:
-                ep.set_tuning(tuning)
+            configure(ep)
             n, steps, wall, res = time_form(ep, batch, args, rep, band=False)
         plain = {"n": n, "steps": steps, "wall": wall, "res": res}
     # ---- learned band, device-resident --------------------------------------
@@ -414,8 +425,7 @@ def main():
     geno = None
     if form == "band":
         eb = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp, pipeline_chunks=args.pipeline_chunks)
-        if tuning:
-            eb.set_tuning(tuning)
+        configure(eb)
         train_rep = train_band(eb, args, rank)
         if args.save_weights and rank == 0:
             eb.band_save(args.save_weights)
@@ -435,8 +445,11 @@ def main():
         return [s_["ms_fp32"] + s_["ms_fp64"] for s_ in run["steps"]]
 
     # ---- end to end through the public API (host buffers) ---------------------
-    e2e_eng = eb if eb is not None else PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp,
-                                                      pipeline_chunks=args.pipeline_chunks)
+    if eb is not None:
+        e2e_eng = eb
+    else:
+        e2e_eng = PairHMMEngine(device=local, haps_per_warp=args.haps_per_warp, pipeline_chunks=args.pipeline_chunks)
+        configure(e2e_eng)
     # the caller's view of a SamRecord batch: when every read base has the same
     # gap-open and gap-continuation qualities they go as three bytes
     gaps = None if args.per_base_gaps else batch.uniform_gaps()
@@ -501,7 +514,8 @@ def main():
                        "l2": f"inputs {batch.nbytes() / 1e9:.2f} GB > 126 MB L2, no flush",
                        "parallelism": f"dp{world} (independent regions, one replica per GPU)",
                        "generate_s": round(t_gen, 1),
-                       "launch_shapes": tuning or "engine defaults (2 haplotypes per warp, 4 warps per block)"},
+                       "launch_shapes": tuning or "engine defaults (2 haplotypes per warp, 4 warps per block)",
+                       "long_read_kernel": long_tuning or "engine default (4 warps per pair, reads of 512 bases on)"},
         }
         if plain is not None:
             pl = plain["steps"][-1]

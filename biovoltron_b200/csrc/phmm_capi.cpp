@@ -395,6 +395,19 @@ bv_status bv_phmm_get_tuning(bv_phmm_ctx* ctx, bv_phmm_tune_entry* out, int32_t*
   return guard(ctx, [&] { return ctx->engine.get_tuning(out, num_out); });
 }
 
+bv_status bv_phmm_set_long_warps(bv_phmm_ctx* ctx, int32_t warps) {
+  if (!ctx) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.set_long_warps(warps); });
+}
+
+int32_t bv_phmm_get_long_warps(const bv_phmm_ctx* ctx) { return ctx ? ctx->engine.long_warps() : 0; }
+
+bv_status bv_phmm_autotune_long(bv_phmm_ctx* ctx, const bv_region_batch* sample, int32_t repeats, int32_t* warps_out,
+                                double* ms_out) {
+  if (!ctx || !sample || !warps_out || !ms_out) return BV_ERR_INVALID_ARG;
+  return guard(ctx, [&] { return ctx->engine.autotune_long(*sample, repeats, warps_out, ms_out); });
+}
+
 bv_status bv_phmm_host_register(bv_phmm_ctx* ctx, void* ptr, size_t bytes) {
   if (!ctx || !ptr || bytes == 0) return BV_ERR_INVALID_ARG;
   cudaError_t e = cudaSetDevice(ctx->engine.device());

@@ -286,7 +286,7 @@ bv_status Engine::plan(const bv_region_batch& b) {
       n_cells_ += rl * hap_bases;
       max_read = std::max(max_read, rl);
       if (all_f64) {
-        auto& list = rl >= kLongRows ? f64_long_items_ : f64_items_;
+        auto& list = rl >= long_rows() ? f64_long_items_ : f64_items_;
         for (int64_t k = 0; k < nh; ++k)
           list.push_back(PairRef{(int32_t)r, (int32_t)(h0 + k), res + (r - r0) * nh + k});
         continue;
@@ -354,11 +354,11 @@ bv_status Engine::plan(const bv_region_batch& b) {
   // FP64 long reads: one block per pair, longest pairs first (the long list is
   // read from its far end, so the host list is in ascending order of cells)
   long_plan_ = LaunchPlan{};
-  if (max_read >= kLongRows) {
-    long_smem_ = long_smem_bytes(rp.hap_bytes);
+  if (max_read >= long_rows()) {
+    long_smem_ = long_smem_bytes(rp.hap_bytes, long_warps_);
     if (long_smem_ <= 227 * 1024) {
-      BV_CUDA(prepare_long(long_smem_), "kernel attribute");
-      long_plan_.grid = sms_ * std::max(1, long_blocks_per_sm(long_smem_));
+      BV_CUDA(prepare_long(long_smem_, long_warps_), "kernel attribute");
+      long_plan_.grid = sms_ * std::max(1, long_blocks_per_sm(long_smem_, long_warps_));
       long_plan_.hap_bytes = rp.hap_bytes;
       long_plan_.bnd_cols = rp.bnd_cols;
       long_plan_.f64 = true;
@@ -510,7 +510,7 @@ bv_status Engine::enqueue_kernels(bool capturing) {
   p.out = d_out_.as<double>();
   p.rescue = d_rescue_.as<PairRef>();
   p.rescue_cap = std::max<int64_t>(n_results_, 1);
-  p.long_rows = long_plan_.grid > 0 ? kLongRows : 0;
+  p.long_rows = long_plan_.grid > 0 ? long_rows() : 0;
   p.warps_per_block = kThreadsPerBlock / kWarp;  // band-path fallback and audit launches
   BV_CUDA(rec(ev_[2]), "event");
   if (band_enabled()) {
@@ -564,7 +564,7 @@ bv_status Engine::enqueue_kernels(bool capturing) {
       KernelParams q = p;
       q.hap_bytes = long_plan_.hap_bytes;
       q.bnd_cols = long_plan_.bnd_cols;
-      BV_CUDA(launch_forward_long(q, long_plan_.grid, long_smem_, stream_), "FP64 long-read launch");
+      BV_CUDA(launch_forward_long(q, long_plan_.grid, long_smem_, long_warps_, stream_), "FP64 long-read launch");
     }
     BV_CUDA(launch_forward(lp.variant, p, lp.grid, stream_), "FP64 forward launch");
     p.cells_ctr = nullptr;

@@ -184,6 +184,12 @@ class Engine {
   bv_status autotune(const bv_region_batch& sample, int repeats, bv_phmm_tune_entry* out, int32_t* n_out);
   bv_status set_tuning(const bv_phmm_tune_entry* entries, int32_t n);
   bv_status get_tuning(bv_phmm_tune_entry* out, int32_t* n_out);
+  // Warps per pair of the FP64 long-read kernel (2, 4 or 8; reads of at least
+  // 128 x warps bases take it), set directly or chosen by timing the FP64 pass
+  // of a sample for each (ms[0..2]: 2, 4, 8 warps; 0 where not timed).
+  bv_status set_long_warps(int warps);
+  int long_warps() const { return long_warps_; }
+  bv_status autotune_long(const bv_region_batch& sample, int repeats, int32_t* warps_out, double* ms_out);
 
  private:
   bv_status validate(const bv_region_batch& b);
@@ -222,7 +228,9 @@ class Engine {
   std::vector<PairRef> f64_long_items_;  // the long reads among them, ascending cells (the list's far end first)
   std::vector<LaunchPlan> plans_;
   LaunchPlan rescue_plan_;
-  LaunchPlan long_plan_;  // FP64 long reads, a block of kLongWarps warps per pair (grid 0: none)
+  LaunchPlan long_plan_;  // FP64 long reads, a block of long_warps_ warps per pair (grid 0: none)
+  int long_warps_ = kLongWarps;  // 2, 4 or 8; reads of at least long_rows() bases take the long kernel
+  int long_rows() const { return long_warps_ * 128; }
   int long_smem_ = 0;
   int64_t n_results_ = 0;
   int64_t n_cells_ = 0;

@@ -145,4 +145,77 @@ bv_status Engine::autotune(const bv_region_batch& sample, int repeats, bv_phmm_t
   return BV_OK;
 }
 
+bv_status Engine::set_long_warps(int warps) {
+  if (!long_warps_valid(warps)) return fail(BV_ERR_INVALID_ARG, "long-read warps per pair must be 2, 4 or 8");
+  if (warps != long_warps_) {
+    long_warps_ = warps;
+    ++config_version_;
+    staged_ = false;  // the FP64 lists and launch plan depend on it: stage again
+    destroy_graph();
+  }
+  return BV_OK;
+}
+
+// The long-read kernel's shape: for each candidate warps per pair (and with
+// it the long-read edge, 128 x warps bases) the sample is staged in FP64 mode
+// -- every pair on the FP64 kernels, long reads on the long-read kernel, the
+// rest on the one-warp kernel -- and its FP64 pass timed (repeats runs after
+// a warm-up, median); the fastest is installed.
+bv_status Engine::autotune_long(const bv_region_batch& sample, int repeats, int32_t* warps_out, double* ms_out) {
+  if (!warps_out || !ms_out) return fail(BV_ERR_INVALID_ARG, "null output");
+  if (repeats < 1 || repeats > 64) return fail(BV_ERR_INVALID_ARG, "repeats out of range");
+  if (band_enabled()) return fail(BV_ERR_INVALID_ARG, "autotune runs the full-DP path: disable the band first");
+  const int cands[3] = {2, 4, 8};
+  for (int c = 0; c < 3; ++c) ms_out[c] = 0.0;
+  const int saved_warps = long_warps_;
+  const int32_t saved_precision = opt_.precision;
+  opt_.precision = BV_PRECISION_F64;
+  int best = saved_warps;
+  double best_ms = 1e300;
+  bv_status s = BV_OK;
+  for (int c = 0; c < 3 && s == BV_OK; ++c) {
+    long_warps_ = cands[c];
+    s = stage(sample);
+    if (s != BV_OK) break;
+    if (long_plan_.grid == 0) continue;  // no read this long, or its haplotypes too long for the kernel
+    std::vector<float> t;
+    for (int k = 0; k <= repeats && s == BV_OK; ++k) {  // the first run warms up
+      s = enqueue_kernels(false);
+      if (s != BV_OK) break;
+      cudaError_t e = cudaStreamSynchronize(stream_);
+      if (e != cudaSuccess) {
+        s = cuda_fail(e, "tune sync");
+        break;
+      }
+      Counters cc{};
+      e = cudaMemcpy(&cc, d_counters_.get(), sizeof(cc), cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) {
+        s = cuda_fail(e, "tune counters");
+        break;
+      }
+      if (cc.status != 0) {
+        s = status_fail(cc.status);
+        break;
+      }
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev_[3], ev_[4]);
+      if (k > 0) t.push_back(ms);
+    }
+    if (s != BV_OK || t.empty()) break;
+    std::nth_element(t.begin(), t.begin() + t.size() / 2, t.end());
+    ms_out[c] = t[t.size() / 2];
+    if (ms_out[c] < best_ms) {
+      best_ms = ms_out[c];
+      best = cands[c];
+    }
+  }
+  opt_.precision = saved_precision;
+  long_warps_ = s == BV_OK ? best : saved_warps;
+  staged_ = false;  // the sample was staged in FP64 mode
+  destroy_graph();
+  ++config_version_;
+  *warps_out = long_warps_;
+  return s;
+}
+
 }  // namespace bvphmm

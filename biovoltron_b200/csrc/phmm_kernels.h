@@ -34,14 +34,17 @@ struct KernelParams {
   int long_rows;          // > 0: FP32 results of reads this long or longer go to the FP64 list's long part
 };
 
-// Long reads in FP64: a block of kLongWarps warps per pair (phmm_long.cu);
-// reads from kLongRows bases on (four strips of 128 rows) take it.
+// Long reads in FP64: a block of `warps` warps per pair (phmm_long.cu; 2, 4
+// or 8, kLongWarps by default, chosen per context by the long-read tuner);
+// reads of at least warps x 128 bases (as many strips of 128 rows as the
+// block has warps) take it.
 constexpr int kLongWarps = 4;
 constexpr int kLongRows = kLongWarps * 128;
-int long_smem_bytes(int hap_bytes);
-cudaError_t prepare_long(int smem);
-int long_blocks_per_sm(int smem);
-cudaError_t launch_forward_long(const KernelParams& p, int grid, int smem, cudaStream_t st);
+bool long_warps_valid(int warps);
+int long_smem_bytes(int hap_bytes, int warps);
+cudaError_t prepare_long(int smem, int warps);
+int long_blocks_per_sm(int smem, int warps);
+cudaError_t launch_forward_long(const KernelParams& p, int grid, int smem, int warps, cudaStream_t st);
 
 // Variant table: (precision, rows per lane, multi-strip, two haplotypes per
 // warp).  Paired variants exist for FP32 single strip only.

@@ -379,23 +379,40 @@ __global__ void __launch_bounds__(K * kWarp) k_forward_long(KernelParams p) {
 
 }  // namespace
 
-int long_smem_bytes(int hap_bytes) { return hap_bytes + LongLayout<kLongWarps>::kBytes; }
-
-cudaError_t prepare_long(int smem) {
-  return raise_dynamic_smem(reinterpret_cast<const void*>(&k_forward_long<kLongWarps>), smem);
-}
-
-int long_blocks_per_sm(int smem) {
+// The kernel for `warps` warps per pair (2, 4 or 8; long_warps_valid).
+namespace {
+template <int K>
+int smem_for(int hap_bytes) { return hap_bytes + LongLayout<K>::kBytes; }
+template <int K>
+int blocks_for(int smem) {
   int nb = 0;
-  if (prepare_long(smem) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_forward_long<kLongWarps>, kLongWarps * kWarp, smem) !=
-      cudaSuccess)
-    return 0;
+  if (raise_dynamic_smem(reinterpret_cast<const void*>(&k_forward_long<K>), smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_forward_long<K>, K * kWarp, smem) != cudaSuccess) return 0;
   return nb;
 }
+}  // namespace
 
-cudaError_t launch_forward_long(const KernelParams& p, int grid, int smem, cudaStream_t st) {
-  k_forward_long<kLongWarps><<<grid, kLongWarps * kWarp, smem, st>>>(p);
+bool long_warps_valid(int warps) { return warps == 2 || warps == 4 || warps == 8; }
+
+int long_smem_bytes(int hap_bytes, int warps) {
+  return warps == 2 ? smem_for<2>(hap_bytes) : warps == 8 ? smem_for<8>(hap_bytes) : smem_for<4>(hap_bytes);
+}
+
+cudaError_t prepare_long(int smem, int warps) {
+  const void* f = warps == 2   ? reinterpret_cast<const void*>(&k_forward_long<2>)
+                  : warps == 8 ? reinterpret_cast<const void*>(&k_forward_long<8>)
+                               : reinterpret_cast<const void*>(&k_forward_long<4>);
+  return raise_dynamic_smem(f, smem);
+}
+
+int long_blocks_per_sm(int smem, int warps) {
+  return warps == 2 ? blocks_for<2>(smem) : warps == 8 ? blocks_for<8>(smem) : blocks_for<4>(smem);
+}
+
+cudaError_t launch_forward_long(const KernelParams& p, int grid, int smem, int warps, cudaStream_t st) {
+  if (warps == 2) k_forward_long<2><<<grid, 2 * kWarp, smem, st>>>(p);
+  else if (warps == 8) k_forward_long<8><<<grid, 8 * kWarp, smem, st>>>(p);
+  else k_forward_long<4><<<grid, 4 * kWarp, smem, st>>>(p);
   return cudaGetLastError();
 }
 

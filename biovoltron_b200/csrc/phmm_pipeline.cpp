@@ -27,6 +27,7 @@ bv_status Engine::mirror_config(Engine& src) {
   }
   band_opt_ = src.band_opt_;
   std::copy(src.tune_, src.tune_ + kTuneBins + 1, tune_);
+  long_warps_ = src.long_warps_;
   staged_ = false;
   destroy_graph();
   mirrored_version_ = src.config_version_;

@@ -179,6 +179,9 @@ def load() -> C.CDLL:
         "bv_phmm_genotype_staged": (C.c_int, [V, P(RegionBatchC), P(GenotypeBatch), V, V, V, V, P(C.c_double)]),
         "bv_phmm_debug_jacobian_table": (C.c_int, [V, C.c_int]),
         "bv_phmm_debug_chunks": (C.c_int64, [P(RegionBatchC), C.c_int32, V, C.c_int64]),
+        "bv_phmm_set_long_warps": (C.c_int, [V, C.c_int32]),
+        "bv_phmm_get_long_warps": (C.c_int32, [V]),
+        "bv_phmm_autotune_long": (C.c_int, [V, P(RegionBatchC), C.c_int32, V, V]),
         "bv_phmm_get_transitions": (C.c_int, [V, P(C.c_double)]),
         "bv_phmm_plan_partition": (C.c_int64, [P(RegionBatchC), C.c_int32, C.c_int32, V, V, V]),
         "bv_phmm_compute_regions_multi": (C.c_int, [P(V), C.c_int32, P(RegionBatchC), V, P(Stats)]),

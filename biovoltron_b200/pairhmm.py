@@ -295,6 +295,25 @@ class PairHMMEngine:
         self._check(self.lib.bv_phmm_set_tuning(self.h, arr, len(entries)))
         self._staged = None
 
+    def set_long_warps(self, warps: int):
+        """Warps per pair of the FP64 long-read kernel (2, 4 or 8; reads of at
+        least 128 x warps bases take it)."""
+        self._check(self.lib.bv_phmm_set_long_warps(self.h, int(warps)))
+        self._staged = None
+
+    def long_warps(self) -> int:
+        return int(self.lib.bv_phmm_get_long_warps(self.h))
+
+    def autotune_long(self, sample: RegionBatch, repeats: int = 3) -> dict:
+        """Times the FP64 pass of `sample` with 2, 4 and 8 warps per long-read
+        pair and installs the fastest (bv_phmm_autotune_long)."""
+        v = _BatchView(sample)
+        warps = C.c_int32(0)
+        ms = np.zeros(3, np.float64)
+        self._check(self.lib.bv_phmm_autotune_long(self.h, C.byref(v.c), repeats, C.byref(warps), _ptr(ms)))
+        self._staged = None
+        return {"warps_per_pair": int(warps.value), "fp64_ms": {2: float(ms[0]), 4: float(ms[1]), 8: float(ms[2])}}
+
     def host_register(self, arr: np.ndarray):
         self._check(self.lib.bv_phmm_host_register(self.h, _ptr(arr), arr.nbytes))
 

@@ -423,6 +423,17 @@ bv_status bv_phmm_autotune(bv_phmm_ctx* ctx, const bv_region_batch* sample, int3
  * not listed keep their values (defaults: two haplotypes per warp, 4 warps). */
 bv_status bv_phmm_set_tuning(bv_phmm_ctx* ctx, const bv_phmm_tune_entry* entries, int32_t num);
 bv_status bv_phmm_get_tuning(bv_phmm_ctx* ctx, bv_phmm_tune_entry* out, int32_t* num_out);
+/* The FP64 long-read kernel: a block of `warps` warps per pair (2, 4 or 8;
+ * default 4) runs reads of at least 128 x warps bases, strip w of every
+ * group of `warps` strips on warp w.  bv_phmm_autotune_long stages `sample`
+ * in FP64 mode for each choice (the long-read edge moves with it), times the
+ * FP64 pass (`repeats` runs, median), installs the fastest and writes it to
+ * *warps_out and the times to ms_out[0..2] (2, 4, 8 warps; 0 where the
+ * sample has no read that long).  No counterpart in the reference. */
+bv_status bv_phmm_set_long_warps(bv_phmm_ctx* ctx, int32_t warps);
+int32_t bv_phmm_get_long_warps(const bv_phmm_ctx* ctx);
+bv_status bv_phmm_autotune_long(bv_phmm_ctx* ctx, const bv_region_batch* sample, int32_t repeats, int32_t* warps_out,
+                                double* ms_out);
 
 /* --- the scalar PairHMM model ----------------------------------------------
  * Replaces PairHMM::compute_likelihoods(haplotypes, reads, trans)

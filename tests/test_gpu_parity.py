@@ -94,6 +94,32 @@ def test_config2_full_length_long_reads(oracle):
         assert st["rescued"] == b.n_pairs
 
 
+def test_long_read_warps_per_pair_and_tuner(oracle):
+    """The FP64 long-read kernel with 2, 4 and 8 warps per pair (reads of at
+    least 256, 512 and 1024 bases take it, the rest the one-warp kernel)
+    against the rescaled FP64 oracle; the long-read tuner times the three,
+    installs one, and the call in the default precision still matches."""
+    from biovoltron_b200.pairhmm import PairHMMEngine
+    b = W.config2(seed=29, n_pairs=8, max_read=3000, max_hap=4000)
+    truth = oracle.log10_rescaled(TestcaseArray.for_batch(b))
+    with PairHMMEngine(device=0, precision="f64") as e:
+        assert e.long_warps() == 4
+        for k in (2, 4, 8):
+            e.set_long_warps(k)
+            assert e.long_warps() == k
+            got = e.compute_regions(b)
+            assert np.max(np.abs(got - truth)) <= 1e-9, (k, got - truth)
+        with pytest.raises(RuntimeError):
+            e.set_long_warps(3)
+    with PairHMMEngine(device=0) as e:
+        rep = e.autotune_long(b, repeats=2)
+        print("long-read tuner", rep)
+        assert rep["warps_per_pair"] in (2, 4, 8) and e.long_warps() == rep["warps_per_pair"]
+        assert all(v > 0 for v in rep["fp64_ms"].values())
+        got = e.compute_regions(b)
+        assert np.max(np.abs(got - truth)) <= 1e-9
+
+
 def test_long_read_lengths_around_the_group_boundaries(oracle):
     """Reads whose strip counts fall on either side of a group of four strips
     (and of the long-read threshold of 512 bases), mixed with short reads in
