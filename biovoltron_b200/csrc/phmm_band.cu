@@ -768,6 +768,7 @@ __global__ void __launch_bounds__(256) k_band_route(BandParams p, int pass) {
       const int H = (int)(p.batch.hap_off[h + 1] - p.batch.hap_off[h]);
       band = route_band(p, pi, R, H, cls, d_lo);
       slot = band ? cls * kRBuckets + min(R / kRBucketRows, kRBuckets - 1) : kSlotFull + full_variant(R);
+      if (pass == 0 && p.banded) p.banded[pi] = 0;  // set by band_outcome when the band's result stands
       if (pass == 0 || band) local = atomicAdd(&cnt[slot], 1u);
     }
     __syncthreads();
@@ -860,6 +861,7 @@ __device__ __forceinline__ void band_outcome(const BandParams& p, int cls, const
     p.out[it.out] = __longlong_as_double(0x7ff8000000000000ll);
   } else {
     p.out[it.out] = (double)(log10f(tot) - p.tables->log10_init_f);
+    if (p.banded) p.banded[it.out] = 1;
   }
 }
 
@@ -1263,6 +1265,43 @@ __global__ void k_gap_check(const uchar4* __restrict__ quals, long long n, BandC
   if (tid == 0) c->gap_checked = 1u;
 }
 
+// Rescore: a read's pairs are consecutive result slots.  The thread at a
+// read's first slot takes the best result over the read's pairs (NaN: an FP64
+// rescue still to come, left out) and sends every banded pair more than
+// cap_margin log10 units below it to the full DP: such a pair is a read
+// scored against a haplotype it does not come from, and a stretch of the read
+// that does not belong to the haplotype is then partly explained by paths off
+// the band (a long insertion run, or a start far off the diagonal), which the
+// ring test does not see.  The full DP's result replaces the banded one.
+__global__ void k_band_cap(BandParams p) {
+  for (long long pi = blockIdx.x * (long long)blockDim.x + threadIdx.x; pi < p.n_pairs;
+       pi += (long long)gridDim.x * blockDim.x) {
+    const int r = p.pair_read[pi];
+    if (pi > 0 && p.pair_read[pi - 1] == r) continue;
+    long long end = pi;
+    double best = -INFINITY;
+    for (; end < p.n_pairs && p.pair_read[end] == r; ++end) {
+      const double v = p.out[end];
+      if (v > best) best = v;  // NaN compares false
+    }
+    const double cut = best - (double)p.cap_margin;
+    const int R = (int)(p.batch.read_off[r + 1] - p.batch.read_off[r]);
+    const int v = full_variant(R);
+    for (long long j = pi; j < end; ++j) {
+      if (!p.banded[j] || !(p.out[j] < cut)) continue;
+      const unsigned long long q = atomicAdd(&p.bctr->cap_count[v], 1ull);
+      atomicAdd(&p.bctr->cap_flagged, 1ull);
+      if (q < (unsigned long long)p.item_cap) {
+        Unit u{};
+        u.read = r; u.hap0 = p.pair_hap[j]; u.nh = 1; u.out0 = j;
+        p.cap_items[(size_t)v * p.item_cap + q] = u;
+      } else {
+        atomicOr(&p.ctr->status, 4ull);
+      }
+    }
+  }
+}
+
 __global__ void k_audit_units(BandParams p, Unit* units) {
   const unsigned long long n = min(p.bctr->audit_count, (unsigned long long)p.audit_cap);
   for (unsigned long long a = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; a < n;
@@ -1293,6 +1332,13 @@ cudaError_t launch_gap_check(const uchar4* quals, long long n_bases, BandCounter
   if (n_bases <= 0) return cudaSuccess;
   const long long blocks = std::min<long long>((n_bases / 4 + 255) / 256 + 1, (long long)sms * 8);
   k_gap_check<<<(int)blocks, 256, 0, st>>>(quals, n_bases, c);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_band_cap(const BandParams& p, int sms, cudaStream_t st) {
+  if (p.n_pairs <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((p.n_pairs + 255) / 256, (long long)sms * 8);
+  k_band_cap<<<(int)blocks, 256, 0, st>>>(p);
   return cudaGetLastError();
 }
 

@@ -83,7 +83,11 @@ struct BandCounters {
   unsigned long long feat_slow_next;                      // its work-queue head
   unsigned int gap_checked;                               // k_gap_check ran on this batch
   unsigned int gap_mixed;                                 // some base's gap qualities differ from the first base's
+  unsigned long long cap_count[16];                       // banded pairs rescored by the full DP, per variant
+  unsigned long long cap_flagged;                         // their total
 };
+// work-queue slots of the rescore launches (the fallback launches use 0 .. 8, the audit 16 .. 24)
+constexpr int kCapSlot0 = 32;
 
 struct BandParams {
   DeviceBatch batch;
@@ -108,6 +112,9 @@ struct BandParams {
   int fixed_half;
   int margin;                 // diagonals added on both sides of the predicted band
   float edge_threshold;       // promotion when the ring adds more than this share of the likelihood
+  float cap_margin;           // > 0: banded pairs this many log10 units below their read's best are rescored
+  uint8_t* banded;            // [n_pairs] 1 where the result came from the banded kernel
+  Unit* cap_items;            // [9][item_cap] rescore units per full-DP variant
   int audit_period;           // every audit_period-th pair is also scored by the full DP (0: off)
   BandCounters* bctr;
   Counters* ctr;
@@ -143,6 +150,9 @@ cudaError_t launch_mlp_forward(const BandParams& p, int sms, cudaStream_t st);
 cudaError_t launch_band_route(const BandParams& p, int pass, int sms, cudaStream_t st);
 cudaError_t launch_band_scan(BandCounters* c, cudaStream_t st);
 cudaError_t launch_band_dp(const BandParams& p, int width_class, int sms, cudaStream_t st);
+// After the fallback full DP: per read, the banded pairs whose result lies more than cap_margin
+// log10 units below the read's best result go to the rescore lists (cap_items, cap_count).
+cudaError_t launch_band_cap(const BandParams& p, int sms, cudaStream_t st);
 // banded kernels: 128-thread blocks, as many as fit at once (3 per SM for W = 8, 2 for the wider classes)
 inline int band_dp_blocks(int sms, int width_class) { return sms * (width_class == 0 ? 3 : 2); }
 // warp featuriser (the slow path) grid and its per-warp scratch histograms (words)

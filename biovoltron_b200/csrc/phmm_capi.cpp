@@ -263,6 +263,7 @@ void bv_phmm_default_band_options(bv_band_options* o) {
   o->margin = 2;
   o->audit_period = 0;
   o->edge_threshold = 1e-3;
+  o->cap_margin = 12.f;
 }
 
 bv_status bv_phmm_set_band_options(bv_phmm_ctx* ctx, const bv_band_options* o) {

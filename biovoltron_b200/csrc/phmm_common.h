@@ -85,7 +85,7 @@ struct DeviceBatch {
 
 // Device-side counters and status, one block of memory per call.
 struct Counters {
-  unsigned long long unit_next[32];  // work-queue heads, one per launch slot
+  unsigned long long unit_next[48];  // work-queue heads, one per launch slot
   unsigned long long rescue_count;
   unsigned long long rescue_next;
   unsigned long long underflow_count;  // FP64 results that stayed non-positive

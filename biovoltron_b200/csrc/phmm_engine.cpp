@@ -648,9 +648,10 @@ bv_status Engine::finish(bv_phmm_stats* stats) {
     stats->fp32_skipped_cells = (int64_t)c.fp32_skipped_cells;
     stats->underflow = (int64_t)c.underflow_count;
     // band mode: k-mer tables, nibble image, read k-mers, gap check, two featurisers, MLP, route,
-    // scan, route; the banded kernels; the fallback variants; the audit; the FP64 pass
+    // scan, route; the banded kernels; the fallback variants; the rescore check and variants;
+    // the audit; the FP64 pass
     stats->kernel_launches = band_enabled()
-                                 ? 9 + (band_opt_.use_mlp ? 1 : 0) + kBandWidths + 9 +
+                                 ? 9 + (band_opt_.use_mlp ? 1 : 0) + kBandWidths + 9 + (band_opt_.cap_margin > 0 ? 10 : 0) +
                                        (band_opt_.audit_period > 0 ? 11 : 0) + 1
                                  : (int64_t)plans_.size() + 1;
     stats->ms_fp32 = ms32;

@@ -255,7 +255,7 @@ class Engine {
   bv_band_options band_opt_{};
   bool mlp_ready_ = false;
   DevBuf d_pair_read_, d_pair_hap_, d_hap_table_, d_dstar_, d_feat_, d_mlp_out_, d_mlp_, d_bctr_;
-  DevBuf d_kmin_, d_kmax_, d_read_kmers_, d_feat_hist_, d_feat_slow_, d_hap_nib_;
+  DevBuf d_kmin_, d_kmax_, d_read_kmers_, d_feat_hist_, d_feat_slow_, d_hap_nib_, d_banded_, d_cap_items_;
   DevBuf d_band_items_, d_full_items_, d_audit_pairs_, d_audit_units_, d_audit_out_, d_audit_err_;
   long long item_cap_ = 0, full_cap_ = 0, audit_cap_ = 0;
   LaunchPlan full_plans_[9];

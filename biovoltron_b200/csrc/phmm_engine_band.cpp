@@ -22,7 +22,7 @@ int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 bv_status Engine::set_band_options(const bv_band_options& o) {
   if (o.struct_size != (int32_t)sizeof(bv_band_options)) return fail(BV_ERR_INVALID_ARG, "band options size");
   if (o.fixed_half < 0 || o.fixed_half > 15 || o.margin < 0 || o.margin > 15 || o.audit_period < 0 ||
-      !(o.edge_threshold > 0))
+      !(o.edge_threshold > 0) || !(o.cap_margin >= 0.f) || !(o.cap_margin < 1e30f))
     return fail(BV_ERR_INVALID_ARG, "band option out of range");
   if (o.enabled && o.use_mlp && !mlp_ready_) return fail(BV_ERR_INVALID_ARG, "no band MLP weights (train or load)");
   if (o.enabled && constant_transitions(nullptr))
@@ -63,6 +63,9 @@ BandParams Engine::band_params() const {
   p.margin = band_opt_.margin;
   p.edge_threshold = (float)band_opt_.edge_threshold;
   p.audit_period = band_opt_.audit_period;
+  p.cap_margin = band_opt_.cap_margin;
+  p.banded = d_banded_.as<uint8_t>();
+  p.cap_items = d_cap_items_.as<Unit>();
   p.bctr = d_bctr_.as<BandCounters>();
   p.ctr = d_counters_.as<Counters>();
   p.items = d_band_items_.as<BandItem>();
@@ -102,6 +105,8 @@ bv_status Engine::band_prepare() {
   audit_cap_ = band_opt_.audit_period > 0 ? n / band_opt_.audit_period + 1 : 1;
   BV_CUDA(d_band_items_.reserve(sizeof(BandItem) * kBandWidths * item_cap_), "alloc band items");
   BV_CUDA(d_full_items_.reserve(sizeof(Unit) * 9 * full_cap_), "alloc fallback units");
+  BV_CUDA(d_banded_.reserve((size_t)n), "alloc band flags");
+  BV_CUDA(d_cap_items_.reserve(sizeof(Unit) * 9 * (band_opt_.cap_margin > 0 ? full_cap_ : 1)), "alloc rescore units");
   BV_CUDA(d_audit_pairs_.reserve(sizeof(int64_t) * audit_cap_), "alloc audit");
   BV_CUDA(d_audit_units_.reserve(sizeof(Unit) * 9 * audit_cap_), "alloc audit");
   BV_CUDA(d_audit_out_.reserve(sizeof(double) * audit_cap_), "alloc audit");
@@ -166,6 +171,26 @@ bv_status Engine::enqueue_band(bool capturing, KernelParams& kp) {
     kp.rescale_target = 0;
     BV_CUDA(launch_forward(v, kp, lp.grid, stream_), "fallback full DP");
   }
+  if (band_opt_.cap_margin > 0) {
+    // banded pairs far below their read's best result, scored again by the full DP
+    BV_CUDA(launch_band_cap(p, sms_, stream_), "band cap");
+    for (int v = 0; v < 9; ++v) {
+      const LaunchPlan& lp = full_plans_[v];
+      kp.units = d_cap_items_.as<Unit>() + (size_t)v * full_cap_;
+      kp.unit_base = 0;
+      kp.n_units = 0;
+      kp.n_units_dev = &d_bctr_.as<BandCounters>()->cap_count[v];
+      kp.slot = kCapSlot0 + v;
+      kp.from_rescue = 0;
+      kp.hap_bytes = lp.hap_bytes;
+      kp.warp_smem_bytes = lp.warp_smem;
+      kp.bnd = lp.multi ? d_bnd32_.get() : nullptr;
+      kp.bnd_cols = lp.bnd_cols;
+      kp.rescale = 0;
+      kp.rescale_target = 0;
+      BV_CUDA(launch_forward(v, kp, lp.grid, stream_), "rescore full DP");
+    }
+  }
   if (band_opt_.audit_period > 0) {
     BV_CUDA(launch_audit_units(p, d_audit_units_.as<Unit>(), stream_), "audit units");
     // the audit pairs' full DP, on the variant each read length takes
@@ -199,6 +224,7 @@ bv_status Engine::band_stats(bv_phmm_stats* st) {
   st->band_routed_full = (int64_t)bc.fallback_route;
   st->band_cells = (int64_t)bc.band_cells;
   st->band_result_cells = (int64_t)bc.band_result_cells;
+  st->band_rescored = (int64_t)bc.cap_flagged;
   st->band_promoted = 0;
   for (int c = 0; c < kBandWidths; ++c) st->band_promoted += (int64_t)bc.promoted[c];
   const long long na = std::min<long long>((long long)bc.audit_count, audit_cap_);
@@ -261,8 +287,18 @@ bv_status Engine::band_routes(int64_t n, int32_t* d_lo, int32_t* width, int32_t*
   rl.resize(nr + nl);
   if (nl) BV_CUDA(cudaMemcpy(rl.data() + nr, d_rescue_.as<PairRef>() + (std::max<int64_t>(n_results_, 1) - (int64_t)nl),
                              sizeof(PairRef) * nl, cudaMemcpyDeviceToHost), "rescue list");
+  if (band_opt_.cap_margin > 0) {
+    for (int v = 0; v < 9; ++v) {
+      const unsigned long long cnt = std::min<unsigned long long>(bc.cap_count[v], (unsigned long long)full_cap_);
+      std::vector<Unit> u(cnt);
+      if (cnt) BV_CUDA(cudaMemcpy(u.data(), d_cap_items_.as<Unit>() + (size_t)v * full_cap_, sizeof(Unit) * cnt,
+                                  cudaMemcpyDeviceToHost), "rescore units");
+      for (const auto& x : u)
+        if (x.out0 >= 0 && x.out0 < n && route[x.out0] == 0) route[x.out0] = 4;
+    }
+  }
   for (const auto& x : rl)
-    if (x.out >= 0 && x.out < n && route[x.out] == 0) route[x.out] = 3;
+    if (x.out >= 0 && x.out < n && (route[x.out] == 0 || route[x.out] == 4)) route[x.out] = 3;
   return BV_OK;
 }
 

@@ -41,6 +41,7 @@ void add_stats(bv_phmm_stats& t, const bv_phmm_stats& s) {
   t.rescued_cells += s.rescued_cells;
   t.band_result_cells += s.band_result_cells;
   t.fp32_skipped_cells += s.fp32_skipped_cells;
+  t.band_rescored += s.band_rescored;
   t.underflow += s.underflow;
   t.band_pairs += s.band_pairs;
   t.band_fallback += s.band_fallback;

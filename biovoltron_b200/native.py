@@ -48,7 +48,7 @@ class Stats(C.Structure):
         ("band_routed_full", C.c_int64), ("audit_pairs", C.c_int64), ("audit_max_err", C.c_double),
         ("audit_p99_err", C.c_double), ("band_promoted", C.c_int64), ("ms_seed", C.c_double),
         ("ms_full", C.c_double), ("rescued_cells", C.c_int64), ("band_result_cells", C.c_int64),
-        ("fp32_skipped_cells", C.c_int64),
+        ("fp32_skipped_cells", C.c_int64), ("band_rescored", C.c_int64),
     ]
 
     def as_dict(self):
@@ -58,7 +58,7 @@ class Stats(C.Structure):
 class BandOptions(C.Structure):
     _fields_ = [("struct_size", C.c_int32), ("enabled", C.c_int32), ("use_mlp", C.c_int32),
                 ("fixed_half", C.c_int32), ("margin", C.c_int32), ("audit_period", C.c_int32),
-                ("edge_threshold", C.c_double), ("reserved", C.c_int32 * 6)]
+                ("edge_threshold", C.c_double), ("cap_margin", C.c_float), ("reserved", C.c_int32 * 5)]
 
 
 class BandTrainOptions(C.Structure):

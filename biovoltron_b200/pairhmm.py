@@ -184,12 +184,12 @@ class PairHMMEngine:
         return list(arr) if self.lib.bv_phmm_get_transitions(self.h, arr) else None
 
     def set_band_options(self, enabled: bool = True, use_mlp: bool = False, fixed_half: int = 8, margin: int = 2,
-                         audit_period: int = 0, edge_threshold: float = 1e-3):
+                         audit_period: int = 0, edge_threshold: float = 1e-3, cap_margin: float = 12.0):
         """Routes pairs through the banded kernel (see bv_band_options)."""
         o = N.BandOptions()
         self.lib.bv_phmm_default_band_options(C.byref(o))
         o.enabled, o.use_mlp, o.fixed_half, o.margin = int(enabled), int(use_mlp), fixed_half, margin
-        o.audit_period, o.edge_threshold = audit_period, edge_threshold
+        o.audit_period, o.edge_threshold, o.cap_margin = audit_period, edge_threshold, cap_margin
         self._check(self.lib.bv_phmm_set_band_options(self.h, C.byref(o)))
 
     # --- learned band: training and weights ---------------------------------

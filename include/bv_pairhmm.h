@@ -105,6 +105,8 @@ typedef struct bv_phmm_stats {
                                 ring); band_cells adds the inner band the ring test recomputes */
   int64_t fp32_skipped_cells; /* cells of the pairs' remaining strips that the FP32 full DP left to the FP64
                                  pass when a strip proved the FP32 result below the rescue threshold */
+  int64_t band_rescored;      /* banded pairs scored again by the full DP, being more than
+                                 bv_band_options.cap_margin below their read's best result */
 } bv_phmm_stats;
 
 typedef struct bv_phmm_ctx bv_phmm_ctx;
@@ -144,7 +146,12 @@ typedef struct bv_band_options {
   int32_t margin;
   int32_t audit_period;
   double edge_threshold;   /* largest share of the likelihood the ring may add (default 1e-3) */
-  int32_t reserved[6];
+  float cap_margin;        /* a banded pair whose result lies more than this many log10 units below its
+                              read's best result is scored again by the full DP (default 12; 0: off) --
+                              such a pair's alternatives off the band (a stretch of the read that does not
+                              belong to the haplotype, explained by a long insertion) can carry a share of
+                              its likelihood the ring test does not see */
+  int32_t reserved[5];
 } bv_band_options;
 
 void bv_phmm_default_band_options(bv_band_options* opts);
@@ -329,8 +336,10 @@ bv_status bv_phmm_band_labels(bv_phmm_ctx* ctx, const bv_region_batch* batch, fl
                               int32_t* hi, float* features, int32_t* kmin, int32_t* kmax);
 /* After bv_phmm_run_staged in band mode: per result slot the route taken
  * (0 banded, 1 full DP from the router, 2 banded then sent to the full DP by
- * the edge check, 3 banded then recomputed in FP64) and, for routes 0, 2 and
- * 3, the band's first diagonal and width.  For testing and analysis. */
+ * the edge check, 3 banded then recomputed in FP64, 4 banded then scored
+ * again by the full DP for lying far below its read's best) and, for routes
+ * 0, 2, 3 and 4, the band's first diagonal and width.  For testing and
+ * analysis. */
 bv_status bv_phmm_band_routes(bv_phmm_ctx* ctx, int64_t n, int32_t* d_lo, int32_t* width, int32_t* route);
 /* Number of FP32 MLP parameters: W1[128][80], b1[128], W2[128][128], b2[128],
  * W3[2][128], b3[2], weights as [output][input], in that order. */
