@@ -14,7 +14,9 @@ distribution, its own seed); then every step scores the whole batch with the
 learned band (featuriser, BF16 MLP, banded forward pass with the ring test
 -- the band widened by 4 or 8 diagonals per side is the result, a ring share
 above the threshold widens the band, after 32 diagonals the full DP takes the
-pair -- and a sampled audit against the full DP) and FP32 with FP64 rescue.  The plain
+pair; banded pairs more than --cap-margin log10 units below their read's best
+are then scored again by the full DP -- and a sampled audit against the full
+DP) and FP32 with FP64 rescue.  The plain
 full-DP kernels score the same batch in the same run for the comparison.
 
 * value        pairs/s of the full chosen form with the batch resident in HBM
@@ -360,6 +362,9 @@ def main():
     ap.add_argument("--fixed-half", type=int, default=-1,
                     help=">= 0: band of seed diagonal +- this many diagonals (and the 11-mer extent), no MLP")
     ap.add_argument("--margin", type=int, default=2, help="diagonals added on both sides of the predicted band")
+    ap.add_argument("--cap-margin", type=float, default=12.0,
+                    help="banded pairs more than this many log10 units below their read's best are scored "
+                         "again by the full DP (0: off)")
     ap.add_argument("--pipeline-chunks", type=int, default=0,
                     help="region chunks of the end-to-end call (0: the library default, one per 4M pairs; 1: one pass)")
     ap.add_argument("--per-base-gaps", action="store_true",
@@ -431,10 +436,11 @@ def main():
             eb.band_save(args.save_weights)
         if args.fixed_half >= 0:  # seed-centred band of +-fixed_half diagonals instead of the MLP's
             eb.set_band_options(use_mlp=False, fixed_half=args.fixed_half, margin=args.margin,
-                                edge_threshold=args.edge_threshold, audit_period=args.audit_period)
+                                edge_threshold=args.edge_threshold, audit_period=args.audit_period,
+                                cap_margin=args.cap_margin)
         else:
             eb.set_band_options(use_mlp=True, margin=args.margin, edge_threshold=args.edge_threshold,
-                                audit_period=args.audit_period)
+                                audit_period=args.audit_period, cap_margin=args.cap_margin)
         n, steps, wall, res = time_form(eb, batch, args, rep, band=True)
         band = {"n": n, "steps": steps, "wall": wall, "res": res}
         geno = genotype_staged_timing(eb, batch)
@@ -549,6 +555,8 @@ def main():
                 "band_pairs": int(last["band_pairs"]), "routed_full": int(last["band_routed_full"]),
                 "edge_fallback": int(last["band_fallback"]), "promoted": int(last["band_promoted"]),
                 "fallback_rate": (int(last["band_routed_full"]) + int(last["band_fallback"])) / max(n, 1),
+                # banded pairs far below their read's best, scored again by the full DP
+                "rescored": int(last["band_rescored"]),
                 "band_cells": band_cells, "band_result_cells": result_cells,
                 # computed cells per second of the banded kernels (band + ring + inner band)
                 "gcups_computed_banded_dp": band_cells / (ms_band / 1e3) / 1e9 if ms_band > 0 else None,
