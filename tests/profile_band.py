@@ -33,6 +33,8 @@ def main():
     ap.add_argument("--half", type=int, default=6)
     ap.add_argument("--margin", type=int, default=2)
     ap.add_argument("--threshold", type=float, default=1e-3)
+    ap.add_argument("--cap-margin", type=float, default=12.0,
+                    help="rescore banded pairs this many log10 units below their read's best (0: off)")
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--weights", default="")
     ap.add_argument("--train-regions", type=int, default=0)
@@ -57,7 +59,8 @@ def main():
         use_mlp = bool(a.weights) and os.path.exists(a.weights)
         if use_mlp:
             e.band_load(a.weights)
-        e.set_band_options(use_mlp=use_mlp, fixed_half=a.half, margin=a.margin, edge_threshold=a.threshold)
+        e.set_band_options(use_mlp=use_mlp, fixed_half=a.half, margin=a.margin, edge_threshold=a.threshold,
+                           cap_margin=a.cap_margin)
         e.stage(b)
         for _ in range(a.runs):
             print(json.dumps({"band": e.run()}))
