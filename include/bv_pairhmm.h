@@ -150,7 +150,9 @@ typedef struct bv_band_options {
                               read's best result is scored again by the full DP (default 12; 0: off) --
                               such a pair's alternatives off the band (a stretch of the read that does not
                               belong to the haplotype, explained by a long insertion) can carry a share of
-                              its likelihood the ring test does not see */
+                              its likelihood the ring test does not see.  A read's results are its
+                              pairs in the batch (testcases: a run of consecutive testcases sharing
+                              the read); a read scored against one haplotype is never rescored */
   int32_t reserved[5];
 } bv_band_options;
 
