@@ -185,7 +185,11 @@ class PairHMMEngine:
 
     def set_band_options(self, enabled: bool = True, use_mlp: bool = False, fixed_half: int = 8, margin: int = 2,
                          audit_period: int = 0, edge_threshold: float = 1e-3, cap_margin: float = 12.0):
-        """Routes pairs through the banded kernel (see bv_band_options)."""
+        """Routes pairs through the banded kernel (see bv_band_options).
+
+        cap_margin: banded pairs whose result lies more than this many log10
+        units below their read's best result are scored again by the full DP
+        (0 switches the rescore off)."""
         o = N.BandOptions()
         self.lib.bv_phmm_default_band_options(C.byref(o))
         o.enabled, o.use_mlp, o.fixed_half, o.margin = int(enabled), int(use_mlp), fixed_half, margin

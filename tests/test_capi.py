@@ -47,6 +47,19 @@ def test_default_options_and_abi():
     assert lib.bv_phmm_status_string(N.BV_ERR_INVALID_ARG) == b"invalid argument"
 
 
+def test_default_band_options():
+    """The ctypes mirror has the C struct's size, and the defaults are the
+    documented ones: fixed band of +-8 diagonals, margin 2, ring threshold
+    1e-3, no audit, rescore 12 log10 units below the read's best."""
+    lib = N.load()
+    o = N.BandOptions()
+    lib.bv_phmm_default_band_options(C.byref(o))
+    assert o.struct_size == C.sizeof(N.BandOptions) == 56
+    assert (o.enabled, o.use_mlp, o.fixed_half, o.margin, o.audit_period) == (1, 0, 8, 2, 0)
+    assert o.edge_threshold == 1e-3 and o.cap_margin == 12.0
+    assert list(o.reserved) == [0] * 5
+
+
 def test_create_rejects_bad_options_before_touching_a_device():
     lib = N.load()
     h = C.c_void_p()
