@@ -169,6 +169,18 @@ extern "C" bv_status bv_phmm_forward_f64_noalloc(int device, const bv_phmm_devic
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) return BV_ERR_NO_DEVICE;
   if (cudaSetDevice(device) != cudaSuccess) return BV_ERR_NO_DEVICE;
+  // every call reads its status back and waits for the stream, which a stream
+  // capture forbids: a capturing stream is refused before anything is enqueued
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cs) != cudaSuccess) {
+    cudaGetLastError();
+    cudaSetDevice(prev);
+    return BV_ERR_UNSUPPORTED;
+  }
+  if (cs != cudaStreamCaptureStatusNone) {
+    cudaSetDevice(prev);
+    return BV_ERR_UNSUPPORTED;
+  }
   unsigned char* scratch = nullptr;
   bv_status s = setup_device(device, &scratch);
   if (s == BV_OK) {

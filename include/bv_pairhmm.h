@@ -383,7 +383,9 @@ bv_status bv_phmm_band_mlp_infer(bv_phmm_ctx* ctx, const float* x, int64_t n, fl
  * or whose indices are out of range gets NaN and makes the call return
  * BV_ERR_INVALID_ARG); reads of any length.
  * The call runs on `stream` (a cudaStream_t, NULL = legacy default stream)
- * and returns after the stream has finished it.  The first call on a device
+ * and returns after the stream has finished it, so it cannot be captured into
+ * a CUDA graph: a call on a capturing stream returns BV_ERR_UNSUPPORTED
+ * before enqueuing anything (the capture stays valid).  The first call on a device
  * sets that device up (finds the scratch array's device address, copies the
  * probability tables into it, synchronously): make it before any stream
  * capture.  Under lazy module loading (the CUDA default since 12.2) that
